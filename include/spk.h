@@ -1,0 +1,234 @@
+/*
+ * spk.h -- C ABI of libspk, the B200 (sm_100a) k-mer counting library for the
+ * spades-rs assembler.
+ *
+ * The library replaces the k-mer counting hot path of spades-rs:
+ *   - the two-tier Bloom prefilter    (src/bloom.rs:13-131, TwoTierFilter),
+ *   - Stage 2 Bloom population        (src/assemble.rs:129-161),
+ *   - Stage 3 solid k-mer count table (src/assemble.rs:166-242),
+ *   - the solid-k-mer cutoff and set  (src/assemble.rs:286-292, 692-735),
+ *   - (k+1)-mer edges implied by      (src/graph.rs:78-102),
+ *   - the per-k loop of multi-k runs  (src/multik.rs:109-178).
+ * The reference computes all of this on host threads; here everything runs on
+ * one GPU and the host only moves buffers across this boundary.
+ *
+ * Conventions
+ *   - Every call returns an int status; SPK_OK (0) is success.  On failure
+ *     spk_last_error() returns a message for the calling thread.  No call
+ *     aborts the process.
+ *   - k-mer keys are passed as little-endian u64 limbs of the reference
+ *     Kmer256 (src/dna.rs:134-138): limb 0 = lo bits 0..63, limb 1 = lo bits
+ *     64..127, limb 2 = hi bits 0..63, limb 3 = hi bits 64..127.  Lists of
+ *     k-mers use ceil(k/32) limbs per key; "k256" entry points always use 4.
+ *   - Lists are sorted ascending in Kmer256 order (lexicographic on (lo, hi),
+ *     src/dna.rs:137), which is sequence order for a fixed k.
+ *   - Input host buffers are borrowed for the duration of a call.  Results
+ *     are owned by the library until spk_result_free.
+ *   - A context may be used from one host thread at a time, except the
+ *     spk_submit / spk_poll / spk_wait family, which is thread-safe.
+ *   - The packed read layout is the reference PackedReads store
+ *     (src/packed_reads.rs:42-59, 547-578): 2 bits per base, A=0 C=1 G=2 T=3,
+ *     first base in the two most significant bits of a byte, every read
+ *     starting on a byte boundary at offsets[i] with lengths[i] bases.
+ */
+#ifndef SPK_H
+#define SPK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPK_VERSION 1
+
+/* Status codes. */
+enum spk_status {
+  SPK_OK = 0,
+  SPK_E_INVALID_ARG = 1,  /* null pointer, size mismatch, read out of bounds */
+  SPK_E_INVALID_K = 2,    /* k outside the supported range (src/main.rs:11-30) */
+  SPK_E_OOM = 3,          /* device memory exhausted */
+  SPK_E_TABLE_FULL = 4,   /* count table overflowed after regrow attempts */
+  SPK_E_TIMEOUT = 5,      /* a bounded device-side wait expired */
+  SPK_E_CUDA = 6,         /* CUDA runtime error */
+  SPK_E_NO_DEVICE = 7,    /* no usable sm_100 device */
+  SPK_E_ADMISSION = 8,    /* serving: job can never fit the HBM budget */
+  SPK_E_NOT_READY = 9,    /* serving: job not finished within the wait */
+  SPK_E_NOT_FOUND = 10    /* serving: unknown ticket */
+};
+
+typedef struct spk_ctx spk_ctx;
+typedef struct spk_bloom spk_bloom;
+typedef struct spk_result spk_result;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* spk_last_error(void);
+int spk_version(void);
+
+/* The CLI rule for k (src/main.rs:11-30): odd and in 11..=127.  Returns
+ * SPK_OK or SPK_E_INVALID_K with the reference's wording in spk_last_error().
+ * spk_count itself accepts any 1 <= k <= 127, as src/dna.rs does. */
+int spk_validate_k(uint32_t k);
+
+/* ---- context ------------------------------------------------------------ */
+int spk_ctx_create(int device, spk_ctx** out);
+int spk_ctx_destroy(spk_ctx* ctx);
+/* Device memory currently held by the context's pools, in bytes. */
+int spk_ctx_memory(spk_ctx* ctx, uint64_t* reserved_bytes, uint64_t* free_bytes);
+/* Runs the context's work on a caller-owned cudaStream_t (NULL restores the
+ * context's own stream), so callers can order libspk work with their own
+ * kernels and time it with events on that stream. */
+int spk_ctx_set_stream(spk_ctx* ctx, void* cuda_stream);
+
+/* ---- TwoTierFilter (src/bloom.rs:13-131) --------------------------------
+ * A device-resident two-tier Bloom filter with the reference's bit layout,
+ * hash (src/bloom.rs:61-78) and seeds (src/bloom.rs:84-86).  Batched calls
+ * have exactly the result of calling the reference method once per key in
+ * array order. */
+/* TwoTierFilter::new (src/bloom.rs:26-43): rounds capacity up to 64-bit words. */
+int spk_bloom_create(spk_ctx* ctx, uint64_t capacity_bits, spk_bloom** out);
+int spk_bloom_destroy(spk_bloom* bloom);
+/* size_bits of src/bloom.rs:15 and memory_usage_bytes of src/bloom.rs:129-131. */
+uint64_t spk_bloom_size_bits(const spk_bloom* bloom);
+uint64_t spk_bloom_memory_usage_bytes(const spk_bloom* bloom);
+/* TwoTierFilter::insert (src/bloom.rs:48-50), one key per element.
+ * out_promoted[i] (nullable) = the bool the reference returns. */
+int spk_bloom_insert_u64(spk_bloom* bloom, const uint64_t* keys, size_t n, uint8_t* out_promoted);
+/* TwoTierFilter::insert_kmer256 (src/bloom.rs:83-107); keys are 4 limbs each. */
+int spk_bloom_insert_k256(spk_bloom* bloom, const uint64_t* keys4, size_t n, uint8_t* out_promoted);
+/* TwoTierFilter::is_solid (src/bloom.rs:54-56). */
+int spk_bloom_is_solid_u64(spk_bloom* bloom, const uint64_t* keys, size_t n, uint8_t* out);
+/* TwoTierFilter::is_solid_kmer256 (src/bloom.rs:111-126). */
+int spk_bloom_is_solid_k256(spk_bloom* bloom, const uint64_t* keys4, size_t n, uint8_t* out);
+/* Copy the tiers (seen_bits / solid_bits of src/bloom.rs:19-21) to the host;
+ * each buffer holds size_bits/64 words and may be NULL. */
+int spk_bloom_download(spk_bloom* bloom, uint64_t* seen, uint64_t* solid);
+
+/* ---- counting (src/assemble.rs:129-292, src/graph.rs:78-102) ------------ */
+#define SPK_F_EDGES      0x1u  /* build the (k+1)-mer edge list */
+#define SPK_F_REF_SOLID  0x2u  /* also build the reference-semantics solid tier */
+#define SPK_F_KEEP_BLOOM 0x4u  /* keep the Bloom tiers for spk_result_bloom */
+
+typedef struct spk_count_opts {
+  uint64_t bloom_bits;    /* bits per tier; 0 = 512 Mi (src/assemble.rs:84) */
+  uint32_t min_count;     /* 0 = adaptive cutoff (src/assemble.rs:692-735), else fixed */
+  uint32_t list_min_count;/* smallest count kept in the sorted k-mer list (default 2) */
+  double min_coverage;    /* min_coverage of the adaptive cutoff (default 5.0) */
+  uint32_t flags;         /* SPK_F_* (default SPK_F_EDGES | SPK_F_KEEP_BLOOM) */
+  uint32_t table_log2;    /* 0 = size the count table from the Bloom fill; else start
+                             with 2^table_log2 slots (it still grows on overflow) */
+} spk_count_opts;
+
+void spk_count_opts_default(spk_count_opts* opts);
+
+/* Counts canonical k-mers of the packed reads for each k in ks[0..n_k).
+ * Replaces Stages 2-3 of run_assembly_with_packed_reads
+ * (src/assemble.rs:122-292) for one k, and the per-k loop of
+ * run_multik_assembly (src/multik.rs:109-178) for several.  Host buffers are
+ * copied to the device inside the call. */
+int spk_count(spk_ctx* ctx, const uint8_t* data, size_t data_len, const uint64_t* offsets,
+              const uint32_t* lengths, size_t n_reads, const uint32_t* ks, int n_k,
+              const spk_count_opts* opts, spk_result** out);
+/* Same with the packed reads already resident on the context's device.
+ * d_data must have data_len + 64 readable bytes (the tail is ignored). */
+int spk_count_device(spk_ctx* ctx, const uint8_t* d_data, size_t data_len,
+                     const uint64_t* d_offsets, const uint32_t* d_lengths, size_t n_reads,
+                     const uint32_t* ks, int n_k, const spk_count_opts* opts, spk_result** out);
+
+typedef struct spk_result_info {
+  uint32_t k;
+  uint32_t cutoff;               /* solid threshold used (src/assemble.rs:286) */
+  uint64_t occurrences;          /* k-mer positions per pass */
+  uint64_t admitted_occurrences; /* positions admitted to the table */
+  uint64_t n_table;              /* distinct admitted k-mers (the HashMap's len) */
+  uint64_t n_list;               /* k-mers with count >= list_min_count */
+  uint64_t n_solid;              /* k-mers with count >= cutoff */
+  uint64_t n_edges;              /* canonical (k+1)-mer edges */
+  uint64_t n_singletons;         /* admitted k-mers with count 1 */
+  uint64_t bloom_size_bits;
+  uint64_t seen_popcount;
+  uint64_t twice_popcount;
+  uint64_t table_capacity;
+  uint32_t table_regrows;
+  uint32_t kernel_launches;      /* libspk kernels launched for this k */
+  float ms_bloom, ms_count, ms_finish, ms_sort, ms_edges, ms_total; /* device time per phase */
+  float ms_bloom_kernel;         /* the Stage 2 insert kernel alone */
+  float ms_count_kernel;         /* the Stage 3 count kernel alone (last attempt) */
+} spk_result_info;
+
+int spk_result_count(const spk_result* res, int* n_k);
+int spk_result_info_get(const spk_result* res, int k_index, spk_result_info* info);
+/* Solid k-mers (count >= cutoff), sorted.  *n_inout: capacity in, count out.
+ * keys_out gets ceil(k/32) limbs per key; either output may be NULL to query n. */
+int spk_result_solid(spk_result* res, int k_index, uint64_t* keys_out, uint32_t* counts_out,
+                     size_t* n_inout);
+/* Sorted (k-mer, count) list of every k-mer with count >= max(min_count, list_min_count). */
+int spk_result_kmers(spk_result* res, int k_index, uint32_t min_count, uint64_t* keys_out,
+                     uint32_t* counts_out, size_t* n_inout);
+/* Canonical (k+1)-mer edges, sorted, ceil((k+1)/32) limbs each. */
+int spk_result_edges(spk_result* res, int k_index, uint64_t* edges_out, size_t* n_inout);
+/* Bloom tiers of the count: seen (bit-exact with src/bloom.rs:95-97), the
+ * twice tier, and the reference-semantics solid tier (SPK_F_REF_SOLID).  Each
+ * buffer holds bloom_size_bits/64 words and may be NULL. */
+int spk_result_bloom(spk_result* res, int k_index, uint64_t* seen, uint64_t* twice,
+                     uint64_t* ref_solid);
+
+/* Device-resident count table for a downstream graph build on the same
+ * device (the input of CompactedGraph::build, src/graph.rs:65-69).  Open
+ * addressing, linear probing: slot s holds key limbs keys[s*key_stride ..],
+ * count counts[s] (0 = empty).  Valid until spk_result_free. */
+typedef struct spk_table_view {
+  const uint64_t* keys;   /* device pointer; limbs hold the sequence value, see below */
+  const uint32_t* counts; /* device pointer */
+  uint64_t capacity;
+  uint32_t key_limbs;     /* ceil(k/32) */
+  uint32_t key_stride;    /* limbs per slot */
+  uint32_t k;
+  uint32_t cutoff;
+  /* Keys are stored as the 2k-bit sequence value (first base most
+   * significant), little-endian limbs.  For k <= 64 that equals the Kmer256
+   * limbs; for k > 64 the Kmer256 form is (value >> 2(k-64), value & mask). */
+} spk_table_view;
+int spk_result_table_view(spk_result* res, int k_index, spk_table_view* view);
+
+int spk_result_free(spk_result* res);
+
+/* ---- batched and serving entry points ---------------------------------- */
+/* One counting job: a read set and its k values.  Host buffers must stay
+ * valid until the job completes (spk_wait returns or spk_poll reports done). */
+typedef struct spk_job {
+  const uint8_t* data;
+  size_t data_len;
+  const uint64_t* offsets;
+  const uint32_t* lengths;
+  size_t n_reads;
+  const uint32_t* ks;
+  int n_k;
+  spk_count_opts opts;
+} spk_job;
+
+/* Counts several independent read sets in one batched device pass (samples
+ * of uneven size, each with its own Bloom and table).  results[i] receives
+ * job i's result, identical to spk_count on that job alone. */
+int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, spk_result** results);
+
+/* Serving loop.  spk_serve_start starts a scheduler thread that admits
+ * submitted jobs while their estimated HBM need fits in hbm_budget_bytes
+ * (0 = 90% of the device memory free at start) and at most max_inflight jobs
+ * run concurrently on separate streams. */
+int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight);
+int spk_serve_stop(spk_ctx* ctx);
+/* Estimated device bytes a job needs (Bloom + table + reads + outputs). */
+int spk_job_hbm_estimate(const spk_job* job, uint64_t* bytes);
+int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket);
+/* *done = 1 when the job finished (successfully or not). */
+int spk_poll(spk_ctx* ctx, uint64_t ticket, int* done);
+/* Waits up to timeout_ms (<0: forever) and hands over the result.  Returns
+ * the job's own status if it failed.  latency_ms (nullable) = submit->done. */
+int spk_wait(spk_ctx* ctx, uint64_t ticket, int timeout_ms, spk_result** out, double* latency_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPK_H */

@@ -1,0 +1,205 @@
+// ora_capi.cpp -- C entry points of the CPU oracle for the Python test suite
+// (ctypes).  TEST INFRASTRUCTURE ONLY: loaded by tests/, the smoke check and
+// the CPU-baseline leg of bench.py; never by the product library.
+//
+// k-mer keys cross this boundary as little-endian u64 limbs of the reference
+// Kmer256 (dna.rs:138): limb 0 = lo bits 0..63, limb 1 = lo bits 64..127,
+// limb 2 = hi bits 0..63, limb 3 = hi bits 64..127.  A k-mer list uses
+// ceil(k/32) limbs per key.
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "spk_oracle.h"
+
+using namespace ora;
+
+static inline unsigned nlimbs(unsigned k) { return (k + 31) / 32; }
+static inline Kmer256 from_limbs(const uint64_t* l, unsigned n) {
+  uint64_t w[4] = {0, 0, 0, 0};
+  for (unsigned i = 0; i < n && i < 4; i++) w[i] = l[i];
+  Kmer256 x;
+  x.lo = ((u128)w[1] << 64) | w[0];
+  x.hi = ((u128)w[3] << 64) | w[2];
+  return x;
+}
+static inline void to_limbs(const Kmer256& x, uint64_t* l, unsigned n) {
+  uint64_t w[4] = {(uint64_t)x.lo, (uint64_t)(x.lo >> 64), (uint64_t)x.hi, (uint64_t)(x.hi >> 64)};
+  for (unsigned i = 0; i < n && i < 4; i++) l[i] = w[i];
+}
+
+extern "C" {
+
+// ---- dna.rs ---------------------------------------------------------------
+int ora_base_to_2bit(uint8_t b) { return base_to_2bit(b); }
+uint64_t ora_revcomp_u64(uint64_t x, unsigned k) { return revcomp_kmer_u64(x, k); }
+uint64_t ora_canonical_u64(uint64_t x, unsigned k, int* is_rc) {
+  bool r = false;
+  uint64_t c = canonical_kmer_u64(x, k, &r);
+  if (is_rc) *is_rc = r;
+  return c;
+}
+int ora_string_to_kmer(const uint8_t* s, size_t len, unsigned k, uint64_t* out) {
+  return string_to_kmer(s, len, k, out) ? 1 : 0;
+}
+int ora_k256_from_bytes(const uint8_t* s, size_t len, unsigned k, uint64_t* out4) {
+  Kmer256 x;
+  if (!k256_from_bytes(s, len, k, &x)) return 0;
+  to_limbs(x, out4, 4);
+  return 1;
+}
+void ora_k256_to_string(const uint64_t* in4, unsigned k, char* out) {
+  std::string s = k256_to_string(from_limbs(in4, 4), k);
+  memcpy(out, s.data(), s.size());
+}
+void ora_k256_revcomp(const uint64_t* in4, unsigned k, uint64_t* out4) {
+  to_limbs(k256_revcomp(from_limbs(in4, 4), k), out4, 4);
+}
+int ora_k256_canonical(const uint64_t* in4, unsigned k, uint64_t* out4) {
+  bool r = false;
+  to_limbs(k256_canonical(from_limbs(in4, 4), k, &r), out4, 4);
+  return r ? 1 : 0;
+}
+void ora_k256_extend_right(const uint64_t* in4, uint8_t b, unsigned k, uint64_t* out4) {
+  to_limbs(k256_extend_right(from_limbs(in4, 4), b, k), out4, 4);
+}
+void ora_k256_prepend_left(const uint64_t* in4, uint8_t a, unsigned k, uint64_t* out4) {
+  to_limbs(k256_prepend_left(from_limbs(in4, 4), a, k), out4, 4);
+}
+
+// ---- bloom.rs -------------------------------------------------------------
+uint64_t ora_hash_kmer256(const uint64_t* in4, uint64_t seed) {
+  return hash_kmer256(from_limbs(in4, 4), seed);
+}
+void ora_hash_batch(const uint64_t* keys4, size_t n, uint64_t seed, uint64_t* out) {
+  for (size_t i = 0; i < n; i++) out[i] = hash_kmer256(from_limbs(keys4 + 4 * i, 4), seed);
+}
+void* ora_bloom_new(uint64_t capacity_bits) { return new TwoTierFilter(capacity_bits); }
+void ora_bloom_free(void* f) { delete (TwoTierFilter*)f; }
+uint64_t ora_bloom_size_bits(void* f) { return ((TwoTierFilter*)f)->size_bits; }
+uint64_t ora_bloom_num_words(void* f) { return ((TwoTierFilter*)f)->num_words; }
+uint64_t ora_bloom_memory_usage_bytes(void* f) { return ((TwoTierFilter*)f)->memory_usage_bytes(); }
+int ora_bloom_insert_k256(void* f, const uint64_t* in4) {
+  return ((TwoTierFilter*)f)->insert_kmer256(from_limbs(in4, 4)) ? 1 : 0;
+}
+int ora_bloom_is_solid_k256(void* f, const uint64_t* in4) {
+  return ((TwoTierFilter*)f)->is_solid_kmer256(from_limbs(in4, 4)) ? 1 : 0;
+}
+int ora_bloom_insert_u64(void* f, uint64_t x) { return ((TwoTierFilter*)f)->insert(x) ? 1 : 0; }
+int ora_bloom_is_solid_u64(void* f, uint64_t x) { return ((TwoTierFilter*)f)->is_solid(x) ? 1 : 0; }
+void ora_bloom_download(void* f, uint64_t* seen, uint64_t* solid) {
+  TwoTierFilter* t = (TwoTierFilter*)f;
+  if (seen) memcpy(seen, t->seen.data(), t->num_words * 8);
+  if (solid) memcpy(solid, t->solid.data(), t->num_words * 8);
+}
+
+// ---- packed_reads.rs ------------------------------------------------------
+void* ora_packed_new() { return new PackedReads(); }
+void ora_packed_free(void* p) { delete (PackedReads*)p; }
+void ora_packed_pack_clean(void* p, const uint8_t* s, size_t len) { ((PackedReads*)p)->pack_clean(s, len); }
+void ora_packed_ingest_read(void* p, const uint8_t* s, size_t len) { ((PackedReads*)p)->ingest_read(s, len); }
+// Reads are passed as one concatenated buffer plus per-read lengths.
+void* ora_packed_from_paired(const char* r1, const uint64_t* l1, size_t n1, const char* r2,
+                             const uint64_t* l2, size_t n2) {
+  std::vector<std::string> a, b;
+  size_t o = 0;
+  for (size_t i = 0; i < n1; i++) { a.emplace_back(r1 + o, l1[i]); o += l1[i]; }
+  o = 0;
+  for (size_t i = 0; i < n2; i++) { b.emplace_back(r2 + o, l2[i]); o += l2[i]; }
+  return new PackedReads(from_paired_slices(a, b));
+}
+void ora_packed_sizes(void* p, uint64_t* n_reads, uint64_t* data_len, uint64_t* pe_count,
+                      uint64_t* n_sidecar) {
+  PackedReads* r = (PackedReads*)p;
+  *n_reads = r->size();
+  *data_len = r->data.size();
+  *pe_count = r->pe_count;
+  *n_sidecar = r->ambiguous_sidecar.size();
+}
+void ora_packed_copy(void* p, uint8_t* data, uint64_t* offsets, uint32_t* lengths) {
+  PackedReads* r = (PackedReads*)p;
+  if (data) memcpy(data, r->data.data(), r->data.size());
+  if (offsets) memcpy(offsets, r->offsets.data(), r->offsets.size() * 8);
+  if (lengths) memcpy(lengths, r->lengths.data(), r->lengths.size() * 4);
+}
+size_t ora_packed_get_read(void* p, size_t idx, uint8_t* out) {
+  std::vector<uint8_t> buf;
+  ((PackedReads*)p)->get_read(idx, buf);
+  if (out) memcpy(out, buf.data(), buf.size());
+  return buf.size();
+}
+
+// ---- assemble.rs Stages 2-3 -------------------------------------------------
+// threads == 0 selects the serial restatement; threads >= 1 the threaded one.
+void* ora_count(const uint8_t* data, size_t data_len, const uint64_t* offsets,
+                const uint32_t* lengths, size_t n_reads, unsigned k, uint64_t bloom_bits,
+                int mode, int threads, int keep_bloom) {
+  PackedReads pr;
+  pr.data.assign(data, data + data_len);
+  pr.offsets.assign(offsets, offsets + n_reads);
+  pr.lengths.assign(lengths, lengths + n_reads);
+  CountResult* r = new CountResult();
+  if (threads <= 0) {
+    count_serial(pr, k, bloom_bits, (Mode)mode, r);
+    if (!keep_bloom) { r->seen.clear(); r->solid.clear(); }
+  } else {
+    count_threaded(pr, k, bloom_bits, threads, (Mode)mode, keep_bloom != 0, r);
+  }
+  return r;
+}
+void ora_count_free(void* r) { delete (CountResult*)r; }
+size_t ora_count_size(void* r, uint32_t min_count) {
+  size_t n = 0;
+  for (auto& e : ((CountResult*)r)->table) n += e.count >= min_count;
+  return n;
+}
+size_t ora_count_table(void* r, unsigned k, uint32_t min_count, uint64_t* keys, uint32_t* counts) {
+  unsigned L = nlimbs(k);
+  size_t n = 0;
+  for (auto& e : ((CountResult*)r)->table) {
+    if (e.count < min_count) continue;
+    if (keys) to_limbs(e.key, keys + n * L, L);
+    if (counts) counts[n] = e.count;
+    n++;
+  }
+  return n;
+}
+size_t ora_count_bloom_words(void* r) { return ((CountResult*)r)->seen.size(); }
+void ora_count_bloom(void* r, uint64_t* seen, uint64_t* solid) {
+  CountResult* c = (CountResult*)r;
+  if (seen) memcpy(seen, c->seen.data(), c->seen.size() * 8);
+  if (solid) memcpy(solid, c->solid.data(), c->solid.size() * 8);
+}
+// out: occurrences, admitted_occurrences, stage2 s, stage3 s, total s
+void ora_count_stats(void* r, double* out) {
+  CountResult* c = (CountResult*)r;
+  out[0] = (double)c->occurrences;
+  out[1] = (double)c->admitted_occurrences;
+  out[2] = c->seconds_stage2;
+  out[3] = c->seconds_stage3;
+  out[4] = c->seconds_total;
+}
+
+uint32_t ora_cutoff(const uint32_t* counts, size_t n, double min_coverage) {
+  std::vector<uint32_t> v(counts, counts + n);
+  return determine_solid_kmer_cutoff(v, min_coverage);
+}
+
+// Edge list for a sorted solid set.  Returns the number of edges; the caller
+// frees *out with ora_free.  Edge keys use ceil((k+1)/32) limbs.
+size_t ora_edges(const uint64_t* solid_keys, size_t n, unsigned k, uint64_t** out) {
+  unsigned L = nlimbs(k), Le = nlimbs(k + 1);
+  std::vector<Kmer256> s(n);
+  for (size_t i = 0; i < n; i++) s[i] = from_limbs(solid_keys + i * L, L);
+  std::sort(s.begin(), s.end());
+  std::vector<Kmer256> e = edges(s, k);
+  uint64_t* o = (uint64_t*)malloc(std::max<size_t>(e.size(), 1) * Le * 8);
+  for (size_t i = 0; i < e.size(); i++) to_limbs(e[i], o + i * Le, Le);
+  *out = o;
+  return e.size();
+}
+void ora_free(void* p) { free(p); }
+
+}  // extern "C"

@@ -1,0 +1,412 @@
+// spk_api.cu -- C ABI entry points of libspk (declared in include/spk.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "spk_internal.h"
+
+namespace spk {
+
+// ---- errors -------------------------------------------------------------------
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return SPK_E_OOM;
+  return SPK_E_CUDA;
+}
+
+// ---- FastMod constants (Granlund & Montgomery 1994, Fig. 4.1, N = 64) ---------
+FastMod make_fastmod(uint64_t d) {
+  FastMod f{};
+  f.d = d;
+  f.pow2 = (d & (d - 1)) == 0;
+  f.mask = d - 1;
+  unsigned l = 0;
+  while (l < 64 && (1ULL << l) < d) l++;  // l = ceil(log2 d)
+  typedef unsigned __int128 u128;
+  const u128 two_l = (u128)1 << l;
+  f.mprime = (uint64_t)((((u128)1 << 64) * (two_l - d)) / d + 1);
+  f.sh1 = l < 1 ? l : 1;
+  f.sh2 = l >= 1 ? l - 1 : 0;
+  return f;
+}
+
+// ---- device memory --------------------------------------------------------------
+int DevBuf::alloc(size_t n, cudaStream_t s) {
+  release();
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMallocAsync(&p, n, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+    // Give cached pool memory back to the driver once and retry.
+    cudaMemPool_t pool;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      cudaStreamSynchronize(s);
+      cudaMemPoolTrimTo(pool, 0);
+      e = cudaMallocAsync(&p, n, s);
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      char msg[128];
+      snprintf(msg, sizeof msg, "device allocation of %zu bytes failed", n);
+      return fail(SPK_E_OOM, msg);
+    }
+  }
+  bytes = n;
+  st = s;
+  return SPK_OK;
+}
+void DevBuf::release() {
+  if (p) cudaFreeAsync(p, st);
+  p = nullptr;
+  bytes = 0;
+}
+
+int bloom_create(spk_ctx* ctx, uint64_t capacity_bits, spk_bloom** out);
+int bloom_insert(spk_bloom* b, const uint64_t* keys, size_t n, int wide, uint8_t* promoted);
+int bloom_query(spk_bloom* b, const uint64_t* keys, size_t n, int wide, uint8_t* out);
+int bloom_download(spk_bloom* b, uint64_t* seen, uint64_t* solid);
+void serve_shutdown(spk_ctx* ctx);
+
+static int use_device(spk_ctx* ctx) {
+  if (!ctx) return fail(SPK_E_INVALID_ARG, "null context");
+  SPK_CUDA(cudaSetDevice(ctx->device));
+  return SPK_OK;
+}
+
+static int check_ks(const uint32_t* ks, int n_k) {
+  if (!ks || n_k < 1) return fail(SPK_E_INVALID_ARG, "at least one k is required");
+  for (int i = 0; i < n_k; i++)
+    if (ks[i] < 1 || ks[i] > 127)
+      return fail(SPK_E_INVALID_K, "k=" + std::to_string(ks[i]) + " is outside 1..=127");
+  return SPK_OK;
+}
+
+// Copies packed reads to the device (data padded so that k-mer windows may
+// read whole 64-bit words past the last byte).
+int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t data_len,
+                 const uint64_t* offsets, const uint32_t* lengths, size_t n_reads, ReadsView* rv) {
+  int rc;
+  const size_t padded = ((data_len + 7) / 8) * 8 + 64;
+  if ((rc = res->reads.alloc(padded, st))) return rc;
+  if ((rc = res->offs.alloc(std::max<size_t>(n_reads, 1) * 8, st))) return rc;
+  if ((rc = res->lens.alloc(std::max<size_t>(n_reads, 1) * 4, st))) return rc;
+  SPK_CUDA(cudaMemsetAsync(res->reads.as<uint8_t>() + (padded - 72), 0, 72, st));
+  if (data_len) SPK_CUDA(cudaMemcpyAsync(res->reads.p, data, data_len, cudaMemcpyHostToDevice, st));
+  if (n_reads) {
+    SPK_CUDA(cudaMemcpyAsync(res->offs.p, offsets, n_reads * 8, cudaMemcpyHostToDevice, st));
+    SPK_CUDA(cudaMemcpyAsync(res->lens.p, lengths, n_reads * 4, cudaMemcpyHostToDevice, st));
+  }
+  rv->words = res->reads.as<uint64_t>();
+  rv->offsets = res->offs.as<uint64_t>();
+  rv->lengths = res->lens.as<uint32_t>();
+  rv->n_reads = n_reads;
+  rv->byte_base = 0;
+  rv->data_len = data_len;
+  rv->err = nullptr;
+  return SPK_OK;
+}
+
+}  // namespace spk
+
+using namespace spk;
+
+extern "C" {
+
+const char* spk_last_error(void) { return g_err.c_str(); }
+int spk_version(void) { return SPK_VERSION; }
+
+// src/main.rs:11-30
+int spk_validate_k(uint32_t k) {
+  if (k < 11) return fail(SPK_E_INVALID_K, "k=" + std::to_string(k) + " is too small; minimum is 11");
+  if (k > 127)
+    return fail(SPK_E_INVALID_K, "k=" + std::to_string(k) + " exceeds maximum of 127 (Kmer256 limit)");
+  if (k % 2 == 0)
+    return fail(SPK_E_INVALID_K, "k=" + std::to_string(k) + " is even; SPAdes requires an odd k-mer size");
+  return SPK_OK;
+}
+
+int spk_ctx_create(int device, spk_ctx** out) {
+  if (!out) return fail(SPK_E_INVALID_ARG, "null output pointer");
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(SPK_E_NO_DEVICE, "no CUDA device is available");
+  }
+  if (device < 0 || device >= n) return fail(SPK_E_INVALID_ARG, "device index out of range");
+  cudaDeviceProp prop;
+  SPK_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fail(SPK_E_NO_DEVICE, std::string("libspk is built for sm_100a; device is ") + prop.name);
+  SPK_CUDA(cudaSetDevice(device));
+  auto* c = new spk_ctx();
+  c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  c->l2_bytes = prop.l2CacheSize;
+  e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  c->stream = c->own_stream;
+  if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&c->pool, device);
+  if (e == cudaSuccess) {
+    uint64_t thr = ~0ULL;  // keep freed blocks cached in the pool
+    e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_pinned, 1 << 16);
+  if (e != cudaSuccess) {
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return cuda_fail(e, "context setup");
+  }
+  *out = c;
+  return SPK_OK;
+}
+
+int spk_ctx_destroy(spk_ctx* ctx) {
+  if (!ctx) return SPK_OK;
+  cudaSetDevice(ctx->device);
+  serve_shutdown(ctx);
+  ctx->scratch.release();
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  cudaStreamDestroy(ctx->own_stream);
+  if (ctx->pool) cudaMemPoolTrimTo(ctx->pool, 0);
+  delete ctx;
+  return SPK_OK;
+}
+
+int spk_ctx_memory(spk_ctx* ctx, uint64_t* reserved_bytes, uint64_t* free_bytes) {
+  int rc;
+  if ((rc = use_device(ctx))) return rc;
+  if (reserved_bytes) {
+    uint64_t v = 0;
+    SPK_CUDA(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &v));
+    *reserved_bytes = v;
+  }
+  if (free_bytes) {
+    size_t f = 0, t = 0;
+    SPK_CUDA(cudaMemGetInfo(&f, &t));
+    *free_bytes = f;
+  }
+  return SPK_OK;
+}
+
+int spk_ctx_set_stream(spk_ctx* ctx, void* cuda_stream) {
+  int rc;
+  if ((rc = use_device(ctx))) return rc;
+  SPK_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+  return SPK_OK;
+}
+
+// ---- TwoTierFilter ------------------------------------------------------------
+int spk_bloom_create(spk_ctx* ctx, uint64_t capacity_bits, spk_bloom** out) {
+  int rc;
+  if (!out) return fail(SPK_E_INVALID_ARG, "null output pointer");
+  if ((rc = use_device(ctx))) return rc;
+  return bloom_create(ctx, capacity_bits, out);
+}
+int spk_bloom_destroy(spk_bloom* b) {
+  if (!b) return SPK_OK;
+  cudaSetDevice(b->ctx->device);
+  b->seen.release();
+  b->solid.release();
+  cudaStreamSynchronize(b->ctx->stream);
+  delete b;
+  return SPK_OK;
+}
+uint64_t spk_bloom_size_bits(const spk_bloom* b) { return b ? b->size_bits : 0; }
+uint64_t spk_bloom_memory_usage_bytes(const spk_bloom* b) { return b ? b->num_words * 8 * 2 : 0; }
+
+static int bloom_call(spk_bloom* b, const uint64_t* keys, size_t n, int wide, uint8_t* out,
+                      bool insert) {
+  int rc;
+  if (!b) return fail(SPK_E_INVALID_ARG, "null filter");
+  if (n && !keys) return fail(SPK_E_INVALID_ARG, "null keys");
+  if (!insert && n && !out) return fail(SPK_E_INVALID_ARG, "null output");
+  if ((rc = use_device(b->ctx))) return rc;
+  return insert ? bloom_insert(b, keys, n, wide, out) : bloom_query(b, keys, n, wide, out);
+}
+int spk_bloom_insert_u64(spk_bloom* b, const uint64_t* keys, size_t n, uint8_t* out_promoted) {
+  return bloom_call(b, keys, n, 0, out_promoted, true);
+}
+int spk_bloom_insert_k256(spk_bloom* b, const uint64_t* keys4, size_t n, uint8_t* out_promoted) {
+  return bloom_call(b, keys4, n, 1, out_promoted, true);
+}
+int spk_bloom_is_solid_u64(spk_bloom* b, const uint64_t* keys, size_t n, uint8_t* out) {
+  return bloom_call(b, keys, n, 0, out, false);
+}
+int spk_bloom_is_solid_k256(spk_bloom* b, const uint64_t* keys4, size_t n, uint8_t* out) {
+  return bloom_call(b, keys4, n, 1, out, false);
+}
+int spk_bloom_download(spk_bloom* b, uint64_t* seen, uint64_t* solid) {
+  int rc;
+  if (!b) return fail(SPK_E_INVALID_ARG, "null filter");
+  if ((rc = use_device(b->ctx))) return rc;
+  return bloom_download(b, seen, solid);
+}
+
+// ---- counting -------------------------------------------------------------------
+void spk_count_opts_default(spk_count_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof *o);
+  o->bloom_bits = 512ULL << 20;  // src/assemble.rs:84
+  o->min_count = 0;
+  o->list_min_count = 2;
+  o->min_coverage = 5.0;         // src/assemble.rs:82
+  o->flags = SPK_F_EDGES | SPK_F_KEEP_BLOOM;
+}
+
+static spk_count_opts resolve_opts(const spk_count_opts* o) {
+  spk_count_opts r;
+  spk_count_opts_default(&r);
+  if (o) r = *o;
+  if (!r.bloom_bits) r.bloom_bits = 512ULL << 20;
+  if (!r.list_min_count) r.list_min_count = 2;
+  return r;
+}
+
+int spk_count(spk_ctx* ctx, const uint8_t* data, size_t data_len, const uint64_t* offsets,
+              const uint32_t* lengths, size_t n_reads, const uint32_t* ks, int n_k,
+              const spk_count_opts* opts, spk_result** out) {
+  int rc;
+  if (!out) return fail(SPK_E_INVALID_ARG, "null output pointer");
+  *out = nullptr;
+  if ((rc = use_device(ctx))) return rc;
+  if ((rc = check_ks(ks, n_k))) return rc;
+  if (n_reads && (!offsets || !lengths)) return fail(SPK_E_INVALID_ARG, "null offsets/lengths");
+  if (data_len && !data) return fail(SPK_E_INVALID_ARG, "null data");
+  auto* res = new spk_result();
+  res->ctx = ctx;
+  res->stream = ctx->stream;
+  res->opts = resolve_opts(opts);
+  ReadsView rv;
+  rc = upload_reads(res, ctx->stream, data, data_len, offsets, lengths, n_reads, &rv);
+  if (!rc) rc = count_pipeline(ctx, ctx->stream, rv, 0, ks, n_k, res->opts, res);
+  if (rc) {
+    spk_result_free(res);
+    return rc;
+  }
+  // The reads are not needed after counting.
+  res->reads.release();
+  res->offs.release();
+  res->lens.release();
+  *out = res;
+  return SPK_OK;
+}
+
+int spk_count_device(spk_ctx* ctx, const uint8_t* d_data, size_t data_len,
+                     const uint64_t* d_offsets, const uint32_t* d_lengths, size_t n_reads,
+                     const uint32_t* ks, int n_k, const spk_count_opts* opts, spk_result** out) {
+  int rc;
+  if (!out) return fail(SPK_E_INVALID_ARG, "null output pointer");
+  *out = nullptr;
+  if ((rc = use_device(ctx))) return rc;
+  if ((rc = check_ks(ks, n_k))) return rc;
+  if (n_reads && (!d_offsets || !d_lengths || !d_data))
+    return fail(SPK_E_INVALID_ARG, "null device pointer");
+  auto* res = new spk_result();
+  res->ctx = ctx;
+  res->stream = ctx->stream;
+  res->opts = resolve_opts(opts);
+  ReadsView rv;
+  const uintptr_t a = (uintptr_t)d_data;
+  rv.words = (const uint64_t*)(a & ~(uintptr_t)7);
+  rv.byte_base = a & 7;
+  rv.offsets = d_offsets;
+  rv.lengths = d_lengths;
+  rv.n_reads = n_reads;
+  rv.data_len = data_len;
+  rv.err = nullptr;
+  rc = count_pipeline(ctx, ctx->stream, rv, 0, ks, n_k, res->opts, res);
+  if (rc) {
+    spk_result_free(res);
+    return rc;
+  }
+  *out = res;
+  return SPK_OK;
+}
+
+static int get_k(const spk_result* res, int ki) {
+  if (!res) return fail(SPK_E_INVALID_ARG, "null result");
+  if (ki < 0 || ki >= (int)res->ks.size()) return fail(SPK_E_INVALID_ARG, "k index out of range");
+  return use_device(res->ctx);
+}
+
+int spk_result_count(const spk_result* res, int* n_k) {
+  if (!res || !n_k) return fail(SPK_E_INVALID_ARG, "null argument");
+  *n_k = (int)res->ks.size();
+  return SPK_OK;
+}
+int spk_result_info_get(const spk_result* res, int ki, spk_result_info* info) {
+  int rc;
+  if ((rc = get_k(res, ki))) return rc;
+  if (!info) return fail(SPK_E_INVALID_ARG, "null info");
+  *info = res->ks[ki]->info;
+  return SPK_OK;
+}
+int spk_result_solid(spk_result* res, int ki, uint64_t* keys, uint32_t* counts, size_t* n) {
+  int rc;
+  if ((rc = get_k(res, ki))) return rc;
+  if (!n) return fail(SPK_E_INVALID_ARG, "null size pointer");
+  return download_list(res, ki, 0, true, keys, counts, n);
+}
+int spk_result_kmers(spk_result* res, int ki, uint32_t min_count, uint64_t* keys, uint32_t* counts,
+                     size_t* n) {
+  int rc;
+  if ((rc = get_k(res, ki))) return rc;
+  if (!n) return fail(SPK_E_INVALID_ARG, "null size pointer");
+  return download_list(res, ki, min_count, false, keys, counts, n);
+}
+int spk_result_edges(spk_result* res, int ki, uint64_t* edges, size_t* n) {
+  int rc;
+  if ((rc = get_k(res, ki))) return rc;
+  if (!n) return fail(SPK_E_INVALID_ARG, "null size pointer");
+  return download_edges(res, ki, edges, n);
+}
+int spk_result_bloom(spk_result* res, int ki, uint64_t* seen, uint64_t* twice, uint64_t* ref_solid) {
+  int rc;
+  if ((rc = get_k(res, ki))) return rc;
+  return download_bloom(res, ki, seen, twice, ref_solid);
+}
+int spk_result_table_view(spk_result* res, int ki, spk_table_view* v) {
+  int rc;
+  if ((rc = get_k(res, ki))) return rc;
+  if (!v) return fail(SPK_E_INVALID_ARG, "null view");
+  KResult& kr = *res->ks[ki];
+  v->keys = kr.table.keys;
+  v->counts = kr.table.counts;
+  v->capacity = kr.table.capacity;
+  v->key_limbs = (uint32_t)kr.nl;
+  v->key_stride = kr.table.stride;
+  v->k = kr.k;
+  v->cutoff = kr.info.cutoff;
+  return SPK_OK;
+}
+int spk_result_free(spk_result* res) {
+  if (!res) return SPK_OK;
+  cudaSetDevice(res->ctx->device);
+  cudaStream_t st = res->stream;
+  res->ks.clear();
+  res->reads.release();
+  res->offs.release();
+  res->lens.release();
+  cudaStreamSynchronize(st);
+  if (res->own_stream) cudaStreamDestroy(st);
+  delete res;
+  return SPK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+// spk_internal.h -- host-side structures shared by the libspk translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/spk.h"
+#include "spk_device.cuh"
+
+namespace spk {
+
+// ---- errors -----------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+#define SPK_CUDA(call)                                  \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return ::spk::cuda_fail(_e, #call); \
+  } while (0)
+
+// Host construction of the division constants of FastMod.
+FastMod make_fastmod(uint64_t d);
+
+// ---- device memory ------------------------------------------------------------
+// Stream-ordered allocations from the device's memory pool (cudaMallocAsync),
+// with the pool's release threshold raised so freed blocks stay cached
+// between jobs instead of returning to the driver.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p; bytes = o.bytes; st = o.st;
+      o.p = nullptr; o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  int alloc(size_t n, cudaStream_t s);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---- packed reads on the device --------------------------------------------
+struct ReadsView {
+  const uint64_t* words;    // packed bytes viewed as 64-bit words (8-byte aligned base)
+  const uint64_t* offsets;  // byte offset of each read, relative to byte_base
+  const uint32_t* lengths;  // bases per read
+  uint64_t n_reads;
+  uint64_t byte_base;       // byte offset of data[0] from `words`
+  uint64_t data_len;        // bytes of packed data; reads beyond it are rejected
+  int* err;                 // device error word: bit 2 set for an out-of-bounds read
+};
+
+// ---- count table --------------------------------------------------------------
+struct TableView {
+  uint64_t* keys;     // capacity * stride limbs (sequence value V)
+  uint32_t* counts;   // capacity
+  uint32_t* state;    // capacity (NL >= 3 only): 0 empty, 1 claiming, 2 ready
+  uint64_t capacity;  // power of two
+  uint32_t log2cap;
+  uint32_t stride;    // limbs per slot: NL, or 4 for NL == 3
+  uint32_t max_probe;
+  uint32_t pad;
+  int* err;           // device error word (bit 0: probe limit, bit 1: wait timeout)
+};
+
+// ---- per-k result ---------------------------------------------------------------
+struct KResult {
+  uint32_t k = 0;
+  int nl = 0;
+  spk_result_info info{};
+  FastMod fm{};
+  uint64_t num_words = 0;
+  DevBuf tiers;       // (seen, twice) word pairs, num_words * 16 bytes
+  DevBuf twice;       // compact twice tier, num_words * 8 bytes
+  DevBuf ref_solid;   // reference-semantics solid tier (SPK_F_REF_SOLID)
+  DevBuf tkeys, tcounts, tstate;  // count table
+  TableView table{};
+  DevBuf list[5];     // sorted k-mer list: limbs 0..nl-1 (SoA), counts in list[4]
+  DevBuf edges[4];    // sorted edge list: limbs (SoA)
+  int nle = 0;        // limbs per edge key
+  uint32_t list_min = 2;  // smallest count in the list
+};
+
+struct spk_result_impl;
+
+}  // namespace spk
+
+// ---- opaque handles --------------------------------------------------------------
+struct spk_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream in use (own_stream or a caller's)
+  cudaStream_t own_stream = nullptr;
+  cudaMemPool_t pool = nullptr;
+  int sm_count = 0;
+  size_t l2_bytes = 0;
+  spk::DevBuf scratch;      // small device scratch (counters, flags)
+  uint64_t* h_pinned = nullptr;  // small pinned host staging area
+  // serving
+  struct Server* server = nullptr;
+  std::mutex serve_mu;
+};
+
+struct spk_bloom {
+  spk_ctx* ctx = nullptr;
+  uint64_t size_bits = 0, num_words = 0;
+  spk::FastMod fm{};
+  spk::DevBuf seen, solid;
+};
+
+struct spk_result {
+  spk_ctx* ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  spk_count_opts opts{};
+  std::vector<std::unique_ptr<spk::KResult>> ks;
+  spk::DevBuf reads;  // device copy of the packed reads (when copied in by spk_count)
+  spk::DevBuf offs, lens;
+};
+
+namespace spk {
+// Count pipeline on device-resident reads (spk_count.cu).  `res` is filled
+// with one KResult per k.
+int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t max_len,
+                   const uint32_t* ks, int n_k, const spk_count_opts& o, spk_result* res);
+// Host copies of result lists (spk_count.cu).
+int download_list(spk_result* res, int ki, uint32_t min_count, bool solid_only, uint64_t* keys,
+                  uint32_t* counts, size_t* n_inout);
+int download_edges(spk_result* res, int ki, uint64_t* out, size_t* n_inout);
+int download_bloom(spk_result* res, int ki, uint64_t* seen, uint64_t* twice, uint64_t* ref_solid);
+// Radix sort of SoA keys (spk_sort.cu): keys[0..nl) limbs (least significant
+// first) and optional u32 values, sorted ascending by the low nbits of the
+// key.  The buffers may be swapped with temporaries.
+int radix_sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
+                    DevBuf* vals, uint32_t* launches = nullptr);
+// Exclusive scan of u32 in place (spk_sort.cu).
+int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches = nullptr);
+// Ordered compaction of a sorted SoA list into AoS Kmer256 limbs; *m is the
+// number of kept items (synchronises st).
+int ordered_convert(cudaStream_t st, int nl, uint64_t n, unsigned k, DevBuf* limbs,
+                    const uint32_t* cin, uint32_t min_count, DevBuf* out, DevBuf* cout,
+                    uint64_t* h_staging, uint64_t* m);
+}  // namespace spk

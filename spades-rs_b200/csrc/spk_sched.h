@@ -1,0 +1,169 @@
+// spk_sched.h -- admission scheduler of the serving loop (host-only C++).
+//
+// Jobs are admitted in arrival order while (a) their estimated device-memory
+// need fits the remaining HBM budget and (b) fewer than max_inflight jobs
+// run.  A job whose need exceeds the whole budget is rejected at once
+// (SPK_E_ADMISSION) instead of blocking the queue forever.  The runner
+// callback executes one job (on its own CUDA stream in libspk; a fake in the
+// CPU tests) on a worker thread; when it returns, its memory and slot are
+// released and the next jobs are admitted.  No CUDA here, so the policy is
+// tested on machines without a GPU.
+#pragma once
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace spk {
+
+struct SchedJob {
+  uint64_t ticket = 0;
+  uint64_t need = 0;                 // estimated device bytes
+  std::function<int(void**)> run;    // returns status, sets an opaque result
+  std::chrono::steady_clock::time_point t_submit, t_start, t_done;
+  bool done = false;
+  int status = 0;
+  void* result = nullptr;
+};
+
+class Scheduler {
+ public:
+  enum { kAdmissionError = 8 /* SPK_E_ADMISSION */ };
+
+  Scheduler(uint64_t budget, int max_inflight)
+      : budget_(budget), max_inflight_(max_inflight < 1 ? 1 : max_inflight) {
+    thread_ = std::thread([this] { loop(); });
+  }
+  ~Scheduler() { stop(); }
+
+  void stop() {
+    {
+      std::unique_lock<std::mutex> l(mu_);
+      if (stopping_) return;
+      stopping_ = true;
+      cv_.notify_all();
+    }
+    if (thread_.joinable()) thread_.join();
+    std::unique_lock<std::mutex> l(mu_);
+    // Queued jobs that were never admitted end as cancelled (admission error).
+    for (auto& j : queue_) {
+      j->done = true;
+      j->status = kAdmissionError;
+      j->t_start = j->t_done = std::chrono::steady_clock::now();
+    }
+    queue_.clear();
+    done_cv_.notify_all();
+    // Running jobs finish on their own worker threads.
+    done_cv_.wait(l, [&] { return inflight_ == 0; });
+  }
+
+  uint64_t submit(uint64_t need, std::function<int(void**)> run) {
+    std::unique_lock<std::mutex> l(mu_);
+    auto j = std::make_shared<SchedJob>();
+    j->ticket = ++next_ticket_;
+    j->need = need;
+    j->run = std::move(run);
+    j->t_submit = std::chrono::steady_clock::now();
+    jobs_[j->ticket] = j;
+    if (need > budget_) {  // can never fit: fail now rather than block the queue
+      j->done = true;
+      j->status = kAdmissionError;
+      j->t_start = j->t_done = j->t_submit;
+    } else {
+      queue_.push_back(j);
+    }
+    cv_.notify_all();
+    return j->ticket;
+  }
+
+  // 1 = done, 0 = running/queued, -1 = unknown ticket
+  int poll(uint64_t ticket) {
+    std::unique_lock<std::mutex> l(mu_);
+    auto it = jobs_.find(ticket);
+    if (it == jobs_.end()) return -1;
+    return it->second->done ? 1 : 0;
+  }
+
+  // Waits up to timeout_ms (< 0: forever).  Returns -1 unknown ticket, 0 not
+  // ready, 1 done (the job is removed and its fields copied out).
+  int wait(uint64_t ticket, int timeout_ms, int* status, void** result, double* latency_ms) {
+    std::unique_lock<std::mutex> l(mu_);
+    auto it = jobs_.find(ticket);
+    if (it == jobs_.end()) return -1;
+    auto j = it->second;
+    auto pred = [&] { return j->done; };
+    if (timeout_ms < 0) done_cv_.wait(l, pred);
+    else if (!done_cv_.wait_for(l, std::chrono::milliseconds(timeout_ms), pred)) return 0;
+    if (status) *status = j->status;
+    if (result) *result = j->result;
+    if (latency_ms)
+      *latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
+    jobs_.erase(ticket);
+    return 1;
+  }
+
+  uint64_t in_use() {
+    std::unique_lock<std::mutex> l(mu_);
+    return in_use_;
+  }
+  int inflight() {
+    std::unique_lock<std::mutex> l(mu_);
+    return inflight_;
+  }
+  int peak_inflight() {
+    std::unique_lock<std::mutex> l(mu_);
+    return peak_inflight_;
+  }
+
+ private:
+  void loop() {
+    std::unique_lock<std::mutex> l(mu_);
+    for (;;) {
+      cv_.wait(l, [&] {
+        return stopping_ || (!queue_.empty() && inflight_ < max_inflight_ &&
+                             in_use_ + queue_.front()->need <= budget_);
+      });
+      if (stopping_) break;
+      auto j = queue_.front();
+      queue_.pop_front();
+      in_use_ += j->need;
+      inflight_++;
+      if (inflight_ > peak_inflight_) peak_inflight_ = inflight_;
+      j->t_start = std::chrono::steady_clock::now();
+      std::thread([this, j] {
+        void* r = nullptr;
+        int st = j->run(&r);
+        std::unique_lock<std::mutex> l2(mu_);
+        j->status = st;
+        j->result = r;
+        j->t_done = std::chrono::steady_clock::now();
+        j->done = true;
+        in_use_ -= j->need;
+        inflight_--;
+        cv_.notify_all();
+        done_cv_.notify_all();
+      }).detach();
+    }
+  }
+
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::deque<std::shared_ptr<SchedJob>> queue_;
+  std::map<uint64_t, std::shared_ptr<SchedJob>> jobs_;
+  std::thread thread_;
+  uint64_t budget_;
+  uint64_t in_use_ = 0;
+  uint64_t next_ticket_ = 0;
+  int max_inflight_;
+  int inflight_ = 0;
+  int peak_inflight_ = 0;
+  bool stopping_ = false;
+};
+
+}  // namespace spk

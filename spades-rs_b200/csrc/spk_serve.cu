@@ -1,0 +1,181 @@
+// spk_serve.cu -- serving loop: admission by HBM budget, concurrent jobs on
+// separate streams, results kept resident until the caller takes them.
+//
+// spades-rs has no serving mode; this is the request loop around the counting
+// path that keeps count tables resident for the downstream graph build
+// (CompactedGraph::build, src/graph.rs:65-69).  The admission rule follows
+// the reference's memory governor idea (src/memory.rs:25-92: budget a share
+// of the available memory, size the Bloom to it), applied to HBM.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "spk_internal.h"
+#include "spk_sched.h"
+
+struct Server {
+  spk::Scheduler* sched = nullptr;
+  uint64_t budget = 0;
+};
+
+namespace spk {
+
+int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t data_len,
+                 const uint64_t* offsets, const uint32_t* lengths, size_t n_reads, ReadsView* rv);
+
+static uint64_t next_pow2_u64(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// Device bytes a job is expected to hold at its peak: reads, both Bloom
+// tiers plus the compact twice tier, and a count table plus list sized for
+// distinct admitted k-mers of up to 15% of the occurrences (at 20-200x
+// coverage the measured share is 2-10%).  A job that outgrows the estimate
+// still runs; it only makes concurrent jobs less likely to fit.
+uint64_t job_estimate(const spk_job& j) {
+  spk_count_opts o = j.opts;
+  const uint64_t bloom_bits = o.bloom_bits ? o.bloom_bits : (512ULL << 20);
+  const uint64_t words = std::max<uint64_t>((bloom_bits + 63) / 64, 1);
+  uint64_t bytes = j.data_len + 64 + j.n_reads * 12;
+  uint64_t total_bases = 0;
+  // Bases from the packed length (4 per byte) bound the occurrences.
+  total_bases = (uint64_t)j.data_len * 4;
+  uint64_t peak_k = 0;
+  for (int i = 0; i < j.n_k; i++) {
+    const uint32_t k = j.ks ? j.ks[i] : 31;
+    const uint64_t occ = total_bases;
+    const uint64_t cap = std::max<uint64_t>(next_pow2_u64(2 * (occ * 15 / 100) + 1024), 1024);
+    const uint64_t nl = (k + 31) / 32, stride = nl == 3 ? 4 : nl;
+    uint64_t b = words * 24 + (o.flags & SPK_F_REF_SOLID ? words * 8 : 0);
+    b += cap * (stride * 8 + 4 + (nl >= 3 ? 4 : 0));  // table
+    b += cap * (nl * 8 + 4) * 2;                       // list + sort temporaries
+    // Results of earlier k stay resident while later k run.
+    peak_k += b;
+  }
+  return bytes + peak_k;
+}
+
+static int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out) {
+  cudaSetDevice(ctx->device);
+  cudaStream_t st;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(e, "job stream");
+  auto* res = new spk_result();
+  res->ctx = ctx;
+  res->stream = st;
+  res->own_stream = true;
+  res->opts = j.opts;
+  if (!res->opts.bloom_bits) res->opts.bloom_bits = 512ULL << 20;
+  if (!res->opts.list_min_count) res->opts.list_min_count = 2;
+  ReadsView rv;
+  int rc = upload_reads(res, st, j.data, j.data_len, j.offsets, j.lengths, j.n_reads, &rv);
+  if (!rc) rc = count_pipeline(ctx, st, rv, 0, ks.data(), (int)ks.size(), res->opts, res);
+  res->reads.release();
+  res->offs.release();
+  res->lens.release();
+  if (rc) {
+    spk_result_free(res);
+    return rc;
+  }
+  *out = res;
+  return SPK_OK;
+}
+
+void serve_shutdown(spk_ctx* ctx) {
+  std::unique_lock<std::mutex> l(ctx->serve_mu);
+  if (!ctx->server) return;
+  ctx->server->sched->stop();
+  delete ctx->server->sched;
+  delete ctx->server;
+  ctx->server = nullptr;
+}
+
+}  // namespace spk
+
+using namespace spk;
+
+extern "C" {
+
+int spk_job_hbm_estimate(const spk_job* job, uint64_t* bytes) {
+  if (!job || !bytes) return fail(SPK_E_INVALID_ARG, "null argument");
+  *bytes = job_estimate(*job);
+  return SPK_OK;
+}
+
+int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight) {
+  if (!ctx) return fail(SPK_E_INVALID_ARG, "null context");
+  SPK_CUDA(cudaSetDevice(ctx->device));
+  std::unique_lock<std::mutex> l(ctx->serve_mu);
+  if (ctx->server) return fail(SPK_E_INVALID_ARG, "serving loop already running");
+  if (!hbm_budget_bytes) {
+    size_t f = 0, t = 0;
+    SPK_CUDA(cudaMemGetInfo(&f, &t));
+    hbm_budget_bytes = (uint64_t)(f * 0.9);
+  }
+  auto* s = new Server();
+  s->budget = hbm_budget_bytes;
+  s->sched = new Scheduler(hbm_budget_bytes, max_inflight > 0 ? max_inflight : 4);
+  ctx->server = s;
+  return SPK_OK;
+}
+
+int spk_serve_stop(spk_ctx* ctx) {
+  if (!ctx) return fail(SPK_E_INVALID_ARG, "null context");
+  serve_shutdown(ctx);
+  return SPK_OK;
+}
+
+int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket) {
+  if (!ctx || !job || !ticket) return fail(SPK_E_INVALID_ARG, "null argument");
+  if (!job->ks || job->n_k < 1) return fail(SPK_E_INVALID_ARG, "job has no k");
+  for (int i = 0; i < job->n_k; i++)
+    if (job->ks[i] < 1 || job->ks[i] > 127) return fail(SPK_E_INVALID_K, "k outside 1..=127");
+  std::unique_lock<std::mutex> l(ctx->serve_mu);
+  if (!ctx->server) return fail(SPK_E_INVALID_ARG, "serving loop not started");
+  spk_job j = *job;
+  std::vector<uint32_t> ks(job->ks, job->ks + job->n_k);
+  const uint64_t need = job_estimate(j);
+  *ticket = ctx->server->sched->submit(need, [ctx, j, ks](void** out) { return run_job(ctx, j, ks, out); });
+  return SPK_OK;
+}
+
+int spk_poll(spk_ctx* ctx, uint64_t ticket, int* done) {
+  if (!ctx || !done) return fail(SPK_E_INVALID_ARG, "null argument");
+  std::unique_lock<std::mutex> l(ctx->serve_mu);
+  if (!ctx->server) return fail(SPK_E_INVALID_ARG, "serving loop not started");
+  int r = ctx->server->sched->poll(ticket);
+  if (r < 0) return fail(SPK_E_NOT_FOUND, "unknown ticket");
+  *done = r;
+  return SPK_OK;
+}
+
+int spk_wait(spk_ctx* ctx, uint64_t ticket, int timeout_ms, spk_result** out, double* latency_ms) {
+  if (!ctx || !out) return fail(SPK_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  Scheduler* sched;
+  {
+    std::unique_lock<std::mutex> l(ctx->serve_mu);
+    if (!ctx->server) return fail(SPK_E_INVALID_ARG, "serving loop not started");
+    sched = ctx->server->sched;
+  }
+  int status = 0;
+  void* r = nullptr;
+  int w = sched->wait(ticket, timeout_ms, &status, &r, latency_ms);
+  if (w < 0) return fail(SPK_E_NOT_FOUND, "unknown ticket");
+  if (w == 0) return fail(SPK_E_NOT_READY, "job not finished");
+  if (status == SPK_E_ADMISSION)
+    return fail(SPK_E_ADMISSION, "job needs more device memory than the serving budget");
+  if (status) return status;
+  *out = (spk_result*)r;
+  return SPK_OK;
+}
+
+// Batched counting of independent samples.  Each sample gets its own Bloom
+// and table; the samples run concurrently on a pool of streams.
+int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, spk_result** results);
+
+}  // extern "C"

@@ -1,0 +1,380 @@
+// spk_sort.cu -- LSD radix sort of multi-limb keys (SoA) and an ordered
+// stream compaction, both written for this library.
+//
+// Sort: 8-bit digits, one pass per digit of the significant bits.  Each pass
+// is a tile histogram, one exclusive scan over (digit, tile) and a stable
+// scatter.  Inside a tile, items are ranked per warp with __match_any_sync on
+// the digit, then offset by the per-warp prefix of each digit, so equal
+// digits keep their input order (stability across passes).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <utility>
+
+#include "spk_internal.h"
+
+namespace spk {
+
+constexpr unsigned FULLM = 0xffffffffu;
+constexpr int RS_BLOCK = 256;
+constexpr int RS_WARPS = RS_BLOCK / 32;
+constexpr int RS_IPT = 8;
+constexpr int RS_TILE = RS_BLOCK * RS_IPT;  // 2048 items
+
+__global__ void __launch_bounds__(RS_BLOCK) k_rs_hist(const uint64_t* __restrict__ limb, uint64_t n,
+                                                       unsigned sh, uint32_t* __restrict__ hist,
+                                                       uint32_t ntiles) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+#pragma unroll
+  for (int j = 0; j < RS_IPT; j++) {
+    const uint64_t i = base + j * RS_BLOCK + threadIdx.x;
+    if (i < n) atomicAdd(&h[(unsigned)(__ldg(limb + i) >> sh) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of n u32 values in place, one block of 1024 threads.  Used
+// for short arrays (the per-chunk sums of scan_u32).
+__global__ void __launch_bounds__(1024) k_scan_u32(uint32_t* __restrict__ a, uint64_t n) {
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t carry_s;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (uint64_t base = 0; base < n; base += 1024) {
+    const uint64_t i = base + threadIdx.x;
+    const uint32_t v = i < n ? a[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t t = __shfl_up_sync(FULLM, x, d);
+      if ((int)lane >= d) x += t;
+    }
+    if (lane == 31) ws[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t y = ws[lane];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        uint32_t t = __shfl_up_sync(FULLM, y, d);
+        if ((int)lane >= d) y += t;
+      }
+      ws[lane] = y;
+    }
+    __syncthreads();
+    const uint32_t carry = carry_s;
+    const uint32_t excl = carry + (warp ? ws[warp - 1] : 0u) + x - v;
+    if (i < n) a[i] = excl;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry_s = carry + ws[31];
+    __syncthreads();
+  }
+}
+
+// Multi-block exclusive scan: chunk sums, a scan of the sums, then a
+// block-wide scan of every chunk with its offset.
+constexpr int SC_BLOCK = 256, SC_IPT = 16, SC_CHUNK = SC_BLOCK * SC_IPT;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* ws, uint32_t* total) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t t = __shfl_up_sync(FULLM, x, d);
+    if ((int)lane >= d) x += t;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  uint32_t pre = 0, tot = 0;
+  for (unsigned w = 0; w < blockDim.x / 32; w++) {
+    const uint32_t s = ws[w];
+    if (w < warp) pre += s;
+    tot += s;
+  }
+  __syncthreads();
+  if (total) *total = tot;
+  return pre + x - v;
+}
+
+__global__ void __launch_bounds__(SC_BLOCK) k_scan_reduce(const uint32_t* __restrict__ a, uint64_t n,
+                                                           uint32_t* __restrict__ sums) {
+  __shared__ uint32_t ws[SC_BLOCK / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * SC_CHUNK;
+  uint32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < SC_IPT; j++) {
+    const uint64_t i = base + j * SC_BLOCK + threadIdx.x;
+    if (i < n) s += a[i];
+  }
+  uint32_t tot;
+  block_excl_scan(s, ws, &tot);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SC_BLOCK) k_scan_apply(uint32_t* __restrict__ a, uint64_t n,
+                                                          const uint32_t* __restrict__ sums) {
+  __shared__ uint32_t ws[SC_BLOCK / 32];
+  // Thread t owns the contiguous items [t*IPT, t*IPT + IPT) of the chunk.
+  const uint64_t base = (uint64_t)blockIdx.x * SC_CHUNK + (uint64_t)threadIdx.x * SC_IPT;
+  uint32_t v[SC_IPT];
+  uint32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < SC_IPT; j++) {
+    v[j] = base + j < n ? a[base + j] : 0u;
+    s += v[j];
+  }
+  uint32_t run = sums[blockIdx.x] + block_excl_scan(s, ws, nullptr);
+#pragma unroll
+  for (int j = 0; j < SC_IPT; j++) {
+    if (base + j < n) a[base + j] = run;
+    run += v[j];
+  }
+}
+
+int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches) {
+  const uint64_t nb = (n + SC_CHUNK - 1) / SC_CHUNK;
+  int rc;
+  if (sums.bytes < nb * 4 && (rc = sums.alloc(nb * 4, st))) return rc;
+  k_scan_reduce<<<(unsigned)nb, SC_BLOCK, 0, st>>>(a, n, sums.as<uint32_t>());
+  k_scan_u32<<<1, 1024, 0, st>>>(sums.as<uint32_t>(), nb);
+  k_scan_apply<<<(unsigned)nb, SC_BLOCK, 0, st>>>(a, n, sums.as<uint32_t>());
+  SPK_CUDA(cudaGetLastError());
+  if (launches) *launches += 3;
+  return SPK_OK;
+}
+
+template <int NL, bool HASV>
+__global__ void __launch_bounds__(RS_BLOCK) k_rs_scatter(
+    const uint64_t* __restrict__ s0, const uint64_t* __restrict__ s1, const uint64_t* __restrict__ s2,
+    const uint64_t* __restrict__ s3, const uint32_t* __restrict__ sv, uint64_t* __restrict__ d0,
+    uint64_t* __restrict__ d1, uint64_t* __restrict__ d2, uint64_t* __restrict__ d3,
+    uint32_t* __restrict__ dv, uint64_t n, unsigned dlimb, unsigned sh,
+    const uint32_t* __restrict__ offs, uint32_t ntiles) {
+  __shared__ uint32_t wh[RS_WARPS][256];
+  __shared__ uint32_t goff[256];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = lanemask_lt();
+  const uint64_t base = (uint64_t)blockIdx.x * RS_TILE + warp * (32 * RS_IPT);
+
+  uint64_t key[RS_IPT][NL];
+  uint32_t val[RS_IPT], dig[RS_IPT], rank[RS_IPT];
+#pragma unroll
+  for (int r = 0; r < RS_IPT; r++) {
+    const uint64_t i = base + r * 32 + lane;
+    const bool ok = i < n;
+#pragma unroll
+    for (int j = 0; j < NL; j++) {
+      const uint64_t* s = j == 0 ? s0 : j == 1 ? s1 : j == 2 ? s2 : s3;
+      key[r][j] = ok ? __ldg(s + i) : 0;
+    }
+    val[r] = (HASV && ok) ? __ldg(sv + i) : 0u;
+    uint64_t dl = 0;
+#pragma unroll
+    for (int j = 0; j < NL; j++)
+      if ((unsigned)j == dlimb) dl = key[r][j];
+    dig[r] = ok ? (unsigned)(dl >> sh) & 255u : 0xFFFFFFFFu;
+  }
+  for (int j = threadIdx.x; j < RS_WARPS * 256; j += RS_BLOCK) (&wh[0][0])[j] = 0;
+  goff[threadIdx.x] = offs[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RS_IPT; r++) {
+    const bool ok = dig[r] != 0xFFFFFFFFu;
+    const unsigned vm = __ballot_sync(FULLM, ok);
+    unsigned peers = 0;
+    if (ok) {
+      peers = __match_any_sync(vm, dig[r]);
+      rank[r] = wh[warp][dig[r]] + __popc(peers & lt);
+    }
+    __syncwarp();
+    if (ok && lane == (unsigned)(__ffs(peers) - 1)) wh[warp][dig[r]] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  {
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) {
+      const uint32_t x = wh[w][threadIdx.x];
+      wh[w][threadIdx.x] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RS_IPT; r++) {
+    if (dig[r] == 0xFFFFFFFFu) continue;
+    const uint64_t p = (uint64_t)goff[dig[r]] + wh[warp][dig[r]] + rank[r];
+    d0[p] = key[r][0];
+    if (NL > 1) d1[p] = key[r][NL > 1 ? 1 : 0];
+    if (NL > 2) d2[p] = key[r][NL > 2 ? 2 : 0];
+    if (NL > 3) d3[p] = key[r][NL > 3 ? 3 : 0];
+    if (HASV) dv[p] = val[r];
+  }
+}
+
+template <int NL>
+static void launch_scatter(cudaStream_t st, uint64_t* src[4], uint32_t* sv, uint64_t* dst[4],
+                           uint32_t* dv, uint64_t n, unsigned dlimb, unsigned sh,
+                           const uint32_t* offs, uint32_t ntiles) {
+  if (sv)
+    k_rs_scatter<NL, true><<<ntiles, RS_BLOCK, 0, st>>>(src[0], src[1], src[2], src[3], sv, dst[0],
+                                                      dst[1], dst[2], dst[3], dv, n, dlimb, sh,
+                                                      offs, ntiles);
+  else
+    k_rs_scatter<NL, false><<<ntiles, RS_BLOCK, 0, st>>>(src[0], src[1], src[2], src[3], nullptr,
+                                                       dst[0], dst[1], dst[2], dst[3], nullptr, n,
+                                                       dlimb, sh, offs, ntiles);
+}
+
+int radix_sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
+                    DevBuf* vals, uint32_t* launches) {
+  if (n <= 1) return SPK_OK;
+  if (n >= (1ULL << 32)) return fail(SPK_E_INVALID_ARG, "sort: more than 2^32 items");
+  const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+  int rc;
+  DevBuf tk[4], tv, hist, sums;
+  for (int j = 0; j < nl; j++)
+    if ((rc = tk[j].alloc(n * 8, st))) return rc;
+  if (vals && (rc = tv.alloc(n * 4, st))) return rc;
+  if ((rc = hist.alloc((uint64_t)256 * ntiles * 4, st))) return rc;
+  uint64_t* a[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t* b[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int j = 0; j < nl; j++) { a[j] = keys[j].as<uint64_t>(); b[j] = tk[j].as<uint64_t>(); }
+  uint32_t* av = vals ? vals->as<uint32_t>() : nullptr;
+  uint32_t* bv = vals ? tv.as<uint32_t>() : nullptr;
+  const unsigned passes = (nbits + 7) / 8;
+  for (unsigned p = 0; p < passes; p++) {
+    const unsigned bit = 8 * p, dlimb = bit / 64, sh = bit % 64;
+    k_rs_hist<<<ntiles, RS_BLOCK, 0, st>>>(a[dlimb], n, sh, hist.as<uint32_t>(), ntiles);
+    if ((rc = scan_u32(st, hist.as<uint32_t>(), (uint64_t)256 * ntiles, sums, launches))) return rc;
+    if (launches) *launches += 2;
+    switch (nl) {
+      case 1: launch_scatter<1>(st, a, av, b, bv, n, dlimb, sh, hist.as<uint32_t>(), ntiles); break;
+      case 2: launch_scatter<2>(st, a, av, b, bv, n, dlimb, sh, hist.as<uint32_t>(), ntiles); break;
+      case 3: launch_scatter<3>(st, a, av, b, bv, n, dlimb, sh, hist.as<uint32_t>(), ntiles); break;
+      default: launch_scatter<4>(st, a, av, b, bv, n, dlimb, sh, hist.as<uint32_t>(), ntiles); break;
+    }
+    SPK_CUDA(cudaGetLastError());
+    for (int j = 0; j < nl; j++) std::swap(a[j], b[j]);
+    std::swap(av, bv);
+  }
+  if (passes & 1) {  // sorted data sits in the temporaries: hand them over
+    for (int j = 0; j < nl; j++) std::swap(keys[j], tk[j]);
+    if (vals) std::swap(*vals, tv);
+  }
+  return SPK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ordered compaction with conversion of sequence values to Kmer256 limbs.
+// Item i of a sorted SoA list is kept when cin == nullptr or cin[i] >=
+// min_count; kept items are written in list order as AoS Kmer256 limbs.
+// ---------------------------------------------------------------------------
+constexpr int OC_BLOCK = 256, OC_IPT = 16, OC_TILE = OC_BLOCK * OC_IPT;
+
+__global__ void __launch_bounds__(OC_BLOCK) k_oc_count(const uint32_t* __restrict__ cin, uint64_t n,
+                                                        uint32_t min_count,
+                                                        uint32_t* __restrict__ bc) {
+  __shared__ uint32_t s;
+  if (threadIdx.x == 0) s = 0;
+  __syncthreads();
+  uint32_t c = 0;
+  const uint64_t base = (uint64_t)blockIdx.x * OC_TILE;
+  for (int j = 0; j < OC_IPT; j++) {
+    const uint64_t i = base + j * OC_BLOCK + threadIdx.x;
+    c += i < n && (cin == nullptr || cin[i] >= min_count);
+  }
+  atomicAdd(&s, c);
+  __syncthreads();
+  if (threadIdx.x == 0) bc[blockIdx.x] = s;
+}
+
+template <int NL>
+__global__ void __launch_bounds__(OC_BLOCK) k_oc_write(const uint64_t* l0, const uint64_t* l1,
+                                                        const uint64_t* l2, const uint64_t* l3,
+                                                        const uint32_t* __restrict__ cin, uint64_t n,
+                                                        unsigned k, uint32_t min_count,
+                                                        const uint32_t* __restrict__ bc,
+                                                        uint64_t* __restrict__ out,
+                                                        uint32_t* __restrict__ cout) {
+  __shared__ uint32_t ws[OC_BLOCK / 32];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // Thread t owns the contiguous items [t*IPT, t*IPT+IPT) of the tile.
+  const uint64_t base = (uint64_t)blockIdx.x * OC_TILE + (uint64_t)threadIdx.x * OC_IPT;
+  uint32_t keepmask = 0;
+#pragma unroll
+  for (int j = 0; j < OC_IPT; j++) {
+    const uint64_t i = base + j;
+    if (i < n && (cin == nullptr || cin[i] >= min_count)) keepmask |= 1u << j;
+  }
+  const uint32_t c = __popc(keepmask);
+  uint32_t x = c;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t t = __shfl_up_sync(FULLM, x, d);
+    if ((int)lane >= d) x += t;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  uint32_t wpre = 0;
+  for (unsigned w = 0; w < warp; w++) wpre += ws[w];
+  uint64_t p = (uint64_t)bc[blockIdx.x] + wpre + x - c;
+#pragma unroll 1
+  for (int j = 0; j < OC_IPT; j++) {
+    if (!(keepmask & (1u << j))) continue;
+    const uint64_t i = base + j;
+    Seq<NL> V;
+    V.v[0] = l0[i];
+    if (NL > 1) V.v[NL > 1 ? 1 : 0] = l1[i];
+    if (NL > 2) V.v[NL > 2 ? 2 : 0] = l2[i];
+    if (NL > 3) V.v[NL > 3 ? 3 : 0] = l3[i];
+    uint64_t w[4];
+    kmer256_limbs<NL>(V, k, w);
+#pragma unroll
+    for (int q = 0; q < NL; q++) out[p * NL + q] = w[q];
+    if (cout) cout[p] = cin[i];
+    p++;
+  }
+}
+
+// Returns the number of kept items in *m (host value; synchronises st).
+int ordered_convert(cudaStream_t st, int nl, uint64_t n, unsigned k, DevBuf* limbs,
+                    const uint32_t* cin, uint32_t min_count, DevBuf* out, DevBuf* cout,
+                    uint64_t* h_staging, uint64_t* m) {
+  int rc;
+  const uint32_t nt = (uint32_t)std::max<uint64_t>((n + OC_TILE - 1) / OC_TILE, 1);
+  DevBuf bc;
+  if ((rc = bc.alloc((uint64_t)(nt + 1) * 4, st))) return rc;
+  SPK_CUDA(cudaMemsetAsync(bc.p, 0, (uint64_t)(nt + 1) * 4, st));
+  if (n) {
+    k_oc_count<<<nt, OC_BLOCK, 0, st>>>(cin, n, min_count, bc.as<uint32_t>());
+  }
+  DevBuf sums;
+  if ((rc = scan_u32(st, bc.as<uint32_t>(), nt + 1, sums))) return rc;
+  SPK_CUDA(cudaMemcpyAsync(h_staging, bc.as<uint32_t>() + nt, 4, cudaMemcpyDeviceToHost, st));
+  SPK_CUDA(cudaStreamSynchronize(st));
+  *m = (uint64_t)((uint32_t*)h_staging)[0];
+  if ((rc = out->alloc(std::max<uint64_t>(*m, 1) * nl * 8, st))) return rc;
+  if (cout && (rc = cout->alloc(std::max<uint64_t>(*m, 1) * 4, st))) return rc;
+  if (n && *m) {
+    const uint64_t* p[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int j = 0; j < nl; j++) p[j] = limbs[j].as<uint64_t>();
+    uint64_t* o = out->as<uint64_t>();
+    uint32_t* oc = cout ? cout->as<uint32_t>() : nullptr;
+    switch (nl) {
+      case 1: k_oc_write<1><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
+      case 2: k_oc_write<2><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
+      case 3: k_oc_write<3><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
+      default: k_oc_write<4><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
+    }
+    SPK_CUDA(cudaGetLastError());
+  }
+  return SPK_OK;
+}
+
+}  // namespace spk

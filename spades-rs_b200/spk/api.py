@@ -1,0 +1,442 @@
+"""Reference-shaped Python API over libspk (see package docstring)."""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass, field
+from typing import Dict, Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from ._lib import (SPK_F_EDGES, SPK_F_KEEP_BLOOM, CountOpts, JobC, ResultInfo, SpkError,
+                   TableView, check, lib, u8p, u32p, u64p, vp)
+
+Kmer256 = Tuple[int, int]  # (lo, hi) as in src/dna.rs:138
+
+_M64 = (1 << 64) - 1
+
+
+def nlimbs(k: int) -> int:
+    """u64 limbs per k-mer key in lists: ceil(k/32)."""
+    return (k + 31) // 32
+
+
+def limbs_from_kmer256(x: Kmer256, n: int = 4) -> List[int]:
+    lo, hi = x
+    w = [lo & _M64, (lo >> 64) & _M64, hi & _M64, (hi >> 64) & _M64]
+    return w[:n]
+
+
+def kmer256_from_limbs(row) -> Kmer256:
+    w = [int(v) for v in row] + [0] * (4 - len(row))
+    return (w[0] | (w[1] << 64), w[2] | (w[3] << 64))
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+# ---------------------------------------------------------------------------
+# Context
+# ---------------------------------------------------------------------------
+class Context:
+    """An spk_ctx: one device, one stream, a cached device memory pool."""
+
+    def __init__(self, device: int = 0):
+        h = vp()
+        check(lib().spk_ctx_create(device, C.byref(h)))
+        self.h = h.value
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().spk_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, cuda_stream: Optional[int]) -> None:
+        """Run this context's work on a caller-owned cudaStream_t (None: its own)."""
+        check(lib().spk_ctx_set_stream(self.h, cuda_stream))
+
+    def memory(self) -> Tuple[int, int]:
+        r, f = C.c_uint64(), C.c_uint64()
+        check(lib().spk_ctx_memory(self.h, C.byref(r), C.byref(f)))
+        return r.value, f.value
+
+
+_DEFAULT: Dict[int, Context] = {}
+_DEFAULT_LOCK = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    with _DEFAULT_LOCK:
+        if device not in _DEFAULT:
+            _DEFAULT[device] = Context(device)
+        return _DEFAULT[device]
+
+
+# ---------------------------------------------------------------------------
+# TwoTierFilter (src/bloom.rs:13-131)
+# ---------------------------------------------------------------------------
+class TwoTierFilter:
+    """Device-resident ``TwoTierFilter``; single-key methods match the reference's.
+
+    Batched methods take numpy arrays and return what per-key calls in array
+    order would return.
+    """
+
+    def __init__(self, capacity_bits: int, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        h = vp()
+        check(lib().spk_bloom_create(self.ctx.h, capacity_bits, C.byref(h)))
+        self.h = h.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().spk_bloom_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def size_bits(self) -> int:
+        return int(lib().spk_bloom_size_bits(self.h))
+
+    def memory_usage_bytes(self) -> int:          # bloom.rs:129-131
+        return int(lib().spk_bloom_memory_usage_bytes(self.h))
+
+    # batched
+    def insert_batch(self, keys) -> np.ndarray:   # bloom.rs:48-50 per key
+        k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1)
+        out = np.zeros(max(k.size, 1), dtype=np.uint8)
+        check(lib().spk_bloom_insert_u64(self.h, _ptr(k, u64p), k.size, _ptr(out, u8p)))
+        return out[: k.size].astype(bool)
+
+    def insert_kmer256_batch(self, keys4) -> np.ndarray:  # bloom.rs:83-107 per key
+        k = np.ascontiguousarray(keys4, dtype=np.uint64).reshape(-1, 4)
+        out = np.zeros(max(k.shape[0], 1), dtype=np.uint8)
+        check(lib().spk_bloom_insert_k256(self.h, _ptr(k, u64p), k.shape[0], _ptr(out, u8p)))
+        return out[: k.shape[0]].astype(bool)
+
+    def is_solid_batch(self, keys) -> np.ndarray:  # bloom.rs:54-56 per key
+        k = np.ascontiguousarray(keys, dtype=np.uint64).reshape(-1)
+        out = np.zeros(max(k.size, 1), dtype=np.uint8)
+        check(lib().spk_bloom_is_solid_u64(self.h, _ptr(k, u64p), k.size, _ptr(out, u8p)))
+        return out[: k.size].astype(bool)
+
+    def is_solid_kmer256_batch(self, keys4) -> np.ndarray:  # bloom.rs:111-126 per key
+        k = np.ascontiguousarray(keys4, dtype=np.uint64).reshape(-1, 4)
+        out = np.zeros(max(k.shape[0], 1), dtype=np.uint8)
+        check(lib().spk_bloom_is_solid_k256(self.h, _ptr(k, u64p), k.shape[0], _ptr(out, u8p)))
+        return out[: k.shape[0]].astype(bool)
+
+    # single key, reference names
+    def insert(self, kmer: int) -> bool:
+        return bool(self.insert_batch(np.array([kmer], dtype=np.uint64))[0])
+
+    def is_solid(self, kmer: int) -> bool:
+        return bool(self.is_solid_batch(np.array([kmer], dtype=np.uint64))[0])
+
+    def insert_kmer256(self, kmer: Kmer256) -> bool:
+        return bool(self.insert_kmer256_batch(np.array([limbs_from_kmer256(kmer)], dtype=np.uint64))[0])
+
+    def is_solid_kmer256(self, kmer: Kmer256) -> bool:
+        return bool(self.is_solid_kmer256_batch(np.array([limbs_from_kmer256(kmer)], dtype=np.uint64))[0])
+
+    def download(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(seen_bits, solid_bits) word arrays of src/bloom.rs:19-21."""
+        n = self.size_bits // 64
+        seen = np.zeros(n, dtype=np.uint64)
+        solid = np.zeros(n, dtype=np.uint64)
+        check(lib().spk_bloom_download(self.h, _ptr(seen, u64p), _ptr(solid, u64p)))
+        return seen, solid
+
+
+# ---------------------------------------------------------------------------
+# Packed reads (src/packed_reads.rs:42-59)
+# ---------------------------------------------------------------------------
+_CODE = np.full(256, 255, dtype=np.uint8)
+for _c, _v in zip(b"AaCcGgTt", (0, 0, 1, 1, 2, 2, 3, 3)):
+    _CODE[_c] = _v
+
+
+@dataclass
+class PackedReads:
+    """The reference PackedReads layout: 2-bit MSB-first bytes, byte-aligned reads."""
+
+    data: np.ndarray
+    offsets: np.ndarray
+    lengths: np.ndarray
+    pe_count: int = 0
+
+    def __len__(self) -> int:
+        return int(self.lengths.size)
+
+    @staticmethod
+    def from_clean_reads(reads: Iterable) -> "PackedReads":
+        """pack_clean (src/packed_reads.rs:547-578) of each read, in order; non-ACGT bytes are skipped."""
+        codes, offsets, lengths, data_parts = [], [], [], []
+        off = 0
+        for r in reads:
+            b = np.frombuffer(r.encode() if isinstance(r, str) else bytes(r), dtype=np.uint8)
+            c = _CODE[b]
+            c = c[c != 255]
+            n = c.size
+            nb = (n + 3) // 4
+            pad = np.zeros(nb * 4, dtype=np.uint8)
+            pad[:n] = c
+            q = pad.reshape(-1, 4) if nb else pad.reshape(0, 4)
+            packed = (q[:, 0] << 6) | (q[:, 1] << 4) | (q[:, 2] << 2) | q[:, 3]
+            data_parts.append(packed.astype(np.uint8))
+            offsets.append(off)
+            lengths.append(n)
+            off += nb
+        data = np.concatenate(data_parts) if data_parts else np.zeros(0, np.uint8)
+        return PackedReads(data, np.array(offsets, dtype=np.uint64), np.array(lengths, dtype=np.uint32))
+
+    def get_read(self, idx: int) -> str:
+        """get_read (src/packed_reads.rs:592-613)."""
+        n = int(self.lengths[idx])
+        o = int(self.offsets[idx])
+        by = self.data[o:o + (n + 3) // 4]
+        codes = np.stack([(by >> 6) & 3, (by >> 4) & 3, (by >> 2) & 3, by & 3], axis=1).reshape(-1)[:n]
+        return bytes(np.frombuffer(b"ACGT", dtype=np.uint8)[codes]).decode()
+
+
+# ---------------------------------------------------------------------------
+# Counting
+# ---------------------------------------------------------------------------
+def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: int = 2,
+              min_coverage: float = 5.0, flags: Optional[int] = None,
+              table_log2: int = 0) -> CountOpts:
+    o = CountOpts()
+    lib().spk_count_opts_default(C.byref(o))
+    o.bloom_bits = bloom_bits
+    o.min_count = min_count
+    o.list_min_count = list_min_count
+    o.min_coverage = min_coverage
+    o.table_log2 = table_log2
+    if flags is not None:
+        o.flags = flags
+    return o
+
+
+class CountResult:
+    """Owner of an spk_result: per-k solid lists, edges, Bloom tiers and stats."""
+
+    def __init__(self, h, ctx: Context):
+        self.h = h
+        self.ctx = ctx
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().spk_result_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        n = C.c_int()
+        check(lib().spk_result_count(self.h, C.byref(n)))
+        return n.value
+
+    def info(self, ki: int = 0) -> dict:
+        i = ResultInfo()
+        check(lib().spk_result_info_get(self.h, ki, C.byref(i)))
+        return i.as_dict()
+
+    def _list(self, fn, ki, *extra, with_counts=True):
+        k = self.info(ki)["k"]
+        L = nlimbs(k)
+        n = C.c_size_t(0)
+        check(fn(self.h, ki, *extra, None, None, C.byref(n)) if with_counts else fn(self.h, ki, *extra, None, C.byref(n)))
+        m = n.value
+        keys = np.zeros((max(m, 1), L), dtype=np.uint64)
+        counts = np.zeros(max(m, 1), dtype=np.uint32)
+        n = C.c_size_t(m)
+        if with_counts:
+            check(fn(self.h, ki, *extra, _ptr(keys, u64p), _ptr(counts, u32p), C.byref(n)))
+        else:
+            check(fn(self.h, ki, *extra, _ptr(keys, u64p), C.byref(n)))
+        return keys[: n.value], counts[: n.value]
+
+    def solid(self, ki: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+        """Sorted (keys, counts) of the solid k-mers (count >= cutoff, src/assemble.rs:288-292)."""
+        return self._list(lib().spk_result_solid, ki)
+
+    def kmers(self, ki: int = 0, min_count: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+        """Sorted (keys, counts) of every listed k-mer with count >= min_count."""
+        return self._list(lib().spk_result_kmers, ki, C.c_uint32(min_count))
+
+    def edges(self, ki: int = 0) -> np.ndarray:
+        """Sorted canonical (k+1)-mer edges, ceil((k+1)/32) limbs each."""
+        k = self.info(ki)["k"]
+        L = nlimbs(k + 1)
+        n = C.c_size_t(0)
+        check(lib().spk_result_edges(self.h, ki, None, C.byref(n)))
+        m = n.value
+        e = np.zeros((max(m, 1), L), dtype=np.uint64)
+        n = C.c_size_t(m)
+        check(lib().spk_result_edges(self.h, ki, _ptr(e, u64p), C.byref(n)))
+        return e[: n.value]
+
+    def bloom(self, ki: int = 0, ref_solid: bool = False):
+        """(seen, twice[, ref_solid]) Bloom word arrays of this k."""
+        n = self.info(ki)["bloom_size_bits"] // 64
+        seen = np.zeros(n, dtype=np.uint64)
+        twice = np.zeros(n, dtype=np.uint64)
+        rs = np.zeros(n, dtype=np.uint64) if ref_solid else None
+        check(lib().spk_result_bloom(self.h, ki, _ptr(seen, u64p), _ptr(twice, u64p),
+                                     _ptr(rs, u64p) if ref_solid else None))
+        return (seen, twice, rs) if ref_solid else (seen, twice)
+
+    def table_view(self, ki: int = 0) -> dict:
+        v = TableView()
+        check(lib().spk_result_table_view(self.h, ki, C.byref(v)))
+        return {name: getattr(v, name) for name, _ in v._fields_}
+
+
+def _as_arrays(packed):
+    if isinstance(packed, PackedReads):
+        return packed.data, packed.offsets, packed.lengths
+    data, offsets, lengths = packed
+    return data, offsets, lengths
+
+
+def count(packed, ks: Sequence[int] | int, ctx: Optional[Context] = None, **opt_kw) -> CountResult:
+    """spk_count on host-resident packed reads (copied to the device inside the call)."""
+    ctx = ctx or default_context()
+    data, offsets, lengths = _as_arrays(packed)
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    lengths = np.ascontiguousarray(lengths, dtype=np.uint32)
+    if offsets.size != lengths.size:
+        raise SpkError(1, "offsets and lengths differ in size")
+    ks_arr = np.ascontiguousarray(np.atleast_1d(ks), dtype=np.uint32)
+    o = make_opts(**opt_kw)
+    h = vp()
+    check(lib().spk_count(ctx.h, data.ctypes.data if data.size else None, data.size,
+                          offsets.ctypes.data if offsets.size else None,
+                          lengths.ctypes.data if lengths.size else None, lengths.size,
+                          _ptr(ks_arr, u32p), ks_arr.size, C.byref(o), C.byref(h)))
+    return CountResult(h.value, ctx)
+
+
+def count_device(d_data: int, data_len: int, d_offsets: int, d_lengths: int, n_reads: int,
+                 ks, ctx: Optional[Context] = None, **opt_kw) -> CountResult:
+    """spk_count_device: packed reads already resident on the device (raw pointers)."""
+    ctx = ctx or default_context()
+    ks_arr = np.ascontiguousarray(np.atleast_1d(ks), dtype=np.uint32)
+    o = make_opts(**opt_kw)
+    h = vp()
+    check(lib().spk_count_device(ctx.h, d_data, data_len, d_offsets, d_lengths, n_reads,
+                                 _ptr(ks_arr, u32p), ks_arr.size, C.byref(o), C.byref(h)))
+    return CountResult(h.value, ctx)
+
+
+def count_solid_kmers(packed, k: int, bloom_bits: int = 512 << 20,
+                      ctx: Optional[Context] = None) -> Dict[Kmer256, int]:
+    """The Stage 2-3 seam: HashMap<Kmer256, u32> of the admitted k-mers with count >= 2.
+
+    Replaces src/assemble.rs:129-242 (without error correction) for one k.
+    """
+    r = count(packed, [k], ctx=ctx, bloom_bits=bloom_bits, flags=0)
+    try:
+        keys, counts = r.kmers(0)
+        return {kmer256_from_limbs(row): int(c) for row, c in zip(keys, counts)}
+    finally:
+        r.close()
+
+
+# ---------------------------------------------------------------------------
+# Batched and serving
+# ---------------------------------------------------------------------------
+@dataclass
+class Job:
+    """One counting job (spk_job); arrays are kept alive for the job's lifetime."""
+
+    packed: object
+    ks: Sequence[int]
+    opts: dict = field(default_factory=dict)
+
+    def to_c(self) -> JobC:
+        data, offsets, lengths = _as_arrays(self.packed)
+        self._data = np.ascontiguousarray(data, dtype=np.uint8)
+        self._off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self._len = np.ascontiguousarray(lengths, dtype=np.uint32)
+        self._ks = np.ascontiguousarray(np.atleast_1d(self.ks), dtype=np.uint32)
+        j = JobC()
+        j.data = self._data.ctypes.data if self._data.size else None
+        j.data_len = self._data.size
+        j.offsets = self._off.ctypes.data if self._off.size else None
+        j.lengths = self._len.ctypes.data if self._len.size else None
+        j.n_reads = self._len.size
+        j.ks = self._ks.ctypes.data
+        j.n_k = self._ks.size
+        j.opts = make_opts(**self.opts)
+        return j
+
+
+def count_batch(jobs: List[Job], ctx: Optional[Context] = None) -> List[CountResult]:
+    ctx = ctx or default_context()
+    cj = (JobC * len(jobs))(*[j.to_c() for j in jobs])
+    outs = (vp * len(jobs))()
+    check(lib().spk_count_batch(ctx.h, cj, len(jobs), outs))
+    return [CountResult(outs[i], ctx) for i in range(len(jobs))]
+
+
+class Server:
+    """The serving loop: jobs admitted by HBM budget, run concurrently, results resident."""
+
+    def __init__(self, ctx: Optional[Context] = None, hbm_budget_bytes: int = 0, max_inflight: int = 4):
+        self.ctx = ctx or default_context()
+        check(lib().spk_serve_start(self.ctx.h, hbm_budget_bytes, max_inflight))
+        self._jobs: Dict[int, Job] = {}
+        self._cjobs: Dict[int, JobC] = {}
+
+    def stop(self):
+        if self.ctx is not None and getattr(self.ctx, "h", None):
+            lib().spk_serve_stop(self.ctx.h)
+
+    @staticmethod
+    def estimate(job: Job) -> int:
+        cj = job.to_c()
+        b = C.c_uint64()
+        check(lib().spk_job_hbm_estimate(C.byref(cj), C.byref(b)))
+        return b.value
+
+    def submit(self, job: Job) -> int:
+        cj = job.to_c()
+        t = C.c_uint64()
+        check(lib().spk_submit(self.ctx.h, C.byref(cj), C.byref(t)))
+        self._jobs[t.value] = job
+        self._cjobs[t.value] = cj
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        d = C.c_int()
+        check(lib().spk_poll(self.ctx.h, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> Tuple[CountResult, float]:
+        h = vp()
+        lat = C.c_double()
+        rc = lib().spk_wait(self.ctx.h, ticket, timeout_ms, C.byref(h), C.byref(lat))
+        if rc != 9:  # SPK_E_NOT_READY keeps the job (and its host buffers) alive
+            self._jobs.pop(ticket, None)
+            self._cjobs.pop(ticket, None)
+        check(rc)
+        return CountResult(h.value, self.ctx), lat.value

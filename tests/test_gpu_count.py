@@ -1,0 +1,223 @@
+"""GPU parity of the counting path (spk_count, through the C ABI) against the
+oracle and the golden fixtures.  Integer work: every comparison is bit-exact.
+
+What is compared (per k):
+  * the seen tier, bit for bit (src/bloom.rs:95-97 is order-free);
+  * the full count table (every admitted k-mer and its count) against the
+    order-free twice-tier oracle, and the sorted (k-mer, count) list for
+    count >= 2 against the reference-semantics oracle (src/assemble.rs:129-242);
+  * the (k+1)-mer edge list (src/graph.rs:78-102);
+  * the reference-semantics solid tier as a counted difference.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from helpers import ecoli_packed, load_npz, nlimbs, rows, synth_small_packed
+
+pytestmark = pytest.mark.gpu
+
+ALL = 0x1 | 0x2 | 0x4  # SPK_F_EDGES | SPK_F_REF_SOLID | SPK_F_KEEP_BLOOM
+
+
+def sha(words):
+    return hashlib.sha256(np.asarray(words, dtype=np.uint64).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def spk(spk_lib):
+    return spk_lib
+
+
+def occ(lengths, k):
+    L = np.asarray(lengths, dtype=np.int64)
+    return int(np.clip(L - k + 1, 0, None).sum())
+
+
+def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True):
+    """Full GPU result vs the C++ oracle (twice semantics for the table, reference
+    semantics for the count >= 2 list)."""
+    r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=ALL)
+    info = r.info(0)
+    tw = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE)
+    ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_REF)
+    tk, tc = tw.table(1)
+    gk, gc = r.kmers(0, 1)
+    np.testing.assert_array_equal(gk, tk)
+    np.testing.assert_array_equal(gc, tc)
+    rk, rc = ref.table(2)
+    g2k, g2c = r.kmers(0, 2)
+    np.testing.assert_array_equal(g2k, rk)
+    np.testing.assert_array_equal(g2c, rc)
+    seen, twice, ref_solid = r.bloom(0, ref_solid=True)
+    oseen, otwice = tw.bloom()
+    np.testing.assert_array_equal(seen, oseen)
+    np.testing.assert_array_equal(twice, otwice)
+    # reference-semantics solid tier: a subset of the twice tier; its difference
+    # against the serial reference is reported and bounded
+    _, oref_solid = ref.bloom()
+    assert not np.any(ref_solid & ~twice)
+    diff = int(np.unpackbits((ref_solid ^ oref_solid).view(np.uint8)).sum())
+    pop = int(np.unpackbits(oref_solid.view(np.uint8)).sum())
+    assert diff <= max(64, pop // 50), (diff, pop)
+    assert info["occurrences"] == occ(lens, k)
+    assert info["admitted_occurrences"] == int(tc.astype(np.int64).sum())
+    assert info["n_table"] == tk.shape[0]
+    assert info["n_singletons"] == int((tc == 1).sum())
+    assert info["cutoff"] == ora.cutoff(tc, 5.0)
+    if edges:
+        sk, sc = r.solid(0)
+        e = r.edges(0)
+        np.testing.assert_array_equal(e, ora.edges(sk, k))
+    r.close()
+    return info
+
+
+GOLDEN = ["counts_ecoli_1K_k21.npz", "counts_ecoli_1K_k31.npz", "counts_ecoli_1K_k55.npz",
+          "counts_synth_k55.npz", "counts_synth_k77.npz", "counts_synth_k32.npz",
+          "counts_synth_k64.npz"]
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_count_matches_golden(spk, name):
+    g = load_npz(name)
+    k, bits = int(g["k"]), int(g["bloom_bits"])
+    if "ecoli" in name:
+        data, offs, lens, _ = ecoli_packed()
+    else:
+        data, offs, lens = synth_small_packed()
+    r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=ALL)
+    gk, gc = r.kmers(0, 1)
+    np.testing.assert_array_equal(gk, g["twice_keys"])
+    np.testing.assert_array_equal(gc, g["twice_counts"])
+    g2k, g2c = r.kmers(0, 2)
+    np.testing.assert_array_equal(g2k, g["ge2_keys"])
+    np.testing.assert_array_equal(g2c, g["ge2_counts"])
+    seen, twice = r.bloom(0)
+    assert sha(seen) == str(g["seen_sha"][0])
+    assert sha(twice) == str(g["twice_sha"][0])
+    if "edges" in g:
+        # edges over the count >= 2 set
+        r2 = spk.count((data, offs, lens), [k], bloom_bits=bits, min_count=2)
+        np.testing.assert_array_equal(r2.edges(0), g["edges"])
+
+
+@pytest.mark.parametrize("k", [1, 11, 15, 21, 31, 32, 33, 47, 55, 63, 64, 65, 77, 96, 99, 127])
+def test_count_all_key_widths(spk, ora, k):
+    data, offs, lens = synth_small_packed()
+    check_against_oracle(spk, ora, data, offs, lens, k, 1 << 20)
+
+
+@pytest.mark.parametrize("bits", [64, 100, 100_003, 12345 * 64 + 17, (1 << 22) + 64])
+def test_count_bloom_sizes(spk, ora, bits):
+    """Non-power-of-two sizes use the invariant-divisor path; 64 bits admits everything."""
+    data, offs, lens, _ = ecoli_packed()
+    check_against_oracle(spk, ora, data, offs, lens, 31, bits)
+
+
+def packed_from(reads):
+    import spk as _spk
+    p = _spk.PackedReads.from_clean_reads(reads)
+    return p.data, p.offsets, p.lengths
+
+
+def test_homopolymer_and_tandem_repeats(spk, ora):
+    """Hot keys: identical k-mers inside a warp go through the aggregated add."""
+    reads = ["A" * 150] * 40 + ["AC" * 75] * 40 + ["ACGT" * 40] * 40 + ["T" * 97] * 7
+    data, offs, lens = packed_from(reads)
+    for k in (21, 33, 55, 77):
+        check_against_oracle(spk, ora, data, offs, lens, k, 1 << 16)
+
+
+def test_all_read_lengths_and_offsets(spk, ora):
+    """Read lengths 0..200 (every byte-boundary case) at several k."""
+    rng = np.random.default_rng(9)
+    reads = ["".join(rng.choice(list("ACGT"), n)) for n in range(201)] * 2
+    data, offs, lens = packed_from(reads)
+    for k in (1, 17, 32, 33, 64, 65, 127):
+        check_against_oracle(spk, ora, data, offs, lens, k, 1 << 18)
+
+
+def test_empty_and_short_inputs(spk):
+    r = spk.count((np.zeros(0, np.uint8), np.zeros(0, np.uint64), np.zeros(0, np.uint32)), [31])
+    i = r.info(0)
+    assert i["occurrences"] == 0 and i["n_list"] == 0 and i["n_edges"] == 0
+    assert r.kmers(0)[0].shape[0] == 0 and r.edges(0).shape[0] == 0
+    data, offs, lens = packed_from(["ACGT" * 5, "A" * 30, "ACGTACGTAC"])
+    r = spk.count((data, offs, lens), [31])
+    assert r.info(0)["occurrences"] == 0
+    data, offs, lens = packed_from(["ACGTTGCAAC" * 3 + "A"])
+    r = spk.count((data, offs, lens), [31], list_min_count=1)
+    i = r.info(0)
+    assert i["occurrences"] == 1 and i["n_list"] <= 1
+
+
+def test_table_regrow(spk, ora):
+    """A deliberately undersized table overflows its probe limit; the host
+    regrows it and recounts, with the same result."""
+    data, offs, lens = synth_small_packed()
+    want = spk.count((data, offs, lens), [55], bloom_bits=1 << 20, list_min_count=1)
+    r = spk.count((data, offs, lens), [55], bloom_bits=1 << 20, list_min_count=1, table_log2=4)
+    assert r.info(0)["table_regrows"] > 0
+    a, b = want.kmers(0, 1), r.kmers(0, 1)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+
+
+def test_invalid_inputs(spk):
+    data, offs, lens = packed_from(["ACGT" * 20])
+    with pytest.raises(spk.SpkError) as e:
+        spk.count((data, offs + np.uint64(100), lens), [21])
+    assert e.value.code == 1
+    for bad_k in (0, 128, 500):
+        with pytest.raises(spk.SpkError) as e:
+            spk.count((data, offs, lens), [bad_k])
+        assert e.value.code == 2
+    with pytest.raises(spk.SpkError):
+        spk.count((data, offs, lens), [])
+
+
+def test_multik_equals_single_k(spk):
+    """One call over several k (the per-k loop of src/multik.rs:109-178) gives,
+    per k, exactly the single-k result."""
+    data, offs, lens = synth_small_packed()
+    ks = [21, 33, 55, 77]
+    multi = spk.count((data, offs, lens), ks, bloom_bits=1 << 22)
+    for i, k in enumerate(ks):
+        one = spk.count((data, offs, lens), [k], bloom_bits=1 << 22)
+        for a, b in zip(multi.kmers(i), one.kmers(0)):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(multi.edges(i), one.edges(0))
+
+
+def test_count_device_pointers(spk):
+    """spk_count_device on device-resident reads, including an unaligned base pointer."""
+    import torch
+    data, offs, lens = synth_small_packed()
+    host = spk.count((data, offs, lens), [55], bloom_bits=1 << 22)
+    for shift in (0, 3):
+        buf = torch.zeros(data.size + 64 + shift, dtype=torch.uint8, device="cuda")
+        buf[shift:shift + data.size] = torch.from_numpy(data).cuda()
+        d_off = torch.from_numpy(offs.astype(np.int64)).cuda()
+        d_len = torch.from_numpy(lens.astype(np.int32)).cuda()
+        torch.cuda.synchronize()
+        r = spk.count_device(buf.data_ptr() + shift, data.size, d_off.data_ptr(), d_len.data_ptr(),
+                             lens.size, [55], bloom_bits=1 << 22)
+        for a, b in zip(r.kmers(0), host.kmers(0)):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_solid_cutoff_and_seam(spk, ora):
+    """count_solid_kmers (the Stage 2-3 seam) returns the HashMap of count >= 2
+    k-mers; the solid list applies the adaptive cutoff (src/assemble.rs:286-292)."""
+    data, offs, lens, _ = ecoli_packed()
+    m = spk.count_solid_kmers((data, offs, lens), 31, bloom_bits=16 << 20)
+    ref = ora.count(data, offs, lens, 31, 16 << 20, mode=ora.MODE_REF)
+    rk, rc = ref.table(2)
+    assert m == {spk.kmer256_from_limbs(k): int(c) for k, c in zip(rk, rc)}
+    r = spk.count((data, offs, lens), [31], bloom_bits=16 << 20)
+    sk, sc = r.solid(0)
+    cut = r.info(0)["cutoff"]
+    assert np.all(sc >= cut)
+    assert sk.shape[0] == int((rc >= cut).sum())
