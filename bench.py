@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Headline benchmark: canonical k-mer counting of the 5 Mb x 100x read set at
+k = 55 on B200 (Gk-mers/s), with the reference algorithm's CPU restatement
+timed beside it.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One step = one complete counting job on one read set: Bloom population,
+twice-tier admission and count table, adaptive cutoff, sorted solid list and
+(k+1)-mer edge list (src/assemble.rs:129-292, src/graph.rs:78-102).  With N
+GPUs (torchrun) every rank counts its own copy of the read set (replicas, no
+data-path collective); value = all ranks' k-mer occurrences / max time.
+
+Output: one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "spades-rs_b200")]
+
+METRIC = "Gk-mers/s at k=55 (5Mb,100x) batched vs plain on 1 B200; p50/p99 job latency"
+K = 55
+L2_FLUSH_BYTES = 512 << 20  # > the 126 MB L2, written between timed steps
+# Algorithmic bytes per k-mer occurrence, counted at the 32-byte sector
+# granularity of random DRAM/L2 accesses ("Roofline").
+#   Stage 2 insert: 3 random Bloom word-pair sectors + the packed-read stream.
+#   Stage 3 count:  3 random twice-tier sectors + the stream, and for each
+#                   admitted occurrence one key sector and one count sector.
+SECTOR = 32
+
+
+def stream_bytes_per_occ(read_len=150, k=K):
+    return ((read_len + 3) // 4 + 12) / (read_len - k + 1)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                smax = float(c[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"), c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU arm
+# ---------------------------------------------------------------------------
+def cpu_sample(packed, target_occ):
+    """The first reads of the workload holding about target_occ k-mer occurrences."""
+    import numpy as np
+    per = np.clip(packed.lengths.astype(np.int64) - K + 1, 0, None)
+    n = int(np.searchsorted(np.cumsum(per), target_occ)) + 1
+    n = min(n, packed.lengths.size)
+    end = int(packed.offsets[n - 1]) + (int(packed.lengths[n - 1]) + 3) // 4
+    return packed.data[:end], packed.offsets[:n], packed.lengths[:n], int(per[:n].sum())
+
+
+def run_cpu_baseline(packed, steps, warmup, target_occ, bloom_bits):
+    """The reference algorithm (C++ restatement of src/assemble.rs:129-242 with
+    the rayon chunking and sharded maps) on all host cores."""
+    from oracle import ora
+    data, offs, lens, occ = cpu_sample(packed, target_occ)
+    threads = os.cpu_count() or 1
+    times = []
+    for i in range(warmup + steps):
+        r = ora.count(data, offs, lens, K, bloom_bits, mode=ora.MODE_REF, threads=threads,
+                      keep_bloom=False)
+        st = r.stats()
+        if i >= warmup:
+            times.append(st["seconds_total"])
+        r.table(2)
+    sec = sum(times) / len(times)
+    return {"value": occ / sec / 1e9, "unit": "Gk-mers/s", "cores": threads, "kind": "port",
+            "seconds_per_step": sec,
+            "sample": f"first {lens.size} reads of the workload ({occ} k-mer occurrences, "
+                      f"{occ / 320_000_064:.1%} of it), full-size Bloom ({bloom_bits} bits/tier); "
+                      f"C++ restatement of spades-rs Stages 2-3, {threads} threads, timed from "
+                      f"packed reads in RAM to the sorted count>=2 list"}
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="spk", choices=["spk", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="genome scale (1.0 = the 5 Mb set)")
+    ap.add_argument("--bloom-bits", type=int, default=512 << 20)
+    ap.add_argument("--cpu-occ", type=int, default=96_000_000,
+                    help="k-mer occurrences in the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    assert args.warmup >= 1
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import numpy as np
+    from spk import synth
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        s = synth.c2(args.scale)
+        cb = run_cpu_baseline(s.packed, args.steps, args.warmup, args.cpu_occ, args.bloom_bits)
+        line = {"metric": METRIC, "value": cb["value"], "unit": "Gk-mers/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": cb["seconds_per_step"] * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": "c2 sample: " + cb["sample"], "k": K,
+                           "bloom_bits": args.bloom_bits},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "Gk-mers/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import spk
+
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+
+    t0 = time.time()
+    s = synth.c2(args.scale)
+    p = s.packed
+    occ = synth.occurrences(p, K)
+    log(f"[rank {rank}] generated {len(p)} reads, {occ} occurrences in {time.time() - t0:.1f}s")
+
+    ctx = spk.Context(local_rank)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    dev = torch.device("cuda", local_rank)
+    d_data = torch.zeros(p.data.size + 64, dtype=torch.uint8, device=dev)
+    d_data[: p.data.size] = torch.from_numpy(p.data).to(dev)
+    d_off = torch.from_numpy(p.offsets.view(np.int64)).to(dev)
+    d_len = torch.from_numpy(p.lengths.view(np.int32)).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
+
+    def device_step():
+        return spk.count_device(d_data.data_ptr(), p.data.size, d_off.data_ptr(), d_len.data_ptr(),
+                                p.lengths.size, [K], ctx=ctx, **opts)
+
+    for _ in range(args.warmup):
+        device_step().close()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    clk = Clocks(local_rank)
+    barrier()
+    step_ms, infos = [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)  # evict the previous step's tables from L2 (outside the timing)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = device_step()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        infos.append(r.info(0))
+        r.close()
+    barrier()
+    clocks = clk.stop()
+
+    ms = sum(step_ms) / len(step_ms)
+    bloom_ms = sum(i["ms_bloom_kernel"] for i in infos) / len(infos)
+    count_ms = sum(i["ms_count_kernel"] for i in infos) / len(infos)
+    launches = sum(i["kernel_launches"] for i in infos) // len(infos)
+    info = infos[-1]
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = occ * world / (ms / 1e3) / 1e9
+
+    # e2e: host buffers (pinned) through spk_count, H2D and the D2H of the
+    # solid list inside the timing
+    e2e = None
+    if not args.no_e2e:
+        h_data = torch.from_numpy(p.data).pin_memory()
+        h_off = torch.from_numpy(p.offsets.view(np.int64)).pin_memory()
+        h_len = torch.from_numpy(p.lengths.view(np.int32)).pin_memory()
+        packed_pinned = (h_data.numpy(), h_off.numpy().view(np.uint64), h_len.numpy().view(np.uint32))
+        e2e_ms, d2h = [], 0
+        for i in range(args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = spk.count(packed_pinned, [K], ctx=ctx, **opts)
+            keys, counts = r.solid(0)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= args.warmup:
+                e2e_ms.append(e0.elapsed_time(e1))
+            d2h = keys.nbytes + counts.nbytes
+            r.close()
+        em = sum(e2e_ms) / len(e2e_ms)
+        if world > 1:
+            t = torch.tensor([em], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            em = float(t.item())
+        e2e = {"value": occ * world / (em / 1e3) / 1e9, "unit": "Gk-mers/s", "ms_per_step": em,
+               "h2d_bytes_per_step": int(p.data.nbytes + p.offsets.nbytes + p.lengths.nbytes),
+               "d2h_bytes_per_step": int(d2h)}
+
+    # roofline of the dominant kernel (largest share of the step)
+    f_adm = info["admitted_occurrences"] / max(info["occurrences"], 1)
+    sb = stream_bytes_per_occ()
+    bytes_bloom = occ * (3 * SECTOR + sb)
+    bytes_count = occ * (3 * SECTOR + sb + f_adm * 2 * SECTOR)
+    if count_ms >= bloom_ms:
+        kname, kms, kbytes = "k_count_pass", count_ms, bytes_count
+    else:
+        kname, kms, kbytes = "k_bloom_pass", bloom_ms, bytes_bloom
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            pk = json.load(f)
+        peak, peak_src = float(pk["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = kbytes / (kms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "dram_traffic_c2_k55.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes,
+                "kernel_ms": kms, "kernel_share": kms / ms,
+                "phases_ms": {"bloom_kernel": bloom_ms, "count_kernel": count_ms,
+                              "bloom_phase": info["ms_bloom"], "count_phase": info["ms_count"],
+                              "cutoff_compact": info["ms_finish"], "sort": info["ms_sort"],
+                              "edges": info["ms_edges"]}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = run_cpu_baseline(p, 1, 1, args.cpu_occ, args.bloom_bits)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gk-mers/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": "c2: 5 Mb genome (50% GC, 20 repeats of 1-5 kb at 99% identity), "
+                                   "2x150 bp pairs at 100x, substitution errors 0.1%->1.0% along the "
+                                   "read; canonical k=55; Bloom 512 Mi bits/tier; adaptive cutoff; "
+                                   "sorted solid list + (k+1)-mer edges",
+                       "k": K, "reads": int(len(p)), "occurrences_per_gpu": occ,
+                       "bloom_bits": args.bloom_bits, "l2": "flushed between steps (512 MiB write)",
+                       "parallelism": f"replicas x{world} (one read set per GPU, no collective)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks,
+            "result": {"n_solid": info["n_solid"], "n_list": info["n_list"],
+                       "n_table": info["n_table"], "n_edges": info["n_edges"],
+                       "cutoff": info["cutoff"], "admitted_fraction": f_adm,
+                       "table_capacity": info["table_capacity"]},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

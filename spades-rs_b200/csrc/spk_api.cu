@@ -103,7 +103,9 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
   if ((rc = res->reads.alloc(padded, st))) return rc;
   if ((rc = res->offs.alloc(std::max<size_t>(n_reads, 1) * 8, st))) return rc;
   if ((rc = res->lens.alloc(std::max<size_t>(n_reads, 1) * 4, st))) return rc;
-  SPK_CUDA(cudaMemsetAsync(res->reads.as<uint8_t>() + (padded - 72), 0, 72, st));
+  // Zero the tail from the last whole word of data to the end of the padding.
+  const size_t tail = data_len & ~(size_t)7;
+  SPK_CUDA(cudaMemsetAsync(res->reads.as<uint8_t>() + tail, 0, padded - tail, st));
   if (data_len) SPK_CUDA(cudaMemcpyAsync(res->reads.p, data, data_len, cudaMemcpyHostToDevice, st));
   if (n_reads) {
     SPK_CUDA(cudaMemcpyAsync(res->offs.p, offsets, n_reads * 8, cudaMemcpyHostToDevice, st));

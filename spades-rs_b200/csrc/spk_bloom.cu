@@ -72,14 +72,16 @@ __global__ void __launch_bounds__(kB) k_api_first(BloomKeys K, FastMod fm,
       pos_out[op] = pos[s];
       init_out[op] = (uint8_t)((seen[pos[s] >> 6] >> (pos[s] & 63)) & 1);
       uint64_t h = mix64(pos[s]) & mmask;
-      for (;;) {
+      // The map has at least twice as many slots as operations, so a free or
+      // matching slot is always found within mmask + 1 probes.
+      for (uint64_t probe = 0; probe <= mmask; probe++) {
         unsigned long long cur = mkeys[h];
         if (cur == ~0ULL) cur = atomicCAS(mkeys + h, ~0ULL, (unsigned long long)pos[s]);
         if (cur == ~0ULL || cur == pos[s]) {
           atomicMin(mvals + h, (unsigned long long)op);
           break;
         }
-        h = (h + 1) & mmask;  // the map has twice as many slots as operations
+        h = (h + 1) & mmask;
       }
     }
   }
@@ -102,7 +104,7 @@ __global__ void __launch_bounds__(kB) k_api_apply(uint64_t n, const uint64_t* __
       const uint64_t op = 3 * i + s;
       pos[s] = pos_in[op];
       uint64_t h = mix64(pos[s]) & mmask;
-      while (mkeys[h] != pos[s]) h = (h + 1) & mmask;
+      for (uint64_t probe = 0; probe <= mmask && mkeys[h] != pos[s]; probe++) h = (h + 1) & mmask;
       const bool before = init_in[op] || mvals[h] < op;
       all &= before;
     }
