@@ -109,6 +109,8 @@ int spk_bloom_download(spk_bloom* bloom, uint64_t* seen, uint64_t* solid);
 #define SPK_F_EDGES      0x1u  /* build the (k+1)-mer edge list */
 #define SPK_F_REF_SOLID  0x2u  /* also build the reference-semantics solid tier */
 #define SPK_F_KEEP_BLOOM 0x4u  /* keep the Bloom tiers for spk_result_bloom */
+#define SPK_F_DIRECT     0x8u  /* Stage 2 with direct random-access atomics instead of
+                                  partition-and-apply (same result; used to cross-check) */
 
 typedef struct spk_count_opts {
   uint64_t bloom_bits;    /* bits per tier; 0 = 512 Mi (src/assemble.rs:84) */
@@ -118,6 +120,8 @@ typedef struct spk_count_opts {
   uint32_t flags;         /* SPK_F_* (default SPK_F_EDGES | SPK_F_KEEP_BLOOM) */
   uint32_t table_log2;    /* 0 = size the count table from the Bloom fill; else start
                              with 2^table_log2 slots (it still grows on overflow) */
+  uint64_t max_chunk_occ; /* k-mer occurrences per streamed chunk of Stage 2 (bounds its
+                             temporary memory at 12 bytes per occurrence); 0 = 2^30 */
 } spk_count_opts;
 
 void spk_count_opts_default(spk_count_opts* opts);

@@ -40,6 +40,9 @@ constexpr int kBlock = 256;
 constexpr uint64_t kEmpty = ~0ULL;
 constexpr uint32_t kMaxProbe = 4096;
 constexpr int kSpinLimit = 1 << 22;
+// Occurrences per streamed chunk of the partitioned Stage 2 (4 bytes of
+// staged operation per Bloom bit: 12 bytes per occurrence).
+constexpr uint64_t kMaxChunkOcc = 1ULL << 30;
 
 struct alignas(16) U128 {
   unsigned long long x, y;
@@ -168,12 +171,14 @@ __global__ void __launch_bounds__(kBlock) k_bloom_pass(ReadsView R, unsigned k, 
 // 2. Split the compact twice tier out of the word pairs; popcount both tiers.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_tier_finish(const U128* __restrict__ tiers, uint64_t n,
+                                                         uint64_t* __restrict__ seen,
                                                          uint64_t* __restrict__ twice,
                                                          unsigned long long* __restrict__ pops) {
   uint64_t cs = 0, ct = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     U128 t = tiers[i];
+    seen[i] = t.x;
     twice[i] = t.y;
     cs += __popcll(t.x);
     ct += __popcll(t.y);
@@ -649,34 +654,46 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   uint32_t launches = 0;
   SPK_CUDA(cudaEventRecord(e0.e, st));
   // ---- Stage 2 ----
-  if ((rc = kr.tiers.alloc(kr.num_words * 16, st))) return rc;
-  SPK_CUDA(cudaMemsetAsync(kr.tiers.p, 0, kr.num_words * 16, st));
   const bool ref = (o.flags & SPK_F_REF_SOLID) != 0;
-  if (ref) {
-    if ((rc = kr.ref_solid.alloc(kr.num_words * 8, st))) return rc;
-    SPK_CUDA(cudaMemsetAsync(kr.ref_solid.p, 0, kr.num_words * 8, st));
+  kr.partitioned = !ref && !(o.flags & SPK_F_DIRECT) && partitioned_bloom_ok(kr.num_words);
+  if (kr.partitioned) {
+    SPK_CUDA(cudaEventRecord(kb0.e, st));
+    if ((rc = bloom_partitioned(ctx, st, rv, k, kr, su + S_OCC, su + S_POPS, errp, host, &launches,
+                                o.max_chunk_occ ? o.max_chunk_occ : kMaxChunkOcc)))
+      return rc;
+    SPK_CUDA(cudaEventRecord(kb1.e, st));
+  } else {
+    if ((rc = kr.tiers.alloc(kr.num_words * 16, st))) return rc;
+    SPK_CUDA(cudaMemsetAsync(kr.tiers.p, 0, kr.num_words * 16, st));
+    if (ref) {
+      if ((rc = kr.ref_solid.alloc(kr.num_words * 8, st))) return rc;
+      SPK_CUDA(cudaMemsetAsync(kr.ref_solid.p, 0, kr.num_words * 8, st));
+    }
+    U128* tiers = kr.tiers.as<U128>();
+    unsigned long long* refp = ref ? kr.ref_solid.as<unsigned long long>() : nullptr;
+    SPK_CUDA(cudaEventRecord(kb0.e, st));
+    switch (nl) {
+      case 1: launch_bloom<1>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+      case 2: launch_bloom<2>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+      case 3: launch_bloom<3>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+      default: launch_bloom<4>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+    }
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaEventRecord(kb1.e, st));
+    if ((rc = kr.seen.alloc(kr.num_words * 8, st))) return rc;
+    if ((rc = kr.twice.alloc(kr.num_words * 8, st))) return rc;
+    k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.seen.as<uint64_t>(),
+                                                      kr.twice.as<uint64_t>(), su + S_POPS);
+    SPK_CUDA(cudaGetLastError());
+    kr.tiers.release();
+    launches += 2;
   }
-  U128* tiers = kr.tiers.as<U128>();
-  unsigned long long* refp = ref ? kr.ref_solid.as<unsigned long long>() : nullptr;
-  SPK_CUDA(cudaEventRecord(kb0.e, st));
-  switch (nl) {
-    case 1: launch_bloom<1>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-    case 2: launch_bloom<2>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-    case 3: launch_bloom<3>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-    default: launch_bloom<4>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-  }
-  SPK_CUDA(cudaGetLastError());
-  SPK_CUDA(cudaEventRecord(kb1.e, st));
-  launches += 2;
-  if ((rc = kr.twice.alloc(kr.num_words * 8, st))) return rc;
-  k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.twice.as<uint64_t>(),
-                                                    su + S_POPS);
-  SPK_CUDA(cudaGetLastError());
   SPK_CUDA(cudaEventRecord(e1.e, st));
   SPK_CUDA(cudaMemcpyAsync(host, sw, 5 * 8, cudaMemcpyDeviceToHost, st));
   SPK_CUDA(cudaStreamSynchronize(st));
   if ((int)host[S_ERR] & 4)
     return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
+  if ((int)host[S_ERR] & 8) return fail(SPK_E_TABLE_FULL, "Bloom partition overflow");
   info.occurrences = host[S_OCC];
   info.seen_popcount = host[S_POPS];
   info.twice_popcount = host[S_POPS + 1];
@@ -772,7 +789,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   }
   SPK_CUDA(cudaEventRecord(e5.e, st));
   if (!(o.flags & SPK_F_KEEP_BLOOM)) {
-    kr.tiers.release();
+    kr.seen.release();
     kr.twice.release();
   }
   SPK_CUDA(cudaEventRecord(e6.e, st));
@@ -845,26 +862,12 @@ int download_edges(spk_result* res, int ki, uint64_t* out, size_t* n_inout) {
                   n_inout);
 }
 
-__global__ void k_split_tiers(const U128* __restrict__ t, uint64_t n, uint64_t* __restrict__ seen) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    seen[i] = t[i].x;
-}
-
 int download_bloom(spk_result* res, int ki, uint64_t* seen, uint64_t* twice, uint64_t* ref_solid) {
   KResult& kr = *res->ks[ki];
   cudaStream_t st = res->stream;
-  if (!kr.tiers.p) return fail(SPK_E_INVALID_ARG, "Bloom tiers were not kept (SPK_F_KEEP_BLOOM)");
+  if (!kr.seen.p) return fail(SPK_E_INVALID_ARG, "Bloom tiers were not kept (SPK_F_KEEP_BLOOM)");
   const uint64_t n = kr.num_words;
-  int rc;
-  if (seen) {
-    DevBuf tmp;
-    if ((rc = tmp.alloc(n * 8, st))) return rc;
-    k_split_tiers<<<grid_for(res->ctx, 4), kBlock, 0, st>>>(kr.tiers.as<U128>(), n, tmp.as<uint64_t>());
-    SPK_CUDA(cudaGetLastError());
-    SPK_CUDA(cudaMemcpyAsync(seen, tmp.p, n * 8, cudaMemcpyDeviceToHost, st));
-    SPK_CUDA(cudaStreamSynchronize(st));
-  }
+  if (seen) SPK_CUDA(cudaMemcpyAsync(seen, kr.seen.p, n * 8, cudaMemcpyDeviceToHost, st));
   if (twice) SPK_CUDA(cudaMemcpyAsync(twice, kr.twice.p, n * 8, cudaMemcpyDeviceToHost, st));
   if (ref_solid) {
     if (!kr.ref_solid.p) return fail(SPK_E_INVALID_ARG, "reference solid tier not built (SPK_F_REF_SOLID)");

@@ -88,8 +88,10 @@ struct KResult {
   spk_result_info info{};
   FastMod fm{};
   uint64_t num_words = 0;
-  DevBuf tiers;       // (seen, twice) word pairs, num_words * 16 bytes
+  DevBuf tiers;       // (seen, twice) word pairs of the direct Stage 2 kernel
+  DevBuf seen;        // compact seen tier, num_words * 8 bytes
   DevBuf twice;       // compact twice tier, num_words * 8 bytes
+  bool partitioned = false;  // Stage 2 ran as partition-and-apply
   DevBuf ref_solid;   // reference-semantics solid tier (SPK_F_REF_SOLID)
   DevBuf tkeys, tcounts, tstate;  // count table
   TableView table{};
@@ -145,6 +147,11 @@ int download_list(spk_result* res, int ki, uint32_t min_count, bool solid_only, 
                   uint32_t* counts, size_t* n_inout);
 int download_edges(spk_result* res, int ki, uint64_t* out, size_t* n_inout);
 int download_bloom(spk_result* res, int ki, uint64_t* seen, uint64_t* twice, uint64_t* ref_solid);
+// Partitioned Stage 2 (spk_part.cu).
+bool partitioned_bloom_ok(uint64_t num_words);
+int bloom_partitioned(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
+                      KResult& kr, unsigned long long* occ, unsigned long long* pops, int* errp,
+                      uint64_t* host, uint32_t* launches, uint64_t max_chunk_occ);
 // Radix sort of SoA keys (spk_sort.cu): keys[0..nl) limbs (least significant
 // first) and optional u32 values, sorted ascending by the low nbits of the
 // key.  The buffers may be swapped with temporaries.

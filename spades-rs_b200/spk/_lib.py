@@ -11,6 +11,7 @@ _LIB = None
 SPK_F_EDGES = 0x1
 SPK_F_REF_SOLID = 0x2
 SPK_F_KEEP_BLOOM = 0x4
+SPK_F_DIRECT = 0x8
 
 STATUS = {
     0: "SPK_OK", 1: "SPK_E_INVALID_ARG", 2: "SPK_E_INVALID_K", 3: "SPK_E_OOM",
@@ -36,7 +37,8 @@ class SpkError(RuntimeError):
 class CountOpts(C.Structure):
     _fields_ = [("bloom_bits", C.c_uint64), ("min_count", C.c_uint32),
                 ("list_min_count", C.c_uint32), ("min_coverage", C.c_double),
-                ("flags", C.c_uint32), ("table_log2", C.c_uint32)]
+                ("flags", C.c_uint32), ("table_log2", C.c_uint32),
+                ("max_chunk_occ", C.c_uint64)]
 
 
 class ResultInfo(C.Structure):

@@ -18,7 +18,8 @@ from helpers import ecoli_packed, load_npz, nlimbs, rows, synth_small_packed
 
 pytestmark = pytest.mark.gpu
 
-ALL = 0x1 | 0x2 | 0x4  # SPK_F_EDGES | SPK_F_REF_SOLID | SPK_F_KEEP_BLOOM
+ALL = 0x1 | 0x2 | 0x4  # SPK_F_EDGES | SPK_F_REF_SOLID | SPK_F_KEEP_BLOOM (direct Stage 2)
+PART = 0x1 | 0x4       # SPK_F_EDGES | SPK_F_KEEP_BLOOM (partitioned Stage 2)
 
 
 def sha(words):
@@ -35,14 +36,26 @@ def occ(lengths, k):
     return int(np.clip(L - k + 1, 0, None).sum())
 
 
-def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True):
+def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
     """Full GPU result vs the C++ oracle (twice semantics for the table, reference
-    semantics for the count >= 2 list)."""
-    r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=ALL)
-    info = r.info(0)
+    semantics for the count >= 2 list), for both Stage 2 implementations."""
     tw = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE)
-    ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_REF)
     tk, tc = tw.table(1)
+    oseen, otwice = tw.bloom()
+    p = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=PART, **kw)
+    pk, pc = p.kmers(0, 1)
+    np.testing.assert_array_equal(pk, tk)
+    np.testing.assert_array_equal(pc, tc)
+    ps, pt = p.bloom(0)
+    np.testing.assert_array_equal(ps, oseen)
+    np.testing.assert_array_equal(pt, otwice)
+    pinfo = p.info(0)
+    r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=ALL, **kw)
+    info = r.info(0)
+    for key in ("occurrences", "admitted_occurrences", "n_table", "n_list", "n_solid", "n_edges",
+                "seen_popcount", "twice_popcount", "cutoff"):
+        assert pinfo[key] == info[key], key
+    ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_REF)
     gk, gc = r.kmers(0, 1)
     np.testing.assert_array_equal(gk, tk)
     np.testing.assert_array_equal(gc, tc)
@@ -51,7 +64,6 @@ def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True):
     np.testing.assert_array_equal(g2k, rk)
     np.testing.assert_array_equal(g2c, rc)
     seen, twice, ref_solid = r.bloom(0, ref_solid=True)
-    oseen, otwice = tw.bloom()
     np.testing.assert_array_equal(seen, oseen)
     np.testing.assert_array_equal(twice, otwice)
     # reference-semantics solid tier: a subset of the twice tier; its difference
@@ -70,7 +82,9 @@ def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True):
         sk, sc = r.solid(0)
         e = r.edges(0)
         np.testing.assert_array_equal(e, ora.edges(sk, k))
+        np.testing.assert_array_equal(p.edges(0), e)
     r.close()
+    p.close()
     return info
 
 
@@ -79,15 +93,16 @@ GOLDEN = ["counts_ecoli_1K_k21.npz", "counts_ecoli_1K_k31.npz", "counts_ecoli_1K
           "counts_synth_k64.npz"]
 
 
+@pytest.mark.parametrize("flags", [PART, ALL], ids=["partitioned", "direct"])
 @pytest.mark.parametrize("name", GOLDEN)
-def test_count_matches_golden(spk, name):
+def test_count_matches_golden(spk, name, flags):
     g = load_npz(name)
     k, bits = int(g["k"]), int(g["bloom_bits"])
     if "ecoli" in name:
         data, offs, lens, _ = ecoli_packed()
     else:
         data, offs, lens = synth_small_packed()
-    r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=ALL)
+    r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=flags)
     gk, gc = r.kmers(0, 1)
     np.testing.assert_array_equal(gk, g["twice_keys"])
     np.testing.assert_array_equal(gc, g["twice_counts"])
@@ -221,3 +236,10 @@ def test_solid_cutoff_and_seam(spk, ora):
     cut = r.info(0)["cutoff"]
     assert np.all(sc >= cut)
     assert sk.shape[0] == int((rc >= cut).sum())
+
+
+@pytest.mark.parametrize("chunk", [1000, 50_000, 333_333])
+def test_stage2_streamed_in_chunks(spk, ora, chunk):
+    """Stage 2 streamed in several chunks (accumulating into the tiers) gives the same result."""
+    data, offs, lens = synth_small_packed()
+    check_against_oracle(spk, ora, data, offs, lens, 55, 1 << 20, max_chunk_occ=chunk)
