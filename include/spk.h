@@ -157,8 +157,10 @@ typedef struct spk_result_info {
   uint32_t table_regrows;
   uint32_t kernel_launches;      /* libspk kernels launched for this k */
   float ms_bloom, ms_count, ms_finish, ms_sort, ms_edges, ms_total; /* device time per phase */
-  float ms_bloom_kernel;         /* the Stage 2 insert kernel alone */
+  float ms_bloom_kernel;         /* the Stage 2 kernels alone */
   float ms_count_kernel;         /* the Stage 3 count kernel alone (last attempt) */
+  uint32_t stage2_partitioned;   /* 1: Stage 2 ran as partition-and-apply */
+  uint32_t stage2_fallback;      /* 1: a partition overflowed and Stage 2 was redone directly */
 } spk_result_info;
 
 int spk_result_count(const spk_result* res, int* n_k);

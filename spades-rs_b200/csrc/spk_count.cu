@@ -655,45 +655,58 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   SPK_CUDA(cudaEventRecord(e0.e, st));
   // ---- Stage 2 ----
   const bool ref = (o.flags & SPK_F_REF_SOLID) != 0;
-  kr.partitioned = !ref && !(o.flags & SPK_F_DIRECT) && partitioned_bloom_ok(kr.num_words);
-  if (kr.partitioned) {
-    SPK_CUDA(cudaEventRecord(kb0.e, st));
-    if ((rc = bloom_partitioned(ctx, st, rv, k, kr, su + S_OCC, su + S_POPS, errp, host, &launches,
-                                o.max_chunk_occ ? o.max_chunk_occ : kMaxChunkOcc)))
-      return rc;
-    SPK_CUDA(cudaEventRecord(kb1.e, st));
-  } else {
-    if ((rc = kr.tiers.alloc(kr.num_words * 16, st))) return rc;
-    SPK_CUDA(cudaMemsetAsync(kr.tiers.p, 0, kr.num_words * 16, st));
-    if (ref) {
-      if ((rc = kr.ref_solid.alloc(kr.num_words * 8, st))) return rc;
-      SPK_CUDA(cudaMemsetAsync(kr.ref_solid.p, 0, kr.num_words * 8, st));
+  auto stage2 = [&](bool partitioned) -> int {
+    int rc2;
+    kr.partitioned = partitioned;
+    SPK_CUDA(cudaMemsetAsync(sw, 0, 8 * 8, st));  // occ, adm, pops, err
+    if (partitioned) {
+      SPK_CUDA(cudaEventRecord(kb0.e, st));
+      if ((rc2 = bloom_partitioned(ctx, st, rv, k, kr, su + S_OCC, su + S_POPS, errp, host,
+                                   &launches, o.max_chunk_occ ? o.max_chunk_occ : kMaxChunkOcc)))
+        return rc2;
+      SPK_CUDA(cudaEventRecord(kb1.e, st));
+    } else {
+      if ((rc2 = kr.tiers.alloc(kr.num_words * 16, st))) return rc2;
+      SPK_CUDA(cudaMemsetAsync(kr.tiers.p, 0, kr.num_words * 16, st));
+      if (ref) {
+        if ((rc2 = kr.ref_solid.alloc(kr.num_words * 8, st))) return rc2;
+        SPK_CUDA(cudaMemsetAsync(kr.ref_solid.p, 0, kr.num_words * 8, st));
+      }
+      U128* tiers = kr.tiers.as<U128>();
+      unsigned long long* refp = ref ? kr.ref_solid.as<unsigned long long>() : nullptr;
+      SPK_CUDA(cudaEventRecord(kb0.e, st));
+      switch (nl) {
+        case 1: launch_bloom<1>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+        case 2: launch_bloom<2>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+        case 3: launch_bloom<3>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+        default: launch_bloom<4>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
+      }
+      SPK_CUDA(cudaGetLastError());
+      SPK_CUDA(cudaEventRecord(kb1.e, st));
+      if ((rc2 = kr.seen.alloc(kr.num_words * 8, st))) return rc2;
+      if ((rc2 = kr.twice.alloc(kr.num_words * 8, st))) return rc2;
+      k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.seen.as<uint64_t>(),
+                                                        kr.twice.as<uint64_t>(), su + S_POPS);
+      SPK_CUDA(cudaGetLastError());
+      kr.tiers.release();
+      launches += 2;
     }
-    U128* tiers = kr.tiers.as<U128>();
-    unsigned long long* refp = ref ? kr.ref_solid.as<unsigned long long>() : nullptr;
-    SPK_CUDA(cudaEventRecord(kb0.e, st));
-    switch (nl) {
-      case 1: launch_bloom<1>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-      case 2: launch_bloom<2>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-      case 3: launch_bloom<3>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-      default: launch_bloom<4>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-    }
-    SPK_CUDA(cudaGetLastError());
-    SPK_CUDA(cudaEventRecord(kb1.e, st));
-    if ((rc = kr.seen.alloc(kr.num_words * 8, st))) return rc;
-    if ((rc = kr.twice.alloc(kr.num_words * 8, st))) return rc;
-    k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.seen.as<uint64_t>(),
-                                                      kr.twice.as<uint64_t>(), su + S_POPS);
-    SPK_CUDA(cudaGetLastError());
-    kr.tiers.release();
-    launches += 2;
+    SPK_CUDA(cudaMemcpyAsync(host, sw, 5 * 8, cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    return SPK_OK;
+  };
+  const bool want_part = !ref && !(o.flags & SPK_F_DIRECT) && partitioned_bloom_ok(kr.num_words);
+  if ((rc = stage2(want_part))) return rc;
+  if (want_part && ((int)host[S_ERR] & 8)) {
+    // A partition received more operations than its region holds (a few
+    // k-mers with huge multiplicity): redo Stage 2 with the direct kernel.
+    info.stage2_fallback = 1;
+    if ((rc = stage2(false))) return rc;
   }
   SPK_CUDA(cudaEventRecord(e1.e, st));
-  SPK_CUDA(cudaMemcpyAsync(host, sw, 5 * 8, cudaMemcpyDeviceToHost, st));
-  SPK_CUDA(cudaStreamSynchronize(st));
   if ((int)host[S_ERR] & 4)
     return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
-  if ((int)host[S_ERR] & 8) return fail(SPK_E_TABLE_FULL, "Bloom partition overflow");
+  info.stage2_partitioned = kr.partitioned ? 1 : 0;
   info.occurrences = host[S_OCC];
   info.seen_popcount = host[S_POPS];
   info.twice_popcount = host[S_POPS + 1];

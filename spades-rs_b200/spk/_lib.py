@@ -51,7 +51,8 @@ class ResultInfo(C.Structure):
                 ("kernel_launches", C.c_uint32), ("ms_bloom", C.c_float), ("ms_count", C.c_float),
                 ("ms_finish", C.c_float), ("ms_sort", C.c_float), ("ms_edges", C.c_float),
                 ("ms_total", C.c_float), ("ms_bloom_kernel", C.c_float),
-                ("ms_count_kernel", C.c_float)]
+                ("ms_count_kernel", C.c_float), ("stage2_partitioned", C.c_uint32),
+                ("stage2_fallback", C.c_uint32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

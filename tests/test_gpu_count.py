@@ -243,3 +243,19 @@ def test_stage2_streamed_in_chunks(spk, ora, chunk):
     """Stage 2 streamed in several chunks (accumulating into the tiers) gives the same result."""
     data, offs, lens = synth_small_packed()
     check_against_oracle(spk, ora, data, offs, lens, 55, 1 << 20, max_chunk_occ=chunk)
+
+
+def test_partition_overflow_falls_back(spk, ora):
+    """Two distinct canonical k-mers (k = 1) pile every Bloom operation into one
+    partition; Stage 2 reruns with the direct kernel and the result is unchanged."""
+    data, offs, lens = synth_small_packed()
+    r = spk.count((data, offs, lens), [1], bloom_bits=1 << 20, list_min_count=1, flags=PART)
+    assert r.info(0)["stage2_fallback"] == 1
+    check_against_oracle(spk, ora, data, offs, lens, 1, 1 << 20)
+
+
+def test_default_path_is_partitioned(spk):
+    data, offs, lens = synth_small_packed()
+    r = spk.count((data, offs, lens), [55])
+    i = r.info(0)
+    assert i["stage2_partitioned"] == 1 and i["stage2_fallback"] == 0
