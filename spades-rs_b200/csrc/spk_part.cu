@@ -167,8 +167,12 @@ __global__ void __launch_bounds__(AP_BLOCK) k_bloom_apply(const uint32_t* __rest
                                                           uint64_t num_words, int accumulate,
                                                           unsigned long long* __restrict__ seen,
                                                           unsigned long long* __restrict__ twice,
-                                                          unsigned long long* __restrict__ pops) {
+                                                          unsigned long long* __restrict__ pops,
+                                                          const int* __restrict__ err) {
   extern __shared__ uint32_t sm[];
+  // After an overflow some reserved slots were never written; the host
+  // discards this pass and reruns Stage 2 directly, so do nothing here.
+  if (*err & 8) return;
   uint32_t* s_seen = sm;                    // 2 * kPartWords u32
   uint32_t* s_twice = sm + 2 * kPartWords;  // 2 * kPartWords u32
   uint64_t cs = 0, ct = 0;
@@ -191,7 +195,7 @@ __global__ void __launch_bounds__(AP_BLOCK) k_bloom_apply(const uint32_t* __rest
     const uint64_t n = cur[b] < cap ? (uint64_t)cur[b] : cap;
     const uint32_t* po = ops + (uint64_t)b * cap;
     for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t v = __ldcs(po + i);
+      const uint32_t v = __ldcs(po + i) & ((1u << kPartBits) - 1);
       const uint32_t bit = 1u << (v & 31);
       const uint32_t prev = atomicOr(&s_seen[v >> 5], bit);
       if (prev & bit) atomicOr(&s_twice[v >> 5], bit);
@@ -298,8 +302,9 @@ int bloom_partitioned(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsign
   chunk_occ.push_back(acc);
   uint64_t max_occ = 0;
   for (uint64_t c : chunk_occ) max_occ = std::max(max_occ, c);
-  // each partition receives about 3 occ / parts operations; 6 sigma + slack
-  const double mean = 3.0 * (double)max_occ / parts;
+  // A full partition receives 3 occ * kPartWords / num_words operations on
+  // average (the last one may be shorter); 6 sigma + slack.
+  const double mean = 3.0 * (double)max_occ * std::min<double>(1.0, (double)kPartWords / (double)kr.num_words);
   const uint64_t cap = (uint64_t)(mean + 6.0 * std::sqrt(mean + 1.0)) + 4096;
   DevBuf ops, cur;
   if ((rc = ops.alloc(cap * parts * 4, st))) return rc;
@@ -330,7 +335,7 @@ int bloom_partitioned(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsign
     k_bloom_apply<<<grid, AP_BLOCK, 4 * kPartWords * 4, st>>>(
         ops.as<uint32_t>(), cur.as<unsigned long long>(), cap, parts, kr.num_words, c > 0 ? 1 : 0,
         kr.seen.as<unsigned long long>(), kr.twice.as<unsigned long long>(),
-        last ? pops : nullptr);
+        last ? pops : nullptr, errp);
     SPK_CUDA(cudaGetLastError());
     *launches += 2;
   }
