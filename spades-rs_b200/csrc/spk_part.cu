@@ -27,68 +27,111 @@ namespace spk {
 
 constexpr unsigned FULLP = 0xffffffffu;
 constexpr int SO_BLOCK = 512;
-constexpr int SO_ROUNDS = 8;                       // position rounds staged per flush
-constexpr int SO_STAGE = SO_ROUNDS * 3 * SO_BLOCK; // staged operations (48 KiB)
 constexpr uint32_t kPartBits = 19;                 // 512 Ki bits per partition
 constexpr uint32_t kPartWords = 1u << (kPartBits - 6);
 constexpr uint32_t kNoOp = 0xFFFFFFFFu;
+constexpr uint32_t kChunk = 64;                    // slots a CTA claims per partition at a time
+constexpr uint32_t kMaxParts = 4096;
 constexpr int AP_BLOCK = 1024;
 
 struct OpSink {
   uint32_t* ops;              // P regions of `cap` operations
-  unsigned long long* cur;    // per-partition fill (relative)
+  unsigned long long* cur;    // per-partition claimed slots (relative)
   uint64_t cap;
   uint32_t parts;
   int* err;                   // bit 3: a partition region overflowed
 };
 
-__device__ __forceinline__ void flush_ops(const OpSink& S, uint32_t* stage, int n, uint32_t* hist) {
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < S.parts; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const uint32_t v = stage[i];
-    if (v != kNoOp) atomicAdd(&hist[v >> kPartBits], 1u);
-  }
-  __syncthreads();
-  for (uint32_t b = threadIdx.x; b < S.parts; b += blockDim.x) {
-    const uint32_t c = hist[b];
-    if (!c) continue;
-    const unsigned long long base = atomicAdd(S.cur + b, (unsigned long long)c);
-    if (base + c > S.cap) {
-      atomicOr(S.err, 8);
-      hist[b] = kNoOp;
+// Per-CTA bump allocation of partition slots.  s_cur[b]/s_end[b] delimit the
+// CTA's current chunk of partition b.  An operation takes a slot with one
+// shared atomic and stores straight to global memory; the L2 merges the
+// 4-byte stores of all CTAs into full sectors.  Operations that find their
+// chunk exhausted go to a small overflow list and are placed at the next
+// CTA-wide refill, which claims `overflow + kChunk` slots at once.
+struct Bump {
+  uint32_t* s_cur;   // parts
+  uint32_t* s_end;   // parts
+  uint32_t* s_ovf;   // overflow ops (partition << 32 | bit offset packed as two u32)
+  uint32_t* s_ovn;   // [0] overflow count
+};
+
+__device__ __forceinline__ void bump_put(const OpSink& S, const Bump& B, uint32_t pos, uint32_t ovf_cap) {
+  const uint32_t b = pos >> kPartBits;
+  const uint32_t payload = pos & ((1u << kPartBits) - 1);
+  const uint32_t r = atomicAdd(&B.s_cur[b], 1u);
+  if (r < B.s_end[b]) {
+    S.ops[(uint64_t)b * S.cap + r] = payload;
+  } else {
+    const uint32_t q = atomicAdd(B.s_ovn, 1u);
+    if (q < ovf_cap) {
+      B.s_ovf[2 * q] = b;
+      B.s_ovf[2 * q + 1] = payload;
     } else {
-      hist[b] = (uint32_t)base;
+      atomicOr(S.err, 8);  // cannot happen with ovf_cap >= ops per round
     }
   }
+}
+
+// CTA-wide: claim new chunks for exhausted partitions, then place the
+// overflow list.  Dead partitions (region full) keep s_end = 0 and drop ops.
+__device__ __forceinline__ void bump_refill(const OpSink& S, const Bump& B, uint32_t* s_base) {
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const uint32_t v = stage[i];
-    if (v == kNoOp) continue;
-    const uint32_t b = v >> kPartBits;
-    if (hist[b] == kNoOp) continue;
-    const uint32_t r = atomicAdd(&hist[b], 1u);
-    S.ops[(uint64_t)b * S.cap + r] = v & ((1u << kPartBits) - 1);
+  const uint32_t nov = min(*B.s_ovn, (uint32_t)(3 * SO_BLOCK));
+  if (nov) {
+    for (uint32_t b = threadIdx.x; b < S.parts; b += blockDim.x) {
+      const uint32_t c = B.s_cur[b], e = B.s_end[b];
+      if (c > e) {  // exhausted with (c - e) overflowed operations
+        const uint32_t need = c - e;
+        const unsigned long long base = atomicAdd(S.cur + b, (unsigned long long)(need + kChunk));
+        if (base + need + kChunk > S.cap) {
+          atomicOr(S.err, 8);
+          s_base[b] = kNoOp;
+          B.s_cur[b] = 0;
+          B.s_end[b] = 0;
+        } else {
+          s_base[b] = (uint32_t)base;  // overflow ops take [base, base + need)
+          B.s_cur[b] = (uint32_t)base + need;
+          B.s_end[b] = (uint32_t)(base + need + kChunk);
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nov; i += blockDim.x) {
+      const uint32_t b = B.s_ovf[2 * i], payload = B.s_ovf[2 * i + 1];
+      if (s_base[b] == kNoOp) continue;
+      const uint32_t r = atomicAdd(&s_base[b], 1u);
+      S.ops[(uint64_t)b * S.cap + r] = payload;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *B.s_ovn = 0;
   }
   __syncthreads();
 }
 
 // One pass over the reads: three Bloom operations per k-mer occurrence.  The
 // CTA walks groups of SO_BLOCK reads; each warp scans its 32 reads and all
-// warps step through positions in lockstep rounds so the staging buffer can
-// be flushed by the whole CTA.
+// warps step through positions in lockstep rounds (so refills can be
+// CTA-wide).
 template <int NL>
 __global__ void __launch_bounds__(SO_BLOCK) k_stream_ops(ReadsView R, unsigned k, FastMod fm,
                                                          OpSink S,
                                                          unsigned long long* __restrict__ occ_out) {
   extern __shared__ uint32_t smem[];
-  uint32_t* stage = smem;                 // SO_STAGE
-  uint32_t* hist = smem + SO_STAGE;       // S.parts
+  Bump B;
+  B.s_cur = smem;
+  B.s_end = smem + S.parts;
+  uint32_t* s_base = smem + 2 * S.parts;
+  B.s_ovf = smem + 3 * S.parts;               // 2 * 3 * SO_BLOCK
+  B.s_ovn = smem + 3 * S.parts + 6 * SO_BLOCK;
   __shared__ uint32_t s_rounds;
+  for (uint32_t b = threadIdx.x; b < S.parts; b += blockDim.x) {
+    B.s_cur[b] = 0;
+    B.s_end[b] = 0;
+  }
+  if (threadIdx.x == 0) *B.s_ovn = 0;
+  __syncthreads();
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint64_t occ = 0;
-  int slot = 0;
   for (uint64_t g = (uint64_t)blockIdx.x * SO_BLOCK; g < R.n_reads; g += (uint64_t)gridDim.x * SO_BLOCK) {
     const uint64_t r = g + warp * 32 + lane;
     uint32_t len = 0;
@@ -125,7 +168,6 @@ __global__ void __launch_bounds__(SO_BLOCK) k_stream_ops(ReadsView R, unsigned k
       }
       const uint64_t o = __shfl_sync(FULLP, off, j);
       const uint32_t e = __shfl_sync(FULLP, excl, j);
-      uint32_t* dst = stage + slot * 3 * SO_BLOCK + 3 * threadIdx.x;
       if (p < total) {
         occ++;
         const uint64_t bitpos = 8ull * (R.byte_base + o) + 2ull * (uint64_t)(p - e);
@@ -134,24 +176,19 @@ __global__ void __launch_bounds__(SO_BLOCK) k_stream_ops(ReadsView R, unsigned k
         uint64_t w4[4];
         kmer256_limbs<NL>(C, k, w4);
         const HashPre hp = hash_pre(w4);
-        const uint64_t p0 = fastmod(fm, hash_seed(hp, kSeed1));
-        const uint64_t p1 = fastmod(fm, hash_seed(hp, kSeed2));
-        const uint64_t p2 = fastmod(fm, hash_seed(hp, kSeed3));
-        dst[0] = (uint32_t)p0;  // < 2^31: partition in bits 19..30, bit offset below
-        dst[1] = (uint32_t)p1;
-        dst[2] = (uint32_t)p2;
-      } else {
-        dst[0] = dst[1] = dst[2] = kNoOp;
+        // bit positions < 2^31: partition in bits 19..30, bit offset below
+        bump_put(S, B, (uint32_t)fastmod(fm, hash_seed(hp, kSeed1)), 3 * SO_BLOCK);
+        bump_put(S, B, (uint32_t)fastmod(fm, hash_seed(hp, kSeed2)), 3 * SO_BLOCK);
+        bump_put(S, B, (uint32_t)fastmod(fm, hash_seed(hp, kSeed3)), 3 * SO_BLOCK);
       }
-      if (++slot == SO_ROUNDS) {
-        flush_ops(S, stage, SO_STAGE, hist);
-        slot = 0;
-      }
+      bump_refill(S, B, s_base);
     }
-    __syncthreads();
   }
-  if (slot) flush_ops(S, stage, slot * 3 * SO_BLOCK, hist);
-  // warp-reduce occurrences
+  // mark the unused tail of every claimed chunk
+  for (uint32_t b = threadIdx.x; b < S.parts; b += blockDim.x) {
+    const uint32_t c = B.s_cur[b], e = B.s_end[b];
+    for (uint32_t q = c; q < e; q++) S.ops[(uint64_t)b * S.cap + q] = kNoOp;
+  }
 #pragma unroll
   for (int d = 16; d >= 1; d >>= 1) occ += __shfl_xor_sync(FULLP, occ, d);
   if (lane == 0 && occ) atomicAdd(occ_out, (unsigned long long)occ);
@@ -195,7 +232,9 @@ __global__ void __launch_bounds__(AP_BLOCK) k_bloom_apply(const uint32_t* __rest
     const uint64_t n = cur[b] < cap ? (uint64_t)cur[b] : cap;
     const uint32_t* po = ops + (uint64_t)b * cap;
     for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t v = __ldcs(po + i) & ((1u << kPartBits) - 1);
+      const uint32_t raw = __ldcs(po + i);
+      if (raw == kNoOp) continue;  // unused tail of a claimed chunk
+      const uint32_t v = raw & ((1u << kPartBits) - 1);
       const uint32_t bit = 1u << (v & 31);
       const uint32_t prev = atomicOr(&s_seen[v >> 5], bit);
       if (prev & bit) atomicOr(&s_twice[v >> 5], bit);
@@ -239,7 +278,7 @@ __global__ void __launch_bounds__(256) k_occ_units(const uint32_t* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-size_t stream_ops_smem(uint32_t parts) { return (SO_STAGE + (size_t)parts) * 4; }
+size_t stream_ops_smem(uint32_t parts) { return (3 * (size_t)parts + 6 * SO_BLOCK + 1) * 4; }
 
 uint32_t bloom_parts(uint64_t num_words) {
   return (uint32_t)((num_words + kPartWords - 1) / kPartWords);
@@ -247,7 +286,7 @@ uint32_t bloom_parts(uint64_t num_words) {
 
 // Largest filter the partitioned path takes (the staging histogram must fit
 // next to the staging buffer): 4096 partitions = 2 Gi bits per tier.
-bool partitioned_bloom_ok(uint64_t num_words) { return bloom_parts(num_words) <= 4096; }
+bool partitioned_bloom_ok(uint64_t num_words) { return bloom_parts(num_words) <= kMaxParts; }
 
 template <int NL>
 static int launch_stream(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
@@ -303,9 +342,12 @@ int bloom_partitioned(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsign
   uint64_t max_occ = 0;
   for (uint64_t c : chunk_occ) max_occ = std::max(max_occ, c);
   // A full partition receives 3 occ * kPartWords / num_words operations on
-  // average (the last one may be shorter); 6 sigma + slack.
+  // average (the last one may be shorter).  Genomic k-mers arrive in clumps
+  // of ~coverage occurrences, so the spread is far above Poisson: allow 25%,
+  // plus one claimed-but-unfilled chunk per CTA.  A region that still
+  // overflows makes the host redo Stage 2 with the direct kernel.
   const double mean = 3.0 * (double)max_occ * std::min<double>(1.0, (double)kPartWords / (double)kr.num_words);
-  const uint64_t cap = (uint64_t)(mean + 6.0 * std::sqrt(mean + 1.0)) + 4096;
+  const uint64_t cap = (uint64_t)(mean * 1.25) + (uint64_t)ctx->sm_count * 4 * kChunk * 2 + 65536;
   DevBuf ops, cur;
   if ((rc = ops.alloc(cap * parts * 4, st))) return rc;
   if ((rc = cur.alloc((uint64_t)parts * 8, st))) return rc;
