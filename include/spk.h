@@ -109,8 +109,11 @@ int spk_bloom_download(spk_bloom* bloom, uint64_t* seen, uint64_t* solid);
 #define SPK_F_EDGES      0x1u  /* build the (k+1)-mer edge list */
 #define SPK_F_REF_SOLID  0x2u  /* also build the reference-semantics solid tier */
 #define SPK_F_KEEP_BLOOM 0x4u  /* keep the Bloom tiers for spk_result_bloom */
-#define SPK_F_DIRECT     0x8u  /* Stage 2 with direct random-access atomics instead of
-                                  partition-and-apply (same result; used to cross-check) */
+#define SPK_F_GATED      0x8u  /* the reference's two-pass schedule: Stage 3 counts only
+                                  occurrences admitted by the final Bloom.  Same result as
+                                  the default one-pass schedule (which counts every k-mer
+                                  and admits singletons afterwards) with a table that holds
+                                  only admitted k-mers, for read sets too large for that */
 
 typedef struct spk_count_opts {
   uint64_t bloom_bits;    /* bits per tier; 0 = 512 Mi (src/assemble.rs:84) */
@@ -118,10 +121,8 @@ typedef struct spk_count_opts {
   uint32_t list_min_count;/* smallest count kept in the sorted k-mer list (default 2) */
   double min_coverage;    /* min_coverage of the adaptive cutoff (default 5.0) */
   uint32_t flags;         /* SPK_F_* (default SPK_F_EDGES | SPK_F_KEEP_BLOOM) */
-  uint32_t table_log2;    /* 0 = size the count table from the Bloom fill; else start
-                             with 2^table_log2 slots (it still grows on overflow) */
-  uint64_t max_chunk_occ; /* k-mer occurrences per streamed chunk of Stage 2 (bounds its
-                             temporary memory at 12 bytes per occurrence); 0 = 2^30 */
+  uint32_t table_log2;    /* 0 = size the count table automatically; else start with
+                             2^table_log2 slots (it still grows on overflow) */
 } spk_count_opts;
 
 void spk_count_opts_default(spk_count_opts* opts);
@@ -159,8 +160,8 @@ typedef struct spk_result_info {
   float ms_bloom, ms_count, ms_finish, ms_sort, ms_edges, ms_total; /* device time per phase */
   float ms_bloom_kernel;         /* the Stage 2 kernels alone */
   float ms_count_kernel;         /* the Stage 3 count kernel alone (last attempt) */
-  uint32_t stage2_partitioned;   /* 1: Stage 2 ran as partition-and-apply */
-  uint32_t stage2_fallback;      /* 1: a partition overflowed and Stage 2 was redone directly */
+  uint32_t fused;                /* 1: one-pass schedule, 0: gated two-pass schedule */
+  uint32_t reserved;
 } spk_result_info;
 
 int spk_result_count(const spk_result* res, int* n_k);
@@ -182,14 +183,16 @@ int spk_result_bloom(spk_result* res, int k_index, uint64_t* seen, uint64_t* twi
 
 /* Device-resident count table for a downstream graph build on the same
  * device (the input of CompactedGraph::build, src/graph.rs:65-69).  Open
- * addressing, linear probing: slot s holds key limbs keys[s*key_stride ..],
- * count counts[s] (0 = empty).  Valid until spk_result_free. */
+ * addressing with linear probing from slot hash_kmer256(key, seed 1) >>
+ * (64 - log2(capacity)) (src/bloom.rs:61-78, seed src/bloom.rs:84).  Slot s
+ * starts at slots + s * slot_bytes with key_limbs u64 key limbs, followed by
+ * a u32 count at byte key_limbs * 8: 0 = empty, bit 31 set = a k-mer seen
+ * once that the Bloom did not admit.  Valid until spk_result_free. */
 typedef struct spk_table_view {
-  const uint64_t* keys;   /* device pointer; limbs hold the sequence value, see below */
-  const uint32_t* counts; /* device pointer */
+  const void* slots;      /* device pointer */
   uint64_t capacity;
   uint32_t key_limbs;     /* ceil(k/32) */
-  uint32_t key_stride;    /* limbs per slot */
+  uint32_t slot_bytes;
   uint32_t k;
   uint32_t cutoff;
   /* Keys are stored as the 2k-bit sequence value (first base most

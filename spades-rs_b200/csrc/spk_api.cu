@@ -388,11 +388,10 @@ int spk_result_table_view(spk_result* res, int ki, spk_table_view* v) {
   if ((rc = get_k(res, ki))) return rc;
   if (!v) return fail(SPK_E_INVALID_ARG, "null view");
   KResult& kr = *res->ks[ki];
-  v->keys = kr.table.keys;
-  v->counts = kr.table.counts;
+  v->slots = kr.table.slots;
   v->capacity = kr.table.capacity;
   v->key_limbs = (uint32_t)kr.nl;
-  v->key_stride = kr.table.stride;
+  v->slot_bytes = kr.table.slot_bytes;
   v->k = kr.k;
   v->cutoff = kr.info.cutoff;
   return SPK_OK;

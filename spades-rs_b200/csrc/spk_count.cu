@@ -2,29 +2,32 @@
 //
 // Replaces Stages 2-3 of run_assembly_with_packed_reads (src/assemble.rs:
 // 129-292) and the implicit edge probes of CompactedGraph::build
-// (src/graph.rs:78-102).  Per k:
-//   1. k_bloom_pass   Stage 2: every canonical k-mer occurrence sets its three
-//                     Bloom bits (src/bloom.rs:83-97).  Seen and twice tiers
-//                     are interleaved per 64-bit word so one 16-byte access
-//                     serves both.
-//   2. k_tier_finish  splits out the compact twice tier, popcounts.
-//   3. k_count_pass   Stage 3: occurrences whose three twice bits are set
-//                     are counted in an open-addressing table in HBM
-//                     (src/assemble.rs:193-207), warp-aggregated.
-//   4. k_table_hist + k_cutoff   src/assemble.rs:692-735 on the device.
-//   5. k_compact      stream compaction of the table into the k-mer list.
-//   6. radix sort     the sorted (k-mer, count) list.
-//   7. k_edges        (k+1)-mer edges between solid k-mers (src/graph.rs:78-102),
-//                     then their sort.
+// (src/graph.rs:78-102).
 //
-// Admission rule.  The reference promotes a k-mer to its solid tier only when
-// an insert finds all three seen bits already set, which depends on the
-// order of the rayon chunks (src/bloom.rs:95-106).  The GPU keeps an
+// Admission.  The reference promotes a k-mer to its solid tier only when an
+// insert finds all three seen bits already set, which depends on the order of
+// the rayon chunks (src/bloom.rs:95-106), and counts (Stage 3) every
+// occurrence of a k-mer whose three solid bits are set.  The GPU keeps an
 // order-free twice tier instead: a seen-tier fetch_or that finds its bit set
-// also sets that bit in the twice tier.  Every k-mer that occurs at least
-// twice gets all three twice bits, so the count >= 2 list is exact and equals
-// the reference's.  The reference-semantics solid tier is still produced on
-// request (SPK_F_REF_SOLID).
+// also sets that bit in the twice tier.  The admitted set is every k-mer whose
+// three twice bits are set; it contains every k-mer that occurs at least twice,
+// so the count >= 2 list is exact and equals the reference's.  The
+// reference-semantics solid tier is still produced on request
+// (SPK_F_REF_SOLID).
+//
+// Two schedules compute that same admitted table:
+//   fused (default)  one pass over the reads: each canonical k-mer occurrence
+//                    sets its three Bloom bits and is counted in a table that
+//                    holds every distinct k-mer.  Afterwards each k-mer seen
+//                    once is kept only if its three twice bits are set (a
+//                    k-mer seen twice always has them).  One read pass and no
+//                    per-occurrence Bloom query.
+//   gated            (SPK_F_GATED) the reference's two passes: Stage 2 fills
+//                    the Bloom, Stage 3 counts only occurrences whose three
+//                    twice bits are set.  The table then holds only admitted
+//                    k-mers, which bounds memory on very large read sets.
+// Both are followed by the cutoff (src/assemble.rs:692-735), a compaction of
+// the table into the k-mer list, a radix sort and the edge list.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,13 +43,57 @@ constexpr int kBlock = 256;
 constexpr uint64_t kEmpty = ~0ULL;
 constexpr uint32_t kMaxProbe = 4096;
 constexpr int kSpinLimit = 1 << 22;
-// Occurrences per streamed chunk of the partitioned Stage 2 (4 bytes of
-// staged operation per Bloom bit: 12 bytes per occurrence).
-constexpr uint64_t kMaxChunkOcc = 1ULL << 30;
+constexpr uint32_t kRejected = 0x80000000u;  // count flag: a singleton the twice tier does not admit
 
 struct alignas(16) U128 {
   unsigned long long x, y;
 };
+
+// ---------------------------------------------------------------------------
+// Count table slots: one slot per 16/32/64 bytes, key limbs first, the count
+// right after them, so a lookup and its increment touch one DRAM sector.
+//   NL = 1 (k <= 32):  16 B  key[1] count pad
+//   NL = 2 (k <= 64):  32 B  key[2] count pad pad
+//   NL = 3 (k <= 96):  32 B  key[3] count state
+//   NL = 4 (k <= 127): 64 B  key[4] count state pad...
+// ---------------------------------------------------------------------------
+template <int NL>
+struct Slot {
+  static constexpr uint32_t bytes = NL == 1 ? 16 : (NL <= 3 ? 32 : 64);
+  static constexpr uint32_t count_off = NL * 8;
+  static constexpr uint32_t state_off = NL * 8 + 4;
+};
+__host__ __device__ constexpr uint32_t slot_bytes(int nl) { return nl == 1 ? 16 : (nl <= 3 ? 32 : 64); }
+
+template <int NL>
+__device__ __forceinline__ uint64_t* slot_key(const TableView& t, uint64_t s) {
+  return (uint64_t*)(t.slots + s * Slot<NL>::bytes);
+}
+template <int NL>
+__device__ __forceinline__ uint32_t* slot_count(const TableView& t, uint64_t s) {
+  return (uint32_t*)(t.slots + s * Slot<NL>::bytes + Slot<NL>::count_off);
+}
+template <int NL>
+__device__ __forceinline__ uint32_t* slot_state(const TableView& t, uint64_t s) {
+  return (uint32_t*)(t.slots + s * Slot<NL>::bytes + Slot<NL>::state_off);
+}
+
+// Empty slots: keys of <= 128 bits hold the all-ones sentinel (no canonical
+// k-mer equals it: for k < 32 / k < 64 the top bits are unused, for k = 32 /
+// 64 all-ones is poly-T whose reverse complement poly-A is smaller); wider
+// keys are empty while their state word is 0.  Counts start at 0.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_table_init(uint8_t* __restrict__ slots, uint64_t cap) {
+  const uint64_t words = cap * Slot<NL>::bytes / 16;
+  ulonglong2* p = (ulonglong2*)slots;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < words;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    ulonglong2 v = make_ulonglong2(0ULL, 0ULL);
+    if (NL == 1) v = make_ulonglong2(~0ULL, 0ULL);                        // key | count, pad
+    if (NL == 2 && (i & 1) == 0) v = make_ulonglong2(~0ULL, ~0ULL);       // key limbs
+    p[i] = v;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Position iteration.  A warp takes 32 consecutive reads, scans their k-mer
@@ -117,9 +164,176 @@ __device__ __forceinline__ void warp_add_u64(unsigned long long* dst, uint64_t v
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, (unsigned long long)v);
 }
 
+// The three seen fetch_or of src/bloom.rs:95-97 on interleaved (seen, twice)
+// word pairs; a fetch_or that finds its bit already set also sets the twice
+// bit.  Returns whether all three bits were already seen (src/bloom.rs:99).
+__device__ __forceinline__ bool bloom_insert3(U128* __restrict__ tiers, const uint64_t pos[3]) {
+  U128 t[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) t[i] = tiers[pos[i] >> 6];
+  bool allprev = true;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const uint64_t w = pos[i] >> 6;
+    const unsigned long long bit = 1ULL << (pos[i] & 63);
+    bool prev;
+    if (t[i].x & bit) {
+      // Seen bits are only ever set, so a set bit read here (even from a
+      // stale cached line) was set by an earlier insert.
+      prev = true;
+      if (!(t[i].y & bit)) atomicOr(&tiers[w].y, bit);
+    } else {
+      const unsigned long long p = atomicOr(&tiers[w].x, bit);
+      prev = (p & bit) != 0;
+      if (prev) atomicOr(&tiers[w].y, bit);
+    }
+    allprev &= prev;
+  }
+  return allprev;
+}
+
+__device__ __forceinline__ void ref_promote(unsigned long long* __restrict__ ref_solid,
+                                            const uint64_t pos[3]) {  // src/bloom.rs:99-103
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const unsigned long long bit = 1ULL << (pos[i] & 63);
+    unsigned long long* a = ref_solid + (pos[i] >> 6);
+    if (!(*a & bit)) atomicOr(a, bit);
+  }
+}
+
 // ---------------------------------------------------------------------------
-// 1. Stage 2: Bloom population (src/assemble.rs:141-157, src/bloom.rs:83-107)
+// Count table operations
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t table_home(const TableView& t, uint64_t raw0) {
+  return raw0 >> (64 - t.log2cap);
+}
+
+// Adds n to key C.  Keys of <= 128 bits claim a slot with one 64- or 128-bit
+// CAS against the sentinel; wider keys claim the state word, publish the key
+// and mark the slot ready.
+template <int NL>
+__device__ __forceinline__ void table_add(const TableView& t, const Seq<NL>& C, uint64_t home,
+                                          uint32_t n) {
+  const uint64_t mask = t.capacity - 1;
+  for (uint32_t i = 0; i < t.max_probe; i++) {
+    const uint64_t s = (home + i) & mask;
+    uint64_t* kp = slot_key<NL>(t, s);
+    if (NL == 1) {
+      unsigned long long cur = __ldcg((const unsigned long long*)kp);
+      if (cur == C.v[0]) { atomicAdd(slot_count<NL>(t, s), n); return; }
+      if (cur == kEmpty) {
+        unsigned long long old = atomicCAS((unsigned long long*)kp, kEmpty, (unsigned long long)C.v[0]);
+        if (old == kEmpty || old == C.v[0]) { atomicAdd(slot_count<NL>(t, s), n); return; }
+      }
+    } else if (NL == 2) {
+      ulonglong2 cur = __ldcg((const ulonglong2*)kp);
+      if (cur.x != kEmpty && cur.y != kEmpty) {
+        // A settled key (a 16-byte load may tear only while a slot is being
+        // claimed, and a claimed slot never changes afterwards).
+        if (cur.x == C.v[0] && cur.y == C.v[NL - 1]) { atomicAdd(slot_count<NL>(t, s), n); return; }
+        continue;
+      }
+      U128 e{kEmpty, kEmpty}, mine{C.v[0], C.v[NL - 1]};
+      U128 old = atomicCAS((U128*)kp, e, mine);
+      if ((old.x == kEmpty && old.y == kEmpty) || (old.x == mine.x && old.y == mine.y)) {
+        atomicAdd(slot_count<NL>(t, s), n);
+        return;
+      }
+    } else {
+      uint32_t* sp = slot_state<NL>(t, s);
+      uint32_t st = __ldcg(sp);
+      if (st == 0) {
+        uint32_t old = atomicCAS(sp, 0u, 1u);
+        if (old == 0) {
+#pragma unroll
+          for (int j = 0; j < NL; j++) __stcg(kp + j, C.v[j]);
+          atomicAdd(slot_count<NL>(t, s), n);
+          __threadfence();
+          atomicExch(sp, 2u);
+          return;
+        }
+        st = old;
+      }
+      if (st == 1) {
+        int spins = 0;
+        while ((st = *(volatile uint32_t*)sp) != 2u) {
+          if (++spins > kSpinLimit) { atomicOr(t.err, 2); return; }
+          __nanosleep(64);
+        }
+        __threadfence();
+      }
+      bool eq = true;
+#pragma unroll
+      for (int j = 0; j < NL; j++) eq &= __ldcg(kp + j) == C.v[j];
+      if (eq) { atomicAdd(slot_count<NL>(t, s), n); return; }
+    }
+  }
+  atomicOr(t.err, 1);  // probe limit: the host regrows the table and recounts
+}
+
+// Read-only lookup after counting: the count (with the kRejected flag) or 0.
+template <int NL>
+__device__ __forceinline__ uint32_t table_find(const TableView& t, const Seq<NL>& C, uint64_t home) {
+  const uint64_t mask = t.capacity - 1;
+  for (uint32_t i = 0; i < t.max_probe; i++) {
+    const uint64_t s = (home + i) & mask;
+    const uint32_t c = __ldg(slot_count<NL>(t, s));
+    if (c == 0) return 0;  // empty slot ends the probe sequence
+    const uint64_t* kp = slot_key<NL>(t, s);
+    bool eq = true;
+#pragma unroll
+    for (int j = 0; j < NL; j++) eq &= __ldg(kp + j) == C.v[j];
+    if (eq) return c;
+  }
+  return 0;
+}
+
+template <int NL>
+__device__ __forceinline__ void warp_table_add(const TableView& t, bool take, const Seq<NL>& C,
+                                               uint64_t raw0) {
+  const unsigned am = __ballot_sync(FULL, take);
+  if (take) {
+    // Equal keys in the warp (repeats, hot k-mers) become one atomic add.
+    unsigned peers = am;
+#pragma unroll
+    for (int j = 0; j < NL; j++) peers &= __match_any_sync(am, (unsigned long long)C.v[j]);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1))
+      table_add<NL>(t, C, table_home(t, raw0), __popc(peers));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused pass: Stage 2 Bloom population (src/assemble.rs:141-157) and the
+// count of every k-mer (src/assemble.rs:193-207 without the gate) in one walk
+// over the reads.
+// ---------------------------------------------------------------------------
+template <int NL, bool REF>
+__global__ void __launch_bounds__(kBlock) k_fused_pass(ReadsView R, unsigned k, FastMod fm,
+                                                        U128* __restrict__ tiers,
+                                                        unsigned long long* __restrict__ ref_solid,
+                                                        TableView t,
+                                                        unsigned long long* __restrict__ occ_out) {
+  uint64_t occ = 0;
+  auto fn = [&](bool active, uint64_t bitpos) {
+    Seq<NL> C;
+    uint64_t raw[3] = {0, 0, 0};
+    if (active) {
+      occ++;
+      const Seq<NL> V = extract<NL>(R.words, bitpos, k);
+      C = canonical<NL>(V, k);
+      uint64_t pos[3];
+      bloom_positions<NL>(C, k, fm, raw, pos);
+      const bool allprev = bloom_insert3(tiers, pos);
+      if (REF && allprev) ref_promote(ref_solid, pos);
+    }
+    warp_table_add<NL>(t, active, C, raw[0]);
+  };
+  foreach_position(R, k, fn);
+  warp_add_u64(occ_out, occ);
+}
+
+// Gated schedule, Stage 2 alone.
 template <int NL, bool REF>
 __global__ void __launch_bounds__(kBlock) k_bloom_pass(ReadsView R, unsigned k, FastMod fm,
                                                         U128* __restrict__ tiers,
@@ -133,43 +347,40 @@ __global__ void __launch_bounds__(kBlock) k_bloom_pass(ReadsView R, unsigned k, 
     const Seq<NL> C = canonical<NL>(V, k);
     uint64_t raw[3], pos[3];
     bloom_positions<NL>(C, k, fm, raw, pos);
-    U128 t[3];
-#pragma unroll
-    for (int i = 0; i < 3; i++) t[i] = tiers[pos[i] >> 6];
-    bool allprev = true;
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-      const uint64_t w = pos[i] >> 6;
-      const unsigned long long bit = 1ULL << (pos[i] & 63);
-      bool prev;
-      if (t[i].x & bit) {
-        // Seen bits are only ever set, so a set bit read here (even from a
-        // stale cached line) was set by an earlier insert.
-        prev = true;
-        if (!(t[i].y & bit)) atomicOr(&tiers[w].y, bit);
-      } else {
-        const unsigned long long p = atomicOr(&tiers[w].x, bit);
-        prev = (p & bit) != 0;
-        if (prev) atomicOr(&tiers[w].y, bit);
-      }
-      allprev &= prev;
-    }
-    if (REF && allprev) {  // src/bloom.rs:99-103
-#pragma unroll
-      for (int i = 0; i < 3; i++) {
-        const unsigned long long bit = 1ULL << (pos[i] & 63);
-        unsigned long long* a = ref_solid + (pos[i] >> 6);
-        if (!(*a & bit)) atomicOr(a, bit);
-      }
-    }
+    const bool allprev = bloom_insert3(tiers, pos);
+    if (REF && allprev) ref_promote(ref_solid, pos);
   };
   foreach_position(R, k, fn);
   warp_add_u64(occ_out, occ);
 }
 
-// ---------------------------------------------------------------------------
-// 2. Split the compact twice tier out of the word pairs; popcount both tiers.
-// ---------------------------------------------------------------------------
+// Gated schedule, Stage 3: count occurrences whose three twice bits are set
+// (src/assemble.rs:193-207).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_count_pass(ReadsView R, unsigned k, FastMod fm,
+                                                        const uint64_t* __restrict__ twice,
+                                                        TableView t) {
+  auto fn = [&](bool active, uint64_t bitpos) {
+    bool admitted = false;
+    Seq<NL> C;
+    uint64_t raw0 = 0;
+    if (active) {
+      const Seq<NL> V = extract<NL>(R.words, bitpos, k);
+      C = canonical<NL>(V, k);
+      uint64_t raw[3], pos[3];
+      bloom_positions<NL>(C, k, fm, raw, pos);
+      raw0 = raw[0];
+      const uint64_t a = __ldg(twice + (pos[0] >> 6));
+      const uint64_t b = __ldg(twice + (pos[1] >> 6));
+      const uint64_t c = __ldg(twice + (pos[2] >> 6));
+      admitted = ((a >> (pos[0] & 63)) & (b >> (pos[1] & 63)) & (c >> (pos[2] & 63)) & 1) != 0;
+    }
+    warp_table_add<NL>(t, admitted, C, raw0);
+  };
+  foreach_position(R, k, fn);
+}
+
+// Interleaved word pairs -> compact seen and twice tiers, with popcounts.
 __global__ void __launch_bounds__(kBlock) k_tier_finish(const U128* __restrict__ tiers, uint64_t n,
                                                          uint64_t* __restrict__ seen,
                                                          uint64_t* __restrict__ twice,
@@ -188,156 +399,57 @@ __global__ void __launch_bounds__(kBlock) k_tier_finish(const U128* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// 3. Stage 3: count table (src/assemble.rs:175-219)
-// ---------------------------------------------------------------------------
-template <int NL>
-__device__ __forceinline__ uint64_t table_home(const TableView& t, uint64_t raw0) {
-  return raw0 >> (64 - t.log2cap);
-}
-
-// Adds n to key C.  Keys of <= 128 bits are claimed with one 64- or 128-bit
-// CAS against the all-ones sentinel, which no canonical k-mer can equal (for
-// k < 32 / k < 64 the top bits are unused; for k = 32 / 64 all-ones is
-// poly-T, whose reverse complement poly-A is smaller).  Wider keys claim the
-// slot through a state word and publish the key before marking it ready.
-template <int NL>
-__device__ __forceinline__ void table_add(const TableView& t, const Seq<NL>& C, uint64_t home,
-                                          uint32_t n) {
-  const uint64_t mask = t.capacity - 1;
-  for (uint32_t i = 0; i < t.max_probe; i++) {
-    const uint64_t s = (home + i) & mask;
-    if (NL == 1) {
-      unsigned long long* kp = (unsigned long long*)(t.keys + s);
-      unsigned long long cur = __ldcg(kp);
-      if (cur == C.v[0]) { atomicAdd(t.counts + s, n); return; }
-      if (cur == kEmpty) {
-        unsigned long long old = atomicCAS(kp, kEmpty, (unsigned long long)C.v[0]);
-        if (old == kEmpty || old == C.v[0]) { atomicAdd(t.counts + s, n); return; }
-      }
-    } else if (NL == 2) {
-      U128* kp = (U128*)(t.keys + 2 * s);
-      ulonglong2 cur = __ldcg((const ulonglong2*)kp);
-      if (cur.x != kEmpty && cur.y != kEmpty) {
-        // A settled key (a 16-byte load may tear only while a slot is being
-        // claimed, and a claimed slot never changes afterwards).
-        if (cur.x == C.v[0] && cur.y == C.v[NL - 1]) { atomicAdd(t.counts + s, n); return; }
-        continue;
-      }
-      U128 e{kEmpty, kEmpty}, mine{C.v[0], C.v[NL - 1]};
-      U128 old = atomicCAS(kp, e, mine);
-      if ((old.x == kEmpty && old.y == kEmpty) || (old.x == mine.x && old.y == mine.y)) {
-        atomicAdd(t.counts + s, n);
-        return;
-      }
-    } else {
-      uint32_t st = __ldcg(t.state + s);
-      if (st == 0) {
-        uint32_t old = atomicCAS(t.state + s, 0u, 1u);
-        if (old == 0) {
-          uint64_t* kp = t.keys + (uint64_t)t.stride * s;
-#pragma unroll
-          for (int j = 0; j < NL; j++) __stcg(kp + j, C.v[j]);
-          atomicAdd(t.counts + s, n);
-          __threadfence();
-          atomicExch(t.state + s, 2u);
-          return;
-        }
-        st = old;
-      }
-      if (st == 1) {
-        int spins = 0;
-        while ((st = ((volatile uint32_t*)t.state)[s]) != 2u) {
-          if (++spins > kSpinLimit) { atomicOr(t.err, 2); return; }
-          __nanosleep(64);
-        }
-        __threadfence();
-      }
-      const uint64_t* kp = t.keys + (uint64_t)t.stride * s;
-      bool eq = true;
-#pragma unroll
-      for (int j = 0; j < NL; j++) eq &= __ldcg(kp + j) == C.v[j];
-      if (eq) { atomicAdd(t.counts + s, n); return; }
-    }
-  }
-  atomicOr(t.err, 1);  // probe limit: the host regrows the table and recounts
-}
-
-template <int NL>
-__device__ __forceinline__ bool table_find(const TableView& t, const Seq<NL>& C, uint64_t home,
-                                           uint32_t* count) {
-  const uint64_t mask = t.capacity - 1;
-  for (uint32_t i = 0; i < t.max_probe; i++) {
-    const uint64_t s = (home + i) & mask;
-    const uint32_t c = __ldg(t.counts + s);
-    if (c == 0) return false;  // empty slot ends the probe sequence
-    const uint64_t* kp = t.keys + (uint64_t)t.stride * s;
-    bool eq = true;
-#pragma unroll
-    for (int j = 0; j < NL; j++) eq &= __ldg(kp + j) == C.v[j];
-    if (eq) { *count = c; return true; }
-  }
-  return false;
-}
-
-template <int NL>
-__global__ void __launch_bounds__(kBlock) k_count_pass(ReadsView R, unsigned k, FastMod fm,
-                                                        const uint64_t* __restrict__ twice,
-                                                        TableView t,
-                                                        unsigned long long* __restrict__ adm_out) {
-  uint64_t adm = 0;
-  const unsigned lane = threadIdx.x & 31;
-  auto fn = [&](bool active, uint64_t bitpos) {
-    bool admitted = false;
-    Seq<NL> C;
-    uint64_t raw0 = 0;
-    if (active) {
-      const Seq<NL> V = extract<NL>(R.words, bitpos, k);
-      C = canonical<NL>(V, k);
-      uint64_t raw[3], pos[3];
-      bloom_positions<NL>(C, k, fm, raw, pos);
-      raw0 = raw[0];
-      const uint64_t a = __ldg(twice + (pos[0] >> 6));
-      const uint64_t b = __ldg(twice + (pos[1] >> 6));
-      const uint64_t c = __ldg(twice + (pos[2] >> 6));
-      admitted = ((a >> (pos[0] & 63)) & (b >> (pos[1] & 63)) & (c >> (pos[2] & 63)) & 1) != 0;
-    }
-    const unsigned am = __ballot_sync(FULL, admitted);
-    if (admitted) {
-      adm++;
-      // Equal keys in the warp (repeats, hot k-mers) become one atomic add.
-      unsigned peers = am;
-#pragma unroll
-      for (int j = 0; j < NL; j++) peers &= __match_any_sync(am, (unsigned long long)C.v[j]);
-      if (lane == (unsigned)(__ffs(peers) - 1)) table_add<NL>(t, C, table_home<NL>(t, raw0), __popc(peers));
-    }
-  };
-  foreach_position(R, k, fn);
-  warp_add_u64(adm_out, adm);
-}
-
-// ---------------------------------------------------------------------------
-// 4. Count histogram and the adaptive cutoff (src/assemble.rs:692-735)
+// Admission of k-mers seen once, and the count histogram of the admitted
+// table (the input of src/assemble.rs:692-735).
+// sums: [0] admitted k-mers, [1] admitted count-1 k-mers, [2] admitted
+// occurrences (sum of counts).
 // ---------------------------------------------------------------------------
 constexpr int kHistBins = 256;  // counts >= 255 share the last bin
 
-__global__ void __launch_bounds__(kBlock) k_table_hist(const uint32_t* __restrict__ counts,
-                                                        uint64_t cap,
-                                                        unsigned long long* __restrict__ hist) {
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_admit_hist(TableView t, unsigned k, FastMod fm,
+                                                        const uint64_t* __restrict__ twice,
+                                                        int check_singletons,
+                                                        unsigned long long* __restrict__ hist,
+                                                        unsigned long long* __restrict__ sums) {
   __shared__ unsigned sh[kHistBins];
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) sh[i] = 0;
   __syncthreads();
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t c = counts[i];
-    if (c) atomicAdd(&sh[c < kHistBins - 1 ? c : kHistBins - 1], 1u);
+  uint64_t n_adm = 0, n_one = 0, occ = 0;
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < t.capacity;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t* cp = slot_count<NL>(t, s);
+    const uint32_t c = *cp;
+    if (c == 0) continue;
+    if (c == 1 && check_singletons) {
+      Seq<NL> C;
+      const uint64_t* kp = slot_key<NL>(t, s);
+#pragma unroll
+      for (int j = 0; j < NL; j++) C.v[j] = kp[j];
+      uint64_t raw[3], pos[3];
+      bloom_positions<NL>(C, k, fm, raw, pos);
+      bool ok = (__ldg(twice + (pos[0] >> 6)) >> (pos[0] & 63)) & 1;
+      if (ok) ok = (__ldg(twice + (pos[1] >> 6)) >> (pos[1] & 63)) & 1;
+      if (ok) ok = (__ldg(twice + (pos[2] >> 6)) >> (pos[2] & 63)) & 1;
+      if (!ok) {
+        *cp = 1u | kRejected;
+        continue;
+      }
+    }
+    n_adm++;
+    n_one += c == 1;
+    occ += c;
+    atomicAdd(&sh[c < kHistBins - 1 ? c : kHistBins - 1], 1u);
   }
+  warp_add_u64(sums + 0, n_adm);
+  warp_add_u64(sums + 1, n_one);
+  warp_add_u64(sums + 2, occ);
   __syncthreads();
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
     if (sh[i]) atomicAdd(hist + i, (unsigned long long)sh[i]);
 }
 
-// params: [0] fixed cutoff (0 = adaptive), [1] list_min_count
-// out:    [0] cutoff, [1] list threshold
+// out: [0] cutoff, [1] list threshold
 __global__ void k_cutoff(const unsigned long long* __restrict__ hist, uint32_t fixed,
                          uint32_t list_min, uint32_t* __restrict__ out) {
   if (threadIdx.x | blockIdx.x) return;
@@ -374,49 +486,47 @@ __global__ void k_cutoff(const unsigned long long* __restrict__ hist, uint32_t f
 }
 
 // ---------------------------------------------------------------------------
-// 5. Stream compaction of the table into the SoA k-mer list.
-// counters: [0] list length, [1] solid (>= cutoff), [2] count == 1, [3] occupied
+// Stream compaction of the admitted table into the SoA k-mer list.
+// counters: [0] list length, [1] solid (>= cutoff)
 // ---------------------------------------------------------------------------
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_compact(TableView t, const uint32_t* __restrict__ thr,
                                                      uint64_t* o0, uint64_t* o1, uint64_t* o2,
                                                      uint64_t* o3, uint32_t* __restrict__ ocnt,
+                                                     uint64_t out_cap,
                                                      unsigned long long* __restrict__ counters) {
   const uint32_t cutoff = thr[0], lmin = thr[1];
   const unsigned lane = threadIdx.x & 31;
-  uint64_t nsolid = 0, nsingle = 0, nocc = 0;
+  uint64_t nsolid = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   // Uniform trip count per warp so the ballot below sees every lane.
   const uint64_t start = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   for (uint64_t base = start - lane; base < t.capacity; base += stride) {
     const uint64_t s = base + lane;
-    const uint32_t c = s < t.capacity ? t.counts[s] : 0u;
-    nocc += c != 0;
-    nsolid += c >= cutoff && c != 0;
-    nsingle += c == 1;
+    uint32_t c = s < t.capacity ? *slot_count<NL>(t, s) : 0u;
+    if (c & kRejected) c = 0;
+    nsolid += c != 0 && c >= cutoff;
     const bool keep = c != 0 && c >= lmin;
     const unsigned m = __ballot_sync(FULL, keep);
     if (!m) continue;
     unsigned long long pos0 = 0;
     if (lane == (unsigned)(__ffs(m) - 1)) pos0 = atomicAdd(counters + 0, (unsigned long long)__popc(m));
     pos0 = __shfl_sync(FULL, pos0, __ffs(m) - 1);
-    if (keep) {
-      const uint64_t p = pos0 + __popc(m & lanemask_lt());
-      const uint64_t* kp = t.keys + (uint64_t)t.stride * s;
+    const uint64_t p = pos0 + __popc(m & lanemask_lt());
+    if (keep && p < out_cap) {
+      const uint64_t* kp = slot_key<NL>(t, s);
       o0[p] = kp[0];
-      if (NL > 1) o1[p] = kp[1];
-      if (NL > 2) o2[p] = kp[2];
-      if (NL > 3) o3[p] = kp[3];
+      if (NL > 1) o1[p] = kp[NL > 1 ? 1 : 0];
+      if (NL > 2) o2[p] = kp[NL > 2 ? 2 : 0];
+      if (NL > 3) o3[p] = kp[NL > 3 ? 3 : 0];
       ocnt[p] = c;
     }
   }
   warp_add_u64(counters + 1, nsolid);
-  warp_add_u64(counters + 2, nsingle);
-  warp_add_u64(counters + 3, nocc);
 }
 
 // ---------------------------------------------------------------------------
-// 7. (k+1)-mer edges (src/graph.rs:78-102 with OrientedKmer::explicit_seq
+// (k+1)-mer edges (src/graph.rs:78-102 with OrientedKmer::explicit_seq
 // src/graph.rs:24-30).  For a solid k-mer s in orientation o and base b the
 // successor is canonical(explicit(s,o).extend_right(b)) (src/dna.rs:196-221);
 // when it is solid too, the (k+1)-mer explicit(s,o)+b is an edge.  The same
@@ -451,8 +561,8 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
                                                    const uint64_t* l2, const uint64_t* l3,
                                                    const uint32_t* __restrict__ cnt, uint64_t n,
                                                    const uint32_t* __restrict__ thr, TableView t,
-                                                   unsigned k, FastMod fm, uint64_t* e0,
-                                                   uint64_t* e1, uint64_t* e2, uint64_t* e3,
+                                                   unsigned k, uint64_t* e0, uint64_t* e1,
+                                                   uint64_t* e2, uint64_t* e3, uint64_t out_cap,
                                                    unsigned long long* __restrict__ counter) {
   const uint32_t cutoff = thr[0];
   const unsigned lane = threadIdx.x & 31;
@@ -464,9 +574,9 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
     bool solid = false;
     if (i < n) {
       S.v[0] = l0[i];
-      if (NL > 1) S.v[1] = l1[i];
-      if (NL > 2) S.v[2] = l2[i];
-      if (NL > 3) S.v[3] = l3[i];
+      if (NL > 1) S.v[NL > 1 ? 1 : 0] = l1[i];
+      if (NL > 2) S.v[NL > 2 ? 2 : 0] = l2[i];
+      if (NL > 3) S.v[NL > 3 ? 3 : 0] = l3[i];
       solid = cnt[i] >= cutoff;
     }
     for (int o = 0; o < 2; o++) {
@@ -482,14 +592,11 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
         if (ok) {
           const Seq<NL> NB = shl_append<NL>(EX, b, k);
           const Seq<NL> CN = canonical<NL>(NB, k);
-          uint64_t raw[3], pos[3];
           uint64_t w4[4];
           kmer256_limbs<NL>(CN, k, w4);
-          HashPre hp = hash_pre(w4);
-          raw[0] = hash_seed(hp, kSeed1);
-          (void)pos; (void)fm;
-          uint32_t c = 0;
-          if (table_find<NL>(t, CN, table_home<NL>(t, raw[0]), &c) && c >= cutoff) {
+          const HashPre hp = hash_pre(w4);
+          const uint32_t c = table_find<NL>(t, CN, table_home(t, hash_seed(hp, kSeed1)));
+          if (c && !(c & kRejected) && c >= cutoff) {
             E = widen_append<NL, NLE>(EX, b);
             emit = seq_le<NLE>(E, revcomp<NLE>(E, k + 1));
           }
@@ -499,16 +606,28 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
         unsigned long long p0 = 0;
         if (lane == (unsigned)(__ffs(m) - 1)) p0 = atomicAdd(counter, (unsigned long long)__popc(m));
         p0 = __shfl_sync(FULL, p0, __ffs(m) - 1);
-        if (emit) {
-          const uint64_t p = p0 + __popc(m & lanemask_lt());
+        const uint64_t p = p0 + __popc(m & lanemask_lt());
+        if (emit && p < out_cap) {
           e0[p] = E.v[0];
-          if (NLE > 1) e1[p] = E.v[1];
-          if (NLE > 2) e2[p] = E.v[2];
-          if (NLE > 3) e3[p] = E.v[3];
+          if (NLE > 1) e1[p] = E.v[NLE > 1 ? 1 : 0];
+          if (NLE > 2) e2[p] = E.v[NLE > 2 ? 2 : 0];
+          if (NLE > 3) e3[p] = E.v[NLE > 3 ? 3 : 0];
         }
       }
     }
   }
+}
+
+// Occurrences of a read set (sum of max(len - k + 1, 0)).
+__global__ void __launch_bounds__(kBlock) k_occ(const uint32_t* __restrict__ lengths, uint64_t n,
+                                               unsigned k, unsigned long long* __restrict__ out) {
+  uint64_t s = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t len = lengths[i];
+    s += len >= k ? len - k + 1 : 0;
+  }
+  warp_add_u64(out, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -516,6 +635,22 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
 // ---------------------------------------------------------------------------
 static int grid_for(spk_ctx* ctx, int blocks_per_sm) { return ctx->sm_count * blocks_per_sm; }
 
+#define SPK_DISPATCH_NL(nl, F, ...)                 \
+  switch (nl) {                                     \
+    case 1: F<1>(__VA_ARGS__); break;               \
+    case 2: F<2>(__VA_ARGS__); break;               \
+    case 3: F<3>(__VA_ARGS__); break;               \
+    default: F<4>(__VA_ARGS__); break;              \
+  }
+
+template <int NL>
+static void launch_fused(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
+                         const FastMod& fm, U128* tiers, unsigned long long* ref,
+                         const TableView& t, unsigned long long* occ) {
+  const int g = grid_for(ctx, 8);
+  if (ref) k_fused_pass<NL, true><<<g, kBlock, 0, st>>>(rv, k, fm, tiers, ref, t, occ);
+  else k_fused_pass<NL, false><<<g, kBlock, 0, st>>>(rv, k, fm, tiers, nullptr, t, occ);
+}
 template <int NL>
 static void launch_bloom(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
                          const FastMod& fm, U128* tiers, unsigned long long* ref,
@@ -526,33 +661,43 @@ static void launch_bloom(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uns
 }
 template <int NL>
 static void launch_count(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
-                         const FastMod& fm, const uint64_t* twice, const TableView& t,
-                         unsigned long long* adm) {
-  k_count_pass<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(rv, k, fm, twice, t, adm);
+                         const FastMod& fm, const uint64_t* twice, const TableView& t) {
+  k_count_pass<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(rv, k, fm, twice, t);
+}
+template <int NL>
+static void launch_init(spk_ctx* ctx, cudaStream_t st, uint8_t* slots, uint64_t cap) {
+  k_table_init<NL><<<grid_for(ctx, 4), kBlock, 0, st>>>(slots, cap);
+}
+template <int NL>
+static void launch_admit(spk_ctx* ctx, cudaStream_t st, const TableView& t, unsigned k,
+                         const FastMod& fm, const uint64_t* twice, int check,
+                         unsigned long long* hist, unsigned long long* sums) {
+  k_admit_hist<NL><<<grid_for(ctx, 4), kBlock, 0, st>>>(t, k, fm, twice, check, hist, sums);
 }
 template <int NL>
 static void launch_compact(spk_ctx* ctx, cudaStream_t st, const TableView& t, const uint32_t* thr,
-                           uint64_t* o[4], uint32_t* oc, unsigned long long* counters) {
-  k_compact<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(t, thr, o[0], o[1], o[2], o[3], oc, counters);
+                           uint64_t** o, uint32_t* oc, uint64_t out_cap,
+                           unsigned long long* counters) {
+  k_compact<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(t, thr, o[0], o[1], o[2], o[3], oc, out_cap,
+                                                    counters);
 }
 template <int NL, int NLE>
 static void launch_edges_t(spk_ctx* ctx, cudaStream_t st, uint64_t* l[4], const uint32_t* cnt,
                            uint64_t n, const uint32_t* thr, const TableView& t, unsigned k,
-                           const FastMod& fm, uint64_t* e[4], unsigned long long* counter) {
+                           uint64_t* e[4], uint64_t out_cap, unsigned long long* counter) {
   k_edges<NL, NLE><<<grid_for(ctx, 8), kBlock, 0, st>>>(l[0], l[1], l[2], l[3], cnt, n, thr, t, k,
-                                                       fm, e[0], e[1], e[2], e[3], counter);
+                                                       e[0], e[1], e[2], e[3], out_cap, counter);
 }
 static void launch_edges(spk_ctx* ctx, cudaStream_t st, int nl, int nle, uint64_t* l[4],
                          const uint32_t* cnt, uint64_t n, const uint32_t* thr, const TableView& t,
-                         unsigned k, const FastMod& fm, uint64_t* e[4],
-                         unsigned long long* counter) {
-  if (nl == 1 && nle == 1) launch_edges_t<1, 1>(ctx, st, l, cnt, n, thr, t, k, fm, e, counter);
-  else if (nl == 1) launch_edges_t<1, 2>(ctx, st, l, cnt, n, thr, t, k, fm, e, counter);
-  else if (nl == 2 && nle == 2) launch_edges_t<2, 2>(ctx, st, l, cnt, n, thr, t, k, fm, e, counter);
-  else if (nl == 2) launch_edges_t<2, 3>(ctx, st, l, cnt, n, thr, t, k, fm, e, counter);
-  else if (nl == 3 && nle == 3) launch_edges_t<3, 3>(ctx, st, l, cnt, n, thr, t, k, fm, e, counter);
-  else if (nl == 3) launch_edges_t<3, 4>(ctx, st, l, cnt, n, thr, t, k, fm, e, counter);
-  else launch_edges_t<4, 4>(ctx, st, l, cnt, n, thr, t, k, fm, e, counter);
+                         unsigned k, uint64_t* e[4], uint64_t out_cap, unsigned long long* counter) {
+  if (nl == 1 && nle == 1) launch_edges_t<1, 1>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
+  else if (nl == 1) launch_edges_t<1, 2>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
+  else if (nl == 2 && nle == 2) launch_edges_t<2, 2>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
+  else if (nl == 2) launch_edges_t<2, 3>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
+  else if (nl == 3 && nle == 3) launch_edges_t<3, 3>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
+  else if (nl == 3) launch_edges_t<3, 4>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
+  else launch_edges_t<4, 4>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
 }
 
 static uint64_t next_pow2(uint64_t x) {
@@ -561,67 +706,71 @@ static uint64_t next_pow2(uint64_t x) {
   return p;
 }
 
-// Table capacity from the Bloom fill.  With m bits and 3 hashes a filter
-// holding n items has fill 1 - exp(-3n/m), so n = -(m/3) ln(1 - fill).  The
-// twice tier estimates the k-mers seen at least twice (plus collisions, an
-// overestimate); singletons admitted by chance add (twice fill)^3 of the
+// Gated table capacity from the Bloom fill.  With m bits and 3 hashes a
+// filter holding n items has fill 1 - exp(-3n/m), so n = -(m/3) ln(1 - fill).
+// The twice tier estimates the k-mers seen at least twice (plus collisions,
+// an overestimate); singletons admitted by chance add (twice fill)^3 of the
 // rest.  Sized for a load factor of at most 1/2.
-static uint64_t table_capacity(uint64_t m, uint64_t pop_seen, uint64_t pop_twice) {
+static uint64_t gated_capacity(uint64_t m, uint64_t pop_seen, uint64_t pop_twice) {
   const double md = (double)m;
   const double fs = std::min((double)pop_seen / md, 0.999999);
   const double ft = std::min((double)pop_twice / md, 0.999999);
   const double n_all = -(md / 3.0) * std::log1p(-fs);
   const double n2 = -(md / 3.0) * std::log1p(-ft);
   const double est = n2 + std::max(n_all - n2, 0.0) * ft * ft * ft;
-  const uint64_t want = (uint64_t)(est * 2.0) + 1024;
-  return std::max<uint64_t>(next_pow2(want), 1024);
+  return std::max<uint64_t>(next_pow2((uint64_t)(est * 2.0) + 1024), 1024);
+}
+
+// Fused table capacity: every distinct k-mer, unknown before the pass.  At
+// 20-200x coverage and 0.1-1% substitution errors distinct k-mers are 5-35%
+// of the occurrences; the table starts at 30% (load <= ~0.6 after rounding
+// up) and doubles, with a recount, if a probe sequence overflows.
+static uint64_t fused_capacity(uint64_t occ) {
+  return std::max<uint64_t>(next_pow2(occ * 3 / 10 + 1), 1024);
 }
 
 struct Ev {
   cudaEvent_t e = nullptr;
   Ev() { cudaEventCreate(&e); }
   ~Ev() { if (e) cudaEventDestroy(e); }
+  Ev(const Ev&) = delete;
+  Ev& operator=(const Ev&) = delete;
 };
 static float ms_between(const Ev& a, const Ev& b) {
   float ms = 0;
-  if (cudaEventElapsedTime(&ms, a.e, b.e) != cudaSuccess) ms = 0;
+  if (cudaEventElapsedTime(&ms, a.e, b.e) != cudaSuccess) {
+    cudaGetLastError();
+    ms = 0;
+  }
   return ms;
 }
 
-static int alloc_table(KResult& kr, cudaStream_t st, uint64_t cap) {
-  const int nl = kr.nl;
-  const uint32_t stride = nl == 3 ? 4 : nl;
+static int alloc_table(spk_ctx* ctx, KResult& kr, cudaStream_t st, uint64_t cap) {
+  const uint32_t sb = slot_bytes(kr.nl);
   int rc;
-  if ((rc = kr.tkeys.alloc(cap * stride * 8, st))) return rc;
-  if ((rc = kr.tcounts.alloc(cap * 4, st))) return rc;
-  SPK_CUDA(cudaMemsetAsync(kr.tkeys.p, 0xFF, cap * stride * 8, st));
-  SPK_CUDA(cudaMemsetAsync(kr.tcounts.p, 0, cap * 4, st));
-  if (nl >= 3) {
-    if ((rc = kr.tstate.alloc(cap * 4, st))) return rc;
-    SPK_CUDA(cudaMemsetAsync(kr.tstate.p, 0, cap * 4, st));
-  } else {
-    kr.tstate.release();
-  }
+  if ((rc = kr.tslots.alloc(cap * sb, st))) return rc;
+  SPK_DISPATCH_NL(kr.nl, launch_init, ctx, st, kr.tslots.as<uint8_t>(), cap);
+  SPK_CUDA(cudaGetLastError());
   TableView& t = kr.table;
-  t.keys = kr.tkeys.as<uint64_t>();
-  t.counts = kr.tcounts.as<uint32_t>();
-  t.state = nl >= 3 ? kr.tstate.as<uint32_t>() : nullptr;
+  t.slots = kr.tslots.as<uint8_t>();
   t.capacity = cap;
   t.log2cap = 0;
   while ((1ULL << t.log2cap) < cap) t.log2cap++;
-  t.stride = stride;
+  t.slot_bytes = sb;
   t.max_probe = (uint32_t)std::min<uint64_t>(kMaxProbe, cap);
   return SPK_OK;
 }
 
 // Scratch layout (u64 words) in the per-k scratch buffer.
 enum {
-  S_OCC = 0, S_ADM = 1, S_POPS = 2,  /* 2 words */
-  S_ERR = 4,                          /* int */
-  S_THR = 5,                          /* 2 x u32 */
-  S_CNT = 6,                          /* 4 words: list, solid, single, occupied */
+  S_OCC = 0, S_POPS = 1, /* 2 words */
+  S_ERR = 3,             /* int */
+  S_THR = 4,             /* 2 x u32 */
+  S_SUMS = 5,            /* 3 words: admitted, admitted singletons, admitted occurrences */
+  S_CNT = 8,             /* 2 words: list, solid */
   S_EDGES = 10,
-  S_HIST = 16,                        /* 256 words */
+  S_OCC0 = 11,           /* occurrences before the pass */
+  S_HIST = 16,           /* 256 words */
   S_WORDS = 16 + kHistBins
 };
 
@@ -649,101 +798,105 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   int* errp = (int*)(sw + S_ERR);
   ReadsView rv = rv_in;
   rv.err = errp;
+  const bool ref = (o.flags & SPK_F_REF_SOLID) != 0;
+  const bool gated = (o.flags & SPK_F_GATED) != 0;
 
   Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1;
   uint32_t launches = 0;
   SPK_CUDA(cudaEventRecord(e0.e, st));
-  // ---- Stage 2 ----
-  const bool ref = (o.flags & SPK_F_REF_SOLID) != 0;
-  auto stage2 = [&](bool partitioned) -> int {
-    int rc2;
-    kr.partitioned = partitioned;
-    SPK_CUDA(cudaMemsetAsync(sw, 0, 8 * 8, st));  // occ, adm, pops, err
-    if (partitioned) {
-      SPK_CUDA(cudaEventRecord(kb0.e, st));
-      if ((rc2 = bloom_partitioned(ctx, st, rv, k, kr, su + S_OCC, su + S_POPS, errp, host,
-                                   &launches, o.max_chunk_occ ? o.max_chunk_occ : kMaxChunkOcc)))
-        return rc2;
-      SPK_CUDA(cudaEventRecord(kb1.e, st));
-    } else {
-      if ((rc2 = kr.tiers.alloc(kr.num_words * 16, st))) return rc2;
-      SPK_CUDA(cudaMemsetAsync(kr.tiers.p, 0, kr.num_words * 16, st));
-      if (ref) {
-        if ((rc2 = kr.ref_solid.alloc(kr.num_words * 8, st))) return rc2;
-        SPK_CUDA(cudaMemsetAsync(kr.ref_solid.p, 0, kr.num_words * 8, st));
-      }
-      U128* tiers = kr.tiers.as<U128>();
-      unsigned long long* refp = ref ? kr.ref_solid.as<unsigned long long>() : nullptr;
-      SPK_CUDA(cudaEventRecord(kb0.e, st));
-      switch (nl) {
-        case 1: launch_bloom<1>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-        case 2: launch_bloom<2>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-        case 3: launch_bloom<3>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-        default: launch_bloom<4>(ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC); break;
-      }
-      SPK_CUDA(cudaGetLastError());
-      SPK_CUDA(cudaEventRecord(kb1.e, st));
-      if ((rc2 = kr.seen.alloc(kr.num_words * 8, st))) return rc2;
-      if ((rc2 = kr.twice.alloc(kr.num_words * 8, st))) return rc2;
-      k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.seen.as<uint64_t>(),
-                                                        kr.twice.as<uint64_t>(), su + S_POPS);
-      SPK_CUDA(cudaGetLastError());
-      kr.tiers.release();
-      launches += 2;
-    }
-    SPK_CUDA(cudaMemcpyAsync(host, sw, 5 * 8, cudaMemcpyDeviceToHost, st));
-    SPK_CUDA(cudaStreamSynchronize(st));
+
+  // Bloom tiers as interleaved (seen, twice) word pairs.
+  if ((rc = kr.tiers.alloc(kr.num_words * 16, st))) return rc;
+  if (ref && (rc = kr.ref_solid.alloc(kr.num_words * 8, st))) return rc;
+  U128* tiers = kr.tiers.as<U128>();
+  unsigned long long* refp = ref ? kr.ref_solid.as<unsigned long long>() : nullptr;
+  auto reset_tiers = [&]() -> int {
+    SPK_CUDA(cudaMemsetAsync(kr.tiers.p, 0, kr.num_words * 16, st));
+    if (ref) SPK_CUDA(cudaMemsetAsync(kr.ref_solid.p, 0, kr.num_words * 8, st));
     return SPK_OK;
   };
-  const bool want_part = !ref && !(o.flags & SPK_F_DIRECT) && partitioned_bloom_ok(kr.num_words);
-  if ((rc = stage2(want_part))) return rc;
-  if (want_part && ((int)host[S_ERR] & 8)) {
-    // A partition received more operations than its region holds (a few
-    // k-mers with huge multiplicity): redo Stage 2 with the direct kernel.
-    info.stage2_fallback = 1;
-    if ((rc = stage2(false))) return rc;
+  auto fetch = [&](int words) -> int {
+    SPK_CUDA(cudaMemcpyAsync(host, sw, words * 8, cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    if ((int)host[S_ERR] & 4)
+      return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
+    if ((int)host[S_ERR] & 2) return fail(SPK_E_TIMEOUT, "count table: claim wait timed out");
+    return SPK_OK;
+  };
+
+  uint64_t cap = 0;
+  if (!gated) {
+    // ---- fused: Bloom and the count of every k-mer in one pass ----
+    k_occ<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv.lengths, rv.n_reads, k, su + S_OCC0);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    if ((rc = fetch(S_OCC0 + 1))) return rc;
+    cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(host[S_OCC0]);
+    for (int attempt = 0;; attempt++) {
+      if ((rc = reset_tiers())) return rc;
+      if ((rc = alloc_table(ctx, kr, st, cap))) return rc;
+      kr.table.err = errp;
+      SPK_CUDA(cudaMemsetAsync(sw, 0, (S_ERR + 1) * 8, st));
+      SPK_CUDA(cudaEventRecord(kb0.e, st));
+      SPK_DISPATCH_NL(nl, launch_fused, ctx, st, rv, k, kr.fm, tiers, refp, kr.table, su + S_OCC);
+      SPK_CUDA(cudaGetLastError());
+      SPK_CUDA(cudaEventRecord(kb1.e, st));
+      launches += 2;
+      if ((rc = fetch(S_ERR + 1))) return rc;
+      if (!((int)host[S_ERR] & 1)) break;
+      if (attempt >= 24) return fail(SPK_E_TABLE_FULL, "count table overflow after regrow attempts");
+      cap *= 2;
+      info.table_regrows++;
+    }
+  } else {
+    // ---- gated: Stage 2 first ----
+    if ((rc = reset_tiers())) return rc;
+    SPK_CUDA(cudaEventRecord(kb0.e, st));
+    SPK_DISPATCH_NL(nl, launch_bloom, ctx, st, rv, k, kr.fm, tiers, refp, su + S_OCC);
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaEventRecord(kb1.e, st));
+    launches++;
   }
+  // compact tiers (both schedules)
+  if ((rc = kr.seen.alloc(kr.num_words * 8, st))) return rc;
+  if ((rc = kr.twice.alloc(kr.num_words * 8, st))) return rc;
+  k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.seen.as<uint64_t>(),
+                                                    kr.twice.as<uint64_t>(), su + S_POPS);
+  SPK_CUDA(cudaGetLastError());
+  launches++;
+  kr.tiers.release();
   SPK_CUDA(cudaEventRecord(e1.e, st));
-  if ((int)host[S_ERR] & 4)
-    return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
-  info.stage2_partitioned = kr.partitioned ? 1 : 0;
+  if ((rc = fetch(S_POPS + 2))) return rc;
   info.occurrences = host[S_OCC];
   info.seen_popcount = host[S_POPS];
   info.twice_popcount = host[S_POPS + 1];
 
-  // ---- Stage 3 ----
-  uint64_t cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40))
-                              : table_capacity(size_bits, info.seen_popcount, info.twice_popcount);
-  for (int attempt = 0;; attempt++) {
-    if ((rc = alloc_table(kr, st, cap))) return rc;
-    kr.table.err = errp;
-    SPK_CUDA(cudaMemsetAsync(sw + S_ADM, 0, 8, st));
-    SPK_CUDA(cudaMemsetAsync(errp, 0, 8, st));
-    SPK_CUDA(cudaEventRecord(kc0.e, st));
-    switch (nl) {
-      case 1: launch_count<1>(ctx, st, rv, k, kr.fm, kr.twice.as<uint64_t>(), kr.table, su + S_ADM); break;
-      case 2: launch_count<2>(ctx, st, rv, k, kr.fm, kr.twice.as<uint64_t>(), kr.table, su + S_ADM); break;
-      case 3: launch_count<3>(ctx, st, rv, k, kr.fm, kr.twice.as<uint64_t>(), kr.table, su + S_ADM); break;
-      default: launch_count<4>(ctx, st, rv, k, kr.fm, kr.twice.as<uint64_t>(), kr.table, su + S_ADM); break;
+  if (gated) {
+    // ---- gated: Stage 3 over admitted occurrences ----
+    cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40))
+                       : gated_capacity(size_bits, info.seen_popcount, info.twice_popcount);
+    for (int attempt = 0;; attempt++) {
+      if ((rc = alloc_table(ctx, kr, st, cap))) return rc;
+      kr.table.err = errp;
+      SPK_CUDA(cudaMemsetAsync(errp, 0, 8, st));
+      SPK_CUDA(cudaEventRecord(kc0.e, st));
+      SPK_DISPATCH_NL(nl, launch_count, ctx, st, rv, k, kr.fm, kr.twice.as<uint64_t>(), kr.table);
+      SPK_CUDA(cudaGetLastError());
+      SPK_CUDA(cudaEventRecord(kc1.e, st));
+      launches += 2;
+      if ((rc = fetch(S_ERR + 1))) return rc;
+      if (!((int)host[S_ERR] & 1)) break;
+      if (attempt >= 24) return fail(SPK_E_TABLE_FULL, "count table overflow after regrow attempts");
+      cap *= 2;
+      info.table_regrows++;
     }
-    SPK_CUDA(cudaGetLastError());
-    SPK_CUDA(cudaEventRecord(kc1.e, st));
-    launches++;
-    SPK_CUDA(cudaMemcpyAsync(host, sw, 5 * 8, cudaMemcpyDeviceToHost, st));
-    SPK_CUDA(cudaStreamSynchronize(st));
-    const int err = (int)host[S_ERR];
-    if (err & 2) return fail(SPK_E_TIMEOUT, "count table: claim wait timed out");
-    if (!(err & 1)) break;
-    if (attempt >= 24) return fail(SPK_E_TABLE_FULL, "count table overflow after regrow attempts");
-    cap *= 2;
-    info.table_regrows++;
   }
-  info.admitted_occurrences = host[S_ADM];
   info.table_capacity = cap;
   SPK_CUDA(cudaEventRecord(e2.e, st));
 
-  // ---- cutoff + compaction ----
-  k_table_hist<<<grid_for(ctx, 4), kBlock, 0, st>>>(kr.table.counts, cap, su + S_HIST);
+  // ---- admission of singletons, histogram, cutoff ----
+  SPK_DISPATCH_NL(nl, launch_admit, ctx, st, kr.table, k, kr.fm, kr.twice.as<uint64_t>(),
+                  gated ? 0 : 1, su + S_HIST, su + S_SUMS);
   uint32_t fixed = o.min_count;
   if (!fixed && o.min_coverage > 5.0) {  // src/assemble.rs:693-694
     double v = std::max(o.min_coverage * 0.35, 2.0);
@@ -751,30 +904,37 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   }
   uint32_t* thr = (uint32_t*)(sw + S_THR);
   k_cutoff<<<1, 32, 0, st>>>(su + S_HIST, fixed, o.list_min_count ? o.list_min_count : 2, thr);
-  uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
-  for (int j = 0; j < nl; j++) {
-    if ((rc = kr.list[j].alloc(cap * 8, st))) return rc;
-    lp[j] = kr.list[j].as<uint64_t>();
-  }
-  if ((rc = kr.list[4].alloc(cap * 4, st))) return rc;
-  switch (nl) {
-    case 1: launch_compact<1>(ctx, st, kr.table, thr, lp, kr.list[4].as<uint32_t>(), su + S_CNT); break;
-    case 2: launch_compact<2>(ctx, st, kr.table, thr, lp, kr.list[4].as<uint32_t>(), su + S_CNT); break;
-    case 3: launch_compact<3>(ctx, st, kr.table, thr, lp, kr.list[4].as<uint32_t>(), su + S_CNT); break;
-    default: launch_compact<4>(ctx, st, kr.table, thr, lp, kr.list[4].as<uint32_t>(), su + S_CNT); break;
-  }
   SPK_CUDA(cudaGetLastError());
-  launches += 3;
-  SPK_CUDA(cudaEventRecord(e3.e, st));
-  SPK_CUDA(cudaMemcpyAsync(host, sw, S_EDGES * 8, cudaMemcpyDeviceToHost, st));
-  SPK_CUDA(cudaStreamSynchronize(st));
+  launches += 2;
+  if ((rc = fetch(S_WORDS))) return rc;
   const uint32_t* hthr = (const uint32_t*)(host + S_THR);
   info.cutoff = hthr[0];
   kr.list_min = hthr[1];
+  info.n_table = host[S_SUMS + 0];
+  info.n_singletons = host[S_SUMS + 1];
+  info.admitted_occurrences = host[S_SUMS + 2];
+  // List length from the histogram: exact for thresholds below the last bin,
+  // an upper bound otherwise (the compaction counts exactly).
+  uint64_t n_list = 0;
+  for (int c = 0; c < kHistBins; c++)
+    if ((uint32_t)c >= kr.list_min || c == kHistBins - 1) n_list += host[S_HIST + c];
+
+  // ---- compaction ----
+  uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int j = 0; j < nl; j++) {
+    if ((rc = kr.list[j].alloc(std::max<uint64_t>(n_list, 1) * 8, st))) return rc;
+    lp[j] = kr.list[j].as<uint64_t>();
+  }
+  if ((rc = kr.list[4].alloc(std::max<uint64_t>(n_list, 1) * 4, st))) return rc;
+  SPK_DISPATCH_NL(nl, launch_compact, ctx, st, kr.table, thr, lp, kr.list[4].as<uint32_t>(), n_list,
+                  su + S_CNT);
+  SPK_CUDA(cudaGetLastError());
+  launches++;
+  SPK_CUDA(cudaEventRecord(e3.e, st));
+  if ((rc = fetch(S_EDGES))) return rc;
   info.n_list = host[S_CNT + 0];
   info.n_solid = host[S_CNT + 1];
-  info.n_singletons = host[S_CNT + 2];
-  info.n_table = host[S_CNT + 3];
+  if (info.n_list > n_list) return fail(SPK_E_CUDA, "k-mer list larger than its histogram count");
 
   // ---- sort ----
   if ((rc = radix_sort_bufs(st, nl, info.n_list, 2 * k, kr.list, &kr.list[4], &launches))) return rc;
@@ -785,18 +945,18 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   kr.nle = (int)((k + 1 + 31) / 32);
   if ((o.flags & SPK_F_EDGES) && info.n_solid > 0) {
     uint64_t* ep[4] = {nullptr, nullptr, nullptr, nullptr};
-    const uint64_t ecap = info.n_solid * 8;
+    const uint64_t ecap = info.n_solid * 8;  // at most 8 canonical edges per solid k-mer
     for (int j = 0; j < kr.nle; j++) {
       if ((rc = kr.edges[j].alloc(ecap * 8, st))) return rc;
       ep[j] = kr.edges[j].as<uint64_t>();
     }
     launch_edges(ctx, st, nl, kr.nle, lp, kr.list[4].as<uint32_t>(), info.n_list, thr, kr.table, k,
-                 kr.fm, ep, su + S_EDGES);
+                 ep, ecap, su + S_EDGES);
     SPK_CUDA(cudaGetLastError());
     launches++;
-    SPK_CUDA(cudaMemcpyAsync(host + S_EDGES, sw + S_EDGES, 8, cudaMemcpyDeviceToHost, st));
-    SPK_CUDA(cudaStreamSynchronize(st));
+    if ((rc = fetch(S_EDGES + 1))) return rc;
     info.n_edges = host[S_EDGES];
+    if (info.n_edges > ecap) return fail(SPK_E_CUDA, "edge list larger than its bound");
     if ((rc = radix_sort_bufs(st, kr.nle, info.n_edges, 2 * (k + 1), kr.edges, nullptr, &launches)))
       return rc;
   }
@@ -814,8 +974,9 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   info.ms_edges = ms_between(e4, e5);
   info.ms_total = ms_between(e0, e6);
   info.ms_bloom_kernel = ms_between(kb0, kb1);
-  info.ms_count_kernel = ms_between(kc0, kc1);
+  info.ms_count_kernel = gated ? ms_between(kc0, kc1) : 0.f;
   info.kernel_launches = launches;
+  info.fused = gated ? 0 : 1;
   return SPK_OK;
 }
 

@@ -69,13 +69,14 @@ struct ReadsView {
 };
 
 // ---- count table --------------------------------------------------------------
+// Open addressing, linear probing; one slot of slot_bytes per entry: key limbs
+// (sequence value V) first, then the u32 count (and a u32 state word for keys
+// wider than 128 bits).  Count 0 marks an empty slot after counting.
 struct TableView {
-  uint64_t* keys;     // capacity * stride limbs (sequence value V)
-  uint32_t* counts;   // capacity
-  uint32_t* state;    // capacity (NL >= 3 only): 0 empty, 1 claiming, 2 ready
+  uint8_t* slots;
   uint64_t capacity;  // power of two
   uint32_t log2cap;
-  uint32_t stride;    // limbs per slot: NL, or 4 for NL == 3
+  uint32_t slot_bytes;
   uint32_t max_probe;
   uint32_t pad;
   int* err;           // device error word (bit 0: probe limit, bit 1: wait timeout)
@@ -88,12 +89,11 @@ struct KResult {
   spk_result_info info{};
   FastMod fm{};
   uint64_t num_words = 0;
-  DevBuf tiers;       // (seen, twice) word pairs of the direct Stage 2 kernel
+  DevBuf tiers;       // (seen, twice) word pairs while counting
   DevBuf seen;        // compact seen tier, num_words * 8 bytes
   DevBuf twice;       // compact twice tier, num_words * 8 bytes
-  bool partitioned = false;  // Stage 2 ran as partition-and-apply
   DevBuf ref_solid;   // reference-semantics solid tier (SPK_F_REF_SOLID)
-  DevBuf tkeys, tcounts, tstate;  // count table
+  DevBuf tslots;      // count table slots
   TableView table{};
   DevBuf list[5];     // sorted k-mer list: limbs 0..nl-1 (SoA), counts in list[4]
   DevBuf edges[4];    // sorted edge list: limbs (SoA)
@@ -147,11 +147,7 @@ int download_list(spk_result* res, int ki, uint32_t min_count, bool solid_only, 
                   uint32_t* counts, size_t* n_inout);
 int download_edges(spk_result* res, int ki, uint64_t* out, size_t* n_inout);
 int download_bloom(spk_result* res, int ki, uint64_t* seen, uint64_t* twice, uint64_t* ref_solid);
-// Partitioned Stage 2 (spk_part.cu).
-bool partitioned_bloom_ok(uint64_t num_words);
-int bloom_partitioned(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
-                      KResult& kr, unsigned long long* occ, unsigned long long* pops, int* errp,
-                      uint64_t* host, uint32_t* launches, uint64_t max_chunk_occ);
+
 // Radix sort of SoA keys (spk_sort.cu): keys[0..nl) limbs (least significant
 // first) and optional u32 values, sorted ascending by the low nbits of the
 // key.  The buffers may be swapped with temporaries.

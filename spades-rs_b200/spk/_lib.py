@@ -11,7 +11,7 @@ _LIB = None
 SPK_F_EDGES = 0x1
 SPK_F_REF_SOLID = 0x2
 SPK_F_KEEP_BLOOM = 0x4
-SPK_F_DIRECT = 0x8
+SPK_F_GATED = 0x8
 
 STATUS = {
     0: "SPK_OK", 1: "SPK_E_INVALID_ARG", 2: "SPK_E_INVALID_K", 3: "SPK_E_OOM",
@@ -37,8 +37,7 @@ class SpkError(RuntimeError):
 class CountOpts(C.Structure):
     _fields_ = [("bloom_bits", C.c_uint64), ("min_count", C.c_uint32),
                 ("list_min_count", C.c_uint32), ("min_coverage", C.c_double),
-                ("flags", C.c_uint32), ("table_log2", C.c_uint32),
-                ("max_chunk_occ", C.c_uint64)]
+                ("flags", C.c_uint32), ("table_log2", C.c_uint32)]
 
 
 class ResultInfo(C.Structure):
@@ -51,17 +50,16 @@ class ResultInfo(C.Structure):
                 ("kernel_launches", C.c_uint32), ("ms_bloom", C.c_float), ("ms_count", C.c_float),
                 ("ms_finish", C.c_float), ("ms_sort", C.c_float), ("ms_edges", C.c_float),
                 ("ms_total", C.c_float), ("ms_bloom_kernel", C.c_float),
-                ("ms_count_kernel", C.c_float), ("stage2_partitioned", C.c_uint32),
-                ("stage2_fallback", C.c_uint32)]
+                ("ms_count_kernel", C.c_float), ("fused", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class TableView(C.Structure):
-    _fields_ = [("keys", C.c_void_p), ("counts", C.c_void_p), ("capacity", C.c_uint64),
-                ("key_limbs", C.c_uint32), ("key_stride", C.c_uint32), ("k", C.c_uint32),
-                ("cutoff", C.c_uint32)]
+    _fields_ = [("slots", C.c_void_p), ("capacity", C.c_uint64), ("key_limbs", C.c_uint32),
+                ("slot_bytes", C.c_uint32), ("k", C.c_uint32), ("cutoff", C.c_uint32)]
 
 
 class JobC(C.Structure):

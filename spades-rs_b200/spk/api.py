@@ -217,7 +217,7 @@ class PackedReads:
 # ---------------------------------------------------------------------------
 def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: int = 2,
               min_coverage: float = 5.0, flags: Optional[int] = None,
-              table_log2: int = 0, max_chunk_occ: int = 0) -> CountOpts:
+              table_log2: int = 0) -> CountOpts:
     o = CountOpts()
     lib().spk_count_opts_default(C.byref(o))
     o.bloom_bits = bloom_bits
@@ -225,7 +225,6 @@ def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: i
     o.list_min_count = list_min_count
     o.min_coverage = min_coverage
     o.table_log2 = table_log2
-    o.max_chunk_occ = max_chunk_occ
     if flags is not None:
         o.flags = flags
     return o

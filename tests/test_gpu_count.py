@@ -18,8 +18,9 @@ from helpers import ecoli_packed, load_npz, nlimbs, rows, synth_small_packed
 
 pytestmark = pytest.mark.gpu
 
-ALL = 0x1 | 0x2 | 0x4  # SPK_F_EDGES | SPK_F_REF_SOLID | SPK_F_KEEP_BLOOM (direct Stage 2)
-PART = 0x1 | 0x4       # SPK_F_EDGES | SPK_F_KEEP_BLOOM (partitioned Stage 2)
+BASE = 0x1 | 0x4        # SPK_F_EDGES | SPK_F_KEEP_BLOOM
+ALL = BASE | 0x2        # ... | SPK_F_REF_SOLID
+GATED = 0x8             # SPK_F_GATED: the two-pass schedule
 
 
 def sha(words):
@@ -38,11 +39,12 @@ def occ(lengths, k):
 
 def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
     """Full GPU result vs the C++ oracle (twice semantics for the table, reference
-    semantics for the count >= 2 list), for both Stage 2 implementations."""
+    semantics for the count >= 2 list), for both schedules: the default
+    one-pass schedule (p, with the reference solid tier r) and the gated one."""
     tw = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE)
     tk, tc = tw.table(1)
     oseen, otwice = tw.bloom()
-    p = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=PART, **kw)
+    p = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=BASE | GATED, **kw)
     pk, pc = p.kmers(0, 1)
     np.testing.assert_array_equal(pk, tk)
     np.testing.assert_array_equal(pc, tc)
@@ -93,7 +95,8 @@ GOLDEN = ["counts_ecoli_1K_k21.npz", "counts_ecoli_1K_k31.npz", "counts_ecoli_1K
           "counts_synth_k64.npz"]
 
 
-@pytest.mark.parametrize("flags", [PART, ALL], ids=["partitioned", "direct"])
+@pytest.mark.parametrize("flags", [BASE, BASE | GATED, ALL, ALL | GATED],
+                         ids=["fused", "gated", "fused-ref", "gated-ref"])
 @pytest.mark.parametrize("name", GOLDEN)
 def test_count_matches_golden(spk, name, flags):
     g = load_npz(name)
@@ -238,24 +241,13 @@ def test_solid_cutoff_and_seam(spk, ora):
     assert sk.shape[0] == int((rc >= cut).sum())
 
 
-@pytest.mark.parametrize("chunk", [1000, 50_000, 333_333])
-def test_stage2_streamed_in_chunks(spk, ora, chunk):
-    """Stage 2 streamed in several chunks (accumulating into the tiers) gives the same result."""
+def test_default_schedule_is_fused(spk):
     data, offs, lens = synth_small_packed()
-    check_against_oracle(spk, ora, data, offs, lens, 55, 1 << 20, max_chunk_occ=chunk)
+    assert spk.count((data, offs, lens), [55]).info(0)["fused"] == 1
+    assert spk.count((data, offs, lens), [55], flags=GATED).info(0)["fused"] == 0
 
 
-def test_partition_overflow_falls_back(spk, ora):
-    """Two distinct canonical k-mers (k = 1) pile every Bloom operation into one
-    partition; Stage 2 reruns with the direct kernel and the result is unchanged."""
+def test_fused_table_regrow(spk, ora):
+    """The one-pass table (every distinct k-mer) starting far too small regrows and recounts."""
     data, offs, lens = synth_small_packed()
-    r = spk.count((data, offs, lens), [1], bloom_bits=1 << 20, list_min_count=1, flags=PART)
-    assert r.info(0)["stage2_fallback"] == 1
-    check_against_oracle(spk, ora, data, offs, lens, 1, 1 << 20)
-
-
-def test_default_path_is_partitioned(spk):
-    data, offs, lens = synth_small_packed()
-    r = spk.count((data, offs, lens), [55])
-    i = r.info(0)
-    assert i["stage2_partitioned"] == 1 and i["stage2_fallback"] == 0
+    check_against_oracle(spk, ora, data, offs, lens, 31, 1 << 20, table_log2=6)
