@@ -167,6 +167,13 @@ int spk_ctx_create(int device, spk_ctx** out) {
     e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_pinned, 1 << 16);
+  // The hot kernels make random 8-32 byte accesses (Bloom words, table
+  // slots); fetch only the 32-byte sector that was asked for.  This is a
+  // limit of this process's context, not a device setting.
+  if (e == cudaSuccess) {
+    cudaError_t g = cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, 32);
+    if (g != cudaSuccess) cudaGetLastError();  // a hint; ignore if unsupported
+  }
   if (e != cudaSuccess) {
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;

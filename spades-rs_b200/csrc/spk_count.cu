@@ -212,22 +212,41 @@ __device__ __forceinline__ uint64_t table_home(const TableView& t, uint64_t raw0
 // Adds n to key C.  Keys of <= 128 bits claim a slot with one 64- or 128-bit
 // CAS against the sentinel; wider keys claim the state word, publish the key
 // and mark the slot ready.
+// The first key words of the home slot, loaded early so the table probe
+// overlaps the Bloom accesses of the same occurrence.
+struct SlotPeek {
+  unsigned long long x, y;
+};
+template <int NL>
+__device__ __forceinline__ SlotPeek table_peek(const TableView& t, uint64_t home) {
+  SlotPeek p{kEmpty, kEmpty};
+  if (NL == 1) p.x = __ldcg((const unsigned long long*)slot_key<NL>(t, home));
+  if (NL == 2) {
+    const ulonglong2 v = __ldcg((const ulonglong2*)slot_key<NL>(t, home));
+    p.x = v.x;
+    p.y = v.y;
+  }
+  return p;
+}
+
 template <int NL>
 __device__ __forceinline__ void table_add(const TableView& t, const Seq<NL>& C, uint64_t home,
-                                          uint32_t n) {
+                                          uint32_t n, const SlotPeek* peek = nullptr) {
   const uint64_t mask = t.capacity - 1;
   for (uint32_t i = 0; i < t.max_probe; i++) {
     const uint64_t s = (home + i) & mask;
     uint64_t* kp = slot_key<NL>(t, s);
     if (NL == 1) {
-      unsigned long long cur = __ldcg((const unsigned long long*)kp);
+      unsigned long long cur = (i == 0 && peek) ? peek->x : __ldcg((const unsigned long long*)kp);
       if (cur == C.v[0]) { atomicAdd(slot_count<NL>(t, s), n); return; }
       if (cur == kEmpty) {
         unsigned long long old = atomicCAS((unsigned long long*)kp, kEmpty, (unsigned long long)C.v[0]);
         if (old == kEmpty || old == C.v[0]) { atomicAdd(slot_count<NL>(t, s), n); return; }
       }
     } else if (NL == 2) {
-      ulonglong2 cur = __ldcg((const ulonglong2*)kp);
+      ulonglong2 cur;
+      if (i == 0 && peek) cur = make_ulonglong2(peek->x, peek->y);
+      else cur = __ldcg((const ulonglong2*)kp);
       if (cur.x != kEmpty && cur.y != kEmpty) {
         // A settled key (a 16-byte load may tear only while a slot is being
         // claimed, and a claimed slot never changes afterwards).
@@ -291,7 +310,7 @@ __device__ __forceinline__ uint32_t table_find(const TableView& t, const Seq<NL>
 
 template <int NL>
 __device__ __forceinline__ void warp_table_add(const TableView& t, bool take, const Seq<NL>& C,
-                                               uint64_t raw0) {
+                                               uint64_t raw0, const SlotPeek* peek = nullptr) {
   const unsigned am = __ballot_sync(FULL, take);
   if (take) {
     // Equal keys in the warp (repeats, hot k-mers) become one atomic add.
@@ -299,7 +318,7 @@ __device__ __forceinline__ void warp_table_add(const TableView& t, bool take, co
 #pragma unroll
     for (int j = 0; j < NL; j++) peers &= __match_any_sync(am, (unsigned long long)C.v[j]);
     if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1))
-      table_add<NL>(t, C, table_home(t, raw0), __popc(peers));
+      table_add<NL>(t, C, table_home(t, raw0), __popc(peers), peek);
   }
 }
 
@@ -318,16 +337,18 @@ __global__ void __launch_bounds__(kBlock) k_fused_pass(ReadsView R, unsigned k, 
   auto fn = [&](bool active, uint64_t bitpos) {
     Seq<NL> C;
     uint64_t raw[3] = {0, 0, 0};
+    SlotPeek peek{kEmpty, kEmpty};
     if (active) {
       occ++;
       const Seq<NL> V = extract<NL>(R.words, bitpos, k);
       C = canonical<NL>(V, k);
       uint64_t pos[3];
       bloom_positions<NL>(C, k, fm, raw, pos);
+      peek = table_peek<NL>(t, table_home(t, raw[0]));
       const bool allprev = bloom_insert3(tiers, pos);
       if (REF && allprev) ref_promote(ref_solid, pos);
     }
-    warp_table_add<NL>(t, active, C, raw[0]);
+    warp_table_add<NL>(t, active, C, raw[0], NL <= 2 ? &peek : nullptr);
   };
   foreach_position(R, k, fn);
   warp_add_u64(occ_out, occ);
@@ -399,47 +420,74 @@ __global__ void __launch_bounds__(kBlock) k_tier_finish(const U128* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// Admission of k-mers seen once, and the count histogram of the admitted
-// table (the input of src/assemble.rs:692-735).
+// One scan of the table: admission of k-mers seen once (their three twice
+// bits), the count histogram of the admitted table (the input of
+// src/assemble.rs:692-735), and the stream compaction of admitted k-mers with
+// count >= lmin into the SoA list.  lmin is known before the cutoff: the
+// adaptive cutoff is never below 2 (src/assemble.rs:692-735).
 // sums: [0] admitted k-mers, [1] admitted count-1 k-mers, [2] admitted
-// occurrences (sum of counts).
+// occurrences (sum of counts), [3] list length.
 // ---------------------------------------------------------------------------
 constexpr int kHistBins = 256;  // counts >= 255 share the last bin
 
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_admit_hist(TableView t, unsigned k, FastMod fm,
-                                                        const uint64_t* __restrict__ twice,
-                                                        int check_singletons,
-                                                        unsigned long long* __restrict__ hist,
-                                                        unsigned long long* __restrict__ sums) {
+__global__ void __launch_bounds__(kBlock) k_admit_compact(TableView t, unsigned k, FastMod fm,
+                                                          const uint64_t* __restrict__ twice,
+                                                          int check_singletons, uint32_t lmin,
+                                                          uint64_t* o0, uint64_t* o1, uint64_t* o2,
+                                                          uint64_t* o3, uint32_t* __restrict__ ocnt,
+                                                          uint64_t out_cap,
+                                                          unsigned long long* __restrict__ hist,
+                                                          unsigned long long* __restrict__ sums) {
   __shared__ unsigned sh[kHistBins];
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) sh[i] = 0;
   __syncthreads();
+  const unsigned lane = threadIdx.x & 31;
   uint64_t n_adm = 0, n_one = 0, occ = 0;
-  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < t.capacity;
-       s += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t* cp = slot_count<NL>(t, s);
-    const uint32_t c = *cp;
-    if (c == 0) continue;
-    if (c == 1 && check_singletons) {
-      Seq<NL> C;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t start = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  // Uniform trip count per warp so the ballot below sees every lane.
+  for (uint64_t base = start - lane; base < t.capacity; base += stride) {
+    const uint64_t s = base + lane;
+    uint32_t c = s < t.capacity ? *slot_count<NL>(t, s) : 0u;
+    if (c & kRejected) c = 0;
+    Seq<NL> C;
+    if (c) {
       const uint64_t* kp = slot_key<NL>(t, s);
 #pragma unroll
       for (int j = 0; j < NL; j++) C.v[j] = kp[j];
+    }
+    if (c == 1 && check_singletons) {
       uint64_t raw[3], pos[3];
       bloom_positions<NL>(C, k, fm, raw, pos);
-      bool ok = (__ldg(twice + (pos[0] >> 6)) >> (pos[0] & 63)) & 1;
-      if (ok) ok = (__ldg(twice + (pos[1] >> 6)) >> (pos[1] & 63)) & 1;
-      if (ok) ok = (__ldg(twice + (pos[2] >> 6)) >> (pos[2] & 63)) & 1;
-      if (!ok) {
-        *cp = 1u | kRejected;
-        continue;
+      const uint64_t a = __ldg(twice + (pos[0] >> 6));
+      const uint64_t b = __ldg(twice + (pos[1] >> 6));
+      const uint64_t d = __ldg(twice + (pos[2] >> 6));
+      if (!((a >> (pos[0] & 63)) & (b >> (pos[1] & 63)) & (d >> (pos[2] & 63)) & 1)) {
+        *slot_count<NL>(t, s) = 1u | kRejected;
+        c = 0;
       }
     }
-    n_adm++;
-    n_one += c == 1;
-    occ += c;
-    atomicAdd(&sh[c < kHistBins - 1 ? c : kHistBins - 1], 1u);
+    if (c) {
+      n_adm++;
+      n_one += c == 1;
+      occ += c;
+      atomicAdd(&sh[c < kHistBins - 1 ? c : kHistBins - 1], 1u);
+    }
+    const bool keep = c != 0 && c >= lmin;
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (!m) continue;
+    unsigned long long pos0 = 0;
+    if (lane == (unsigned)(__ffs(m) - 1)) pos0 = atomicAdd(sums + 3, (unsigned long long)__popc(m));
+    pos0 = __shfl_sync(FULL, pos0, __ffs(m) - 1);
+    const uint64_t p = pos0 + __popc(m & lanemask_lt());
+    if (keep && p < out_cap) {
+      o0[p] = C.v[0];
+      if (NL > 1) o1[p] = C.v[NL > 1 ? 1 : 0];
+      if (NL > 2) o2[p] = C.v[NL > 2 ? 2 : 0];
+      if (NL > 3) o3[p] = C.v[NL > 3 ? 3 : 0];
+      ocnt[p] = c;
+    }
   }
   warp_add_u64(sums + 0, n_adm);
   warp_add_u64(sums + 1, n_one);
@@ -447,6 +495,18 @@ __global__ void __launch_bounds__(kBlock) k_admit_hist(TableView t, unsigned k, 
   __syncthreads();
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
     if (sh[i]) atomicAdd(hist + i, (unsigned long long)sh[i]);
+}
+
+// Solid k-mers of the list (count >= cutoff), for cutoffs the histogram cannot resolve.
+__global__ void __launch_bounds__(256) k_count_solid(const uint32_t* __restrict__ cnt, uint64_t n,
+                                                     const uint32_t* __restrict__ thr,
+                                                     unsigned long long* __restrict__ out) {
+  uint64_t s = 0;
+  const uint32_t cutoff = thr[0];
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    s += cnt[i] >= cutoff;
+  warp_add_u64(out, s);
 }
 
 // out: [0] cutoff, [1] list threshold
@@ -483,46 +543,6 @@ __global__ void k_cutoff(const unsigned long long* __restrict__ hist, uint32_t f
   }
   out[0] = cutoff;
   out[1] = max(1u, min(cutoff, list_min));
-}
-
-// ---------------------------------------------------------------------------
-// Stream compaction of the admitted table into the SoA k-mer list.
-// counters: [0] list length, [1] solid (>= cutoff)
-// ---------------------------------------------------------------------------
-template <int NL>
-__global__ void __launch_bounds__(kBlock) k_compact(TableView t, const uint32_t* __restrict__ thr,
-                                                     uint64_t* o0, uint64_t* o1, uint64_t* o2,
-                                                     uint64_t* o3, uint32_t* __restrict__ ocnt,
-                                                     uint64_t out_cap,
-                                                     unsigned long long* __restrict__ counters) {
-  const uint32_t cutoff = thr[0], lmin = thr[1];
-  const unsigned lane = threadIdx.x & 31;
-  uint64_t nsolid = 0;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  // Uniform trip count per warp so the ballot below sees every lane.
-  const uint64_t start = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  for (uint64_t base = start - lane; base < t.capacity; base += stride) {
-    const uint64_t s = base + lane;
-    uint32_t c = s < t.capacity ? *slot_count<NL>(t, s) : 0u;
-    if (c & kRejected) c = 0;
-    nsolid += c != 0 && c >= cutoff;
-    const bool keep = c != 0 && c >= lmin;
-    const unsigned m = __ballot_sync(FULL, keep);
-    if (!m) continue;
-    unsigned long long pos0 = 0;
-    if (lane == (unsigned)(__ffs(m) - 1)) pos0 = atomicAdd(counters + 0, (unsigned long long)__popc(m));
-    pos0 = __shfl_sync(FULL, pos0, __ffs(m) - 1);
-    const uint64_t p = pos0 + __popc(m & lanemask_lt());
-    if (keep && p < out_cap) {
-      const uint64_t* kp = slot_key<NL>(t, s);
-      o0[p] = kp[0];
-      if (NL > 1) o1[p] = kp[NL > 1 ? 1 : 0];
-      if (NL > 2) o2[p] = kp[NL > 2 ? 2 : 0];
-      if (NL > 3) o3[p] = kp[NL > 3 ? 3 : 0];
-      ocnt[p] = c;
-    }
-  }
-  warp_add_u64(counters + 1, nsolid);
 }
 
 // ---------------------------------------------------------------------------
@@ -670,16 +690,11 @@ static void launch_init(spk_ctx* ctx, cudaStream_t st, uint8_t* slots, uint64_t 
 }
 template <int NL>
 static void launch_admit(spk_ctx* ctx, cudaStream_t st, const TableView& t, unsigned k,
-                         const FastMod& fm, const uint64_t* twice, int check,
-                         unsigned long long* hist, unsigned long long* sums) {
-  k_admit_hist<NL><<<grid_for(ctx, 4), kBlock, 0, st>>>(t, k, fm, twice, check, hist, sums);
-}
-template <int NL>
-static void launch_compact(spk_ctx* ctx, cudaStream_t st, const TableView& t, const uint32_t* thr,
-                           uint64_t** o, uint32_t* oc, uint64_t out_cap,
-                           unsigned long long* counters) {
-  k_compact<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(t, thr, o[0], o[1], o[2], o[3], oc, out_cap,
-                                                    counters);
+                         const FastMod& fm, const uint64_t* twice, int check, uint32_t lmin,
+                         uint64_t** o, uint32_t* oc, uint64_t out_cap, unsigned long long* hist,
+                         unsigned long long* sums) {
+  k_admit_compact<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(t, k, fm, twice, check, lmin, o[0], o[1],
+                                                          o[2], o[3], oc, out_cap, hist, sums);
 }
 template <int NL, int NLE>
 static void launch_edges_t(spk_ctx* ctx, cudaStream_t st, uint64_t* l[4], const uint32_t* cnt,
@@ -766,8 +781,8 @@ enum {
   S_OCC = 0, S_POPS = 1, /* 2 words */
   S_ERR = 3,             /* int */
   S_THR = 4,             /* 2 x u32 */
-  S_SUMS = 5,            /* 3 words: admitted, admitted singletons, admitted occurrences */
-  S_CNT = 8,             /* 2 words: list, solid */
+  S_SUMS = 5,            /* 4 words: admitted, admitted singletons, admitted occurrences, list */
+  S_CNT = 9,             /* solid */
   S_EDGES = 10,
   S_OCC0 = 11,           /* occurrences before the pass */
   S_HIST = 16,           /* 256 words */
@@ -894,18 +909,56 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   info.table_capacity = cap;
   SPK_CUDA(cudaEventRecord(e2.e, st));
 
-  // ---- admission of singletons, histogram, cutoff ----
-  SPK_DISPATCH_NL(nl, launch_admit, ctx, st, kr.table, k, kr.fm, kr.twice.as<uint64_t>(),
-                  gated ? 0 : 1, su + S_HIST, su + S_SUMS);
+  // ---- admission of singletons, histogram, compaction, cutoff ----
   uint32_t fixed = o.min_count;
   if (!fixed && o.min_coverage > 5.0) {  // src/assemble.rs:693-694
     double v = std::max(o.min_coverage * 0.35, 2.0);
     fixed = v >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v;
   }
+  const uint32_t list_min = o.list_min_count ? o.list_min_count : 2;
+  // The list keeps counts >= min(cutoff, list_min).  The adaptive cutoff is
+  // never below 2, so compacting counts >= min(2 or the fixed cutoff,
+  // list_min) keeps a superset; the exact threshold filters downloads.
+  const uint32_t lmin_pre = std::max(1u, std::min(fixed ? fixed : 2u, list_min));
+  kr.list_min = lmin_pre;
+  // List capacity from the Bloom: k-mers seen at least twice (twice-tier
+  // estimate, an overestimate), plus admitted singletons if they are listed.
+  uint64_t lcap;
+  {
+    const double md = (double)size_bits;
+    const double fs = std::min((double)info.seen_popcount / md, 0.999999);
+    const double ft = std::min((double)info.twice_popcount / md, 0.999999);
+    const double n_all = -(md / 3.0) * std::log1p(-fs);
+    const double n2 = -(md / 3.0) * std::log1p(-ft);
+    double est = n2 * 1.25 + 65536;
+    if (kr.list_min <= 1) est += std::max(n_all - n2, 0.0) * ft * ft * ft * 1.5 + 65536;
+    lcap = std::min<uint64_t>((uint64_t)est, cap);
+  }
+  uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int pass = 0;; pass++) {
+    for (int j = 0; j < nl; j++) {
+      if ((rc = kr.list[j].alloc(std::max<uint64_t>(lcap, 1) * 8, st))) return rc;
+      lp[j] = kr.list[j].as<uint64_t>();
+    }
+    if ((rc = kr.list[4].alloc(std::max<uint64_t>(lcap, 1) * 4, st))) return rc;
+    SPK_CUDA(cudaMemsetAsync(sw + S_SUMS, 0, 4 * 8, st));
+    SPK_CUDA(cudaMemsetAsync(sw + S_HIST, 0, kHistBins * 8, st));
+    SPK_DISPATCH_NL(nl, launch_admit, ctx, st, kr.table, k, kr.fm, kr.twice.as<uint64_t>(),
+                    gated ? 0 : 1, lmin_pre, lp, kr.list[4].as<uint32_t>(), lcap, su + S_HIST,
+                    su + S_SUMS);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    if ((rc = fetch(S_SUMS + 4))) return rc;
+    if (host[S_SUMS + 3] <= lcap) break;
+    // Underestimated: size exactly and scan again (rejections are already
+    // marked, so the second scan admits the same k-mers).
+    lcap = host[S_SUMS + 3];
+    if (pass >= 1) return fail(SPK_E_CUDA, "k-mer list size changed between scans");
+  }
   uint32_t* thr = (uint32_t*)(sw + S_THR);
-  k_cutoff<<<1, 32, 0, st>>>(su + S_HIST, fixed, o.list_min_count ? o.list_min_count : 2, thr);
+  k_cutoff<<<1, 32, 0, st>>>(su + S_HIST, fixed, list_min, thr);
   SPK_CUDA(cudaGetLastError());
-  launches += 2;
+  launches++;
   if ((rc = fetch(S_WORDS))) return rc;
   const uint32_t* hthr = (const uint32_t*)(host + S_THR);
   info.cutoff = hthr[0];
@@ -913,31 +966,30 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   info.n_table = host[S_SUMS + 0];
   info.n_singletons = host[S_SUMS + 1];
   info.admitted_occurrences = host[S_SUMS + 2];
-  // List length from the histogram: exact for thresholds below the last bin,
-  // an upper bound otherwise (the compaction counts exactly).
-  uint64_t n_list = 0;
-  for (int c = 0; c < kHistBins; c++)
-    if ((uint32_t)c >= kr.list_min || c == kHistBins - 1) n_list += host[S_HIST + c];
-
-  // ---- compaction ----
-  uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
-  for (int j = 0; j < nl; j++) {
-    if ((rc = kr.list[j].alloc(std::max<uint64_t>(n_list, 1) * 8, st))) return rc;
-    lp[j] = kr.list[j].as<uint64_t>();
+  kr.list_len = host[S_SUMS + 3];
+  auto hist_from = [&](uint32_t c0) {
+    uint64_t ns = 0;
+    for (int c = (int)c0; c < kHistBins; c++) ns += host[S_HIST + c];
+    return ns;
+  };
+  info.n_list = kr.list_min == lmin_pre ? kr.list_len : hist_from(kr.list_min);
+  if (kr.list_min != lmin_pre && kr.list_min >= (uint32_t)(kHistBins - 1))
+    return fail(SPK_E_INVALID_ARG, "list_min_count above 254 needs a fixed min_count");
+  if (info.cutoff < (uint32_t)(kHistBins - 1)) {
+    info.n_solid = hist_from(info.cutoff);
+  } else {
+    SPK_CUDA(cudaMemsetAsync(sw + S_CNT, 0, 8, st));
+    k_count_solid<<<grid_for(ctx, 2), 256, 0, st>>>(kr.list[4].as<uint32_t>(), kr.list_len, thr,
+                                                   su + S_CNT);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    if ((rc = fetch(S_CNT + 1))) return rc;
+    info.n_solid = host[S_CNT];
   }
-  if ((rc = kr.list[4].alloc(std::max<uint64_t>(n_list, 1) * 4, st))) return rc;
-  SPK_DISPATCH_NL(nl, launch_compact, ctx, st, kr.table, thr, lp, kr.list[4].as<uint32_t>(), n_list,
-                  su + S_CNT);
-  SPK_CUDA(cudaGetLastError());
-  launches++;
   SPK_CUDA(cudaEventRecord(e3.e, st));
-  if ((rc = fetch(S_EDGES))) return rc;
-  info.n_list = host[S_CNT + 0];
-  info.n_solid = host[S_CNT + 1];
-  if (info.n_list > n_list) return fail(SPK_E_CUDA, "k-mer list larger than its histogram count");
 
   // ---- sort ----
-  if ((rc = radix_sort_bufs(st, nl, info.n_list, 2 * k, kr.list, &kr.list[4], &launches))) return rc;
+  if ((rc = radix_sort_bufs(st, nl, kr.list_len, 2 * k, kr.list, &kr.list[4], &launches))) return rc;
   for (int j = 0; j < nl; j++) lp[j] = kr.list[j].as<uint64_t>();
   SPK_CUDA(cudaEventRecord(e4.e, st));
 
@@ -950,7 +1002,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
       if ((rc = kr.edges[j].alloc(ecap * 8, st))) return rc;
       ep[j] = kr.edges[j].as<uint64_t>();
     }
-    launch_edges(ctx, st, nl, kr.nle, lp, kr.list[4].as<uint32_t>(), info.n_list, thr, kr.table, k,
+    launch_edges(ctx, st, nl, kr.nle, lp, kr.list[4].as<uint32_t>(), kr.list_len, thr, kr.table, k,
                  ep, ecap, su + S_EDGES);
     SPK_CUDA(cudaGetLastError());
     launches++;
@@ -1026,7 +1078,7 @@ int download_list(spk_result* res, int ki, uint32_t min_count, bool solid_only, 
                   uint32_t* counts, size_t* n_inout) {
   KResult& kr = *res->ks[ki];
   const uint32_t minc = solid_only ? kr.info.cutoff : std::max(min_count, kr.list_min);
-  return copy_out(res, kr.nl, kr.list, kr.list[4].as<uint32_t>(), kr.info.n_list, kr.k, minc,
+  return copy_out(res, kr.nl, kr.list, kr.list[4].as<uint32_t>(), kr.list_len, kr.k, minc,
                   keys, counts, n_inout);
 }
 

@@ -98,7 +98,8 @@ struct KResult {
   DevBuf list[5];     // sorted k-mer list: limbs 0..nl-1 (SoA), counts in list[4]
   DevBuf edges[4];    // sorted edge list: limbs (SoA)
   int nle = 0;        // limbs per edge key
-  uint32_t list_min = 2;  // smallest count in the list
+  uint32_t list_min = 2;  // smallest count downloads of the list return
+  uint64_t list_len = 0;  // entries in the list buffers (may include counts below list_min)
 };
 
 struct spk_result_impl;

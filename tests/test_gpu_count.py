@@ -251,3 +251,19 @@ def test_fused_table_regrow(spk, ora):
     """The one-pass table (every distinct k-mer) starting far too small regrows and recounts."""
     data, offs, lens = synth_small_packed()
     check_against_oracle(spk, ora, data, offs, lens, 31, 1 << 20, table_log2=6)
+
+
+def test_list_threshold_above_two(spk, ora):
+    """list_min_count above 2 with the adaptive cutoff: the list and its length
+    hold exactly the k-mers with count >= min(list_min_count, cutoff)."""
+    data, offs, lens = synth_small_packed()
+    ref = ora.count(data, offs, lens, 55, 1 << 20, mode=ora.MODE_TWICE)
+    tk, tc = ref.table(1)
+    r = spk.count((data, offs, lens), [55], bloom_bits=1 << 20, list_min_count=5)
+    i = r.info(0)
+    thr = min(5, i["cutoff"])
+    keys, counts = r.kmers(0)
+    np.testing.assert_array_equal(keys, tk[tc >= thr])
+    np.testing.assert_array_equal(counts, tc[tc >= thr])
+    assert i["n_list"] == int((tc >= thr).sum())
+    assert i["n_solid"] == int((tc >= i["cutoff"]).sum())
