@@ -31,10 +31,12 @@ METRIC = "Gk-mers/s at k=55 (5Mb,100x) batched vs plain on 1 B200; p50/p99 job l
 K = 55
 L2_FLUSH_BYTES = 512 << 20  # > the 126 MB L2, written between timed steps
 # Algorithmic bytes per k-mer occurrence, counted at the 32-byte sector
-# granularity of random DRAM/L2 accesses ("Roofline").
+# granularity of random DRAM/L2 accesses.
+#   fused pass:     the packed-read stream, 3 random Bloom word-pair sectors
+#                   and the one-sector count-table slot.
 #   Stage 2 insert: 3 random Bloom word-pair sectors + the packed-read stream.
 #   Stage 3 count:  3 random twice-tier sectors + the stream, and for each
-#                   admitted occurrence one key sector and one count sector.
+#                   admitted occurrence one table slot sector.
 SECTOR = 32
 
 
@@ -269,12 +271,21 @@ def main():
     # roofline of the dominant kernel (largest share of the step)
     f_adm = info["admitted_occurrences"] / max(info["occurrences"], 1)
     sb = stream_bytes_per_occ()
-    bytes_bloom = occ * (3 * SECTOR + sb)
-    bytes_count = occ * (3 * SECTOR + sb + f_adm * 2 * SECTOR)
-    if count_ms >= bloom_ms:
-        kname, kms, kbytes = "k_count_pass", count_ms, bytes_count
+    if info["fused"]:
+        # One pass: the read stream, three Bloom word-pair sectors and the
+        # one-sector table slot of every occurrence.
+        kname, kms = "k_fused_pass", bloom_ms
+        kbytes = occ * (sb + 3 * SECTOR + SECTOR)
+    elif count_ms >= bloom_ms:
+        kname, kms = "k_count_pass", count_ms
+        kbytes = occ * (3 * SECTOR + sb + f_adm * SECTOR)
     else:
-        kname, kms, kbytes = "k_bloom_pass", bloom_ms, bytes_bloom
+        kname, kms = "k_bloom_pass", bloom_ms
+        kbytes = occ * (3 * SECTOR + sb)
+    # Whole job against the design-independent 217 B per occurrence of the
+    # reference's two-pass algorithm (stream x2, Bloom insert + query, table,
+    # output).
+    job_bytes_per_occ = 2 * sb + 6 * SECTOR + f_adm * SECTOR + 0.3
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         with open(peaks_path) as f:
@@ -292,6 +303,9 @@ def main():
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes,
                 "kernel_ms": kms, "kernel_share": kms / ms,
+                "job": {"bytes_per_occurrence": job_bytes_per_occ,
+                        "achieved": value * job_bytes_per_occ / world,
+                        "frac": value * job_bytes_per_occ / world / peak},
                 "phases_ms": {"bloom_kernel": bloom_ms, "count_kernel": count_ms,
                               "bloom_phase": info["ms_bloom"], "count_phase": info["ms_count"],
                               "cutoff_compact": info["ms_finish"], "sort": info["ms_sort"],

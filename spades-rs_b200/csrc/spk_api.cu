@@ -74,6 +74,41 @@ void DevBuf::release() {
   bytes = 0;
 }
 
+// ---- pinned staging blocks ----------------------------------------------------
+uint64_t* staging_acquire(spk_ctx* ctx) {
+  std::lock_guard<std::mutex> l(ctx->staging_mu);
+  if (!ctx->staging_free.empty()) {
+    uint64_t* b = ctx->staging_free.back();
+    ctx->staging_free.pop_back();
+    return b;
+  }
+  uint64_t* b = nullptr;
+  if (cudaMallocHost((void**)&b, kStagingBytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  ctx->staging_all.push_back(b);
+  return b;
+}
+void staging_release(spk_ctx* ctx, uint64_t* block) {
+  if (!block) return;
+  std::lock_guard<std::mutex> l(ctx->staging_mu);
+  ctx->staging_free.push_back(block);
+}
+spk_result* result_new(spk_ctx* ctx, cudaStream_t st, bool own_stream) {
+  uint64_t* h = staging_acquire(ctx);
+  if (!h) {
+    fail(SPK_E_OOM, "pinned host staging allocation failed");
+    return nullptr;
+  }
+  auto* res = new spk_result();
+  res->ctx = ctx;
+  res->stream = st;
+  res->own_stream = own_stream;
+  res->h_staging = h;
+  return res;
+}
+
 int bloom_create(spk_ctx* ctx, uint64_t capacity_bits, spk_bloom** out);
 int bloom_insert(spk_bloom* b, const uint64_t* keys, size_t n, int wide, uint8_t* promoted);
 int bloom_query(spk_bloom* b, const uint64_t* keys, size_t n, int wide, uint8_t* out);
@@ -166,7 +201,6 @@ int spk_ctx_create(int device, spk_ctx** out) {
     uint64_t thr = ~0ULL;  // keep freed blocks cached in the pool
     e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_pinned, 1 << 16);
   // The hot kernels make random 8-32 byte accesses (Bloom words, table
   // slots); fetch only the 32-byte sector that was asked for.  This is a
   // limit of this process's context, not a device setting.
@@ -189,7 +223,7 @@ int spk_ctx_destroy(spk_ctx* ctx) {
   serve_shutdown(ctx);
   ctx->scratch.release();
   cudaStreamSynchronize(ctx->stream);
-  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  for (uint64_t* b : ctx->staging_all) cudaFreeHost(b);
   cudaStreamDestroy(ctx->own_stream);
   if (ctx->pool) cudaMemPoolTrimTo(ctx->pool, 0);
   delete ctx;
@@ -297,9 +331,8 @@ int spk_count(spk_ctx* ctx, const uint8_t* data, size_t data_len, const uint64_t
   if ((rc = check_ks(ks, n_k))) return rc;
   if (n_reads && (!offsets || !lengths)) return fail(SPK_E_INVALID_ARG, "null offsets/lengths");
   if (data_len && !data) return fail(SPK_E_INVALID_ARG, "null data");
-  auto* res = new spk_result();
-  res->ctx = ctx;
-  res->stream = ctx->stream;
+  auto* res = result_new(ctx, ctx->stream, false);
+  if (!res) return SPK_E_OOM;
   res->opts = resolve_opts(opts);
   ReadsView rv;
   rc = upload_reads(res, ctx->stream, data, data_len, offsets, lengths, n_reads, &rv);
@@ -326,9 +359,8 @@ int spk_count_device(spk_ctx* ctx, const uint8_t* d_data, size_t data_len,
   if ((rc = check_ks(ks, n_k))) return rc;
   if (n_reads && (!d_offsets || !d_lengths || !d_data))
     return fail(SPK_E_INVALID_ARG, "null device pointer");
-  auto* res = new spk_result();
-  res->ctx = ctx;
-  res->stream = ctx->stream;
+  auto* res = result_new(ctx, ctx->stream, false);
+  if (!res) return SPK_E_OOM;
   res->opts = resolve_opts(opts);
   ReadsView rv;
   const uintptr_t a = (uintptr_t)d_data;
@@ -412,6 +444,7 @@ int spk_result_free(spk_result* res) {
   res->offs.release();
   res->lens.release();
   cudaStreamSynchronize(st);
+  staging_release(res->ctx, res->h_staging);
   if (res->own_stream) cudaStreamDestroy(st);
   delete res;
   return SPK_OK;

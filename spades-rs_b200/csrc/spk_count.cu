@@ -789,7 +789,7 @@ enum {
   S_WORDS = 16 + kHistBins
 };
 
-int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned k,
+int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv_in, unsigned k,
                 const spk_count_opts& o, KResult& kr) {
   kr.k = k;
   kr.nl = (int)((k + 31) / 32);
@@ -809,7 +809,6 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv_in, unsigned 
   uint64_t* sw = scratch.as<uint64_t>();
   SPK_CUDA(cudaMemsetAsync(sw, 0, S_WORDS * 8, st));
   unsigned long long* su = (unsigned long long*)sw;
-  uint64_t* host = ctx->h_pinned;
   int* errp = (int*)(sw + S_ERR);
   ReadsView rv = rv_in;
   rv.err = errp;
@@ -1037,7 +1036,7 @@ int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t 
   (void)max_len;
   for (int i = 0; i < n_k; i++) {
     auto kr = std::make_unique<KResult>();
-    int rc = count_one_k(ctx, st, rv, ks[i], o, *kr);
+    int rc = count_one_k(ctx, st, res->h_staging, rv, ks[i], o, *kr);
     if (rc) return rc;
     res->ks.push_back(std::move(kr));
   }
@@ -1053,7 +1052,7 @@ static int copy_out(spk_result* res, int nl, DevBuf* limbs, const uint32_t* cin,
   DevBuf okeys, ocnt;
   uint64_t m = 0;
   int rc = ordered_convert(st, nl, n, k, limbs, cin, minc, &okeys, cin ? &ocnt : nullptr,
-                           res->ctx->h_pinned, &m);
+                           res->h_staging, &m);
   if (rc) return rc;
   if (!keys && !counts) {
     SPK_CUDA(cudaStreamSynchronize(st));

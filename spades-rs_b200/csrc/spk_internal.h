@@ -115,7 +115,11 @@ struct spk_ctx {
   int sm_count = 0;
   size_t l2_bytes = 0;
   spk::DevBuf scratch;      // small device scratch (counters, flags)
-  uint64_t* h_pinned = nullptr;  // small pinned host staging area
+  // Pinned host staging blocks (kStagingBytes each) for counters read back
+  // during a count.  Every result holds its own block, so jobs that run
+  // concurrently (serving, batches) never share one.
+  std::mutex staging_mu;
+  std::vector<uint64_t*> staging_free, staging_all;
   // serving
   struct Server* server = nullptr;
   std::mutex serve_mu;
@@ -136,9 +140,17 @@ struct spk_result {
   std::vector<std::unique_ptr<spk::KResult>> ks;
   spk::DevBuf reads;  // device copy of the packed reads (when copied in by spk_count)
   spk::DevBuf offs, lens;
+  uint64_t* h_staging = nullptr;  // pinned staging block of this result (from ctx)
 };
 
 namespace spk {
+constexpr size_t kStagingBytes = 1 << 16;
+// A pinned staging block for one result (nullptr if pinned memory is
+// exhausted), and its return to the context's free list.
+uint64_t* staging_acquire(spk_ctx* ctx);
+void staging_release(spk_ctx* ctx, uint64_t* block);
+// A new result on stream st with its own staging block, or nullptr (error set).
+spk_result* result_new(spk_ctx* ctx, cudaStream_t st, bool own_stream);
 // Count pipeline on device-resident reads (spk_count.cu).  `res` is filled
 // with one KResult per k.
 int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t max_len,

@@ -64,10 +64,11 @@ static int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& 
   cudaStream_t st;
   cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   if (e != cudaSuccess) return cuda_fail(e, "job stream");
-  auto* res = new spk_result();
-  res->ctx = ctx;
-  res->stream = st;
-  res->own_stream = true;
+  auto* res = result_new(ctx, st, true);
+  if (!res) {
+    cudaStreamDestroy(st);
+    return SPK_E_OOM;
+  }
   res->opts = j.opts;
   if (!res->opts.bloom_bits) res->opts.bloom_bits = 512ULL << 20;
   if (!res->opts.list_min_count) res->opts.list_min_count = 2;
