@@ -105,6 +105,36 @@ int spk_bloom_is_solid_k256(spk_bloom* bloom, const uint64_t* keys4, size_t n, u
  * each buffer holds size_bits/64 words and may be NULL. */
 int spk_bloom_download(spk_bloom* bloom, uint64_t* seen, uint64_t* solid);
 
+/* Largest n accepted by spk_bloom_insert_k256_noalloc. */
+#define SPK_NOALLOC_MAX_KEYS 65536u
+/* No counterpart in the reference.  The insert_kmer256 batch of
+ * spk_bloom_insert_k256 for callers that must not allocate device memory:
+ * hosts whose HBM is fully committed to their own arena or to resident count
+ * tables (a cudaMalloc would fail there), and hosts with work in flight on
+ * other streams that cannot afford the implicit device synchronisation of
+ * cudaMalloc / cudaFree.  Everything is a device pointer on the current
+ * device and owned by the caller: the two tiers (num_words u64 words each,
+ * size_bits = 64 * num_words as in src/bloom.rs:27-28), n keys of 4 limbs and
+ * the nullable out_promoted (n bytes).  The result equals
+ * spk_bloom_insert_k256 on a filter holding the same tiers.
+ *   - n may be at most SPK_NOALLOC_MAX_KEYS; larger n returns
+ *     SPK_E_INVALID_ARG and does nothing.
+ *   - The work is queued on cuda_stream (NULL = the legacy default stream)
+ *     and the call returns without waiting; the outputs are ready once that
+ *     stream has been synchronised.
+ *   - The library never allocates for this call.  Its scratch (about 10 MiB)
+ *     is a static device array that every GPU holds from the moment the
+ *     library's device code is loaded on it until the process exits.
+ *   - The first call on each device looks up that array's device address;
+ *     make that first call before any stream capture on the device.
+ *   - All calls on a device share the one scratch array, so calls whose work
+ *     overlaps on the GPU (different streams, or different host threads
+ *     without ordering) race and give wrong results: order them on one
+ *     stream or synchronise between them. */
+int spk_bloom_insert_k256_noalloc(uint64_t* d_seen, uint64_t* d_solid, uint64_t num_words,
+                                  const uint64_t* d_keys4, size_t n, uint8_t* d_out_promoted,
+                                  void* cuda_stream);
+
 /* ---- counting (src/assemble.rs:129-292, src/graph.rs:78-102) ------------ */
 #define SPK_F_EDGES      0x1u  /* build the (k+1)-mer edge list */
 #define SPK_F_REF_SOLID  0x2u  /* also build the reference-semantics solid tier */

@@ -219,3 +219,109 @@ int bloom_download(spk_bloom* b, uint64_t* seen, uint64_t* solid) {
 }
 
 }  // namespace spk
+
+// ---------------------------------------------------------------------------
+// spk_bloom_insert_k256_noalloc: the batched insert above with its scratch in
+// a static device array instead of stream-ordered allocations, for callers
+// that cannot allocate device memory (their HBM is committed elsewhere, or an
+// allocation's implicit synchronisation would stall their other streams).
+//
+// Scratch layout for up to SPK_NOALLOC_MAX_KEYS keys (3 operations each):
+//   [map keys: kNaMapSlots u64][map values: kNaMapSlots u64]
+//   [positions: kNaOps u64][bits-before-the-batch flags: kNaOps u8]
+// The map needs a power of two of at least 2 * operations slots, so that
+// every probe sequence of k_api_first finds a free or matching slot.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr uint64_t kNaMaxKeys = SPK_NOALLOC_MAX_KEYS;
+constexpr uint64_t kNaOps = 3 * kNaMaxKeys;
+constexpr uint64_t kNaMapSlots = 524288;  // next power of two >= 2 * kNaOps
+static_assert(kNaMapSlots >= 2 * kNaOps && (kNaMapSlots & (kNaMapSlots - 1)) == 0,
+              "map must hold twice the operations");
+constexpr size_t kNaKeysOff = 0;
+constexpr size_t kNaValsOff = kNaKeysOff + kNaMapSlots * 8;
+constexpr size_t kNaPosOff = kNaValsOff + kNaMapSlots * 8;
+constexpr size_t kNaInitOff = kNaPosOff + kNaOps * 8;
+constexpr size_t kNaBytes = (kNaInitOff + kNaOps + 255) & ~(size_t)255;  // 9.7 MiB
+}  // namespace
+
+// One copy per device, reserved when the library's device code is loaded on
+// that device and held until the process exits.  Host code must not use this
+// name as a pointer (on the host it is only a stand-in for the symbol); it
+// passes the address from cudaGetSymbolAddress to the kernels instead.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+namespace {
+constexpr int kNaMaxDevices = 64;
+struct NaDevice {
+  unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
+  int sm_count = 0;
+  bool ready = false;
+};
+std::mutex g_na_mu;
+NaDevice g_na_dev[kNaMaxDevices];
+
+// Once per device, with that device current: the scratch array's device
+// address and the SM count used to size the grid.
+int noalloc_setup(int dev, NaDevice** out) {
+  std::lock_guard<std::mutex> l(g_na_mu);
+  NaDevice& d = g_na_dev[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return spk::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    if (!p) return spk::fail(SPK_E_CUDA, "cudaGetSymbolAddress returned a null scratch address");
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return spk::cuda_fail(e, "cudaDeviceGetAttribute(multiProcessorCount)");
+    d.scratch = static_cast<unsigned char*>(p);
+    d.sm_count = sms;
+    d.ready = true;
+  }
+  *out = &d;
+  return SPK_OK;
+}
+}  // namespace
+
+extern "C" int spk_bloom_insert_k256_noalloc(uint64_t* d_seen, uint64_t* d_solid, uint64_t num_words,
+                                             const uint64_t* d_keys4, size_t n,
+                                             uint8_t* d_out_promoted, void* cuda_stream) {
+  using namespace spk;
+  if (n > kNaMaxKeys)
+    return fail(SPK_E_INVALID_ARG, "spk_bloom_insert_k256_noalloc: n = " + std::to_string(n) +
+                                       " keys exceeds the maximum of " + std::to_string(kNaMaxKeys) +
+                                       " per call (SPK_NOALLOC_MAX_KEYS)");
+  if (!d_seen || !d_solid) return fail(SPK_E_INVALID_ARG, "null tier pointer");
+  if (num_words == 0) return fail(SPK_E_INVALID_ARG, "num_words must be at least 1");
+  if (num_words > (~0ULL >> 6)) return fail(SPK_E_INVALID_ARG, "num_words too large");
+  if (n && !d_keys4) return fail(SPK_E_INVALID_ARG, "null keys");
+  if (n == 0) return SPK_OK;
+  int dev = 0;
+  SPK_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNaMaxDevices) return fail(SPK_E_INVALID_ARG, "device ordinal above 63");
+  NaDevice* d = nullptr;
+  int rc = noalloc_setup(dev, &d);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  const uint64_t ops = 3 * (uint64_t)n;
+  uint64_t mcap = 1;
+  while (mcap < 2 * ops) mcap <<= 1;  // <= kNaMapSlots because n <= kNaMaxKeys
+  unsigned long long* mk = reinterpret_cast<unsigned long long*>(d->scratch + kNaKeysOff);
+  unsigned long long* mv = reinterpret_cast<unsigned long long*>(d->scratch + kNaValsOff);
+  uint64_t* pos = reinterpret_cast<uint64_t*>(d->scratch + kNaPosOff);
+  uint8_t* init = d->scratch + kNaInitOff;
+  // The previous call's map is still in the array: reset the part this call uses.
+  SPK_CUDA(cudaMemsetAsync(mk, 0xFF, mcap * 8, st));
+  SPK_CUDA(cudaMemsetAsync(mv, 0xFF, mcap * 8, st));
+  const FastMod fm = make_fastmod(num_words * 64);  // src/bloom.rs:27-28
+  BloomKeys K{d_keys4, (uint64_t)n, 1};
+  const unsigned grid = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>((n + kB - 1) / kB, (uint64_t)std::max(d->sm_count, 1) * 8));
+  k_api_first<<<grid, kB, 0, st>>>(K, fm, reinterpret_cast<const unsigned long long*>(d_seen), pos,
+                                   init, mk, mv, mcap - 1);
+  k_api_apply<<<grid, kB, 0, st>>>((uint64_t)n, pos, init, mk, mv, mcap - 1,
+                                   reinterpret_cast<unsigned long long*>(d_seen),
+                                   reinterpret_cast<unsigned long long*>(d_solid), d_out_promoted);
+  SPK_CUDA(cudaGetLastError());
+  return SPK_OK;
+}

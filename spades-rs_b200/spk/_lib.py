@@ -12,6 +12,7 @@ SPK_F_EDGES = 0x1
 SPK_F_REF_SOLID = 0x2
 SPK_F_KEEP_BLOOM = 0x4
 SPK_F_GATED = 0x8
+SPK_NOALLOC_MAX_KEYS = 65536
 
 STATUS = {
     0: "SPK_OK", 1: "SPK_E_INVALID_ARG", 2: "SPK_E_INVALID_K", 3: "SPK_E_OOM",
@@ -86,6 +87,7 @@ _SIGS = [
     ("spk_bloom_is_solid_u64", C.c_int, [vp, u64p, C.c_size_t, u8p]),
     ("spk_bloom_is_solid_k256", C.c_int, [vp, u64p, C.c_size_t, u8p]),
     ("spk_bloom_download", C.c_int, [vp, u64p, u64p]),
+    ("spk_bloom_insert_k256_noalloc", C.c_int, [vp, vp, C.c_uint64, vp, C.c_size_t, vp, vp]),
     ("spk_count_opts_default", None, [C.POINTER(CountOpts)]),
     ("spk_count", C.c_int, [vp, vp, C.c_size_t, vp, vp, C.c_size_t, u32p, C.c_int,
                             C.POINTER(CountOpts), C.POINTER(vp)]),
