@@ -271,7 +271,17 @@ def main():
     # roofline of the dominant kernel (largest share of the step)
     f_adm = info["admitted_occurrences"] / max(info["occurrences"], 1)
     sb = stream_bytes_per_occ()
-    if info["fused"]:
+    if info["schedule"] == 2 and count_ms >= bloom_ms:
+        # Count-first: the read stream and a read-modify-write of the table
+        # slot's sector (read + write back) per occurrence.
+        kname, kms = "k_count_all", count_ms
+        kbytes = occ * (sb + 2 * SECTOR)
+    elif info["schedule"] == 2:
+        # Bloom tiers from the table: a table scan plus three word-pair
+        # sector read-modify-writes per distinct k-mer.
+        kname, kms = "k_bloom_from_table", bloom_ms
+        kbytes = info["table_capacity"] * 32 + info["n_table"] * 3 * 2 * SECTOR
+    elif info["schedule"] == 1:
         # One pass: the read stream, three Bloom word-pair sectors and the
         # one-sector table slot of every occurrence.
         kname, kms = "k_fused_pass", bloom_ms

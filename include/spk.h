@@ -141,9 +141,16 @@ int spk_bloom_insert_k256_noalloc(uint64_t* d_seen, uint64_t* d_solid, uint64_t 
 #define SPK_F_KEEP_BLOOM 0x4u  /* keep the Bloom tiers for spk_result_bloom */
 #define SPK_F_GATED      0x8u  /* the reference's two-pass schedule: Stage 3 counts only
                                   occurrences admitted by the final Bloom.  Same result as
-                                  the default one-pass schedule (which counts every k-mer
-                                  and admits singletons afterwards) with a table that holds
+                                  the default one-pass schedules (which count every k-mer
+                                  and admit singletons afterwards) with a table that holds
                                   only admitted k-mers, for read sets too large for that */
+
+/* spk_result_info.schedule */
+#define SPK_SCHEDULE_GATED       0u  /* SPK_F_GATED: Bloom pass, then the gated count pass */
+#define SPK_SCHEDULE_FUSED       1u  /* SPK_F_REF_SOLID: one read pass with the per-occurrence
+                                        Bloom inserts the reference solid tier needs */
+#define SPK_SCHEDULE_COUNT_FIRST 2u  /* default: one read pass counting every k-mer; the Bloom
+                                        tiers are derived from the table afterwards */
 
 typedef struct spk_count_opts {
   uint64_t bloom_bits;    /* bits per tier; 0 = 512 Mi (src/assemble.rs:84) */
@@ -188,9 +195,10 @@ typedef struct spk_result_info {
   uint32_t table_regrows;
   uint32_t kernel_launches;      /* libspk kernels launched for this k */
   float ms_bloom, ms_count, ms_finish, ms_sort, ms_edges, ms_total; /* device time per phase */
-  float ms_bloom_kernel;         /* the Stage 2 kernels alone */
-  float ms_count_kernel;         /* the Stage 3 count kernel alone (last attempt) */
-  uint32_t fused;                /* 1: one-pass schedule, 0: gated two-pass schedule */
+  float ms_bloom_kernel;         /* the kernel that fills the Bloom tiers */
+  float ms_count_kernel;         /* the count kernel alone (last attempt; 0 for the fused
+                                    schedule, whose one kernel is ms_bloom_kernel) */
+  uint32_t schedule;             /* SPK_SCHEDULE_* */
   uint32_t reserved;
 } spk_result_info;
 

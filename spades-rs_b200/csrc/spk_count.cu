@@ -15,18 +15,24 @@
 // reference-semantics solid tier is still produced on request
 // (SPK_F_REF_SOLID).
 //
-// Two schedules compute that same admitted table:
-//   fused (default)  one pass over the reads: each canonical k-mer occurrence
-//                    sets its three Bloom bits and is counted in a table that
-//                    holds every distinct k-mer.  Afterwards each k-mer seen
-//                    once is kept only if its three twice bits are set (a
-//                    k-mer seen twice always has them).  One read pass and no
-//                    per-occurrence Bloom query.
-//   gated            (SPK_F_GATED) the reference's two passes: Stage 2 fills
-//                    the Bloom, Stage 3 counts only occurrences whose three
-//                    twice bits are set.  The table then holds only admitted
-//                    k-mers, which bounds memory on very large read sets.
-// Both are followed by the cutoff (src/assemble.rs:692-735), a compaction of
+// Three schedules compute that same admitted table:
+//   count-first  (default) one pass over the reads counts every canonical
+//                k-mer occurrence in a table that holds every distinct
+//                k-mer, with one hash and one table update per occurrence.
+//                The Bloom tiers are then derived from the table (a k-mer
+//                counted c times makes c insert operations on each of its
+//                three bits; the tiers do not depend on their order), and
+//                each k-mer seen once is kept only if its three twice bits
+//                are set (a k-mer seen twice always has them).
+//   fused        (SPK_F_REF_SOLID without SPK_F_GATED) the same single read
+//                pass with the three Bloom insert operations of every
+//                occurrence in it, which the reference-semantics solid tier
+//                needs because it depends on the order of the inserts.
+//   gated        (SPK_F_GATED) the reference's two passes: Stage 2 fills the
+//                Bloom, Stage 3 counts only occurrences whose three twice
+//                bits are set.  The table then holds only admitted k-mers,
+//                which bounds memory on very large read sets.
+// All are followed by the cutoff (src/assemble.rs:692-735), a compaction of
 // the table into the k-mer list, a radix sort and the edge list.
 #include <cuda_runtime.h>
 
@@ -354,6 +360,73 @@ __global__ void __launch_bounds__(kBlock) k_fused_pass(ReadsView R, unsigned k, 
   warp_add_u64(occ_out, occ);
 }
 
+// ---------------------------------------------------------------------------
+// Count-first schedule, pass 1: the count of every canonical k-mer occurrence
+// (src/assemble.rs:193-207 without the gate), with one hash (the table's home
+// slot) and one table update per occurrence and no Bloom work.  Both Bloom
+// tiers depend only on the distinct k-mers and their counts, so
+// k_bloom_from_table derives them from the finished table.
+// ---------------------------------------------------------------------------
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_count_all(ReadsView R, unsigned k, TableView t,
+                                                       unsigned long long* __restrict__ occ_out) {
+  uint64_t occ = 0;
+  auto fn = [&](bool active, uint64_t bitpos) {
+    Seq<NL> C;
+    uint64_t raw0 = 0;
+    SlotPeek peek{kEmpty, kEmpty};
+    if (active) {
+      occ++;
+      const Seq<NL> V = extract<NL>(R.words, bitpos, k);
+      C = canonical<NL>(V, k);
+      uint64_t w4[4];
+      kmer256_limbs<NL>(C, k, w4);
+      raw0 = hash_seed(hash_pre(w4), kSeed1);
+      if (NL <= 2) peek = table_peek<NL>(t, table_home(t, raw0));
+    }
+    warp_table_add<NL>(t, active, C, raw0, NL <= 2 ? &peek : nullptr);
+  };
+  foreach_position(R, k, fn);
+  warp_add_u64(occ_out, occ);
+}
+
+// Count-first schedule, pass 2: the Bloom tiers from the table.  An insert
+// operation sets its seen bit, and its twice bit when the seen bit was
+// already set (src/bloom.rs:95-97 plus the twice tier), so once every
+// occurrence is inserted seen[p] = "some operation hit p" and twice[p] = "at
+// least two operations hit p", whatever the order.  A k-mer counted c times
+// makes c operations on each of its three positions: for c >= 2 all three
+// twice bits are set outright, and a k-mer seen once makes its three
+// operations one after another (so a position it hits twice still gets its
+// twice bit).  The tiers equal those of inserting every occurrence.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_bloom_from_table(TableView t, unsigned k, FastMod fm,
+                                                              U128* __restrict__ tiers) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < t.capacity;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = *slot_count<NL>(t, s);
+    if (c == 0) continue;  // empty slot
+    Seq<NL> C;
+    const uint64_t* kp = slot_key<NL>(t, s);
+#pragma unroll
+    for (int j = 0; j < NL; j++) C.v[j] = kp[j];
+    uint64_t raw[3], pos[3];
+    bloom_positions<NL>(C, k, fm, raw, pos);
+    if (c == 1) {
+      bloom_insert3(tiers, pos);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const uint64_t w = pos[i] >> 6;
+        const unsigned long long bit = 1ULL << (pos[i] & 63);
+        const U128 cur = tiers[w];
+        if (!(cur.x & bit)) atomicOr(&tiers[w].x, bit);
+        if (!(cur.y & bit)) atomicOr(&tiers[w].y, bit);
+      }
+    }
+  }
+}
+
 // Gated schedule, Stage 2 alone.
 template <int NL, bool REF>
 __global__ void __launch_bounds__(kBlock) k_bloom_pass(ReadsView R, unsigned k, FastMod fm,
@@ -672,6 +745,16 @@ static void launch_fused(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uns
   else k_fused_pass<NL, false><<<g, kBlock, 0, st>>>(rv, k, fm, tiers, nullptr, t, occ);
 }
 template <int NL>
+static void launch_count_all(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
+                             const TableView& t, unsigned long long* occ) {
+  k_count_all<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(rv, k, t, occ);
+}
+template <int NL>
+static void launch_bloom_from_table(spk_ctx* ctx, cudaStream_t st, const TableView& t, unsigned k,
+                                    const FastMod& fm, U128* tiers) {
+  k_bloom_from_table<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(t, k, fm, tiers);
+}
+template <int NL>
 static void launch_bloom(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
                          const FastMod& fm, U128* tiers, unsigned long long* ref,
                          unsigned long long* occ) {
@@ -814,6 +897,9 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   rv.err = errp;
   const bool ref = (o.flags & SPK_F_REF_SOLID) != 0;
   const bool gated = (o.flags & SPK_F_GATED) != 0;
+  // The reference-semantics solid tier depends on the order of the inserts,
+  // so it needs the per-occurrence Bloom of the fused pass.
+  const bool count_first = !gated && !ref;
 
   Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1;
   uint32_t launches = 0;
@@ -851,16 +937,30 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
       if ((rc = alloc_table(ctx, kr, st, cap))) return rc;
       kr.table.err = errp;
       SPK_CUDA(cudaMemsetAsync(sw, 0, (S_ERR + 1) * 8, st));
-      SPK_CUDA(cudaEventRecord(kb0.e, st));
-      SPK_DISPATCH_NL(nl, launch_fused, ctx, st, rv, k, kr.fm, tiers, refp, kr.table, su + S_OCC);
-      SPK_CUDA(cudaGetLastError());
-      SPK_CUDA(cudaEventRecord(kb1.e, st));
+      if (count_first) {
+        SPK_CUDA(cudaEventRecord(kc0.e, st));
+        SPK_DISPATCH_NL(nl, launch_count_all, ctx, st, rv, k, kr.table, su + S_OCC);
+        SPK_CUDA(cudaGetLastError());
+        SPK_CUDA(cudaEventRecord(kc1.e, st));
+      } else {
+        SPK_CUDA(cudaEventRecord(kb0.e, st));
+        SPK_DISPATCH_NL(nl, launch_fused, ctx, st, rv, k, kr.fm, tiers, refp, kr.table, su + S_OCC);
+        SPK_CUDA(cudaGetLastError());
+        SPK_CUDA(cudaEventRecord(kb1.e, st));
+      }
       launches += 2;
       if ((rc = fetch(S_ERR + 1))) return rc;
       if (!((int)host[S_ERR] & 1)) break;
       if (attempt >= 24) return fail(SPK_E_TABLE_FULL, "count table overflow after regrow attempts");
       cap *= 2;
       info.table_regrows++;
+    }
+    if (count_first) {
+      SPK_CUDA(cudaEventRecord(kb0.e, st));
+      SPK_DISPATCH_NL(nl, launch_bloom_from_table, ctx, st, kr.table, k, kr.fm, tiers);
+      SPK_CUDA(cudaGetLastError());
+      SPK_CUDA(cudaEventRecord(kb1.e, st));
+      launches++;
     }
   } else {
     // ---- gated: Stage 2 first ----
@@ -1025,9 +1125,9 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   info.ms_edges = ms_between(e4, e5);
   info.ms_total = ms_between(e0, e6);
   info.ms_bloom_kernel = ms_between(kb0, kb1);
-  info.ms_count_kernel = gated ? ms_between(kc0, kc1) : 0.f;
+  info.ms_count_kernel = (gated || count_first) ? ms_between(kc0, kc1) : 0.f;
   info.kernel_launches = launches;
-  info.fused = gated ? 0 : 1;
+  info.schedule = gated ? SPK_SCHEDULE_GATED : count_first ? SPK_SCHEDULE_COUNT_FIRST : SPK_SCHEDULE_FUSED;
   return SPK_OK;
 }
 

@@ -13,6 +13,9 @@ SPK_F_REF_SOLID = 0x2
 SPK_F_KEEP_BLOOM = 0x4
 SPK_F_GATED = 0x8
 SPK_NOALLOC_MAX_KEYS = 65536
+SPK_SCHEDULE_GATED = 0
+SPK_SCHEDULE_FUSED = 1
+SPK_SCHEDULE_COUNT_FIRST = 2
 
 STATUS = {
     0: "SPK_OK", 1: "SPK_E_INVALID_ARG", 2: "SPK_E_INVALID_K", 3: "SPK_E_OOM",
@@ -51,7 +54,7 @@ class ResultInfo(C.Structure):
                 ("kernel_launches", C.c_uint32), ("ms_bloom", C.c_float), ("ms_count", C.c_float),
                 ("ms_finish", C.c_float), ("ms_sort", C.c_float), ("ms_edges", C.c_float),
                 ("ms_total", C.c_float), ("ms_bloom_kernel", C.c_float),
-                ("ms_count_kernel", C.c_float), ("fused", C.c_uint32),
+                ("ms_count_kernel", C.c_float), ("schedule", C.c_uint32),
                 ("reserved", C.c_uint32)]
 
     def as_dict(self):

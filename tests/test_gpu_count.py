@@ -39,8 +39,9 @@ def occ(lengths, k):
 
 def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
     """Full GPU result vs the C++ oracle (twice semantics for the table, reference
-    semantics for the count >= 2 list), for both schedules: the default
-    one-pass schedule (p, with the reference solid tier r) and the gated one."""
+    semantics for the count >= 2 list), for all three schedules: the default
+    count-first one (d), the fused pass that builds the reference solid tier
+    (r) and the gated one (p)."""
     tw = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE)
     tk, tc = tw.table(1)
     oseen, otwice = tw.bloom()
@@ -52,11 +53,20 @@ def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
     np.testing.assert_array_equal(ps, oseen)
     np.testing.assert_array_equal(pt, otwice)
     pinfo = p.info(0)
+    d = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=BASE, **kw)
+    dk, dc = d.kmers(0, 1)
+    np.testing.assert_array_equal(dk, tk)
+    np.testing.assert_array_equal(dc, tc)
+    ds, dt = d.bloom(0)
+    np.testing.assert_array_equal(ds, oseen)
+    np.testing.assert_array_equal(dt, otwice)
+    dinfo = d.info(0)
     r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=ALL, **kw)
     info = r.info(0)
     for key in ("occurrences", "admitted_occurrences", "n_table", "n_list", "n_solid", "n_edges",
                 "seen_popcount", "twice_popcount", "cutoff"):
         assert pinfo[key] == info[key], key
+        assert dinfo[key] == info[key], key
     ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_REF)
     gk, gc = r.kmers(0, 1)
     np.testing.assert_array_equal(gk, tk)
@@ -85,8 +95,10 @@ def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
         e = r.edges(0)
         np.testing.assert_array_equal(e, ora.edges(sk, k))
         np.testing.assert_array_equal(p.edges(0), e)
+        np.testing.assert_array_equal(d.edges(0), e)
     r.close()
     p.close()
+    d.close()
     return info
 
 
@@ -96,7 +108,7 @@ GOLDEN = ["counts_ecoli_1K_k21.npz", "counts_ecoli_1K_k31.npz", "counts_ecoli_1K
 
 
 @pytest.mark.parametrize("flags", [BASE, BASE | GATED, ALL, ALL | GATED],
-                         ids=["fused", "gated", "fused-ref", "gated-ref"])
+                         ids=["count-first", "gated", "fused-ref", "gated-ref"])
 @pytest.mark.parametrize("name", GOLDEN)
 def test_count_matches_golden(spk, name, flags):
     g = load_npz(name)
@@ -241,10 +253,14 @@ def test_solid_cutoff_and_seam(spk, ora):
     assert sk.shape[0] == int((rc >= cut).sum())
 
 
-def test_default_schedule_is_fused(spk):
+def test_schedules(spk):
+    """Count-first by default; the reference solid tier selects the fused pass
+    and SPK_F_GATED the two-pass schedule."""
     data, offs, lens = synth_small_packed()
-    assert spk.count((data, offs, lens), [55]).info(0)["fused"] == 1
-    assert spk.count((data, offs, lens), [55], flags=GATED).info(0)["fused"] == 0
+    assert spk.count((data, offs, lens), [55]).info(0)["schedule"] == 2
+    assert spk.count((data, offs, lens), [55], flags=ALL).info(0)["schedule"] == 1
+    assert spk.count((data, offs, lens), [55], flags=GATED).info(0)["schedule"] == 0
+    assert spk.count((data, offs, lens), [55], flags=ALL | GATED).info(0)["schedule"] == 0
 
 
 def test_fused_table_regrow(spk, ora):
