@@ -144,13 +144,19 @@ int spk_bloom_insert_k256_noalloc(uint64_t* d_seen, uint64_t* d_solid, uint64_t 
                                   the default one-pass schedules (which count every k-mer
                                   and admit singletons afterwards) with a table that holds
                                   only admitted k-mers, for read sets too large for that */
+#define SPK_F_DIRECT     0x10u /* count-first with one global-table atomic per occurrence
+                                  instead of the partitioned passes (k <= 64) */
 
 /* spk_result_info.schedule */
 #define SPK_SCHEDULE_GATED       0u  /* SPK_F_GATED: Bloom pass, then the gated count pass */
 #define SPK_SCHEDULE_FUSED       1u  /* SPK_F_REF_SOLID: one read pass with the per-occurrence
                                         Bloom inserts the reference solid tier needs */
-#define SPK_SCHEDULE_COUNT_FIRST 2u  /* default: one read pass counting every k-mer; the Bloom
+#define SPK_SCHEDULE_COUNT_FIRST 2u  /* one read pass counting every k-mer into the table with
+                                        global atomics (k > 64, or SPK_F_DIRECT); the Bloom
                                         tiers are derived from the table afterwards */
+#define SPK_SCHEDULE_PARTITIONED 3u  /* default for k <= 64: the read pass scatters keys by table
+                                        span, each span is counted in shared memory and written
+                                        once, with the Bloom tiers derived from its counts */
 
 typedef struct spk_count_opts {
   uint64_t bloom_bits;    /* bits per tier; 0 = 512 Mi (src/assemble.rs:84) */
@@ -197,9 +203,14 @@ typedef struct spk_result_info {
   float ms_bloom, ms_count, ms_finish, ms_sort, ms_edges, ms_total; /* device time per phase */
   float ms_bloom_kernel;         /* the kernel that fills the Bloom tiers */
   float ms_count_kernel;         /* the count kernel alone (last attempt; 0 for the fused
-                                    schedule, whose one kernel is ms_bloom_kernel) */
+                                    schedule, whose one kernel is ms_bloom_kernel; the span
+                                    count for the partitioned schedule) */
   uint32_t schedule;             /* SPK_SCHEDULE_* */
-  uint32_t reserved;
+  uint32_t part_rescatters;      /* partitioned: read passes repeated with exact region sizes */
+  uint64_t n_distinct;           /* distinct k-mers in the table before singleton admission
+                                    (n_table plus the rejected singletons) */
+  float ms_scatter_kernel;       /* partitioned: the read pass that scatters keys by span */
+  float reserved_f;
 } spk_result_info;
 
 int spk_result_count(const spk_result* res, int* n_k);
@@ -221,8 +232,11 @@ int spk_result_bloom(spk_result* res, int k_index, uint64_t* seen, uint64_t* twi
 
 /* Device-resident count table for a downstream graph build on the same
  * device (the input of CompactedGraph::build, src/graph.rs:65-69).  Open
- * addressing with linear probing from slot hash_kmer256(key, seed 1) >>
- * (64 - log2(capacity)) (src/bloom.rs:61-78, seed src/bloom.rs:84).  Slot s
+ * addressing with linear probing from slot h = hash_kmer256(key, seed 1) >>
+ * (64 - log2(capacity)) (src/bloom.rs:61-78, seed src/bloom.rs:84); the
+ * table is divided into spans of 2^log2span slots and the probe sequence
+ * wraps inside the span holding h: slot i of the sequence is
+ * (h & ~(span - 1)) | ((h + i) & (span - 1)).  Slot s
  * starts at slots + s * slot_bytes with key_limbs u64 key limbs, followed by
  * a u32 count at byte key_limbs * 8: 0 = empty, bit 31 set = a k-mer seen
  * once that the Bloom did not admit.  Valid until spk_result_free. */
@@ -233,6 +247,8 @@ typedef struct spk_table_view {
   uint32_t slot_bytes;
   uint32_t k;
   uint32_t cutoff;
+  uint32_t log2span;      /* probe sequences wrap inside spans of 2^log2span slots */
+  uint32_t reserved;
   /* Keys are stored as the 2k-bit sequence value (first base most
    * significant), little-endian limbs.  For k <= 64 that equals the Kmer256
    * limbs; for k > 64 the Kmer256 form is (value >> 2(k-64), value & mask). */

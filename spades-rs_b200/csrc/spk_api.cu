@@ -433,6 +433,8 @@ int spk_result_table_view(spk_result* res, int ki, spk_table_view* v) {
   v->slot_bytes = kr.table.slot_bytes;
   v->k = kr.k;
   v->cutoff = kr.info.cutoff;
+  v->log2span = kr.table.log2span;
+  v->reserved = 0;
   return SPK_OK;
 }
 int spk_result_free(spk_result* res) {

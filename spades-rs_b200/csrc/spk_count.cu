@@ -151,6 +151,131 @@ __device__ __forceinline__ void foreach_position(const ReadsView& R, unsigned k,
   }
 }
 
+// The same walk handing every lane U positions per call, f(active[U],
+// bitpos[U]), so that a lane can keep U independent memory operations in
+// flight.  Position u of a call is base + 32u + lane.
+template <int U, class F>
+__device__ __forceinline__ void foreach_position_n(const ReadsView& R, unsigned k, F& f) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t b = warp * 32; b < R.n_reads; b += nwarps * 32) {
+    const uint64_t r = b + lane;
+    uint32_t len = 0;
+    uint64_t off = 0;
+    if (r < R.n_reads) {
+      len = __ldg(R.lengths + r);
+      off = __ldg(R.offsets + r);
+      // get_read slices data[off .. off + ceil(len/4)] (src/packed_reads.rs:600-602)
+      if (off + ((uint64_t)len + 3) / 4 > R.data_len) {
+        atomicOr(R.err, 4);
+        len = 0;
+      }
+    }
+    const uint32_t np = len >= k ? len - k + 1 : 0;
+    uint32_t incl = np;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t t = __shfl_up_sync(FULL, incl, d);
+      if ((int)lane >= d) incl += t;
+    }
+    const uint32_t excl = incl - np;
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    for (uint32_t base = 0; base < total; base += 32 * U) {
+      bool active[U];
+      uint64_t bitpos[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const uint32_t p = base + 32 * u + lane;
+        unsigned j = 0;
+#pragma unroll
+        for (unsigned step = 16; step >= 1; step >>= 1) {
+          uint32_t c = __shfl_sync(FULL, incl, j + step - 1);
+          if (p >= c) j += step;
+        }
+        const uint64_t o = __shfl_sync(FULL, off, j);
+        const uint32_t e = __shfl_sync(FULL, excl, j);
+        active[u] = p < total;
+        bitpos[u] = 8ull * (R.byte_base + o) + 2ull * (uint64_t)(p - e);
+      }
+      f(active, bitpos);
+    }
+  }
+}
+
+// Rolling walk (k <= 64): one read per thread.  The first window of a read
+// is extracted, later windows roll in one base each (extend_right,
+// src/dna.rs:196-221) with the reverse complement rolled alongside, so a
+// position costs a few shifts instead of a full extract and reverse
+// complement.  f(active[U], canonical[U]) gets U consecutive windows of the
+// thread's read per call (all 32 lanes call f; inactive entries are junk).
+template <int NL, int U, class F>
+__device__ __forceinline__ void foreach_read_roll(const ReadsView& R, unsigned k, F& f) {
+  static_assert(NL <= 2, "rolling walk holds keys of up to 128 bits");
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t first = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const unsigned topsh = 2 * k - 2 - 64 * (NL - 1);  // bit of the first base in the top limb
+  const uint64_t topmask = (2 * k - 64 * (NL - 1)) >= 64 ? ~0ULL : ((1ULL << (2 * k - 64 * (NL - 1))) - 1);
+  // Warps walk 32 consecutive reads per round; a warp keeps going while any
+  // of its lanes has windows left, so f sees all 32 lanes.
+  for (uint64_t r0 = first - (threadIdx.x & 31); r0 < R.n_reads; r0 += nthreads) {
+    const uint64_t r = r0 + (threadIdx.x & 31);
+    uint32_t np = 0;
+    uint64_t bit0 = 0;
+    if (r < R.n_reads) {
+      const uint32_t len = __ldg(R.lengths + r);
+      const uint64_t off = __ldg(R.offsets + r);
+      if (off + ((uint64_t)len + 3) / 4 > R.data_len) {  // src/packed_reads.rs:600-602
+        atomicOr(R.err, 4);
+      } else if (len >= k) {
+        np = len - k + 1;
+        bit0 = 8ull * (R.byte_base + off);
+      }
+    }
+    Seq<NL> V, Rc;
+    if (np) {
+      V = extract<NL>(R.words, bit0, k);
+      Rc = revcomp<NL>(V, k);
+    }
+    uint64_t buf = 0, nextbit = bit0 + 2ull * k;
+    unsigned bleft = 0;
+    uint32_t i = 0;
+    for (;;) {
+      if (!__any_sync(FULL, i < np)) break;
+      bool act[U];
+      Seq<NL> C[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        act[u] = i < np;
+        if (act[u]) {
+          if (i > 0) {
+            if (bleft == 0) {
+              buf = extract<1>(R.words, nextbit, 32).v[0];
+              bleft = 32;
+            }
+            const uint64_t b = buf >> 62;
+            buf <<= 2;
+            bleft--;
+            nextbit += 2;
+            if (NL == 1) {
+              V.v[0] = ((V.v[0] << 2) | b) & topmask;
+              Rc.v[0] = (Rc.v[0] >> 2) | ((3 - b) << topsh);
+            } else {
+              V.v[NL - 1] = ((V.v[NL - 1] << 2) | (V.v[0] >> 62)) & topmask;
+              V.v[0] = (V.v[0] << 2) | b;
+              Rc.v[0] = (Rc.v[0] >> 2) | (Rc.v[NL - 1] << 62);
+              Rc.v[NL - 1] = (Rc.v[NL - 1] >> 2) | ((3 - b) << topsh);
+            }
+          }
+          C[u] = seq_le<NL>(V, Rc) ? V : Rc;  // canonical, src/dna.rs:185-192
+          i++;
+        }
+      }
+      f(act, C);
+    }
+  }
+}
+
 template <int NL>
 __device__ __forceinline__ void bloom_positions(const Seq<NL>& C, unsigned k, const FastMod& fm,
                                                 uint64_t raw[3], uint64_t pos[3]) {
@@ -198,6 +323,45 @@ __device__ __forceinline__ bool bloom_insert3(U128* __restrict__ tiers, const ui
   return allprev;
 }
 
+// The Bloom insert operations of U distinct k-mers with counts c[u] (0 =
+// none): a k-mer counted c >= 2 times sets its three seen and twice bits; a
+// k-mer seen once makes its three operations in order (as bloom_insert3).
+// All word pairs are loaded first and all fetch_or issued before their
+// results are used, so a thread keeps up to 3U operations in flight.
+template <int U>
+__device__ __forceinline__ void bloom_ops_distinct(U128* __restrict__ tiers, const uint64_t (&pos)[U][3],
+                                                   const uint32_t (&c)[U]) {
+  U128 t[U][3];
+#pragma unroll
+  for (int u = 0; u < U; u++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) t[u][i] = c[u] ? tiers[pos[u][i] >> 6] : U128{0, 0};
+  unsigned long long prev[U][3];
+#pragma unroll
+  for (int u = 0; u < U; u++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const uint64_t w = pos[u][i] >> 6;
+      const unsigned long long bit = 1ULL << (pos[u][i] & 63);
+      prev[u][i] = 0;
+      if (c[u] >= 2) {
+        if (!(t[u][i].x & bit)) atomicOr(&tiers[w].x, bit);
+        if (!(t[u][i].y & bit)) atomicOr(&tiers[w].y, bit);
+      } else if (c[u] == 1) {
+        // A set seen bit (even from a stale read) was set by an earlier operation.
+        prev[u][i] = (t[u][i].x & bit) ? bit : atomicOr(&tiers[w].x, bit);
+      }
+    }
+#pragma unroll
+  for (int u = 0; u < U; u++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const unsigned long long bit = 1ULL << (pos[u][i] & 63);
+      if (c[u] == 1 && (prev[u][i] & bit) && !(t[u][i].y & bit))
+        atomicOr(&tiers[pos[u][i] >> 6].y, bit);
+    }
+}
+
 __device__ __forceinline__ void ref_promote(unsigned long long* __restrict__ ref_solid,
                                             const uint64_t pos[3]) {  // src/bloom.rs:99-103
 #pragma unroll
@@ -213,6 +377,11 @@ __device__ __forceinline__ void ref_promote(unsigned long long* __restrict__ ref
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t table_home(const TableView& t, uint64_t raw0) {
   return raw0 >> (64 - t.log2cap);
+}
+// Slot i of the probe sequence from `home`: linear, wrapping inside the span.
+__device__ __forceinline__ uint64_t probe_slot(const TableView& t, uint64_t home, uint32_t i) {
+  const uint64_t m = (1ULL << t.log2span) - 1;
+  return (home & ~m) | ((home + i) & m);
 }
 
 // Adds n to key C.  Keys of <= 128 bits claim a slot with one 64- or 128-bit
@@ -238,9 +407,8 @@ __device__ __forceinline__ SlotPeek table_peek(const TableView& t, uint64_t home
 template <int NL>
 __device__ __forceinline__ void table_add(const TableView& t, const Seq<NL>& C, uint64_t home,
                                           uint32_t n, const SlotPeek* peek = nullptr) {
-  const uint64_t mask = t.capacity - 1;
   for (uint32_t i = 0; i < t.max_probe; i++) {
-    const uint64_t s = (home + i) & mask;
+    const uint64_t s = probe_slot(t, home, i);
     uint64_t* kp = slot_key<NL>(t, s);
     if (NL == 1) {
       unsigned long long cur = (i == 0 && peek) ? peek->x : __ldcg((const unsigned long long*)kp);
@@ -300,9 +468,8 @@ __device__ __forceinline__ void table_add(const TableView& t, const Seq<NL>& C, 
 // Read-only lookup after counting: the count (with the kRejected flag) or 0.
 template <int NL>
 __device__ __forceinline__ uint32_t table_find(const TableView& t, const Seq<NL>& C, uint64_t home) {
-  const uint64_t mask = t.capacity - 1;
   for (uint32_t i = 0; i < t.max_probe; i++) {
-    const uint64_t s = (home + i) & mask;
+    const uint64_t s = probe_slot(t, home, i);
     const uint32_t c = __ldg(slot_count<NL>(t, s));
     if (c == 0) return 0;  // empty slot ends the probe sequence
     const uint64_t* kp = slot_key<NL>(t, s);
@@ -427,6 +594,400 @@ __global__ void __launch_bounds__(kBlock) k_bloom_from_table(TableView t, unsign
   }
 }
 
+// ---------------------------------------------------------------------------
+// Partitioned count-first schedule (k <= 64).  The table's spans double as
+// partitions: a k-mer belongs to the span of its home slot (the top bits of
+// hash_kmer256(key, seed 1)).
+//   k_part_scatter  one read pass appends every canonical occurrence to the
+//                   region of its span (one relaxed counter per span; the
+//                   regions' write frontiers stay in L2, so DRAM sees whole
+//                   lines).
+//   k_part_count    one CTA per span counts the span's region in a shared-
+//                   memory copy of the span and writes the span to the table
+//                   (every slot, so the table needs no initialisation).  The
+//                   Bloom insert operations of its distinct k-mers (see
+//                   k_bloom_from_table) are binned by Bloom range: ranges of
+//                   2^19 bits, one u32 operation (bit offset in the range,
+//                   and whether the k-mer was seen twice) appended to the
+//                   range's region with one reservation per (span, range).
+//   k_bloom_apply   one CTA per Bloom range applies its operations to a
+//                   shared-memory copy of the range's seen and twice words
+//                   and writes both tiers out once.
+// The random read-modify-write of a table slot per occurrence becomes a
+// streamed write and read of the key, the table is written once, and every
+// random Bloom update happens in shared memory.
+// ---------------------------------------------------------------------------
+struct PartView {
+  uint64_t* keys;            // region entries, NL u64 limbs each
+  const uint64_t* base;      // region of span p = entries [base[p], base[p + 1])
+  unsigned int* fill;        // entries appended to span p: fill[p * kFillStride]
+  uint64_t uniform;          // > 0: every region holds `uniform` entries and base[p] =
+                             // p * uniform (no lookup); 0: use base[]
+  uint32_t log2parts;        // spans = 2^log2parts
+  uint32_t packed_home;      // 1: entries carry their home slot in the span in the top
+                             // kHomeBits bits of their top limb (keys leave them zero)
+  int* err;                  // bit 3: some region overflowed
+};
+constexpr uint32_t kHomeBits = 13;  // >= log2 of the largest span
+// Whether keys of k (NL limbs) leave the top kHomeBits bits of their top limb free.
+__host__ __device__ constexpr bool home_fits(unsigned k, int nl) {
+  return 2u * k - 64u * (nl - 1) <= 64u - kHomeBits;
+}
+// One fill counter per 32-byte sector, so that claims on different spans
+// never queue behind each other on one L2 line.
+constexpr uint32_t kFillStride = 8;
+
+constexpr int kPartBlock = 512;
+constexpr int kScatterBatch = 4;   // positions per lane in flight in k_part_scatter
+constexpr int kSpanBatch = 2;      // slots per thread in flight in k_part_count's write-out
+constexpr uint32_t kErrRegion = 8;
+
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_part_scatter(ReadsView R, unsigned k, PartView pv,
+                                                          unsigned long long* __restrict__ occ_out) {
+  constexpr int U = kScatterBatch;
+  uint64_t occ = 0;
+  auto fn = [&](const bool (&active)[U], const Seq<NL> (&Cin)[U]) {
+    Seq<NL> C[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) C[u] = Cin[u];
+    uint32_t p[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      p[u] = 0;
+      if (!active[u]) continue;
+      occ++;
+      uint64_t w4[4];
+      kmer256_limbs<NL>(C[u], k, w4);
+      const uint64_t raw0 = hash_seed(hash_pre(w4), kSeed1);
+      p[u] = pv.log2parts ? (uint32_t)(raw0 >> (64 - pv.log2parts)) : 0u;
+      if (pv.packed_home)  // the slot within the span, for k_part_count
+        C[u].v[NL - 1] |= (raw0 << pv.log2parts) >> (64 - kHomeBits) << (64 - kHomeBits);
+    }
+    // U independent claims in flight before any is used.
+    uint64_t i[U], e[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      i[u] = 0;
+      e[u] = 0;
+      if (!active[u]) continue;
+      const uint32_t got = atomicAdd(pv.fill + (uint64_t)p[u] * kFillStride, 1u);
+      if (pv.uniform) {
+        i[u] = (uint64_t)p[u] * pv.uniform + got;
+        e[u] = (uint64_t)(p[u] + 1) * pv.uniform;
+      } else {
+        i[u] = __ldg(pv.base + p[u]) + got;
+        e[u] = __ldg(pv.base + p[u] + 1);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (!active[u]) continue;
+      if (i[u] < e[u]) {
+        if (NL == 1) pv.keys[i[u]] = C[u].v[0];
+        else *(ulonglong2*)(pv.keys + 2 * i[u]) = make_ulonglong2(C[u].v[0], C[u].v[NL - 1]);
+      } else {
+        atomicOr(pv.err, (int)kErrRegion);
+      }
+    }
+  };
+  foreach_read_roll<NL, U>(R, k, fn);
+  warp_add_u64(occ_out, occ);
+}
+
+// Shared-memory slots of one span: keys (8 or 16 bytes) then u32 counts.
+template <int NL>
+struct SpanKey;
+template <>
+struct SpanKey<1> {
+  typedef unsigned long long T;
+};
+template <>
+struct SpanKey<2> {
+  typedef U128 T;
+};
+
+// Adds one occurrence of C to the shared-memory span; false if the span is
+// full.  Empty slots hold the all-ones key (never a canonical k-mer) and are
+// claimed with one 64- or 128-bit CAS, as in table_add.
+template <int NL>
+__device__ __forceinline__ bool span_add(typename SpanKey<NL>::T* keys, uint32_t* cnt, uint32_t mask,
+                                         const Seq<NL>& C, uint32_t home) {
+  for (uint32_t i = 0; i <= mask; i++) {
+    const uint32_t s = (home + i) & mask;
+    if (NL == 1) {
+      unsigned long long* kp = (unsigned long long*)&keys[s];
+      const unsigned long long cur = *(volatile unsigned long long*)kp;
+      if (cur == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
+      if (cur == kEmpty) {
+        const unsigned long long old = atomicCAS(kp, kEmpty, (unsigned long long)C.v[0]);
+        if (old == kEmpty || old == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
+      }
+    } else {
+      U128* kp = (U128*)&keys[s];
+      U128 cur;
+      cur.x = ((volatile unsigned long long*)kp)[0];
+      cur.y = ((volatile unsigned long long*)kp)[1];
+      if (cur.x != kEmpty && cur.y != kEmpty) {
+        // settled (a slot changes once, from empty to its key; a read that
+        // overlaps that change has an empty half and takes the CAS below)
+        if (cur.x == C.v[0] && cur.y == C.v[NL - 1]) { atomicAdd(cnt + s, 1u); return true; }
+        continue;
+      }
+      const U128 e{kEmpty, kEmpty}, mine{C.v[0], C.v[NL - 1]};
+      const U128 old = atomicCAS(kp, e, mine);
+      if ((old.x == kEmpty && old.y == kEmpty) || (old.x == mine.x && old.y == mine.y)) {
+        atomicAdd(cnt + s, 1u);
+        return true;
+      }
+    }
+  }
+  return false;
+}
+
+// Bloom operations binned by range (2^kLog2Range bits of both tiers).
+struct RangeView {
+  uint32_t* ops;             // op = (bit offset in the range << 1) | (k-mer count >= 2)
+  const uint64_t* base;      // range r holds ops [base[r], base[r + 1]) (when uniform == 0)
+  unsigned int* fill;        // ops appended to range r: fill[r * kFillStride]
+  uint64_t uniform;          // > 0: every range holds `uniform` ops, base[r] = r * uniform
+  uint32_t nranges;
+  int* err;                  // bit 4: some range overflowed
+};
+constexpr uint32_t kLog2Range = 19;        // 64 KiB of each tier per range
+constexpr uint32_t kMaxRanges = 4096;      // shared-memory bins of k_part_count
+constexpr uint32_t kErrRange = 16;
+
+__device__ __forceinline__ uint64_t range_base(const RangeView& rv, uint32_t r) {
+  return rv.uniform ? (uint64_t)r * rv.uniform : rv.base[r];
+}
+
+template <int NL, bool OPS>
+__global__ void __launch_bounds__(kPartBlock, 2) k_part_count(PartView pv, TableView t, unsigned k,
+                                                            FastMod fm, U128* __restrict__ tiers,
+                                                            RangeView rv) {
+  typedef typename SpanKey<NL>::T KeyT;
+  extern __shared__ __align__(16) unsigned char span_smem[];
+  const uint32_t S = 1u << t.log2span;
+  KeyT* keys = (KeyT*)span_smem;
+  uint32_t* cnt = (uint32_t*)(span_smem + (size_t)S * sizeof(KeyT));
+  // OPS: per-range op counts, then the next global op index of each range
+  uint32_t* rhist = cnt + S;
+  unsigned long long* rcur = (unsigned long long*)(rhist + ((rv.nranges + 1) & ~1u));
+  const uint32_t nparts = 1u << pv.log2parts;
+  for (uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
+    for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+      if (NL == 1) ((unsigned long long*)keys)[s] = kEmpty;
+      else ((U128*)keys)[s] = U128{kEmpty, kEmpty};
+      cnt[s] = 0;
+    }
+    if (OPS)
+      for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) rhist[r] = 0;
+    __syncthreads();
+    const uint64_t b = pv.base[p];
+    const uint64_t e = min(pv.base[p + 1], b + (uint64_t)pv.fill[(uint64_t)p * kFillStride]);
+    bool full = false;
+    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      Seq<NL> C;
+      if (NL == 1) {
+        C.v[0] = __ldcs(pv.keys + i);
+      } else {
+        const ulonglong2 v = __ldcs((const ulonglong2*)(pv.keys + 2 * i));
+        C.v[0] = v.x;
+        C.v[NL - 1] = v.y;
+      }
+      uint32_t home;
+      if (pv.packed_home) {
+        const uint64_t top = C.v[NL - 1];
+        home = (uint32_t)(top >> (64 - kHomeBits)) >> (kHomeBits - t.log2span);
+        C.v[NL - 1] = top & (~0ULL >> kHomeBits);
+      } else {
+        uint64_t w4[4];
+        kmer256_limbs<NL>(C, k, w4);
+        home = (uint32_t)(table_home(t, hash_seed(hash_pre(w4), kSeed1)) & (S - 1));
+      }
+      if (!span_add<NL>(keys, cnt, S - 1, C, home)) full = true;
+    }
+    if (full) atomicOr(t.err, 1);  // span full: the host regrows the table
+    __syncthreads();
+    const uint64_t g0 = (uint64_t)p << t.log2span;
+    if (OPS) {
+      // Write the span out and count its Bloom operations per range.
+      for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+        const uint32_t c = cnt[s];
+        Seq<NL> C;
+        if (NL == 1) {
+          C.v[0] = c ? ((unsigned long long*)keys)[s] : kEmpty;
+          ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
+          *gp = make_ulonglong2(C.v[0], (unsigned long long)c);
+        } else {
+          const U128 kv = c ? ((U128*)keys)[s] : U128{kEmpty, kEmpty};
+          C.v[0] = kv.x;
+          C.v[NL - 1] = kv.y;
+          ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
+          gp[0] = make_ulonglong2(kv.x, kv.y);
+          gp[1] = make_ulonglong2((unsigned long long)c, 0ULL);
+        }
+        if (!c) continue;
+        uint64_t raw[3], pos[3];
+        bloom_positions<NL>(C, k, fm, raw, pos);
+#pragma unroll
+        for (int j = 0; j < 3; j++) atomicAdd(rhist + (uint32_t)(pos[j] >> kLog2Range), 1u);
+      }
+      __syncthreads();
+      // One reservation per non-empty range.
+      for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) {
+        const uint32_t n = rhist[r];
+        rcur[r] = n ? range_base(rv, r) + atomicAdd(rv.fill + (uint64_t)r * kFillStride, n) : 0ULL;
+      }
+      __syncthreads();
+      // Emit the operations.
+      for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+        const uint32_t c = cnt[s];
+        if (!c) continue;
+        Seq<NL> C;
+        if (NL == 1) {
+          C.v[0] = ((unsigned long long*)keys)[s];
+        } else {
+          const U128 kv = ((U128*)keys)[s];
+          C.v[0] = kv.x;
+          C.v[NL - 1] = kv.y;
+        }
+        uint64_t raw[3], pos[3];
+        bloom_positions<NL>(C, k, fm, raw, pos);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          const uint32_t r = (uint32_t)(pos[j] >> kLog2Range);
+          const uint64_t i = atomicAdd(rcur + r, 1ULL);
+          const uint64_t end = rv.uniform ? (uint64_t)(r + 1) * rv.uniform : rv.base[r + 1];
+          if (i < end)
+            rv.ops[i] = ((uint32_t)(pos[j] & ((1u << kLog2Range) - 1)) << 1) | (c >= 2 ? 1u : 0u);
+          else
+            atomicOr(rv.err, (int)kErrRange);
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    constexpr int U = kSpanBatch;
+    for (uint32_t s0 = threadIdx.x; s0 < S; s0 += U * blockDim.x) {
+      uint32_t c[U];
+      uint64_t pos[U][3];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const uint32_t s = s0 + u * blockDim.x;
+        c[u] = 0;
+        pos[u][0] = pos[u][1] = pos[u][2] = 0;
+        if (s >= S) continue;
+        c[u] = cnt[s];
+        Seq<NL> C;
+        if (NL == 1) {
+          C.v[0] = c[u] ? ((unsigned long long*)keys)[s] : kEmpty;
+          ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
+          *gp = make_ulonglong2(C.v[0], (unsigned long long)c[u]);
+        } else {
+          const U128 kv = c[u] ? ((U128*)keys)[s] : U128{kEmpty, kEmpty};
+          C.v[0] = kv.x;
+          C.v[NL - 1] = kv.y;
+          ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
+          gp[0] = make_ulonglong2(kv.x, kv.y);
+          gp[1] = make_ulonglong2((unsigned long long)c[u], 0ULL);
+        }
+        if (c[u]) {
+          uint64_t raw[3];
+          bloom_positions<NL>(C, k, fm, raw, pos[u]);
+        }
+      }
+      // The Bloom operations of these k-mers (see k_bloom_from_table).
+      bloom_ops_distinct<U>(tiers, pos, c);
+    }
+    __syncthreads();
+  }
+}
+
+// Exact regions after an overflow: base[p] = sum of fill[0..p), base[P] = total.
+// One block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_part_bases(const unsigned int* __restrict__ fill,
+                                                     uint32_t n, uint64_t* __restrict__ base) {
+  __shared__ unsigned long long part[1024];
+  const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+  const uint32_t lo = min(n, threadIdx.x * per), hi = min(n, lo + per);
+  unsigned long long s = 0;
+  for (uint32_t i = lo; i < hi; i++) s += fill[(uint64_t)i * kFillStride];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (uint32_t j = 0; j < blockDim.x; j++) {
+      const unsigned long long v = part[j];
+      part[j] = run;
+      run += v;
+    }
+    base[n] = run;
+  }
+  __syncthreads();
+  unsigned long long run = part[threadIdx.x];
+  for (uint32_t i = lo; i < hi; i++) {
+    base[i] = run;
+    run += fill[(uint64_t)i * kFillStride];
+  }
+}
+
+// Uniform regions: base[p] = p * cap for p = 0..n.
+__global__ void k_part_uniform(uint32_t n, uint64_t cap, uint64_t* __restrict__ base) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    base[i] = i * cap;
+}
+
+// Applies the operations of each Bloom range in shared memory (one u32 word
+// per 32 bits of each tier) and writes the range's seen and twice words,
+// with their popcounts.  An operation of a k-mer seen twice sets both bits;
+// an operation of a k-mer seen once sets its seen bit and, if that bit was
+// already set, its twice bit -- the same tiers as applying every occurrence.
+constexpr int kApplyBlock = 1024;
+__global__ void __launch_bounds__(kApplyBlock) k_bloom_apply(RangeView rv, uint64_t num_words,
+                                                             uint64_t* __restrict__ seen,
+                                                             uint64_t* __restrict__ twice,
+                                                             unsigned long long* __restrict__ pops) {
+  extern __shared__ __align__(16) uint32_t range_smem[];
+  constexpr uint32_t W32 = (1u << kLog2Range) / 32;  // u32 words per tier and range
+  uint32_t* s_seen = range_smem;
+  uint32_t* s_twice = range_smem + W32;
+  uint64_t cs = 0, ct = 0;
+  for (uint32_t r = blockIdx.x; r < rv.nranges; r += gridDim.x) {
+    for (uint32_t i = threadIdx.x; i < 2 * W32; i += blockDim.x) range_smem[i] = 0;
+    __syncthreads();
+    const uint64_t b = range_base(rv, r);
+    const uint64_t end = rv.uniform ? (uint64_t)(r + 1) * rv.uniform : rv.base[r + 1];
+    const uint64_t e = min(end, b + (uint64_t)rv.fill[(uint64_t)r * kFillStride]);
+    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      const uint32_t op = __ldcs(rv.ops + i);
+      const uint32_t off = op >> 1;
+      const uint32_t w = off >> 5, bit = 1u << (off & 31);
+      if (op & 1) {
+        atomicOr(s_seen + w, bit);
+        atomicOr(s_twice + w, bit);
+      } else if (atomicOr(s_seen + w, bit) & bit) {
+        atomicOr(s_twice + w, bit);
+      }
+    }
+    __syncthreads();
+    const uint64_t g0 = (uint64_t)r * (W32 / 2);
+    for (uint32_t i = threadIdx.x; i < W32 / 2 && g0 + i < num_words; i += blockDim.x) {
+      const uint64_t sv = (uint64_t)s_seen[2 * i] | ((uint64_t)s_seen[2 * i + 1] << 32);
+      const uint64_t tv = (uint64_t)s_twice[2 * i] | ((uint64_t)s_twice[2 * i + 1] << 32);
+      seen[g0 + i] = sv;
+      twice[g0 + i] = tv;
+      cs += __popcll(sv);
+      ct += __popcll(tv);
+    }
+    __syncthreads();
+  }
+  warp_add_u64(pops + 0, cs);
+  warp_add_u64(pops + 1, ct);
+}
+
 // Gated schedule, Stage 2 alone.
 template <int NL, bool REF>
 __global__ void __launch_bounds__(kBlock) k_bloom_pass(ReadsView R, unsigned k, FastMod fm,
@@ -503,68 +1064,121 @@ __global__ void __launch_bounds__(kBlock) k_tier_finish(const U128* __restrict__
 // ---------------------------------------------------------------------------
 constexpr int kHistBins = 256;  // counts >= 255 share the last bin
 
+// A table slot: its count, and its key in C (keys of empty slots are junk).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_admit_compact(TableView t, unsigned k, FastMod fm,
+__device__ __forceinline__ uint32_t load_slot(const TableView& t, uint64_t s, Seq<NL>& C) {
+  if (NL == 1) {
+    const ulonglong2 v = __ldcs((const ulonglong2*)slot_key<NL>(t, s));
+    C.v[0] = v.x;
+    return (uint32_t)v.y;
+  }
+  if (NL == 2) {
+    const ulonglong2* q = (const ulonglong2*)slot_key<NL>(t, s);
+    const ulonglong2 a = __ldcs(q), b = __ldcs(q + 1);
+    C.v[0] = a.x;
+    C.v[NL - 1] = a.y;
+    return (uint32_t)b.x;
+  }
+  const uint32_t c = *slot_count<NL>(t, s);
+  const uint64_t* kp = slot_key<NL>(t, s);
+#pragma unroll
+  for (int j = 0; j < NL; j++) C.v[j] = c ? kp[j] : 0;
+  return c;
+}
+
+constexpr int kAdmitBatch = 2;  // slots per lane in flight
+
+template <int NL>
+__global__ void __launch_bounds__(kBlock, 4) k_admit_compact(TableView t, unsigned k, FastMod fm,
                                                           const uint64_t* __restrict__ twice,
                                                           int check_singletons, uint32_t lmin,
                                                           uint64_t* o0, uint64_t* o1, uint64_t* o2,
                                                           uint64_t* o3, uint32_t* __restrict__ ocnt,
                                                           uint64_t out_cap,
                                                           unsigned long long* __restrict__ hist,
-                                                          unsigned long long* __restrict__ sums) {
+                                                          unsigned long long* __restrict__ sums,
+                                                          unsigned long long* __restrict__ rejected) {
+  constexpr int U = kAdmitBatch;
+  constexpr int NW = kBlock / 32;
+  constexpr uint64_t CHUNK = (uint64_t)kBlock * U;
   __shared__ unsigned sh[kHistBins];
+  __shared__ unsigned wkeep[NW];
+  __shared__ unsigned long long cta_base;
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) sh[i] = 0;
   __syncthreads();
-  const unsigned lane = threadIdx.x & 31;
-  uint64_t n_adm = 0, n_one = 0, occ = 0;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t start = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  // Uniform trip count per warp so the ballot below sees every lane.
-  for (uint64_t base = start - lane; base < t.capacity; base += stride) {
-    const uint64_t s = base + lane;
-    uint32_t c = s < t.capacity ? *slot_count<NL>(t, s) : 0u;
-    if (c & kRejected) c = 0;
-    Seq<NL> C;
-    if (c) {
-      const uint64_t* kp = slot_key<NL>(t, s);
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t n_adm = 0, n_one = 0, occ = 0, n_rej = 0;
+  // A CTA scans CHUNK consecutive slots at a time (warp w: 32U of them) and
+  // reserves its list entries with one atomic per chunk.
+  for (uint64_t chunk0 = blockIdx.x * CHUNK; chunk0 < t.capacity; chunk0 += (uint64_t)gridDim.x * CHUNK) {
+    const uint64_t chunk = chunk0 + (uint64_t)warp * 32 * U;
+    uint32_t c[U];
+    Seq<NL> C[U];
 #pragma unroll
-      for (int j = 0; j < NL; j++) C.v[j] = kp[j];
+    for (int u = 0; u < U; u++) {
+      const uint64_t s = chunk + 32 * u + lane;
+      c[u] = s < t.capacity ? load_slot<NL>(t, s, C[u]) : 0u;
+      if (c[u] & kRejected) c[u] = 0;
     }
-    if (c == 1 && check_singletons) {
-      uint64_t raw[3], pos[3];
-      bloom_positions<NL>(C, k, fm, raw, pos);
-      const uint64_t a = __ldg(twice + (pos[0] >> 6));
-      const uint64_t b = __ldg(twice + (pos[1] >> 6));
-      const uint64_t d = __ldg(twice + (pos[2] >> 6));
-      if (!((a >> (pos[0] & 63)) & (b >> (pos[1] & 63)) & (d >> (pos[2] & 63)) & 1)) {
-        *slot_count<NL>(t, s) = 1u | kRejected;
-        c = 0;
+    // Singletons: the three twice bits of every slot in flight together.
+    uint64_t pos[U][3], tw[U][3];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (c[u] == 1 && check_singletons) {
+        uint64_t raw[3];
+        bloom_positions<NL>(C[u], k, fm, raw, pos[u]);
+#pragma unroll
+        for (int j = 0; j < 3; j++) tw[u][j] = __ldg(twice + (pos[u][j] >> 6));
       }
     }
-    if (c) {
-      n_adm++;
-      n_one += c == 1;
-      occ += c;
-      atomicAdd(&sh[c < kHistBins - 1 ? c : kHistBins - 1], 1u);
+    unsigned km[U];
+    unsigned nkeep = 0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (c[u] == 1 && check_singletons &&
+          !((tw[u][0] >> (pos[u][0] & 63)) & (tw[u][1] >> (pos[u][1] & 63)) &
+            (tw[u][2] >> (pos[u][2] & 63)) & 1)) {
+        *slot_count<NL>(t, chunk + 32 * u + lane) = 1u | kRejected;
+        c[u] = 0;
+        n_rej++;
+      }
+      if (c[u]) {
+        n_adm++;
+        n_one += c[u] == 1;
+        occ += c[u];
+        atomicAdd(&sh[c[u] < kHistBins - 1 ? c[u] : kHistBins - 1], 1u);
+      }
+      km[u] = __ballot_sync(FULL, c[u] != 0 && c[u] >= lmin);
+      nkeep += __popc(km[u]);
     }
-    const bool keep = c != 0 && c >= lmin;
-    const unsigned m = __ballot_sync(FULL, keep);
-    if (!m) continue;
-    unsigned long long pos0 = 0;
-    if (lane == (unsigned)(__ffs(m) - 1)) pos0 = atomicAdd(sums + 3, (unsigned long long)__popc(m));
-    pos0 = __shfl_sync(FULL, pos0, __ffs(m) - 1);
-    const uint64_t p = pos0 + __popc(m & lanemask_lt());
-    if (keep && p < out_cap) {
-      o0[p] = C.v[0];
-      if (NL > 1) o1[p] = C.v[NL > 1 ? 1 : 0];
-      if (NL > 2) o2[p] = C.v[NL > 2 ? 2 : 0];
-      if (NL > 3) o3[p] = C.v[NL > 3 ? 3 : 0];
-      ocnt[p] = c;
+    if (lane == 0) wkeep[warp] = nkeep;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tot = 0;
+      for (int w = 0; w < NW; w++) tot += wkeep[w];
+      cta_base = tot ? atomicAdd(sums + 3, (unsigned long long)tot) : 0ULL;
     }
+    __syncthreads();
+    uint64_t p0 = cta_base;
+    for (unsigned w = 0; w < warp; w++) p0 += wkeep[w];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint64_t p = p0 + __popc(km[u] & lanemask_lt());
+      if (((km[u] >> lane) & 1) && p < out_cap) {
+        o0[p] = C[u].v[0];
+        if (NL > 1) o1[p] = C[u].v[NL > 1 ? 1 : 0];
+        if (NL > 2) o2[p] = C[u].v[NL > 2 ? 2 : 0];
+        if (NL > 3) o3[p] = C[u].v[NL > 3 ? 3 : 0];
+        ocnt[p] = c[u];
+      }
+      p0 += __popc(km[u]);
+    }
+    __syncthreads();  // wkeep and cta_base are reused by the next chunk
   }
   warp_add_u64(sums + 0, n_adm);
   warp_add_u64(sums + 1, n_one);
   warp_add_u64(sums + 2, occ);
+  warp_add_u64(rejected, n_rej);
   __syncthreads();
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
     if (sh[i]) atomicAdd(hist + i, (unsigned long long)sh[i]);
@@ -649,12 +1263,71 @@ __device__ __forceinline__ Seq<NLE> widen_append(const Seq<NL>& X, unsigned b) {
   return R;
 }
 
-template <int NL, int NLE>
+// The solid k-mers (count >= cutoff) of a list as a set: open addressing with
+// linear probing over 2^log2cap slots of NL key limbs (k <= 64), all-ones =
+// empty (never a canonical k-mer: all-ones full limbs would be poly-T, whose
+// reverse complement poly-A is smaller, and a partial top limb never has its
+// unused bits set).  Home slot: hash_kmer256(key, seed 1) >> (64 - log2cap).
+// Probed 8 times per solid k-mer by k_edges, it is small enough to stay
+// mostly in L2, unlike the count table.
+struct SetView {
+  uint64_t* keys;
+  uint32_t log2cap;
+};
+
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_solid_set(const uint64_t* l0, const uint64_t* l1,
+                                                       const uint32_t* __restrict__ cnt, uint64_t n,
+                                                       const uint32_t* __restrict__ thr, unsigned k,
+                                                       SetView sv) {
+  const uint32_t cutoff = thr[0];
+  const uint64_t mask = (1ULL << sv.log2cap) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    if (cnt[i] < cutoff) continue;
+    Seq<NL> C;
+    C.v[0] = l0[i];
+    if (NL == 2) C.v[NL - 1] = l1[i];
+    uint64_t w4[4];
+    kmer256_limbs<NL>(C, k, w4);
+    uint64_t h = hash_seed(hash_pre(w4), kSeed1) >> (64 - sv.log2cap);
+    // keys are distinct and the set is at most 2/3 full, so a free slot is found
+    for (uint64_t probe = 0; probe <= mask; probe++, h = (h + 1) & mask) {
+      if (NL == 1) {
+        if (atomicCAS((unsigned long long*)sv.keys + h, kEmpty, (unsigned long long)C.v[0]) == kEmpty)
+          break;
+      } else {
+        const U128 old = atomicCAS((U128*)sv.keys + h, U128{kEmpty, kEmpty}, U128{C.v[0], C.v[NL - 1]});
+        if (old.x == kEmpty && old.y == kEmpty) break;
+      }
+    }
+  }
+}
+
+template <int NL>
+__device__ __forceinline__ bool set_has(const SetView& sv, const Seq<NL>& C, uint64_t raw0) {
+  const uint64_t mask = (1ULL << sv.log2cap) - 1;
+  uint64_t h = raw0 >> (64 - sv.log2cap);
+  for (uint64_t probe = 0; probe <= mask; probe++, h = (h + 1) & mask) {
+    if (NL == 1) {
+      const uint64_t v = __ldg(sv.keys + h);
+      if (v == C.v[0]) return true;
+      if (v == kEmpty) return false;
+    } else {
+      const ulonglong2 v = __ldg((const ulonglong2*)sv.keys + h);
+      if (v.x == C.v[0] && v.y == C.v[NL - 1]) return true;
+      if (v.x == kEmpty && v.y == kEmpty) return false;
+    }
+  }
+  return false;
+}
+
+template <int NL, int NLE, bool SET>
 __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint64_t* l1,
                                                    const uint64_t* l2, const uint64_t* l3,
                                                    const uint32_t* __restrict__ cnt, uint64_t n,
                                                    const uint32_t* __restrict__ thr, TableView t,
-                                                   unsigned k, uint64_t* e0, uint64_t* e1,
+                                                   SetView sv, unsigned k, uint64_t* e0, uint64_t* e1,
                                                    uint64_t* e2, uint64_t* e3, uint64_t out_cap,
                                                    unsigned long long* __restrict__ counter) {
   const uint32_t cutoff = thr[0];
@@ -672,6 +1345,7 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
       if (NL > 3) S.v[NL > 3 ? 3 : 0] = l3[i];
       solid = cnt[i] >= cutoff;
     }
+    uint32_t emits = 0;  // bit 4o + b: the edge of orientation o and base b
     for (int o = 0; o < 2; o++) {
       Seq<NL> EX = S;
       bool ok = solid;
@@ -681,31 +1355,55 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
       }
       for (unsigned b = 0; b < 4; b++) {
         bool emit = false;
-        Seq<NLE> E;
         if (ok) {
           const Seq<NL> NB = shl_append<NL>(EX, b, k);
           const Seq<NL> CN = canonical<NL>(NB, k);
           uint64_t w4[4];
           kmer256_limbs<NL>(CN, k, w4);
           const HashPre hp = hash_pre(w4);
-          const uint32_t c = table_find<NL>(t, CN, table_home(t, hash_seed(hp, kSeed1)));
-          if (c && !(c & kRejected) && c >= cutoff) {
-            E = widen_append<NL, NLE>(EX, b);
+          const uint64_t raw0 = hash_seed(hp, kSeed1);
+          bool solid_nb;
+          if (SET) {
+            solid_nb = set_has<NL>(sv, CN, raw0);
+          } else {
+            const uint32_t c = table_find<NL>(t, CN, table_home(t, raw0));
+            solid_nb = c && !(c & kRejected) && c >= cutoff;
+          }
+          if (solid_nb) {
+            const Seq<NLE> E = widen_append<NL, NLE>(EX, b);
             emit = seq_le<NLE>(E, revcomp<NLE>(E, k + 1));
           }
         }
-        const unsigned m = __ballot_sync(FULL, emit);
-        if (!m) continue;
-        unsigned long long p0 = 0;
-        if (lane == (unsigned)(__ffs(m) - 1)) p0 = atomicAdd(counter, (unsigned long long)__popc(m));
-        p0 = __shfl_sync(FULL, p0, __ffs(m) - 1);
-        const uint64_t p = p0 + __popc(m & lanemask_lt());
-        if (emit && p < out_cap) {
+        if (emit) emits |= 1u << (4 * o + b);
+      }
+    }
+    // One reservation per warp for all its edges, then write them (the
+    // edge (k+1)-mer is rebuilt from the oriented k-mer and the base).
+    const uint32_t ne = __popc(emits);
+    uint32_t incl = ne;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(FULL, incl, d);
+      if ((int)lane >= d) incl += v;
+    }
+    const uint32_t wtot = __shfl_sync(FULL, incl, 31);
+    if (!wtot) continue;
+    unsigned long long wb = 0;
+    if (lane == 0) wb = atomicAdd(counter, (unsigned long long)wtot);
+    uint64_t p = __shfl_sync(FULL, wb, 0) + incl - ne;
+    for (int o = 0; o < 2; o++) {
+      if (!(emits >> (4 * o) & 15u)) continue;
+      const Seq<NL> EX = o ? revcomp<NL>(S, k) : S;
+      for (unsigned b = 0; b < 4; b++) {
+        if (!(emits >> (4 * o + b) & 1u)) continue;
+        const Seq<NLE> E = widen_append<NL, NLE>(EX, b);
+        if (p < out_cap) {
           e0[p] = E.v[0];
           if (NLE > 1) e1[p] = E.v[NLE > 1 ? 1 : 0];
           if (NLE > 2) e2[p] = E.v[NLE > 2 ? 2 : 0];
           if (NLE > 3) e3[p] = E.v[NLE > 3 ? 3 : 0];
         }
+        p++;
       }
     }
   }
@@ -755,6 +1453,43 @@ static void launch_bloom_from_table(spk_ctx* ctx, cudaStream_t st, const TableVi
   k_bloom_from_table<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(t, k, fm, tiers);
 }
 template <int NL>
+static void launch_part_scatter(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
+                                const PartView& pv, unsigned long long* occ) {
+  k_part_scatter<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(rv, k, pv, occ);
+}
+// rv.ops == nullptr: apply the Bloom operations to the interleaved tiers
+// directly; else bin them by range into rv.
+template <int NL>
+static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, const TableView& t,
+                             unsigned k, const FastMod& fm, U128* tiers, const RangeView& rv) {
+  size_t smem = ((size_t)1 << t.log2span) * (sizeof(typename SpanKey<NL>::T) + 4);
+  const uint64_t nparts = 1ULL << pv.log2parts;
+  const int grid = (int)std::min<uint64_t>(nparts, (uint64_t)ctx->sm_count * 2);
+  if (rv.ops) {
+    smem += ((rv.nranges + 1) & ~1u) * 4 + (size_t)rv.nranges * 8;
+    SPK_CUDA(cudaFuncSetAttribute(k_part_count<NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    k_part_count<NL, true><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv);
+  } else {
+    SPK_CUDA(cudaFuncSetAttribute(k_part_count<NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    k_part_count<NL, false><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv);
+  }
+  return SPK_OK;
+}
+static int launch_bloom_apply(spk_ctx* ctx, cudaStream_t st, const RangeView& rv, uint64_t num_words,
+                              uint64_t* seen, uint64_t* twice, unsigned long long* pops) {
+  const size_t smem = (size_t)2 * ((1u << kLog2Range) / 32) * 4;
+  SPK_CUDA(cudaFuncSetAttribute(k_bloom_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = (int)std::min<uint64_t>(rv.nranges, (uint64_t)ctx->sm_count);
+  k_bloom_apply<<<grid, kApplyBlock, smem, st>>>(rv, num_words, seen, twice, pops);
+  return SPK_OK;
+}
+// Spans of the partitioned schedule: 8192 slots of 12 bytes (k <= 32) or
+// 4096 of 20 bytes (k <= 64) in shared memory, two CTAs per SM.
+constexpr uint32_t kPartLog2Span1 = 13, kPartLog2Span2 = 12;
+
+template <int NL>
 static void launch_bloom(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
                          const FastMod& fm, U128* tiers, unsigned long long* ref,
                          unsigned long long* occ) {
@@ -775,27 +1510,36 @@ template <int NL>
 static void launch_admit(spk_ctx* ctx, cudaStream_t st, const TableView& t, unsigned k,
                          const FastMod& fm, const uint64_t* twice, int check, uint32_t lmin,
                          uint64_t** o, uint32_t* oc, uint64_t out_cap, unsigned long long* hist,
-                         unsigned long long* sums) {
+                         unsigned long long* sums, unsigned long long* rejected) {
   k_admit_compact<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(t, k, fm, twice, check, lmin, o[0], o[1],
-                                                          o[2], o[3], oc, out_cap, hist, sums);
+                                                          o[2], o[3], oc, out_cap, hist, sums,
+                                                          rejected);
 }
 template <int NL, int NLE>
 static void launch_edges_t(spk_ctx* ctx, cudaStream_t st, uint64_t* l[4], const uint32_t* cnt,
-                           uint64_t n, const uint32_t* thr, const TableView& t, unsigned k,
-                           uint64_t* e[4], uint64_t out_cap, unsigned long long* counter) {
-  k_edges<NL, NLE><<<grid_for(ctx, 8), kBlock, 0, st>>>(l[0], l[1], l[2], l[3], cnt, n, thr, t, k,
-                                                       e[0], e[1], e[2], e[3], out_cap, counter);
+                           uint64_t n, const uint32_t* thr, const TableView& t, const SetView* sv,
+                           unsigned k, uint64_t* e[4], uint64_t out_cap,
+                           unsigned long long* counter) {
+  if (sv && NL <= 2)
+    k_edges<NL, NLE, true><<<grid_for(ctx, 8), kBlock, 0, st>>>(
+        l[0], l[1], l[2], l[3], cnt, n, thr, t, *sv, k, e[0], e[1], e[2], e[3], out_cap, counter);
+  else
+    k_edges<NL, NLE, false><<<grid_for(ctx, 8), kBlock, 0, st>>>(
+        l[0], l[1], l[2], l[3], cnt, n, thr, t, SetView{nullptr, 0}, k, e[0], e[1], e[2], e[3],
+        out_cap, counter);
 }
+// sv: the solid set (k <= 64), or nullptr to probe the count table.
 static void launch_edges(spk_ctx* ctx, cudaStream_t st, int nl, int nle, uint64_t* l[4],
                          const uint32_t* cnt, uint64_t n, const uint32_t* thr, const TableView& t,
-                         unsigned k, uint64_t* e[4], uint64_t out_cap, unsigned long long* counter) {
-  if (nl == 1 && nle == 1) launch_edges_t<1, 1>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
-  else if (nl == 1) launch_edges_t<1, 2>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
-  else if (nl == 2 && nle == 2) launch_edges_t<2, 2>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
-  else if (nl == 2) launch_edges_t<2, 3>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
-  else if (nl == 3 && nle == 3) launch_edges_t<3, 3>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
-  else if (nl == 3) launch_edges_t<3, 4>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
-  else launch_edges_t<4, 4>(ctx, st, l, cnt, n, thr, t, k, e, out_cap, counter);
+                         const SetView* sv, unsigned k, uint64_t* e[4], uint64_t out_cap,
+                         unsigned long long* counter) {
+  if (nl == 1 && nle == 1) launch_edges_t<1, 1>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
+  else if (nl == 1) launch_edges_t<1, 2>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
+  else if (nl == 2 && nle == 2) launch_edges_t<2, 2>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
+  else if (nl == 2) launch_edges_t<2, 3>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
+  else if (nl == 3 && nle == 3) launch_edges_t<3, 3>(ctx, st, l, cnt, n, thr, t, nullptr, k, e, out_cap, counter);
+  else if (nl == 3) launch_edges_t<3, 4>(ctx, st, l, cnt, n, thr, t, nullptr, k, e, out_cap, counter);
+  else launch_edges_t<4, 4>(ctx, st, l, cnt, n, thr, t, nullptr, k, e, out_cap, counter);
 }
 
 static uint64_t next_pow2(uint64_t x) {
@@ -843,19 +1587,26 @@ static float ms_between(const Ev& a, const Ev& b) {
   return ms;
 }
 
-static int alloc_table(spk_ctx* ctx, KResult& kr, cudaStream_t st, uint64_t cap) {
+// A table of cap slots (a power of two) probed within spans of 2^log2span
+// slots (0: the whole table).  init = false leaves the slots unwritten for a
+// pass that writes every slot itself.
+static int alloc_table(spk_ctx* ctx, KResult& kr, cudaStream_t st, uint64_t cap,
+                       uint32_t log2span = 0, bool init = true) {
   const uint32_t sb = slot_bytes(kr.nl);
   int rc;
   if ((rc = kr.tslots.alloc(cap * sb, st))) return rc;
-  SPK_DISPATCH_NL(kr.nl, launch_init, ctx, st, kr.tslots.as<uint8_t>(), cap);
-  SPK_CUDA(cudaGetLastError());
+  if (init) {
+    SPK_DISPATCH_NL(kr.nl, launch_init, ctx, st, kr.tslots.as<uint8_t>(), cap);
+    SPK_CUDA(cudaGetLastError());
+  }
   TableView& t = kr.table;
   t.slots = kr.tslots.as<uint8_t>();
   t.capacity = cap;
   t.log2cap = 0;
   while ((1ULL << t.log2cap) < cap) t.log2cap++;
+  t.log2span = (log2span && log2span < t.log2cap) ? log2span : t.log2cap;
   t.slot_bytes = sb;
-  t.max_probe = (uint32_t)std::min<uint64_t>(kMaxProbe, cap);
+  t.max_probe = (uint32_t)std::min<uint64_t>(kMaxProbe, 1ULL << t.log2span);
   return SPK_OK;
 }
 
@@ -868,6 +1619,7 @@ enum {
   S_CNT = 9,             /* solid */
   S_EDGES = 10,
   S_OCC0 = 11,           /* occurrences before the pass */
+  S_REJ = 12,            /* singletons the twice tier rejected */
   S_HIST = 16,           /* 256 words */
   S_WORDS = 16 + kHistBins
 };
@@ -900,17 +1652,21 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   // The reference-semantics solid tier depends on the order of the inserts,
   // so it needs the per-occurrence Bloom of the fused pass.
   const bool count_first = !gated && !ref;
+  bool partitioned = count_first && nl <= 2 && !(o.flags & SPK_F_DIRECT);
 
-  Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1;
+  Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1;
   uint32_t launches = 0;
   SPK_CUDA(cudaEventRecord(e0.e, st));
 
-  // Bloom tiers as interleaved (seen, twice) word pairs.
-  if ((rc = kr.tiers.alloc(kr.num_words * 16, st))) return rc;
+  // Bloom tiers as interleaved (seen, twice) word pairs, for the schedules
+  // that update them in place (allocated on first use).
   if (ref && (rc = kr.ref_solid.alloc(kr.num_words * 8, st))) return rc;
-  U128* tiers = kr.tiers.as<U128>();
+  U128* tiers = nullptr;
   unsigned long long* refp = ref ? kr.ref_solid.as<unsigned long long>() : nullptr;
   auto reset_tiers = [&]() -> int {
+    int r2;
+    if (!kr.tiers.p && (r2 = kr.tiers.alloc(kr.num_words * 16, st))) return r2;
+    tiers = kr.tiers.as<U128>();
     SPK_CUDA(cudaMemsetAsync(kr.tiers.p, 0, kr.num_words * 16, st));
     if (ref) SPK_CUDA(cudaMemsetAsync(kr.ref_solid.p, 0, kr.num_words * 8, st));
     return SPK_OK;
@@ -925,14 +1681,123 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   };
 
   uint64_t cap = 0;
+  // Partitioned schedule: Bloom operations binned by range when the ranges'
+  // bins fit in shared memory (else applied in place, as k_bloom_from_table).
+  const uint64_t nranges = (size_bits + (1ULL << kLog2Range) - 1) >> kLog2Range;
+  const bool use_ops = nranges <= kMaxRanges;
+  DevBuf rbase, rfill, ops;
+  RangeView bv{nullptr, nullptr, nullptr, 0, (uint32_t)nranges, errp};
   if (!gated) {
     // ---- fused: Bloom and the count of every k-mer in one pass ----
     k_occ<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv.lengths, rv.n_reads, k, su + S_OCC0);
     SPK_CUDA(cudaGetLastError());
     launches++;
     if ((rc = fetch(S_OCC0 + 1))) return rc;
-    cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(host[S_OCC0]);
-    for (int attempt = 0;; attempt++) {
+    const uint64_t occ0 = host[S_OCC0];
+    cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(occ0);
+    if (partitioned) {
+      // Regions hold 1.5x the mean share of occurrences per span: keep them
+      // within a quarter of the device memory, else count with global atomics.
+      size_t fr = 0, tot = 0;
+      SPK_CUDA(cudaMemGetInfo(&fr, &tot));
+      partitioned = (occ0 + (occ0 >> 1) + (1u << 20)) * (uint64_t)nl * 8 <= tot / 4;
+    }
+    for (int attempt = 0; partitioned; attempt++) {
+      if (!use_ops && (rc = reset_tiers())) return rc;
+      if ((rc = alloc_table(ctx, kr, st, cap, nl == 1 ? kPartLog2Span1 : kPartLog2Span2, false)))
+        return rc;
+      TableView& t = kr.table;
+      t.err = errp;
+      SPK_CUDA(cudaMemsetAsync(sw, 0, (S_ERR + 1) * 8, st));
+      const uint32_t log2parts = t.log2cap - t.log2span;
+      const uint64_t nparts = 1ULL << log2parts;
+      DevBuf base, fill, region;
+      if ((rc = base.alloc((nparts + 1) * 8, st)) || (rc = fill.alloc(nparts * 4 * kFillStride, st)))
+        return rc;
+      const uint64_t per = occ0 / nparts;
+      const uint64_t capu = per + (per >> 1) + 256;
+      if ((rc = region.alloc(nparts * capu * nl * 8, st))) return rc;
+      k_part_uniform<<<64, kBlock, 0, st>>>((uint32_t)nparts, capu, base.as<uint64_t>());
+      SPK_CUDA(cudaMemsetAsync(fill.p, 0, nparts * 4 * kFillStride, st));
+      PartView pv{region.as<uint64_t>(), base.as<uint64_t>(), fill.as<unsigned int>(), capu, log2parts,
+                  home_fits(k, nl) ? 1u : 0u, errp};
+      SPK_CUDA(cudaEventRecord(ks0.e, st));
+      if (nl == 1) launch_part_scatter<1>(ctx, st, rv, k, pv, su + S_OCC);
+      else launch_part_scatter<2>(ctx, st, rv, k, pv, su + S_OCC);
+      SPK_CUDA(cudaGetLastError());
+      launches += 2;  // k_part_uniform, k_part_scatter
+      if ((rc = fetch(S_ERR + 1))) return rc;
+      if ((int)host[S_ERR] & kErrRegion) {
+        // Skewed spans: the fill counters are the exact sizes.  Lay the
+        // regions out by them and scatter again (this cannot overflow).
+        k_part_bases<<<1, 1024, 0, st>>>(fill.as<unsigned int>(), (uint32_t)nparts, base.as<uint64_t>());
+        SPK_CUDA(cudaMemcpyAsync(host + S_WORDS, base.as<uint64_t>() + nparts, 8,
+                                 cudaMemcpyDeviceToHost, st));
+        SPK_CUDA(cudaStreamSynchronize(st));
+        if ((rc = region.alloc(std::max<uint64_t>(host[S_WORDS], 1) * nl * 8, st))) return rc;
+        pv.keys = region.as<uint64_t>();
+        pv.uniform = 0;
+        SPK_CUDA(cudaMemsetAsync(fill.p, 0, nparts * 4 * kFillStride, st));
+        SPK_CUDA(cudaMemsetAsync(sw, 0, (S_ERR + 1) * 8, st));
+        if (nl == 1) launch_part_scatter<1>(ctx, st, rv, k, pv, su + S_OCC);
+        else launch_part_scatter<2>(ctx, st, rv, k, pv, su + S_OCC);
+        SPK_CUDA(cudaGetLastError());
+        launches += 2;  // k_part_bases, k_part_scatter
+        info.part_rescatters++;
+      }
+      SPK_CUDA(cudaEventRecord(ks1.e, st));
+      if (use_ops) {
+        // At most three operations per table slot; each range gets 1.25x its
+        // share of that bound (Bloom positions are uniform over the ranges).
+        const uint64_t share = 3 * cap / nranges + 1;
+        const uint64_t rcap = share + (share >> 2) + 1024;
+        if ((rc = rbase.alloc((nranges + 1) * 8, st)) ||
+            (rc = rfill.alloc(nranges * 4 * kFillStride, st)) || (rc = ops.alloc(nranges * rcap * 4, st)))
+          return rc;
+        SPK_CUDA(cudaMemsetAsync(rfill.p, 0, nranges * 4 * kFillStride, st));
+        bv = RangeView{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), rcap,
+                       (uint32_t)nranges, errp};
+      }
+      SPK_CUDA(cudaEventRecord(kc0.e, st));
+      if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, tiers, bv);
+      else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, tiers, bv);
+      if (rc) return rc;
+      SPK_CUDA(cudaGetLastError());
+      SPK_CUDA(cudaEventRecord(kc1.e, st));
+      launches++;
+      if ((rc = fetch(S_ERR + 1))) return rc;
+      if ((int)host[S_ERR] & kErrRegion) return fail(SPK_E_CUDA, "partition region overflow after resizing");
+      if ((int)host[S_ERR] & 1) {
+        if (attempt >= 24) return fail(SPK_E_TABLE_FULL, "count table overflow after regrow attempts");
+        cap *= 2;
+        info.table_regrows++;
+        continue;
+      }
+      if (use_ops && ((int)host[S_ERR] & kErrRange)) {
+        // A range outgrew its share: lay the ranges out by their exact
+        // counts and count the spans again (the table comes out the same).
+        k_part_bases<<<1, 1024, 0, st>>>(rfill.as<unsigned int>(), (uint32_t)nranges,
+                                         rbase.as<uint64_t>());
+        SPK_CUDA(cudaMemcpyAsync(host + S_WORDS, rbase.as<uint64_t>() + nranges, 8,
+                                 cudaMemcpyDeviceToHost, st));
+        SPK_CUDA(cudaStreamSynchronize(st));
+        if ((rc = ops.alloc(std::max<uint64_t>(host[S_WORDS], 1) * 4, st))) return rc;
+        SPK_CUDA(cudaMemsetAsync(rfill.p, 0, nranges * 4 * kFillStride, st));
+        SPK_CUDA(cudaMemsetAsync(errp, 0, 4, st));
+        bv = RangeView{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), 0,
+                       (uint32_t)nranges, errp};
+        if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, tiers, bv);
+        else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, tiers, bv);
+        if (rc) return rc;
+        SPK_CUDA(cudaGetLastError());
+        launches += 2;  // k_part_bases, k_part_count
+        info.part_rescatters++;
+        if ((rc = fetch(S_ERR + 1))) return rc;
+        if ((int)host[S_ERR] & (kErrRange | 1)) return fail(SPK_E_CUDA, "Bloom range overflow after resizing");
+      }
+      break;
+    }
+    for (int attempt = 0; !partitioned; attempt++) {
       if ((rc = reset_tiers())) return rc;
       if ((rc = alloc_table(ctx, kr, st, cap))) return rc;
       kr.table.err = errp;
@@ -955,7 +1820,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
       cap *= 2;
       info.table_regrows++;
     }
-    if (count_first) {
+    if (count_first && !partitioned) {
       SPK_CUDA(cudaEventRecord(kb0.e, st));
       SPK_DISPATCH_NL(nl, launch_bloom_from_table, ctx, st, kr.table, k, kr.fm, tiers);
       SPK_CUDA(cudaGetLastError());
@@ -971,14 +1836,26 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     SPK_CUDA(cudaEventRecord(kb1.e, st));
     launches++;
   }
-  // compact tiers (both schedules)
+  // the compact tiers (every schedule)
   if ((rc = kr.seen.alloc(kr.num_words * 8, st))) return rc;
   if ((rc = kr.twice.alloc(kr.num_words * 8, st))) return rc;
-  k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.seen.as<uint64_t>(),
-                                                    kr.twice.as<uint64_t>(), su + S_POPS);
-  SPK_CUDA(cudaGetLastError());
-  launches++;
-  kr.tiers.release();
+  if (bv.ops) {
+    // partitioned: apply the binned operations range by range
+    SPK_CUDA(cudaEventRecord(kb0.e, st));
+    if ((rc = launch_bloom_apply(ctx, st, bv, kr.num_words, kr.seen.as<uint64_t>(),
+                                 kr.twice.as<uint64_t>(), su + S_POPS)))
+      return rc;
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaEventRecord(kb1.e, st));
+    launches++;
+    ops.release();
+  } else {
+    k_tier_finish<<<grid_for(ctx, 4), kBlock, 0, st>>>(tiers, kr.num_words, kr.seen.as<uint64_t>(),
+                                                      kr.twice.as<uint64_t>(), su + S_POPS);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    kr.tiers.release();
+  }
   SPK_CUDA(cudaEventRecord(e1.e, st));
   if ((rc = fetch(S_POPS + 2))) return rc;
   info.occurrences = host[S_OCC];
@@ -1041,10 +1918,11 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     }
     if ((rc = kr.list[4].alloc(std::max<uint64_t>(lcap, 1) * 4, st))) return rc;
     SPK_CUDA(cudaMemsetAsync(sw + S_SUMS, 0, 4 * 8, st));
+    SPK_CUDA(cudaMemsetAsync(sw + S_REJ, 0, 8, st));
     SPK_CUDA(cudaMemsetAsync(sw + S_HIST, 0, kHistBins * 8, st));
     SPK_DISPATCH_NL(nl, launch_admit, ctx, st, kr.table, k, kr.fm, kr.twice.as<uint64_t>(),
                     gated ? 0 : 1, lmin_pre, lp, kr.list[4].as<uint32_t>(), lcap, su + S_HIST,
-                    su + S_SUMS);
+                    su + S_SUMS, su + S_REJ);
     SPK_CUDA(cudaGetLastError());
     launches++;
     if ((rc = fetch(S_SUMS + 4))) return rc;
@@ -1064,6 +1942,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   kr.list_min = hthr[1];
   info.n_table = host[S_SUMS + 0];
   info.n_singletons = host[S_SUMS + 1];
+  info.n_distinct = host[S_SUMS + 0] + host[S_REJ];
   info.admitted_occurrences = host[S_SUMS + 2];
   kr.list_len = host[S_SUMS + 3];
   auto hist_from = [&](uint32_t c0) {
@@ -1088,7 +1967,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   SPK_CUDA(cudaEventRecord(e3.e, st));
 
   // ---- sort ----
-  if ((rc = radix_sort_bufs(st, nl, kr.list_len, 2 * k, kr.list, &kr.list[4], &launches))) return rc;
+  if ((rc = sort_bufs(st, nl, kr.list_len, 2 * k, kr.list, &kr.list[4], host, &launches))) return rc;
   for (int j = 0; j < nl; j++) lp[j] = kr.list[j].as<uint64_t>();
   SPK_CUDA(cudaEventRecord(e4.e, st));
 
@@ -1101,14 +1980,33 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
       if ((rc = kr.edges[j].alloc(ecap * 8, st))) return rc;
       ep[j] = kr.edges[j].as<uint64_t>();
     }
-    launch_edges(ctx, st, nl, kr.nle, lp, kr.list[4].as<uint32_t>(), kr.list_len, thr, kr.table, k,
-                 ep, ecap, su + S_EDGES);
+    // For k <= 64 the neighbours are looked up in a set of the solid k-mers
+    // (at most 2/3 full), built from the list; wider keys probe the table.
+    DevBuf set;
+    SetView sv{nullptr, 0};
+    if (nl <= 2) {
+      uint32_t lg = 10;
+      while ((1ULL << lg) < info.n_solid + (info.n_solid >> 1) + 1) lg++;
+      if ((rc = set.alloc((1ULL << lg) * nl * 8, st))) return rc;
+      SPK_CUDA(cudaMemsetAsync(set.p, 0xFF, (1ULL << lg) * nl * 8, st));
+      sv = SetView{set.as<uint64_t>(), lg};
+      if (nl == 1)
+        k_solid_set<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[0], kr.list[4].as<uint32_t>(),
+                                                           kr.list_len, thr, k, sv);
+      else
+        k_solid_set<2><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[1], kr.list[4].as<uint32_t>(),
+                                                           kr.list_len, thr, k, sv);
+      SPK_CUDA(cudaGetLastError());
+      launches++;
+    }
+    launch_edges(ctx, st, nl, kr.nle, lp, kr.list[4].as<uint32_t>(), kr.list_len, thr, kr.table,
+                 nl <= 2 ? &sv : nullptr, k, ep, ecap, su + S_EDGES);
     SPK_CUDA(cudaGetLastError());
     launches++;
     if ((rc = fetch(S_EDGES + 1))) return rc;
     info.n_edges = host[S_EDGES];
     if (info.n_edges > ecap) return fail(SPK_E_CUDA, "edge list larger than its bound");
-    if ((rc = radix_sort_bufs(st, kr.nle, info.n_edges, 2 * (k + 1), kr.edges, nullptr, &launches)))
+    if ((rc = sort_bufs(st, kr.nle, info.n_edges, 2 * (k + 1), kr.edges, nullptr, host, &launches)))
       return rc;
   }
   SPK_CUDA(cudaEventRecord(e5.e, st));
@@ -1126,8 +2024,12 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   info.ms_total = ms_between(e0, e6);
   info.ms_bloom_kernel = ms_between(kb0, kb1);
   info.ms_count_kernel = (gated || count_first) ? ms_between(kc0, kc1) : 0.f;
+  info.ms_scatter_kernel = partitioned ? ms_between(ks0, ks1) : 0.f;
   info.kernel_launches = launches;
-  info.schedule = gated ? SPK_SCHEDULE_GATED : count_first ? SPK_SCHEDULE_COUNT_FIRST : SPK_SCHEDULE_FUSED;
+  info.schedule = gated         ? SPK_SCHEDULE_GATED
+                  : partitioned ? SPK_SCHEDULE_PARTITIONED
+                  : count_first ? SPK_SCHEDULE_COUNT_FIRST
+                                : SPK_SCHEDULE_FUSED;
   return SPK_OK;
 }
 

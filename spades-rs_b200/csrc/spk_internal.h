@@ -71,14 +71,16 @@ struct ReadsView {
 // ---- count table --------------------------------------------------------------
 // Open addressing, linear probing; one slot of slot_bytes per entry: key limbs
 // (sequence value V) first, then the u32 count (and a u32 state word for keys
-// wider than 128 bits).  Count 0 marks an empty slot after counting.
+// wider than 128 bits).  Count 0 marks an empty slot after counting.  The
+// table is divided into spans of 2^log2span slots and a probe sequence wraps
+// inside the span of its home slot (log2span == log2cap: the whole table).
 struct TableView {
   uint8_t* slots;
   uint64_t capacity;  // power of two
   uint32_t log2cap;
   uint32_t slot_bytes;
   uint32_t max_probe;
-  uint32_t pad;
+  uint32_t log2span;
   int* err;           // device error word (bit 0: probe limit, bit 1: wait timeout)
 };
 
@@ -166,6 +168,12 @@ int download_bloom(spk_result* res, int ki, uint64_t* seen, uint64_t* twice, uin
 // key.  The buffers may be swapped with temporaries.
 int radix_sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
                     DevBuf* vals, uint32_t* launches = nullptr);
+// The same result with an MSD split into 65536 buckets by the top 16 bits and
+// a shared-memory sort per bucket (large lists; falls back to the radix sort
+// for short lists and for buckets too large for shared memory).  h_staging:
+// a pinned host staging block (kStagingBytes).
+int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys, DevBuf* vals,
+              uint64_t* h_staging, uint32_t* launches = nullptr);
 // Exclusive scan of u32 in place (spk_sort.cu).
 int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches = nullptr);
 // Ordered compaction of a sorted SoA list into AoS Kmer256 limbs; *m is the

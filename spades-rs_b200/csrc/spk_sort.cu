@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <utility>
+#include <vector>
 
 #include "spk_internal.h"
 
@@ -266,6 +267,229 @@ int radix_sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf*
   if (passes & 1) {  // sorted data sits in the temporaries: hand them over
     for (int j = 0; j < nl; j++) std::swap(keys[j], tk[j]);
     if (vals) std::swap(*vals, tv);
+  }
+  return SPK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Bucket sort: an MSD split on the top 16 significant bits of the key into
+// 65536 buckets, then a bitonic sort of each bucket in shared memory.  The
+// top bits of canonical k-mers and (k+1)-mers spread their lists over the
+// buckets, so a bucket holds ~n/65536 items; a bucket larger than BS_LOCAL
+// items is sorted by the LSD radix sort above instead.  Equal keys do not
+// occur (the lists hold distinct k-mers), so stability is not needed.
+// ---------------------------------------------------------------------------
+constexpr uint32_t BS_BITS = 16;
+constexpr uint32_t BS_NB = 1u << BS_BITS;
+constexpr uint32_t BS_LOCAL = 2048;
+constexpr int BS_BLOCK = 256;
+constexpr uint32_t BS_MAX_BIG = 4096;
+constexpr uint64_t BS_STAGE_WORDS = 1024;  // big-bucket list offset in the host staging block
+
+struct Limbs {
+  uint64_t* p[4];
+};
+
+template <int NL>
+__device__ __forceinline__ uint32_t bs_digit(const Limbs& L, uint64_t i, unsigned limb, unsigned sh) {
+  uint64_t lo = 0, hi = 0;
+#pragma unroll
+  for (int j = 0; j < NL; j++) {
+    if ((unsigned)j == limb) lo = L.p[j][i];
+    if ((unsigned)j == limb + 1) hi = L.p[j][i];
+  }
+  return (uint32_t)(((lo >> sh) | ((hi << 1) << (63 - sh))) & (BS_NB - 1));
+}
+
+template <int NL>
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(Limbs L, uint64_t n, unsigned limb, unsigned sh,
+                                                       uint32_t* __restrict__ hist) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(hist + bs_digit<NL>(L, i, limb, sh), 1u);
+}
+
+template <int NL, bool HASV>
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_scatter(Limbs S, const uint32_t* __restrict__ sv, Limbs D,
+                                                          uint32_t* __restrict__ dv, uint64_t n,
+                                                          unsigned limb, unsigned sh,
+                                                          uint32_t* __restrict__ cur) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = atomicAdd(cur + bs_digit<NL>(S, i, limb, sh), 1u);
+#pragma unroll
+    for (int j = 0; j < NL; j++) D.p[j][p] = S.p[j][i];
+    if (HASV) dv[p] = sv[i];
+  }
+}
+
+// Sorts every bucket of at most BS_LOCAL items from T into D; larger buckets
+// are listed in big[3i..3i+2] = (bucket, offset, size) for the host.
+template <int NL, bool HASV>
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* __restrict__ tv, Limbs D,
+                                                        uint32_t* __restrict__ dv,
+                                                        const uint32_t* __restrict__ off,
+                                                        const uint32_t* __restrict__ size,
+                                                        uint32_t* __restrict__ big,
+                                                        unsigned* __restrict__ nbig) {
+  extern __shared__ __align__(16) uint64_t bs_smem[];
+  uint64_t* sk = bs_smem;                              // NL arrays of BS_LOCAL limbs
+  uint32_t* svl = (uint32_t*)(bs_smem + NL * BS_LOCAL);  // values
+  for (uint32_t b = blockIdx.x; b < BS_NB; b += gridDim.x) {
+    const uint32_t m = size[b];
+    if (m == 0) continue;
+    const uint32_t o = off[b];
+    if (m > BS_LOCAL) {
+      if (threadIdx.x == 0) {
+        const unsigned q = atomicAdd(nbig, 1u);
+        if (q < BS_MAX_BIG) {
+          big[3 * q] = b;
+          big[3 * q + 1] = o;
+          big[3 * q + 2] = m;
+        }
+      }
+      continue;
+    }
+    uint32_t P = 1;
+    while (P < m) P <<= 1;
+    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+      const bool in = i < m;
+#pragma unroll
+      for (int j = 0; j < NL; j++) sk[j * BS_LOCAL + i] = in ? T.p[j][o + i] : ~0ULL;
+      if (HASV) svl[i] = in ? tv[o + i] : 0u;
+    }
+    __syncthreads();
+    for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+      for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+          const uint32_t x = i ^ j;
+          if (x <= i) continue;
+          // a > b on the limbs, most significant first
+          bool gt = false, eq = true;
+#pragma unroll
+          for (int q = NL - 1; q >= 0; q--) {
+            const uint64_t u = sk[q * BS_LOCAL + i], v = sk[q * BS_LOCAL + x];
+            if (eq && u != v) {
+              gt = u > v;
+              eq = false;
+            }
+          }
+          const bool up = (i & kk) == 0;
+          if (gt == up && !eq) {
+#pragma unroll
+            for (int q = 0; q < NL; q++) {
+              const uint64_t t = sk[q * BS_LOCAL + i];
+              sk[q * BS_LOCAL + i] = sk[q * BS_LOCAL + x];
+              sk[q * BS_LOCAL + x] = t;
+            }
+            if (HASV) {
+              const uint32_t t = svl[i];
+              svl[i] = svl[x];
+              svl[x] = t;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+#pragma unroll
+      for (int j = 0; j < NL; j++) D.p[j][o + i] = sk[j * BS_LOCAL + i];
+      if (HASV) dv[o + i] = svl[i];
+    }
+    __syncthreads();
+  }
+}
+
+template <int NL, bool HASV>
+static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* tv, uint64_t n,
+                     unsigned limb, unsigned sh, uint32_t* hist, uint32_t* off, uint32_t* cur,
+                     uint32_t* big, unsigned* nbig, uint32_t* launches) {
+  const unsigned g = (unsigned)std::min<uint64_t>((n + BS_BLOCK - 1) / BS_BLOCK, 148 * 16);
+  k_bs_hist<NL><<<g, BS_BLOCK, 0, st>>>(K, n, limb, sh, hist);
+  SPK_CUDA(cudaMemcpyAsync(off, hist, BS_NB * 4, cudaMemcpyDeviceToDevice, st));
+  DevBuf sums;
+  int rc;
+  if ((rc = scan_u32(st, off, BS_NB, sums, launches))) return rc;
+  SPK_CUDA(cudaMemcpyAsync(cur, off, BS_NB * 4, cudaMemcpyDeviceToDevice, st));
+  k_bs_scatter<NL, HASV><<<g, BS_BLOCK, 0, st>>>(K, v, T, tv, n, limb, sh, cur);
+  const size_t smem = BS_LOCAL * (NL * 8 + (HASV ? 4 : 0));
+  SPK_CUDA(cudaFuncSetAttribute(k_bs_local<NL, HASV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+  k_bs_local<NL, HASV><<<148 * 4, BS_BLOCK, smem, st>>>(T, tv, K, v, off, hist, big, nbig);
+  SPK_CUDA(cudaGetLastError());
+  if (launches) *launches += 3;
+  return SPK_OK;
+}
+
+int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys, DevBuf* vals,
+              uint64_t* h_staging, uint32_t* launches) {
+  if (n < (1u << 18) || nbits < BS_BITS + 8 || !h_staging)
+    return radix_sort_bufs(st, nl, n, nbits, keys, vals, launches);
+  if (n >= (1ULL << 32)) return fail(SPK_E_INVALID_ARG, "sort: more than 2^32 items");
+  int rc;
+  DevBuf tk[4], tv, hist, off, cur, big;
+  Limbs K{}, T{};
+  for (int j = 0; j < nl; j++) {
+    if ((rc = tk[j].alloc(n * 8, st))) return rc;
+    K.p[j] = keys[j].as<uint64_t>();
+    T.p[j] = tk[j].as<uint64_t>();
+  }
+  if (vals && (rc = tv.alloc(n * 4, st))) return rc;
+  if ((rc = hist.alloc(BS_NB * 4, st)) || (rc = off.alloc(BS_NB * 4, st)) ||
+      (rc = cur.alloc(BS_NB * 4, st)) || (rc = big.alloc((3 * BS_MAX_BIG + 1) * 4, st)))
+    return rc;
+  SPK_CUDA(cudaMemsetAsync(hist.p, 0, BS_NB * 4, st));
+  unsigned* nbig = (unsigned*)(big.as<uint32_t>() + 3 * BS_MAX_BIG);
+  SPK_CUDA(cudaMemsetAsync(nbig, 0, 4, st));
+  const unsigned hi_bit = nbits - BS_BITS, limb = hi_bit / 64, sh = hi_bit % 64;
+  uint32_t* v = vals ? vals->as<uint32_t>() : nullptr;
+  uint32_t* tvp = vals ? tv.as<uint32_t>() : nullptr;
+  uint32_t* H = hist.as<uint32_t>();
+  uint32_t* O = off.as<uint32_t>();
+  uint32_t* Cu = cur.as<uint32_t>();
+  uint32_t* B = big.as<uint32_t>();
+  switch (nl * 2 + (vals ? 1 : 0)) {
+    case 2: rc = bs_launch<1, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    case 3: rc = bs_launch<1, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    case 4: rc = bs_launch<2, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    case 5: rc = bs_launch<2, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    case 6: rc = bs_launch<3, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    case 7: rc = bs_launch<3, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    case 8: rc = bs_launch<4, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    default: rc = bs_launch<4, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+  }
+  if (rc) return rc;
+  uint64_t* hs = h_staging + BS_STAGE_WORDS;
+  SPK_CUDA(cudaMemcpyAsync(hs, nbig, 4, cudaMemcpyDeviceToHost, st));
+  SPK_CUDA(cudaStreamSynchronize(st));
+  const unsigned nb = ((unsigned*)hs)[0];
+  if (nb > BS_MAX_BIG) {
+    // Too many large buckets: sort the bucketed copy as a whole instead.
+    for (int j = 0; j < nl; j++)
+      SPK_CUDA(cudaMemcpyAsync(K.p[j], T.p[j], n * 8, cudaMemcpyDeviceToDevice, st));
+    if (vals) SPK_CUDA(cudaMemcpyAsync(v, tvp, n * 4, cudaMemcpyDeviceToDevice, st));
+    return radix_sort_bufs(st, nl, n, nbits, keys, vals, launches);
+  }
+  if (nb == 0) return SPK_OK;
+  SPK_CUDA(cudaMemcpyAsync(hs, B, (size_t)nb * 12, cudaMemcpyDeviceToHost, st));
+  SPK_CUDA(cudaStreamSynchronize(st));
+  std::vector<uint32_t> bl((const uint32_t*)hs, (const uint32_t*)hs + 3 * nb);
+  for (unsigned q = 0; q < nb; q++) {
+    const uint64_t o = bl[3 * q + 1], m = bl[3 * q + 2];
+    DevBuf bk[4], bvv;
+    for (int j = 0; j < nl; j++) {
+      if ((rc = bk[j].alloc(m * 8, st))) return rc;
+      SPK_CUDA(cudaMemcpyAsync(bk[j].p, T.p[j] + o, m * 8, cudaMemcpyDeviceToDevice, st));
+    }
+    if (vals) {
+      if ((rc = bvv.alloc(m * 4, st))) return rc;
+      SPK_CUDA(cudaMemcpyAsync(bvv.p, tvp + o, m * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    if ((rc = radix_sort_bufs(st, nl, m, hi_bit, bk, vals ? &bvv : nullptr, launches))) return rc;
+    for (int j = 0; j < nl; j++)
+      SPK_CUDA(cudaMemcpyAsync(K.p[j] + o, bk[j].p, m * 8, cudaMemcpyDeviceToDevice, st));
+    if (vals) SPK_CUDA(cudaMemcpyAsync(v + o, bvv.p, m * 4, cudaMemcpyDeviceToDevice, st));
   }
   return SPK_OK;
 }

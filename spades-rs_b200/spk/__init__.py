@@ -16,14 +16,17 @@ There is no CPU fallback: importing works anywhere, but every call that
 needs the GPU raises :class:`SpkError` when ``libspk.so`` or the device is
 missing.
 """
-from ._lib import (SPK_F_GATED, SPK_F_EDGES, SPK_F_KEEP_BLOOM, SPK_F_REF_SOLID, SpkError, lib,
-                   lib_path, validate_k)
+from ._lib import (SPK_F_DIRECT, SPK_F_EDGES, SPK_F_GATED, SPK_F_KEEP_BLOOM, SPK_F_REF_SOLID,
+                   SPK_SCHEDULE_COUNT_FIRST, SPK_SCHEDULE_FUSED, SPK_SCHEDULE_GATED,
+                   SPK_SCHEDULE_PARTITIONED, SpkError, lib, lib_path, validate_k)
 from .api import (Context, CountResult, Job, PackedReads, Server, TwoTierFilter, count,
                   count_batch, count_device, count_solid_kmers, default_context, kmer256_from_limbs,
                   limbs_from_kmer256, nlimbs)
 
 __all__ = [
-    "SPK_F_GATED", "SPK_F_EDGES", "SPK_F_KEEP_BLOOM", "SPK_F_REF_SOLID", "SpkError", "lib", "lib_path",
+    "SPK_F_DIRECT", "SPK_F_EDGES", "SPK_F_GATED", "SPK_F_KEEP_BLOOM", "SPK_F_REF_SOLID",
+    "SPK_SCHEDULE_COUNT_FIRST", "SPK_SCHEDULE_FUSED", "SPK_SCHEDULE_GATED", "SPK_SCHEDULE_PARTITIONED",
+    "SpkError", "lib", "lib_path",
     "validate_k", "Context", "CountResult", "Job", "PackedReads", "Server", "TwoTierFilter",
     "count", "count_batch", "count_device", "count_solid_kmers", "default_context",
     "kmer256_from_limbs", "limbs_from_kmer256", "nlimbs",

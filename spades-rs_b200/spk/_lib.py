@@ -12,10 +12,12 @@ SPK_F_EDGES = 0x1
 SPK_F_REF_SOLID = 0x2
 SPK_F_KEEP_BLOOM = 0x4
 SPK_F_GATED = 0x8
+SPK_F_DIRECT = 0x10
 SPK_NOALLOC_MAX_KEYS = 65536
 SPK_SCHEDULE_GATED = 0
 SPK_SCHEDULE_FUSED = 1
 SPK_SCHEDULE_COUNT_FIRST = 2
+SPK_SCHEDULE_PARTITIONED = 3
 
 STATUS = {
     0: "SPK_OK", 1: "SPK_E_INVALID_ARG", 2: "SPK_E_INVALID_K", 3: "SPK_E_OOM",
@@ -55,7 +57,8 @@ class ResultInfo(C.Structure):
                 ("ms_finish", C.c_float), ("ms_sort", C.c_float), ("ms_edges", C.c_float),
                 ("ms_total", C.c_float), ("ms_bloom_kernel", C.c_float),
                 ("ms_count_kernel", C.c_float), ("schedule", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("part_rescatters", C.c_uint32), ("n_distinct", C.c_uint64),
+                ("ms_scatter_kernel", C.c_float), ("reserved_f", C.c_float)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -63,7 +66,8 @@ class ResultInfo(C.Structure):
 
 class TableView(C.Structure):
     _fields_ = [("slots", C.c_void_p), ("capacity", C.c_uint64), ("key_limbs", C.c_uint32),
-                ("slot_bytes", C.c_uint32), ("k", C.c_uint32), ("cutoff", C.c_uint32)]
+                ("slot_bytes", C.c_uint32), ("k", C.c_uint32), ("cutoff", C.c_uint32),
+                ("log2span", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class JobC(C.Structure):

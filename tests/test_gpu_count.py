@@ -21,6 +21,7 @@ pytestmark = pytest.mark.gpu
 BASE = 0x1 | 0x4        # SPK_F_EDGES | SPK_F_KEEP_BLOOM
 ALL = BASE | 0x2        # ... | SPK_F_REF_SOLID
 GATED = 0x8             # SPK_F_GATED: the two-pass schedule
+DIRECT = 0x10           # SPK_F_DIRECT: count-first with global-table atomics
 
 
 def sha(words):
@@ -39,9 +40,10 @@ def occ(lengths, k):
 
 def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
     """Full GPU result vs the C++ oracle (twice semantics for the table, reference
-    semantics for the count >= 2 list), for all three schedules: the default
-    count-first one (d), the fused pass that builds the reference solid tier
-    (r) and the gated one (p)."""
+    semantics for the count >= 2 list), for every schedule: the default one
+    (d: partitioned count-first for k <= 64), count-first with global atomics
+    (x), the fused pass that builds the reference solid tier (r) and the gated
+    one (p)."""
     tw = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE)
     tk, tc = tw.table(1)
     oseen, otwice = tw.bloom()
@@ -61,12 +63,23 @@ def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
     np.testing.assert_array_equal(ds, oseen)
     np.testing.assert_array_equal(dt, otwice)
     dinfo = d.info(0)
+    x = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=BASE | DIRECT, **kw)
+    xk, xc = x.kmers(0, 1)
+    np.testing.assert_array_equal(xk, tk)
+    np.testing.assert_array_equal(xc, tc)
+    xs, xt = x.bloom(0)
+    np.testing.assert_array_equal(xs, oseen)
+    np.testing.assert_array_equal(xt, otwice)
+    xinfo = x.info(0)
     r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=ALL, **kw)
     info = r.info(0)
     for key in ("occurrences", "admitted_occurrences", "n_table", "n_list", "n_solid", "n_edges",
                 "seen_popcount", "twice_popcount", "cutoff"):
         assert pinfo[key] == info[key], key
         assert dinfo[key] == info[key], key
+        assert xinfo[key] == info[key], key
+    assert dinfo["n_distinct"] == xinfo["n_distinct"] >= info["n_table"]
+    assert pinfo["n_distinct"] == pinfo["n_table"]  # the gated table holds admitted k-mers only
     ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_REF)
     gk, gc = r.kmers(0, 1)
     np.testing.assert_array_equal(gk, tk)
@@ -96,9 +109,11 @@ def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
         np.testing.assert_array_equal(e, ora.edges(sk, k))
         np.testing.assert_array_equal(p.edges(0), e)
         np.testing.assert_array_equal(d.edges(0), e)
+        np.testing.assert_array_equal(x.edges(0), e)
     r.close()
     p.close()
     d.close()
+    x.close()
     return info
 
 
@@ -254,10 +269,14 @@ def test_solid_cutoff_and_seam(spk, ora):
 
 
 def test_schedules(spk):
-    """Count-first by default; the reference solid tier selects the fused pass
-    and SPK_F_GATED the two-pass schedule."""
+    """Partitioned count-first by default for k <= 64 and count-first with
+    global atomics above; the reference solid tier selects the fused pass and
+    SPK_F_GATED the two-pass schedule."""
     data, offs, lens = synth_small_packed()
-    assert spk.count((data, offs, lens), [55]).info(0)["schedule"] == 2
+    assert spk.count((data, offs, lens), [55]).info(0)["schedule"] == 3
+    assert spk.count((data, offs, lens), [21]).info(0)["schedule"] == 3
+    assert spk.count((data, offs, lens), [77]).info(0)["schedule"] == 2
+    assert spk.count((data, offs, lens), [55], flags=DIRECT).info(0)["schedule"] == 2
     assert spk.count((data, offs, lens), [55], flags=ALL).info(0)["schedule"] == 1
     assert spk.count((data, offs, lens), [55], flags=GATED).info(0)["schedule"] == 0
     assert spk.count((data, offs, lens), [55], flags=ALL | GATED).info(0)["schedule"] == 0
@@ -283,3 +302,83 @@ def test_list_threshold_above_two(spk, ora):
     np.testing.assert_array_equal(counts, tc[tc >= thr])
     assert i["n_list"] == int((tc >= thr).sum())
     assert i["n_solid"] == int((tc >= i["cutoff"]).sum())
+
+
+@pytest.mark.parametrize("table_log2", [16, 21])
+def test_partition_rescatter_on_skew(spk, ora, table_log2):
+    """A k-mer that makes up most occurrences overflows its span's region:
+    the read pass is repeated with exact region sizes and the result is
+    unchanged."""
+    data, offs, lens = synth_small_packed()
+    # 400 poly-A reads of 150 bases: 48,000 occurrences of one k-mer, more
+    # than its span's region holds next to that span's share of the rest.
+    extra = np.zeros(38 * 400, dtype=np.uint8)
+    d2 = np.concatenate([data[: int(offs[-1]) + (int(lens[-1]) + 3) // 4], extra])
+    o2 = np.concatenate([offs, int(offs[-1]) + (int(lens[-1]) + 3) // 4 + 38 * np.arange(400, dtype=np.uint64)])
+    l2 = np.concatenate([lens, np.full(400, 150, dtype=np.uint32)])
+    info = check_against_oracle(spk, ora, d2, o2.astype(np.uint64), l2.astype(np.uint32), 31,
+                                1 << 20, table_log2=table_log2)
+    r = spk.count((d2, o2.astype(np.uint64), l2.astype(np.uint32)), [31], bloom_bits=1 << 20,
+                  table_log2=table_log2)
+    ri = r.info(0)
+    assert ri["schedule"] == 3 and ri["part_rescatters"] >= 1
+    assert ri["n_table"] == info["n_table"]
+    v = r.table_view(0)
+    assert v["log2span"] == 13 and v["capacity"] == 1 << table_log2  # 8192-slot spans for k <= 32
+
+
+@pytest.mark.parametrize("k,table_log2", [(21, 22), (55, 22), (55, 20), (64, 23)])
+def test_many_spans(spk, ora, k, table_log2):
+    """Tables of hundreds of spans: the result equals the oracle's."""
+    data, offs, lens = synth_small_packed()
+    check_against_oracle(spk, ora, data, offs, lens, k, 1 << 20, table_log2=table_log2)
+    r = spk.count((data, offs, lens), [k], bloom_bits=1 << 20, table_log2=table_log2)
+    v = r.table_view(0)
+    assert r.info(0)["schedule"] == 3 and v["capacity"] == 1 << table_log2
+    assert (table_log2 - v["log2span"]) >= 8
+
+
+def _pack_codes(rows):
+    """Packed reads (src/packed_reads.rs:547-578) from rows of 2-bit codes."""
+    data, offs, lens = [], [], []
+    o = 0
+    for c in rows:
+        c = np.asarray(c, dtype=np.uint8)
+        pad = np.zeros((len(c) + 3) // 4 * 4, dtype=np.uint8)
+        pad[: len(c)] = c
+        q = pad.reshape(-1, 4)
+        data.append((q[:, 0] << 6) | (q[:, 1] << 4) | (q[:, 2] << 2) | q[:, 3])
+        offs.append(o)
+        lens.append(len(c))
+        o += q.shape[0]
+    return np.concatenate(data).astype(np.uint8), np.array(offs, np.uint64), np.array(lens, np.uint32)
+
+
+def test_large_lists_bucket_sort(spk, ora):
+    """Lists long enough for the bucketed sort (2^18 entries and more), with
+    one top-bits bucket far over its shared-memory size (k-mers that start
+    with eight A): the sorted list and edges equal the oracle's."""
+    from spk import synth
+    p = synth.c2(0.05).packed
+    rng = np.random.default_rng(5)
+    rows = []
+    for _ in range(1500):
+        blocks = [np.concatenate([np.zeros(8, np.uint8), rng.integers(0, 4, 8, dtype=np.uint8)])
+                  for _ in range(10)]
+        r = np.concatenate(blocks)[:150]
+        rows += [r, r]  # twice, so that its k-mers are listed (count >= 2)
+    d2, o2, l2 = _pack_codes(rows)
+    data = np.concatenate([p.data, d2])
+    offs = np.concatenate([p.offsets, o2 + np.uint64(p.data.size)])
+    lens = np.concatenate([p.lengths, l2])
+    k, bits = 55, 1 << 26
+    ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE, keep_bloom=False)
+    tk, tc = ref.table(2)
+    assert tk.shape[0] > (1 << 18)
+    assert int((tk[:, 1] >> np.uint64(2 * k - 64 - 16) == 0).sum()) > 2048  # the big bucket
+    r = spk.count((data, offs, lens), [k], bloom_bits=bits)
+    gk, gc = r.kmers(0)
+    np.testing.assert_array_equal(gk, tk)
+    np.testing.assert_array_equal(gc, tc)
+    sk, _ = r.solid(0)
+    np.testing.assert_array_equal(r.edges(0), ora.edges(sk, k))
