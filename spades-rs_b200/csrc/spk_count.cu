@@ -2048,27 +2048,34 @@ int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t 
 // ---------------------------------------------------------------------------
 // Downloads
 // ---------------------------------------------------------------------------
-static int copy_out(spk_result* res, int nl, DevBuf* limbs, const uint32_t* cin, uint64_t n,
-                    unsigned k, uint32_t minc, uint64_t* keys, uint32_t* counts, size_t* n_inout) {
+// The converted list (Kmer256 limbs, kept counts) of the last download of a
+// kind is cached in the result, so that a size query followed by the copy
+// converts once.
+static int copy_out(spk_result* res, KResult& kr, int kind, int nl, DevBuf* limbs, const uint32_t* cin,
+                    uint64_t n, unsigned k, uint32_t minc, uint64_t* keys, uint32_t* counts,
+                    size_t* n_inout) {
   cudaStream_t st = res->stream;
-  DevBuf okeys, ocnt;
-  uint64_t m = 0;
-  int rc = ordered_convert(st, nl, n, k, limbs, cin, minc, &okeys, cin ? &ocnt : nullptr,
-                           res->h_staging, &m);
-  if (rc) return rc;
+  KResult::Conv& cv = kr.conv;
+  if (cv.kind != kind || cv.minc != minc) {
+    cv.kind = -1;
+    int rc = ordered_convert(st, nl, n, k, limbs, cin, minc, &cv.keys, cin ? &cv.cnt : nullptr,
+                             res->h_staging, &cv.n);
+    if (rc) return rc;
+    cv.kind = kind;
+    cv.minc = minc;
+  }
+  const uint64_t m = cv.n;
   if (!keys && !counts) {
-    SPK_CUDA(cudaStreamSynchronize(st));
     *n_inout = m;
     return SPK_OK;
   }
   if (*n_inout < m) {
-    SPK_CUDA(cudaStreamSynchronize(st));
     *n_inout = m;
     return fail(SPK_E_INVALID_ARG, "output buffer too small");
   }
   if (m) {
-    if (keys) SPK_CUDA(cudaMemcpyAsync(keys, okeys.p, m * nl * 8, cudaMemcpyDeviceToHost, st));
-    if (counts && cin) SPK_CUDA(cudaMemcpyAsync(counts, ocnt.p, m * 4, cudaMemcpyDeviceToHost, st));
+    if (keys) SPK_CUDA(cudaMemcpyAsync(keys, cv.keys.p, m * nl * 8, cudaMemcpyDeviceToHost, st));
+    if (counts && cin) SPK_CUDA(cudaMemcpyAsync(counts, cv.cnt.p, m * 4, cudaMemcpyDeviceToHost, st));
   }
   SPK_CUDA(cudaStreamSynchronize(st));
   *n_inout = m;
@@ -2079,13 +2086,13 @@ int download_list(spk_result* res, int ki, uint32_t min_count, bool solid_only, 
                   uint32_t* counts, size_t* n_inout) {
   KResult& kr = *res->ks[ki];
   const uint32_t minc = solid_only ? kr.info.cutoff : std::max(min_count, kr.list_min);
-  return copy_out(res, kr.nl, kr.list, kr.list[4].as<uint32_t>(), kr.list_len, kr.k, minc,
+  return copy_out(res, kr, 0, kr.nl, kr.list, kr.list[4].as<uint32_t>(), kr.list_len, kr.k, minc,
                   keys, counts, n_inout);
 }
 
 int download_edges(spk_result* res, int ki, uint64_t* out, size_t* n_inout) {
   KResult& kr = *res->ks[ki];
-  return copy_out(res, kr.nle, kr.edges, nullptr, kr.info.n_edges, kr.k + 1, 0, out, nullptr,
+  return copy_out(res, kr, 1, kr.nle, kr.edges, nullptr, kr.info.n_edges, kr.k + 1, 0, out, nullptr,
                   n_inout);
 }
 

@@ -102,6 +102,14 @@ struct KResult {
   int nle = 0;        // limbs per edge key
   uint32_t list_min = 2;  // smallest count downloads of the list return
   uint64_t list_len = 0;  // entries in the list buffers (may include counts below list_min)
+  // The last converted download (kind 0: k-mer list with counts >= minc, 1:
+  // edges), kept for the copy that follows a size query.
+  struct Conv {
+    int kind = -1;
+    uint32_t minc = 0;
+    uint64_t n = 0;
+    DevBuf keys, cnt;
+  } conv;
 };
 
 struct spk_result_impl;

@@ -258,28 +258,35 @@ class CountResult:
         check(lib().spk_result_info_get(self.h, ki, C.byref(i)))
         return i.as_dict()
 
-    def _list(self, fn, ki, *extra, with_counts=True):
+    def _list(self, fn, ki, *extra, out=None):
+        """keys (n, ceil(k/32)) u64 and counts (n,) u32.  out = (keys, counts)
+        arrays to fill (C-contiguous, enough rows; pinned host memory makes
+        the copy faster); views of their first n rows are returned."""
         k = self.info(ki)["k"]
         L = nlimbs(k)
         n = C.c_size_t(0)
-        check(fn(self.h, ki, *extra, None, None, C.byref(n)) if with_counts else fn(self.h, ki, *extra, None, C.byref(n)))
+        check(fn(self.h, ki, *extra, None, None, C.byref(n)))
         m = n.value
-        keys = np.zeros((max(m, 1), L), dtype=np.uint64)
-        counts = np.zeros(max(m, 1), dtype=np.uint32)
-        n = C.c_size_t(m)
-        if with_counts:
-            check(fn(self.h, ki, *extra, _ptr(keys, u64p), _ptr(counts, u32p), C.byref(n)))
+        if out is None:
+            keys = np.empty((max(m, 1), L), dtype=np.uint64)
+            counts = np.empty(max(m, 1), dtype=np.uint32)
         else:
-            check(fn(self.h, ki, *extra, _ptr(keys, u64p), C.byref(n)))
+            keys, counts = out
+            if (keys.dtype != np.uint64 or counts.dtype != np.uint32 or keys.ndim != 2
+                    or keys.shape[1] != L or keys.shape[0] < m or counts.shape[0] < m
+                    or not keys.flags.c_contiguous or not counts.flags.c_contiguous):
+                raise SpkError(1, f"output arrays must hold {m} keys of {L} u64 limbs and {m} u32 counts")
+        n = C.c_size_t(max(m, keys.shape[0]) if out is not None else m)
+        check(fn(self.h, ki, *extra, _ptr(keys, u64p), _ptr(counts, u32p), C.byref(n)))
         return keys[: n.value], counts[: n.value]
 
-    def solid(self, ki: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    def solid(self, ki: int = 0, out=None) -> Tuple[np.ndarray, np.ndarray]:
         """Sorted (keys, counts) of the solid k-mers (count >= cutoff, src/assemble.rs:288-292)."""
-        return self._list(lib().spk_result_solid, ki)
+        return self._list(lib().spk_result_solid, ki, out=out)
 
-    def kmers(self, ki: int = 0, min_count: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    def kmers(self, ki: int = 0, min_count: int = 0, out=None) -> Tuple[np.ndarray, np.ndarray]:
         """Sorted (keys, counts) of every listed k-mer with count >= min_count."""
-        return self._list(lib().spk_result_kmers, ki, C.c_uint32(min_count))
+        return self._list(lib().spk_result_kmers, ki, C.c_uint32(min_count), out=out)
 
     def edges(self, ki: int = 0) -> np.ndarray:
         """Sorted canonical (k+1)-mer edges, ceil((k+1)/32) limbs each."""
@@ -288,7 +295,7 @@ class CountResult:
         n = C.c_size_t(0)
         check(lib().spk_result_edges(self.h, ki, None, C.byref(n)))
         m = n.value
-        e = np.zeros((max(m, 1), L), dtype=np.uint64)
+        e = np.empty((max(m, 1), L), dtype=np.uint64)
         n = C.c_size_t(m)
         check(lib().spk_result_edges(self.h, ki, _ptr(e, u64p), C.byref(n)))
         return e[: n.value]
