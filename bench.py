@@ -128,20 +128,193 @@ def run_cpu_baseline(packed, steps, warmup, target_occ, bloom_bits):
 
 
 # ---------------------------------------------------------------------------
+# the other workloads (one JSON line each; the default run is the k=55 one)
+# ---------------------------------------------------------------------------
+def _gk(occ, sec):
+    return occ / sec / 1e9
+
+
+def run_c3(args, ctx, log_rank0):
+    """Multi-k: the 5 Mb x 100x reads (scaled by --scale) at k in {21,33,55,77},
+    one call counting the four k values concurrently against four
+    one-k calls in a row.  Both are device-resident; time = host clock around
+    synchronised calls (the concurrent call runs on several streams)."""
+    import numpy as np
+    import torch
+    import spk
+    from spk import synth
+    ks = [21, 33, 55, 77]
+    p = synth.c2(args.scale).packed
+    occ = sum(synth.occurrences(p, k) for k in ks)
+    dev = torch.device("cuda", 0)
+    d_data = torch.zeros(p.data.size + 64, dtype=torch.uint8, device=dev)
+    d_data[: p.data.size] = torch.from_numpy(p.data).to(dev)
+    d_off = torch.from_numpy(p.offsets.view(np.int64)).to(dev)
+    d_len = torch.from_numpy(p.lengths.view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+    opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
+
+    def run(kset):
+        return spk.count_device(d_data.data_ptr(), p.data.size, d_off.data_ptr(), d_len.data_ptr(),
+                                p.lengths.size, kset, ctx=ctx, **opts)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        out = []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            out.append(time.perf_counter() - t0)
+        return sum(out) / len(out)
+
+    def plain():
+        for k in ks:
+            run([k]).close()
+
+    def multi():
+        run(ks).close()
+
+    t_plain = timed(plain)
+    t_multi = timed(multi)
+    return {"metric": METRIC, "value": _gk(occ, t_multi), "unit": "Gk-mers/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_multi * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": f"c3: the 5 Mb x 100x reads at scale {args.scale}, k in {ks} in "
+                                   "one call (concurrent per-k streams)",
+                       "occurrences": occ, "bloom_bits": args.bloom_bits,
+                       "timing": "host clock around synchronised calls"},
+            "plain": {"what": "one call per k, in a row", "value": _gk(occ, t_plain),
+                      "ms_per_step": t_plain * 1e3},
+            "speedup_vs_plain": t_plain / t_multi}
+
+
+def run_c4(args, ctx, log_rank0):
+    """Batched uneven samples: 64 samples (genome log-uniform 0.5-12 Mb x --scale,
+    GC 30-70%, 20-200x, 0.5% errors), k=33, host buffers in and solid lists
+    out: spk_count_batch against spk_count on one sample after another."""
+    import torch
+    import spk
+    from spk import synth
+    t0 = time.time()
+    ss = synth.c4(64, args.scale)
+    packs = [s.packed for s in ss]
+    occ = sum(synth.occurrences(p, 33) for p in packs)
+    log_rank0(f"c4: {len(packs)} samples, {occ} occurrences, generated in {time.time() - t0:.1f}s")
+    opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
+
+    def plain():
+        for p in packs:
+            r = spk.count(p, [33], ctx=ctx, **opts)
+            r.solid(0)
+            r.close()
+
+    def batched():
+        rs = spk.count_batch([spk.Job(p, [33], dict(opts)) for p in packs], ctx=ctx)
+        for r in rs:
+            r.solid(0)
+            r.close()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        out = []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            a = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            out.append(time.perf_counter() - a)
+        return sum(out) / len(out)
+
+    t_plain = timed(plain)
+    t_batch = timed(batched)
+    return {"metric": METRIC, "value": _gk(occ, t_batch), "unit": "Gk-mers/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": f"c4: 64 samples at genome scale {args.scale}, k=33, "
+                                   "spk_count_batch (host buffers in, solid lists out)",
+                       "occurrences": occ, "bloom_bits": args.bloom_bits,
+                       "timing": "host clock around synchronised calls"},
+            "plain": {"what": "spk_count on one sample after another", "value": _gk(occ, t_plain),
+                      "ms_per_step": t_plain * 1e3},
+            "speedup_vs_plain": t_plain / t_batch}
+
+
+def run_c5(args, ctx, log_rank0):
+    """Serving: counting jobs (isolates 1-8 Mb x --scale at 30-100x; 1 in 4
+    metagenome-like, 20 genomes with log-normal abundances), k=55, arriving
+    as a Poisson process (mean 4 jobs/s), admitted by HBM budget with up to 4
+    in flight; p50/p99 latency from submit to result and throughput."""
+    import numpy as np
+    import spk
+    from spk import synth
+    n_jobs = max(8, args.steps * 4)
+    t0 = time.time()
+    jobs = [synth.c5_job(i, args.scale).packed for i in range(n_jobs)]
+    occ = sum(synth.occurrences(p, 55) for p in jobs)
+    log_rank0(f"c5: {n_jobs} jobs, {occ} occurrences, generated in {time.time() - t0:.1f}s")
+    opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
+    # warm-up: the first job alone
+    spk.count(jobs[0], [55], ctx=ctx, **opts).close()
+    rng = np.random.default_rng(4)
+    gaps = rng.exponential(1.0 / 4.0, n_jobs)
+    srv = spk.Server(ctx, hbm_budget_bytes=0, max_inflight=4)
+    try:
+        start = time.perf_counter()
+        tickets = []
+        for i, p in enumerate(jobs):
+            due = start + gaps[: i + 1].sum()
+            while time.perf_counter() < due:
+                time.sleep(min(0.002, max(0.0, due - time.perf_counter())))
+            tickets.append(srv.submit(spk.Job(p, [55], dict(opts))))
+        lat = []
+        for t in tickets:
+            r, ms = srv.wait(t)
+            r.solid(0)
+            r.close()
+            lat.append(ms)
+        wall = time.perf_counter() - start
+    finally:
+        srv.stop()
+    lat = np.array(lat)
+    return {"metric": METRIC, "value": _gk(occ, wall), "unit": "Gk-mers/s", "n_gpus": 1,
+            "steps": n_jobs, "warmup": 1, "ms_per_step": wall * 1e3 / n_jobs,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": f"c5: {n_jobs} serving jobs at genome scale {args.scale}, k=55, "
+                                   "Poisson arrivals at 4/s, up to 4 in flight",
+                       "occurrences": occ, "bloom_bits": args.bloom_bits,
+                       "timing": "host clock; throughput over the arrival span"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())}}
+
+
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="spk", choices=["spk", "reference"])
-    ap.add_argument("--scale", type=float, default=1.0, help="genome scale (1.0 = the 5 Mb set)")
+    ap.add_argument("--scale", type=float, default=None,
+                    help="genome scale (default 1.0 for c2/c3, 0.05 for c4, 0.02 for c5)")
     ap.add_argument("--bloom-bits", type=int, default=512 << 20)
     ap.add_argument("--cpu-occ", type=int, default=96_000_000,
                     help="k-mer occurrences in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2 (default): k=55 on the 5 Mb x 100x reads; c3: multi-k; "
+                         "c4: 64 batched samples; c5: serving")
     args = ap.parse_args()
     assert args.warmup >= 1
+    if args.scale is None:
+        args.scale = {"c2": 1.0, "c3": 1.0, "c4": 0.05, "c5": 0.02}[args.workload]
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -170,6 +343,16 @@ def main():
 
     import torch
     import spk
+
+    if args.workload != "c2":
+        if rank != 0:
+            return
+        torch.cuda.set_device(local_rank)
+        ctx = spk.Context(local_rank)
+        fn = {"c3": run_c3, "c4": run_c4, "c5": run_c5}[args.workload]
+        print(json.dumps(fn(args, ctx, log)), flush=True)
+        ctx.close()
+        return
 
     if world > 1:
         import datetime

@@ -1,20 +1,80 @@
 // spk_batch.cu -- batched counting of independent samples (spk_count_batch).
+//
+// The samples of a batch are independent jobs (their own Bloom tiers, table
+// and lists).  They run concurrently, each on its own stream with its own
+// staging block, admitted by the serving scheduler (spk_sched.h) while their
+// estimated device memory fits 90% of the free HBM and at most
+// kBatchInflight run at once.  A job's kernels then overlap another job's
+// host decisions (table and list sizing), short kernels and copies, which
+// one-at-a-time counting leaves idle.  Every result is exactly spk_count's
+// on that sample alone: the jobs share nothing but the device.
 #include <cuda_runtime.h>
 
+#include <string>
+#include <vector>
+
 #include "spk_internal.h"
+#include "spk_sched.h"
+
+namespace spk {
+int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out);
+uint64_t job_estimate(const spk_job& j);
+constexpr int kBatchInflight = 4;
+}  // namespace spk
 
 extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, spk_result** results) {
   using namespace spk;
   if (!ctx || (n_jobs > 0 && (!jobs || !results))) return fail(SPK_E_INVALID_ARG, "null argument");
+  if (n_jobs < 0) return fail(SPK_E_INVALID_ARG, "negative job count");
   for (int i = 0; i < n_jobs; i++) results[i] = nullptr;
+  if (n_jobs == 0) return SPK_OK;
   for (int i = 0; i < n_jobs; i++) {
     const spk_job& j = jobs[i];
-    int rc = spk_count(ctx, j.data, j.data_len, j.offsets, j.lengths, j.n_reads, j.ks, j.n_k, &j.opts,
-                       &results[i]);
-    if (rc) {
-      for (int q = 0; q < i; q++) { spk_result_free(results[q]); results[q] = nullptr; }
-      return rc;
+    if (!j.ks || j.n_k < 1) return fail(SPK_E_INVALID_ARG, "job has no k");
+    for (int q = 0; q < j.n_k; q++)
+      if (j.ks[q] < 1 || j.ks[q] > 127) return fail(SPK_E_INVALID_K, "k outside 1..=127");
+    if (j.n_reads && (!j.offsets || !j.lengths)) return fail(SPK_E_INVALID_ARG, "null offsets/lengths");
+    if (j.data_len && !j.data) return fail(SPK_E_INVALID_ARG, "null data");
+  }
+  SPK_CUDA(cudaSetDevice(ctx->device));
+  size_t fr = 0, tot = 0;
+  SPK_CUDA(cudaMemGetInfo(&fr, &tot));
+  // A job larger than the whole budget still runs, alone.
+  uint64_t budget = (uint64_t)(fr * 0.9);
+  for (int i = 0; i < n_jobs; i++) budget = std::max<uint64_t>(budget, job_estimate(jobs[i]));
+  int status = SPK_OK;
+  std::string msg;
+  std::vector<std::string> errs(n_jobs);  // a worker thread's error message
+  {
+    Scheduler sched(budget, kBatchInflight);
+    std::vector<uint64_t> tickets(n_jobs);
+    for (int i = 0; i < n_jobs; i++) {
+      spk_job j = jobs[i];
+      std::vector<uint32_t> ks(j.ks, j.ks + j.n_k);
+      std::string* err = &errs[i];
+      tickets[i] = sched.submit(job_estimate(j), [ctx, j, ks, err](void** out) {
+        const int rc = run_job(ctx, j, ks, out);
+        if (rc) *err = spk_last_error();
+        return rc;
+      });
     }
+    for (int i = 0; i < n_jobs; i++) {
+      int st = 0;
+      void* r = nullptr;
+      sched.wait(tickets[i], -1, &st, &r, nullptr);
+      results[i] = (spk_result*)r;
+      if (st && status == SPK_OK) {
+        status = st;
+        msg = "job " + std::to_string(i) + " of the batch failed: " + errs[i];
+      }
+    }
+  }
+  if (status != SPK_OK) {
+    for (int i = 0; i < n_jobs; i++) {
+      spk_result_free(results[i]);
+      results[i] = nullptr;
+    }
+    return fail(status, msg);
   }
   return SPK_OK;
 }

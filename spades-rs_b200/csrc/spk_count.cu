@@ -39,6 +39,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "spk_internal.h"
 
@@ -2033,15 +2036,65 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   return SPK_OK;
 }
 
+// Device buffers of a k allocated on another stream: stream-ordered frees
+// go to `s` from now on (the allocating stream has been synchronised).
+static void rehome(KResult& kr, cudaStream_t s) {
+  DevBuf* bufs[] = {&kr.tiers, &kr.seen, &kr.twice, &kr.ref_solid, &kr.tslots, &kr.conv.keys,
+                    &kr.conv.cnt};
+  for (DevBuf* b : bufs) b->st = s;
+  for (DevBuf& b : kr.list) b.st = s;
+  for (DevBuf& b : kr.edges) b.st = s;
+}
+
 int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t max_len,
                    const uint32_t* ks, int n_k, const spk_count_opts& o, spk_result* res) {
   (void)max_len;
-  for (int i = 0; i < n_k; i++) {
+  if (n_k == 1) {
     auto kr = std::make_unique<KResult>();
-    int rc = count_one_k(ctx, st, res->h_staging, rv, ks[i], o, *kr);
+    int rc = count_one_k(ctx, st, res->h_staging, rv, ks[0], o, *kr);
     if (rc) return rc;
     res->ks.push_back(std::move(kr));
+    return SPK_OK;
   }
+  // Several k (run_multik_assembly's per-k loop, src/multik.rs:109-178): the
+  // k values are independent, so each counts concurrently on its own stream
+  // and staging block over the same read-only reads, once the reads that st
+  // uploads are ready.
+  cudaEvent_t ready;
+  SPK_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  SPK_CUDA(cudaEventRecord(ready, st));
+  std::vector<std::unique_ptr<KResult>> krs(n_k);
+  std::vector<int> rcs(n_k, SPK_OK);
+  std::vector<std::string> errs(n_k);
+  std::vector<std::thread> th;
+  for (int i = 0; i < n_k; i++) {
+    th.emplace_back([&, i] {
+      cudaSetDevice(ctx->device);
+      cudaStream_t s2 = nullptr;
+      uint64_t* h = staging_acquire(ctx);
+      int rc = SPK_OK;
+      if (!h) rc = fail(SPK_E_OOM, "pinned host staging allocation failed");
+      else if (cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) != cudaSuccess)
+        rc = cuda_fail(cudaGetLastError(), "per-k stream");
+      auto kr = std::make_unique<KResult>();
+      if (!rc && cudaStreamWaitEvent(s2, ready, 0) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "wait");
+      if (!rc) rc = count_one_k(ctx, s2, h, rv, ks[i], o, *kr);
+      if (s2) {
+        cudaStreamSynchronize(s2);
+        rehome(*kr, st);
+        cudaStreamDestroy(s2);
+      }
+      staging_release(ctx, h);
+      if (rc) errs[i] = spk_last_error();
+      rcs[i] = rc;
+      krs[i] = std::move(kr);
+    });
+  }
+  for (auto& t : th) t.join();
+  cudaEventDestroy(ready);
+  for (int i = 0; i < n_k; i++)
+    if (rcs[i]) return fail(rcs[i], "k=" + std::to_string(ks[i]) + ": " + errs[i]);
+  for (int i = 0; i < n_k; i++) res->ks.push_back(std::move(krs[i]));
   return SPK_OK;
 }
 

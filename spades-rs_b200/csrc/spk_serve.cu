@@ -31,35 +31,41 @@ static uint64_t next_pow2_u64(uint64_t x) {
   return p;
 }
 
-// Device bytes a job is expected to hold at its peak: reads, both Bloom
-// tiers plus the compact twice tier, and a count table plus list sized for
-// distinct admitted k-mers of up to 15% of the occurrences (at 20-200x
-// coverage the measured share is 2-10%).  A job that outgrows the estimate
-// still runs; it only makes concurrent jobs less likely to fit.
+// Device bytes a job is expected to hold at its peak (per k, the k values of
+// a job run one after another and earlier results stay resident):
+//   reads                      packed bytes + 12 B per read
+//   Bloom                      both tiers (+ the reference tier)
+//   table                      2^ceil(log2(0.3 occ)) slots, the count-first capacity
+//   partitioned passes         span regions of 1.5 occ keys, Bloom operations of
+//                              3.75 per table slot
+//   list and sort temporaries  twice (key + count) per admitted k-mer, bounded by
+//                              the table
+// Occurrences are bounded by the bases (4 per packed byte).  A job that
+// outgrows the estimate still runs; it only makes concurrent jobs less likely
+// to fit.
 uint64_t job_estimate(const spk_job& j) {
   spk_count_opts o = j.opts;
   const uint64_t bloom_bits = o.bloom_bits ? o.bloom_bits : (512ULL << 20);
   const uint64_t words = std::max<uint64_t>((bloom_bits + 63) / 64, 1);
+  const uint64_t occ = (uint64_t)j.data_len * 4;
   uint64_t bytes = j.data_len + 64 + j.n_reads * 12;
-  uint64_t total_bases = 0;
-  // Bases from the packed length (4 per byte) bound the occurrences.
-  total_bases = (uint64_t)j.data_len * 4;
-  uint64_t peak_k = 0;
+  uint64_t resident = 0, peak = 0;
   for (int i = 0; i < j.n_k; i++) {
     const uint32_t k = j.ks ? j.ks[i] : 31;
-    const uint64_t occ = total_bases;
-    const uint64_t cap = std::max<uint64_t>(next_pow2_u64(2 * (occ * 15 / 100) + 1024), 1024);
-    const uint64_t nl = (k + 31) / 32, stride = nl == 3 ? 4 : nl;
-    uint64_t b = words * 24 + (o.flags & SPK_F_REF_SOLID ? words * 8 : 0);
-    b += cap * (stride * 8 + 4 + (nl >= 3 ? 4 : 0));  // table
-    b += cap * (nl * 8 + 4) * 2;                       // list + sort temporaries
-    // Results of earlier k stay resident while later k run.
-    peak_k += b;
+    const uint64_t nl = (k + 31) / 32;
+    const uint64_t slot = nl == 1 ? 16 : (nl <= 3 ? 32 : 64);
+    const uint64_t cap = std::max<uint64_t>(next_pow2_u64(occ * 3 / 10 + 1), 1024);
+    const uint64_t tiers = words * 16 + (o.flags & SPK_F_REF_SOLID ? words * 8 : 0);
+    const uint64_t table = cap * slot;
+    const uint64_t passes = nl <= 2 ? (occ + occ / 2) * nl * 8 + cap * 15 : words * 16;
+    const uint64_t lists = std::min<uint64_t>(occ / 4, cap) * (nl * 8 + 4) * 2;
+    peak = std::max(peak, resident + tiers + table + passes + lists);
+    resident += tiers + table + lists / 2;
   }
-  return bytes + peak_k;
+  return bytes + peak;
 }
 
-static int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out) {
+int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out) {
   cudaSetDevice(ctx->device);
   cudaStream_t st;
   cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
