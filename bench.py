@@ -92,6 +92,26 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
+# N GPUs: replicas (every rank counts its own copy of the read set, no
+# data-path collective); the step time is the slowest rank's
+# ---------------------------------------------------------------------------
+def max_over_ranks(ms, world, device):
+    """The largest per-step time of all ranks (every rank calls this)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(occ_per_rank, world, ms):
+    """Gk-mers/s of the whole job: all ranks' occurrences over the slowest step."""
+    return occ_per_rank * world / (ms / 1e3) / 1e9
+
+
+# ---------------------------------------------------------------------------
 # reference CPU arm
 # ---------------------------------------------------------------------------
 def cpu_sample(packed, target_occ):
@@ -414,11 +434,8 @@ def main():
     bloom_ms = sum(i["ms_bloom_kernel"] for i in infos) / len(infos)
     count_ms = sum(i["ms_count_kernel"] for i in infos) / len(infos)
     launches = sum(i["kernel_launches"] for i in infos) // len(infos)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = occ * world / (ms / 1e3) / 1e9
+    ms = max_over_ranks(ms, world, dev)
+    value = replica_throughput(occ, world, ms)
 
     # e2e: host buffers (pinned) through spk_count, H2D and the D2H of the
     # solid list inside the timing
@@ -448,11 +465,8 @@ def main():
             d2h = keys.nbytes + counts.nbytes
             r.close()
         em = sum(e2e_ms) / len(e2e_ms)
-        if world > 1:
-            t = torch.tensor([em], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            em = float(t.item())
-        e2e = {"value": occ * world / (em / 1e3) / 1e9, "unit": "Gk-mers/s", "ms_per_step": em,
+        em = max_over_ranks(em, world, dev)
+        e2e = {"value": replica_throughput(occ, world, em), "unit": "Gk-mers/s", "ms_per_step": em,
                "h2d_bytes_per_step": int(p.data.nbytes + p.offsets.nbytes + p.lengths.nbytes),
                "d2h_bytes_per_step": int(d2h)}
 
