@@ -640,8 +640,19 @@ __host__ __device__ constexpr bool home_fits(unsigned k, int nl) {
 // never queue behind each other on one L2 line.
 constexpr uint32_t kFillStride = 8;
 
-constexpr int kPartBlock = 512;
-constexpr int kScatterBatch = 4;   // positions per lane in flight in k_part_scatter
+// Launch shapes of the partitioned passes (build-time tunables).
+#ifndef SPK_PART_BLOCK
+#define SPK_PART_BLOCK 512
+#endif
+#ifndef SPK_PART_CTAS_PER_SM
+#define SPK_PART_CTAS_PER_SM 2
+#endif
+#ifndef SPK_SCATTER_BATCH
+#define SPK_SCATTER_BATCH 4
+#endif
+constexpr int kPartBlock = SPK_PART_BLOCK;
+constexpr int kPartCtasPerSm = SPK_PART_CTAS_PER_SM;
+constexpr int kScatterBatch = SPK_SCATTER_BATCH;  // positions per lane in flight in k_part_scatter
 constexpr int kSpanBatch = 2;      // slots per thread in flight in k_part_count's write-out
 constexpr uint32_t kErrRegion = 8;
 
@@ -710,42 +721,39 @@ struct SpanKey<2> {
   typedef U128 T;
 };
 
-// Adds one occurrence of C to the shared-memory span; false if the span is
-// full.  Empty slots hold the all-ones key (never a canonical k-mer) and are
-// claimed with one 64- or 128-bit CAS, as in table_add.
+// One probe step at slot s of the shared-memory span: true when the
+// occurrence of C is counted there (C found, or s empty and claimed for C).
 template <int NL>
-__device__ __forceinline__ bool span_add(typename SpanKey<NL>::T* keys, uint32_t* cnt, uint32_t mask,
-                                         const Seq<NL>& C, uint32_t home) {
-  for (uint32_t i = 0; i <= mask; i++) {
-    const uint32_t s = (home + i) & mask;
-    if (NL == 1) {
-      unsigned long long* kp = (unsigned long long*)&keys[s];
-      const unsigned long long cur = *(volatile unsigned long long*)kp;
-      if (cur == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
-      if (cur == kEmpty) {
-        const unsigned long long old = atomicCAS(kp, kEmpty, (unsigned long long)C.v[0]);
-        if (old == kEmpty || old == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
-      }
-    } else {
-      U128* kp = (U128*)&keys[s];
-      U128 cur;
-      cur.x = ((volatile unsigned long long*)kp)[0];
-      cur.y = ((volatile unsigned long long*)kp)[1];
-      if (cur.x != kEmpty && cur.y != kEmpty) {
-        // settled (a slot changes once, from empty to its key; a read that
-        // overlaps that change has an empty half and takes the CAS below)
-        if (cur.x == C.v[0] && cur.y == C.v[NL - 1]) { atomicAdd(cnt + s, 1u); return true; }
-        continue;
-      }
-      const U128 e{kEmpty, kEmpty}, mine{C.v[0], C.v[NL - 1]};
-      const U128 old = atomicCAS(kp, e, mine);
-      if ((old.x == kEmpty && old.y == kEmpty) || (old.x == mine.x && old.y == mine.y)) {
-        atomicAdd(cnt + s, 1u);
-        return true;
-      }
+__device__ __forceinline__ bool span_step(typename SpanKey<NL>::T* keys, uint32_t* cnt, uint32_t s,
+                                          const Seq<NL>& C) {
+  if (NL == 1) {
+    unsigned long long* kp = (unsigned long long*)&keys[s];
+    const unsigned long long cur = *(volatile unsigned long long*)kp;
+    if (cur == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
+    if (cur == kEmpty) {
+      const unsigned long long old = atomicCAS(kp, kEmpty, (unsigned long long)C.v[0]);
+      if (old == kEmpty || old == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
     }
+    return false;
+  } else {
+    U128* kp = (U128*)&keys[s];
+    U128 cur;
+    cur.x = ((volatile unsigned long long*)kp)[0];
+    cur.y = ((volatile unsigned long long*)kp)[1];
+    if (cur.x != kEmpty && cur.y != kEmpty) {
+      // settled (a slot changes once, from empty to its key; a read that
+      // overlaps that change has an empty half and takes the CAS below)
+      if (cur.x == C.v[0] && cur.y == C.v[NL - 1]) { atomicAdd(cnt + s, 1u); return true; }
+      return false;
+    }
+    const U128 e{kEmpty, kEmpty}, mine{C.v[0], C.v[NL - 1]};
+    const U128 old = atomicCAS(kp, e, mine);
+    if ((old.x == kEmpty && old.y == kEmpty) || (old.x == mine.x && old.y == mine.y)) {
+      atomicAdd(cnt + s, 1u);
+      return true;
+    }
+    return false;
   }
-  return false;
 }
 
 // Bloom operations binned by range (2^kLog2Range bits of both tiers).
@@ -766,7 +774,7 @@ __device__ __forceinline__ uint64_t range_base(const RangeView& rv, uint32_t r) 
 }
 
 template <int NL, bool OPS>
-__global__ void __launch_bounds__(kPartBlock, 2) k_part_count(PartView pv, TableView t, unsigned k,
+__global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartView pv, TableView t, unsigned k,
                                                             FastMod fm, U128* __restrict__ tiers,
                                                             RangeView rv) {
   typedef typename SpanKey<NL>::T KeyT;
@@ -774,9 +782,10 @@ __global__ void __launch_bounds__(kPartBlock, 2) k_part_count(PartView pv, Table
   const uint32_t S = 1u << t.log2span;
   KeyT* keys = (KeyT*)span_smem;
   uint32_t* cnt = (uint32_t*)(span_smem + (size_t)S * sizeof(KeyT));
-  // OPS: per-range op counts, then the next global op index of each range
+  // OPS: per-range op counts (then the ops emitted so far), and the global
+  // index reserved for each range's ops of this span
   uint32_t* rhist = cnt + S;
-  unsigned long long* rcur = (unsigned long long*)(rhist + ((rv.nranges + 1) & ~1u));
+  unsigned long long* rbase = (unsigned long long*)(rhist + ((rv.nranges + 1) & ~1u));
   const uint32_t nparts = 1u << pv.log2parts;
   for (uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
     for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
@@ -789,27 +798,45 @@ __global__ void __launch_bounds__(kPartBlock, 2) k_part_count(PartView pv, Table
     __syncthreads();
     const uint64_t b = pv.base[p];
     const uint64_t e = min(pv.base[p + 1], b + (uint64_t)pv.fill[(uint64_t)p * kFillStride]);
+    // Each thread keeps one key in flight and makes one probe step per
+    // iteration, taking its next key as soon as the current one is placed:
+    // a warp's steps are then not held back by its longest probe sequence.
     bool full = false;
-    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+    {
+      uint64_t i = b + threadIdx.x;
+      bool have = false;
       Seq<NL> C;
-      if (NL == 1) {
-        C.v[0] = __ldcs(pv.keys + i);
-      } else {
-        const ulonglong2 v = __ldcs((const ulonglong2*)(pv.keys + 2 * i));
-        C.v[0] = v.x;
-        C.v[NL - 1] = v.y;
+      uint32_t home = 0, step = 0;
+      for (;;) {
+        if (!have) {
+          if (i >= e) break;
+          if (NL == 1) {
+            C.v[0] = __ldcs(pv.keys + i);
+          } else {
+            const ulonglong2 v = __ldcs((const ulonglong2*)(pv.keys + 2 * i));
+            C.v[0] = v.x;
+            C.v[NL - 1] = v.y;
+          }
+          i += blockDim.x;
+          if (pv.packed_home) {
+            const uint64_t top = C.v[NL - 1];
+            home = (uint32_t)(top >> (64 - kHomeBits)) >> (kHomeBits - t.log2span);
+            C.v[NL - 1] = top & (~0ULL >> kHomeBits);
+          } else {
+            uint64_t w4[4];
+            kmer256_limbs<NL>(C, k, w4);
+            home = (uint32_t)(table_home(t, hash_seed(hash_pre(w4), kSeed1)) & (S - 1));
+          }
+          have = true;
+          step = 0;
+        }
+        if (span_step<NL>(keys, cnt, (home + step) & (S - 1), C)) {
+          have = false;
+        } else if (++step == S) {
+          full = true;  // every slot probed
+          have = false;
+        }
       }
-      uint32_t home;
-      if (pv.packed_home) {
-        const uint64_t top = C.v[NL - 1];
-        home = (uint32_t)(top >> (64 - kHomeBits)) >> (kHomeBits - t.log2span);
-        C.v[NL - 1] = top & (~0ULL >> kHomeBits);
-      } else {
-        uint64_t w4[4];
-        kmer256_limbs<NL>(C, k, w4);
-        home = (uint32_t)(table_home(t, hash_seed(hash_pre(w4), kSeed1)) & (S - 1));
-      }
-      if (!span_add<NL>(keys, cnt, S - 1, C, home)) full = true;
     }
     if (full) atomicOr(t.err, 1);  // span full: the host regrows the table
     __syncthreads();
@@ -835,36 +862,45 @@ __global__ void __launch_bounds__(kPartBlock, 2) k_part_count(PartView pv, Table
         uint64_t raw[3], pos[3];
         bloom_positions<NL>(C, k, fm, raw, pos);
 #pragma unroll
-        for (int j = 0; j < 3; j++) atomicAdd(rhist + (uint32_t)(pos[j] >> kLog2Range), 1u);
+        for (int j = 0; j < 3; j++) {
+          atomicAdd(rhist + (uint32_t)(pos[j] >> kLog2Range), 1u);
+          // k <= 64: the written-out key's slot keeps the three positions as
+          // (range << kLog2Range | offset), at most 31 bits each
+          if (NL == 2) ((uint32_t*)&keys[s])[j] = (uint32_t)pos[j];
+        }
       }
       __syncthreads();
-      // One reservation per non-empty range.
+      // One reservation per non-empty range; rhist then counts the span's
+      // ops emitted into each range.
       for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) {
         const uint32_t n = rhist[r];
-        rcur[r] = n ? range_base(rv, r) + atomicAdd(rv.fill + (uint64_t)r * kFillStride, n) : 0ULL;
+        rbase[r] = n ? range_base(rv, r) + atomicAdd(rv.fill + (uint64_t)r * kFillStride, n) : 0ULL;
+        rhist[r] = 0;
       }
       __syncthreads();
       // Emit the operations.
       for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
         const uint32_t c = cnt[s];
         if (!c) continue;
-        Seq<NL> C;
-        if (NL == 1) {
-          C.v[0] = ((unsigned long long*)keys)[s];
+        uint32_t pk[3];
+        if (NL == 2) {
+#pragma unroll
+          for (int j = 0; j < 3; j++) pk[j] = ((const uint32_t*)&keys[s])[j];
         } else {
-          const U128 kv = ((U128*)keys)[s];
-          C.v[0] = kv.x;
-          C.v[NL - 1] = kv.y;
+          Seq<NL> C;
+          C.v[0] = ((unsigned long long*)keys)[s];
+          uint64_t raw[3], pos[3];
+          bloom_positions<NL>(C, k, fm, raw, pos);
+#pragma unroll
+          for (int j = 0; j < 3; j++) pk[j] = (uint32_t)pos[j];
         }
-        uint64_t raw[3], pos[3];
-        bloom_positions<NL>(C, k, fm, raw, pos);
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-          const uint32_t r = (uint32_t)(pos[j] >> kLog2Range);
-          const uint64_t i = atomicAdd(rcur + r, 1ULL);
+          const uint32_t r = pk[j] >> kLog2Range;
+          const uint64_t i = rbase[r] + atomicAdd(rhist + r, 1u);
           const uint64_t end = rv.uniform ? (uint64_t)(r + 1) * rv.uniform : rv.base[r + 1];
           if (i < end)
-            rv.ops[i] = ((uint32_t)(pos[j] & ((1u << kLog2Range) - 1)) << 1) | (c >= 2 ? 1u : 0u);
+            rv.ops[i] = ((pk[j] & ((1u << kLog2Range) - 1)) << 1) | (c >= 2 ? 1u : 0u);
           else
             atomicOr(rv.err, (int)kErrRange);
         }
@@ -1265,6 +1301,32 @@ __device__ __forceinline__ Seq<NLE> widen_append(const Seq<NL>& X, unsigned b) {
   R.v[0] = (X.v[0] << 2) | b;
   return R;
 }
+// The reverse complement of X.extend_right(b), from RC = revcomp(X): the
+// complement of b enters at the front (the top two of the 2k bits) and the
+// last base of RC drops out.
+template <int NL>
+__device__ __forceinline__ Seq<NL> shr_prepend(const Seq<NL>& RC, unsigned c, unsigned k) {
+  Seq<NL> R;
+#pragma unroll
+  for (int i = 0; i < NL; i++) R.v[i] = (i + 1 < NL) ? shr2(RC.v[i + 1], RC.v[i], 2) : (RC.v[i] >> 2);
+  const unsigned top = 2u * k - 2u;  // bit of the first base
+#pragma unroll
+  for (int i = 0; i < NL; i++)
+    if ((unsigned)i == (top >> 6)) R.v[i] |= (uint64_t)c << (top & 63);
+  return R;
+}
+// rc(X.extend_right(b)) as a (k+1)-mer: comp(b) in front of RC = revcomp(X).
+template <int NL, int NLE>
+__device__ __forceinline__ Seq<NLE> prepend_wide(const Seq<NL>& RC, unsigned c, unsigned k) {
+  Seq<NLE> R;
+#pragma unroll
+  for (int i = 0; i < NLE; i++) R.v[i] = i < NL ? RC.v[i] : 0;
+  const unsigned top = 2u * k;  // bit of the first base of the (k+1)-mer
+#pragma unroll
+  for (int i = 0; i < NLE; i++)
+    if ((unsigned)i == (top >> 6)) R.v[i] |= (uint64_t)c << (top & 63);
+  return R;
+}
 
 // The solid k-mers (count >= cutoff) of a list as a set: open addressing with
 // linear probing over 2^log2cap slots of NL key limbs (k <= 64), all-ones =
@@ -1349,18 +1411,20 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
       solid = cnt[i] >= cutoff;
     }
     uint32_t emits = 0;  // bit 4o + b: the edge of orientation o and base b
+    Seq<NL> RS;
+    if (solid) RS = revcomp<NL>(S, k);
     for (int o = 0; o < 2; o++) {
-      Seq<NL> EX = S;
+      // the oriented k-mer and its reverse complement
+      const Seq<NL> EX = o ? RS : S;
+      const Seq<NL> RX = o ? S : RS;
       bool ok = solid;
-      if (o == 1 && ok) {
-        EX = revcomp<NL>(S, k);
-        ok = !seq_eq<NL>(EX, S);  // a palindromic k-mer (even k) has one orientation
-      }
+      if (o == 1 && ok) ok = !seq_eq<NL>(RS, S);  // a palindromic k-mer (even k) has one orientation
       for (unsigned b = 0; b < 4; b++) {
         bool emit = false;
         if (ok) {
           const Seq<NL> NB = shl_append<NL>(EX, b, k);
-          const Seq<NL> CN = canonical<NL>(NB, k);
+          const Seq<NL> RB = shr_prepend<NL>(RX, 3u - b, k);
+          const Seq<NL> CN = seq_le<NL>(NB, RB) ? NB : RB;  // canonical, src/dna.rs:185-192
           uint64_t w4[4];
           kmer256_limbs<NL>(CN, k, w4);
           const HashPre hp = hash_pre(w4);
@@ -1374,7 +1438,7 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
           }
           if (solid_nb) {
             const Seq<NLE> E = widen_append<NL, NLE>(EX, b);
-            emit = seq_le<NLE>(E, revcomp<NLE>(E, k + 1));
+            emit = seq_le<NLE>(E, prepend_wide<NL, NLE>(RX, 3u - b, k));
           }
         }
         if (emit) emits |= 1u << (4 * o + b);
@@ -1467,7 +1531,7 @@ static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, 
                              unsigned k, const FastMod& fm, U128* tiers, const RangeView& rv) {
   size_t smem = ((size_t)1 << t.log2span) * (sizeof(typename SpanKey<NL>::T) + 4);
   const uint64_t nparts = 1ULL << pv.log2parts;
-  const int grid = (int)std::min<uint64_t>(nparts, (uint64_t)ctx->sm_count * 2);
+  const int grid = (int)std::min<uint64_t>(nparts, (uint64_t)ctx->sm_count * kPartCtasPerSm);
   if (rv.ops) {
     smem += ((rv.nranges + 1) & ~1u) * 4 + (size_t)rv.nranges * 8;
     SPK_CUDA(cudaFuncSetAttribute(k_part_count<NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1490,7 +1554,13 @@ static int launch_bloom_apply(spk_ctx* ctx, cudaStream_t st, const RangeView& rv
 }
 // Spans of the partitioned schedule: 8192 slots of 12 bytes (k <= 32) or
 // 4096 of 20 bytes (k <= 64) in shared memory, two CTAs per SM.
-constexpr uint32_t kPartLog2Span1 = 13, kPartLog2Span2 = 12;
+#ifndef SPK_PART_LOG2SPAN1
+#define SPK_PART_LOG2SPAN1 13
+#endif
+#ifndef SPK_PART_LOG2SPAN2
+#define SPK_PART_LOG2SPAN2 12
+#endif
+constexpr uint32_t kPartLog2Span1 = SPK_PART_LOG2SPAN1, kPartLog2Span2 = SPK_PART_LOG2SPAN2;
 
 template <int NL>
 static void launch_bloom(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,

@@ -272,15 +272,14 @@ int radix_sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf*
 }
 
 // ---------------------------------------------------------------------------
-// Bucket sort: an MSD split on the top 16 significant bits of the key into
-// 65536 buckets, then a bitonic sort of each bucket in shared memory.  The
-// top bits of canonical k-mers and (k+1)-mers spread their lists over the
-// buckets, so a bucket holds ~n/65536 items; a bucket larger than BS_LOCAL
-// items is sorted by the LSD radix sort above instead.  Equal keys do not
-// occur (the lists hold distinct k-mers), so stability is not needed.
+// Bucket sort: an MSD split on the top b significant bits of the key into 2^b
+// buckets (b chosen for ~128 items per bucket, 8 <= b <= 16), then a bitonic
+// sort of each bucket in shared memory.  The top bits of canonical k-mers
+// and (k+1)-mers spread their lists over the buckets; a bucket larger than
+// BS_LOCAL items is sorted by the LSD radix sort above instead.  Equal keys
+// do not occur (the lists hold distinct k-mers), so stability is not needed.
 // ---------------------------------------------------------------------------
-constexpr uint32_t BS_BITS = 16;
-constexpr uint32_t BS_NB = 1u << BS_BITS;
+constexpr uint32_t BS_MAX_BITS = 16;
 constexpr uint32_t BS_LOCAL = 2048;
 constexpr int BS_BLOCK = 256;
 constexpr uint32_t BS_MAX_BIG = 4096;
@@ -291,32 +290,33 @@ struct Limbs {
 };
 
 template <int NL>
-__device__ __forceinline__ uint32_t bs_digit(const Limbs& L, uint64_t i, unsigned limb, unsigned sh) {
+__device__ __forceinline__ uint32_t bs_digit(const Limbs& L, uint64_t i, unsigned limb, unsigned sh,
+                                             uint32_t nb) {
   uint64_t lo = 0, hi = 0;
 #pragma unroll
   for (int j = 0; j < NL; j++) {
     if ((unsigned)j == limb) lo = L.p[j][i];
     if ((unsigned)j == limb + 1) hi = L.p[j][i];
   }
-  return (uint32_t)(((lo >> sh) | ((hi << 1) << (63 - sh))) & (BS_NB - 1));
+  return (uint32_t)(((lo >> sh) | ((hi << 1) << (63 - sh))) & (nb - 1));
 }
 
 template <int NL>
 __global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(Limbs L, uint64_t n, unsigned limb, unsigned sh,
-                                                       uint32_t* __restrict__ hist) {
+                                                       uint32_t nb, uint32_t* __restrict__ hist) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
-    atomicAdd(hist + bs_digit<NL>(L, i, limb, sh), 1u);
+    atomicAdd(hist + bs_digit<NL>(L, i, limb, sh, nb), 1u);
 }
 
 template <int NL, bool HASV>
 __global__ void __launch_bounds__(BS_BLOCK) k_bs_scatter(Limbs S, const uint32_t* __restrict__ sv, Limbs D,
                                                           uint32_t* __restrict__ dv, uint64_t n,
-                                                          unsigned limb, unsigned sh,
+                                                          unsigned limb, unsigned sh, uint32_t nb,
                                                           uint32_t* __restrict__ cur) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t p = atomicAdd(cur + bs_digit<NL>(S, i, limb, sh), 1u);
+    const uint32_t p = atomicAdd(cur + bs_digit<NL>(S, i, limb, sh, nb), 1u);
 #pragma unroll
     for (int j = 0; j < NL; j++) D.p[j][p] = S.p[j][i];
     if (HASV) dv[p] = sv[i];
@@ -329,13 +329,13 @@ template <int NL, bool HASV>
 __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* __restrict__ tv, Limbs D,
                                                         uint32_t* __restrict__ dv,
                                                         const uint32_t* __restrict__ off,
-                                                        const uint32_t* __restrict__ size,
+                                                        const uint32_t* __restrict__ size, uint32_t nb,
                                                         uint32_t* __restrict__ big,
                                                         unsigned* __restrict__ nbig) {
   extern __shared__ __align__(16) uint64_t bs_smem[];
   uint64_t* sk = bs_smem;                              // NL arrays of BS_LOCAL limbs
   uint32_t* svl = (uint32_t*)(bs_smem + NL * BS_LOCAL);  // values
-  for (uint32_t b = blockIdx.x; b < BS_NB; b += gridDim.x) {
+  for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
     const uint32_t m = size[b];
     if (m == 0) continue;
     const uint32_t o = off[b];
@@ -403,20 +403,21 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* 
 
 template <int NL, bool HASV>
 static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* tv, uint64_t n,
-                     unsigned limb, unsigned sh, uint32_t* hist, uint32_t* off, uint32_t* cur,
-                     uint32_t* big, unsigned* nbig, uint32_t* launches) {
+                     unsigned limb, unsigned sh, uint32_t nb, uint32_t* hist, uint32_t* off,
+                     uint32_t* cur, uint32_t* big, unsigned* nbig, uint32_t* launches) {
   const unsigned g = (unsigned)std::min<uint64_t>((n + BS_BLOCK - 1) / BS_BLOCK, 148 * 16);
-  k_bs_hist<NL><<<g, BS_BLOCK, 0, st>>>(K, n, limb, sh, hist);
-  SPK_CUDA(cudaMemcpyAsync(off, hist, BS_NB * 4, cudaMemcpyDeviceToDevice, st));
+  k_bs_hist<NL><<<g, BS_BLOCK, 0, st>>>(K, n, limb, sh, nb, hist);
+  SPK_CUDA(cudaMemcpyAsync(off, hist, (size_t)nb * 4, cudaMemcpyDeviceToDevice, st));
   DevBuf sums;
   int rc;
-  if ((rc = scan_u32(st, off, BS_NB, sums, launches))) return rc;
-  SPK_CUDA(cudaMemcpyAsync(cur, off, BS_NB * 4, cudaMemcpyDeviceToDevice, st));
-  k_bs_scatter<NL, HASV><<<g, BS_BLOCK, 0, st>>>(K, v, T, tv, n, limb, sh, cur);
+  if ((rc = scan_u32(st, off, nb, sums, launches))) return rc;
+  SPK_CUDA(cudaMemcpyAsync(cur, off, (size_t)nb * 4, cudaMemcpyDeviceToDevice, st));
+  k_bs_scatter<NL, HASV><<<g, BS_BLOCK, 0, st>>>(K, v, T, tv, n, limb, sh, nb, cur);
   const size_t smem = BS_LOCAL * (NL * 8 + (HASV ? 4 : 0));
   SPK_CUDA(cudaFuncSetAttribute(k_bs_local<NL, HASV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem));
-  k_bs_local<NL, HASV><<<148 * 4, BS_BLOCK, smem, st>>>(T, tv, K, v, off, hist, big, nbig);
+  const unsigned gl = (unsigned)std::min<uint32_t>(nb, 148 * 4);
+  k_bs_local<NL, HASV><<<gl, BS_BLOCK, smem, st>>>(T, tv, K, v, off, hist, nb, big, nbig);
   SPK_CUDA(cudaGetLastError());
   if (launches) *launches += 3;
   return SPK_OK;
@@ -424,7 +425,11 @@ static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* t
 
 int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys, DevBuf* vals,
               uint64_t* h_staging, uint32_t* launches) {
-  if (n < (1u << 18) || nbits < BS_BITS + 8 || !h_staging)
+  // ~128 items per bucket (a few bitonic stages each), 2^8 to 2^16 buckets
+  uint32_t bbits = 8;
+  while (bbits < BS_MAX_BITS && (n >> (bbits + 1)) >= 128) bbits++;
+  const uint32_t nb = 1u << bbits;
+  if (n < (1u << 18) || nbits < bbits + 8 || !h_staging)
     return radix_sort_bufs(st, nl, n, nbits, keys, vals, launches);
   if (n >= (1ULL << 32)) return fail(SPK_E_INVALID_ARG, "sort: more than 2^32 items");
   int rc;
@@ -436,13 +441,13 @@ int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
     T.p[j] = tk[j].as<uint64_t>();
   }
   if (vals && (rc = tv.alloc(n * 4, st))) return rc;
-  if ((rc = hist.alloc(BS_NB * 4, st)) || (rc = off.alloc(BS_NB * 4, st)) ||
-      (rc = cur.alloc(BS_NB * 4, st)) || (rc = big.alloc((3 * BS_MAX_BIG + 1) * 4, st)))
+  if ((rc = hist.alloc(nb * 4, st)) || (rc = off.alloc(nb * 4, st)) || (rc = cur.alloc(nb * 4, st)) ||
+      (rc = big.alloc((3 * BS_MAX_BIG + 1) * 4, st)))
     return rc;
-  SPK_CUDA(cudaMemsetAsync(hist.p, 0, BS_NB * 4, st));
+  SPK_CUDA(cudaMemsetAsync(hist.p, 0, nb * 4, st));
   unsigned* nbig = (unsigned*)(big.as<uint32_t>() + 3 * BS_MAX_BIG);
   SPK_CUDA(cudaMemsetAsync(nbig, 0, 4, st));
-  const unsigned hi_bit = nbits - BS_BITS, limb = hi_bit / 64, sh = hi_bit % 64;
+  const unsigned hi_bit = nbits - bbits, limb = hi_bit / 64, sh = hi_bit % 64;
   uint32_t* v = vals ? vals->as<uint32_t>() : nullptr;
   uint32_t* tvp = vals ? tv.as<uint32_t>() : nullptr;
   uint32_t* H = hist.as<uint32_t>();
@@ -450,32 +455,32 @@ int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
   uint32_t* Cu = cur.as<uint32_t>();
   uint32_t* B = big.as<uint32_t>();
   switch (nl * 2 + (vals ? 1 : 0)) {
-    case 2: rc = bs_launch<1, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
-    case 3: rc = bs_launch<1, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
-    case 4: rc = bs_launch<2, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
-    case 5: rc = bs_launch<2, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
-    case 6: rc = bs_launch<3, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
-    case 7: rc = bs_launch<3, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
-    case 8: rc = bs_launch<4, false>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
-    default: rc = bs_launch<4, true>(st, K, v, T, tvp, n, limb, sh, H, O, Cu, B, nbig, launches); break;
+    case 2: rc = bs_launch<1, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 3: rc = bs_launch<1, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 4: rc = bs_launch<2, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 5: rc = bs_launch<2, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 6: rc = bs_launch<3, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 7: rc = bs_launch<3, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 8: rc = bs_launch<4, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    default: rc = bs_launch<4, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
   }
   if (rc) return rc;
   uint64_t* hs = h_staging + BS_STAGE_WORDS;
   SPK_CUDA(cudaMemcpyAsync(hs, nbig, 4, cudaMemcpyDeviceToHost, st));
   SPK_CUDA(cudaStreamSynchronize(st));
-  const unsigned nb = ((unsigned*)hs)[0];
-  if (nb > BS_MAX_BIG) {
+  const unsigned nbig_h = ((unsigned*)hs)[0];
+  if (nbig_h > BS_MAX_BIG) {
     // Too many large buckets: sort the bucketed copy as a whole instead.
     for (int j = 0; j < nl; j++)
       SPK_CUDA(cudaMemcpyAsync(K.p[j], T.p[j], n * 8, cudaMemcpyDeviceToDevice, st));
     if (vals) SPK_CUDA(cudaMemcpyAsync(v, tvp, n * 4, cudaMemcpyDeviceToDevice, st));
     return radix_sort_bufs(st, nl, n, nbits, keys, vals, launches);
   }
-  if (nb == 0) return SPK_OK;
-  SPK_CUDA(cudaMemcpyAsync(hs, B, (size_t)nb * 12, cudaMemcpyDeviceToHost, st));
+  if (nbig_h == 0) return SPK_OK;
+  SPK_CUDA(cudaMemcpyAsync(hs, B, (size_t)nbig_h * 12, cudaMemcpyDeviceToHost, st));
   SPK_CUDA(cudaStreamSynchronize(st));
-  std::vector<uint32_t> bl((const uint32_t*)hs, (const uint32_t*)hs + 3 * nb);
-  for (unsigned q = 0; q < nb; q++) {
+  std::vector<uint32_t> bl((const uint32_t*)hs, (const uint32_t*)hs + 3 * nbig_h);
+  for (unsigned q = 0; q < nbig_h; q++) {
     const uint64_t o = bl[3 * q + 1], m = bl[3 * q + 2];
     DevBuf bk[4], bvv;
     for (int j = 0; j < nl; j++) {
