@@ -1334,11 +1334,18 @@ __device__ __forceinline__ Seq<NLE> prepend_wide(const Seq<NL>& RC, unsigned c, 
 // reverse complement poly-A is smaller, and a partial top limb never has its
 // unused bits set).  Home slot: hash_kmer256(key, seed 1) >> (64 - log2cap).
 // Probed 8 times per solid k-mer by k_edges, it is small enough to stay
-// mostly in L2, unlike the count table.
+// mostly in L2, unlike the count table.  A bit filter of 2^log2filter bits
+// (bit: the low hash bits of each solid k-mer) answers most lookups of
+// k-mers that are not solid with one L2-resident bit.
 struct SetView {
   uint64_t* keys;
   uint32_t log2cap;
+  uint32_t log2filter;
+  uint32_t* filter;
 };
+__device__ __forceinline__ uint64_t filter_bit(const SetView& sv, uint64_t raw0) {
+  return raw0 & ((1ULL << sv.log2filter) - 1);
+}
 
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_solid_set(const uint64_t* l0, const uint64_t* l1,
@@ -1355,7 +1362,10 @@ __global__ void __launch_bounds__(kBlock) k_solid_set(const uint64_t* l0, const 
     if (NL == 2) C.v[NL - 1] = l1[i];
     uint64_t w4[4];
     kmer256_limbs<NL>(C, k, w4);
-    uint64_t h = hash_seed(hash_pre(w4), kSeed1) >> (64 - sv.log2cap);
+    const uint64_t raw0 = hash_seed(hash_pre(w4), kSeed1);
+    const uint64_t fb = filter_bit(sv, raw0);
+    atomicOr(sv.filter + (fb >> 5), 1u << (fb & 31));
+    uint64_t h = raw0 >> (64 - sv.log2cap);
     // keys are distinct and the set is at most 2/3 full, so a free slot is found
     for (uint64_t probe = 0; probe <= mask; probe++, h = (h + 1) & mask) {
       if (NL == 1) {
@@ -1371,6 +1381,8 @@ __global__ void __launch_bounds__(kBlock) k_solid_set(const uint64_t* l0, const 
 
 template <int NL>
 __device__ __forceinline__ bool set_has(const SetView& sv, const Seq<NL>& C, uint64_t raw0) {
+  const uint64_t fb = filter_bit(sv, raw0);
+  if (!((__ldg(sv.filter + (fb >> 5)) >> (fb & 31)) & 1u)) return false;
   const uint64_t mask = (1ULL << sv.log2cap) - 1;
   uint64_t h = raw0 >> (64 - sv.log2cap);
   for (uint64_t probe = 0; probe <= mask; probe++, h = (h + 1) & mask) {
@@ -1598,7 +1610,7 @@ static void launch_edges_t(spk_ctx* ctx, cudaStream_t st, uint64_t* l[4], const 
         l[0], l[1], l[2], l[3], cnt, n, thr, t, *sv, k, e[0], e[1], e[2], e[3], out_cap, counter);
   else
     k_edges<NL, NLE, false><<<grid_for(ctx, 8), kBlock, 0, st>>>(
-        l[0], l[1], l[2], l[3], cnt, n, thr, t, SetView{nullptr, 0}, k, e[0], e[1], e[2], e[3],
+        l[0], l[1], l[2], l[3], cnt, n, thr, t, SetView{nullptr, 0, 0, nullptr}, k, e[0], e[1], e[2], e[3],
         out_cap, counter);
 }
 // sv: the solid set (k <= 64), or nullptr to probe the count table.
@@ -2055,14 +2067,17 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     }
     // For k <= 64 the neighbours are looked up in a set of the solid k-mers
     // (at most 2/3 full), built from the list; wider keys probe the table.
-    DevBuf set;
-    SetView sv{nullptr, 0};
+    DevBuf set, filt;
+    SetView sv{nullptr, 0, 0, nullptr};
     if (nl <= 2) {
-      uint32_t lg = 10;
+      uint32_t lg = 10, lf = 20;
       while ((1ULL << lg) < info.n_solid + (info.n_solid >> 1) + 1) lg++;
-      if ((rc = set.alloc((1ULL << lg) * nl * 8, st))) return rc;
+      while (lf < 30 && (1ULL << lf) < info.n_solid * 16) lf++;  // ~1/16 false positives
+      if ((rc = set.alloc((1ULL << lg) * nl * 8, st)) || (rc = filt.alloc((1ULL << lf) / 8, st)))
+        return rc;
       SPK_CUDA(cudaMemsetAsync(set.p, 0xFF, (1ULL << lg) * nl * 8, st));
-      sv = SetView{set.as<uint64_t>(), lg};
+      SPK_CUDA(cudaMemsetAsync(filt.p, 0, (1ULL << lf) / 8, st));
+      sv = SetView{set.as<uint64_t>(), lg, lf, filt.as<uint32_t>()};
       if (nl == 1)
         k_solid_set<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[0], kr.list[4].as<uint32_t>(),
                                                            kr.list_len, thr, k, sv);

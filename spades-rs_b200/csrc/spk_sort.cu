@@ -323,7 +323,47 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_scatter(Limbs S, const uint32_t
   }
 }
 
-// Sorts every bucket of at most BS_LOCAL items from T into D; larger buckets
+// A bitonic sort of P (a power of two, <= BS_WARP) items in one warp's
+// shared-memory region, ascending on the limbs (most significant last).
+constexpr uint32_t BS_WARP = 256;  // largest bucket one warp sorts
+template <int NL, bool HASV>
+__device__ __forceinline__ void warp_bitonic(uint64_t* sk, uint32_t* svl, uint32_t P) {
+  const unsigned lane = threadIdx.x & 31;
+  for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+    for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = lane; i < P; i += 32) {
+        const uint32_t x = i ^ j;
+        if (x <= i) continue;
+        bool gt = false, eq = true;
+#pragma unroll
+        for (int q = NL - 1; q >= 0; q--) {
+          const uint64_t u = sk[q * BS_WARP + i], v = sk[q * BS_WARP + x];
+          if (eq && u != v) {
+            gt = u > v;
+            eq = false;
+          }
+        }
+        if (gt == ((i & kk) == 0) && !eq) {
+#pragma unroll
+          for (int q = 0; q < NL; q++) {
+            const uint64_t t = sk[q * BS_WARP + i];
+            sk[q * BS_WARP + i] = sk[q * BS_WARP + x];
+            sk[q * BS_WARP + x] = t;
+          }
+          if (HASV) {
+            const uint32_t t = svl[i];
+            svl[i] = svl[x];
+            svl[x] = t;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Sorts every bucket of at most BS_LOCAL items from T into D: buckets of at
+// most BS_WARP items one per warp, the others one per CTA.  Larger buckets
 // are listed in big[3i..3i+2] = (bucket, offset, size) for the host.
 template <int NL, bool HASV>
 __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* __restrict__ tv, Limbs D,
@@ -333,11 +373,50 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* 
                                                         uint32_t* __restrict__ big,
                                                         unsigned* __restrict__ nbig) {
   extern __shared__ __align__(16) uint64_t bs_smem[];
+  // Warp phase: warp w sorts the small buckets b = its global warp index +
+  // j * (all warps), in its own region of BS_WARP items.
+  {
+    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint64_t* wk = bs_smem + (size_t)w * BS_WARP * (NL + (HASV ? 1 : 0));
+    uint32_t* wv = (uint32_t*)(wk + NL * BS_WARP);
+    const uint32_t gw = blockIdx.x * (BS_BLOCK / 32) + w, nw = gridDim.x * (BS_BLOCK / 32);
+    for (uint32_t b = gw; b < nb; b += nw) {
+      const uint32_t m = size[b];
+      if (m == 0 || m > BS_WARP) continue;
+      const uint32_t o = off[b];
+      if (m == 1) {
+        if (lane == 0) {
+#pragma unroll
+          for (int j = 0; j < NL; j++) D.p[j][o] = T.p[j][o];
+          if (HASV) dv[o] = tv[o];
+        }
+        continue;
+      }
+      uint32_t P = 2;
+      while (P < m) P <<= 1;
+      for (uint32_t i = lane; i < P; i += 32) {
+        const bool in = i < m;
+#pragma unroll
+        for (int j = 0; j < NL; j++) wk[j * BS_WARP + i] = in ? T.p[j][o + i] : ~0ULL;
+        if (HASV) wv[i] = in ? tv[o + i] : 0u;
+      }
+      __syncwarp();
+      warp_bitonic<NL, HASV>(wk, wv, P);
+      for (uint32_t i = lane; i < m; i += 32) {
+#pragma unroll
+        for (int j = 0; j < NL; j++) D.p[j][o + i] = wk[j * BS_WARP + i];
+        if (HASV) dv[o + i] = wv[i];
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // CTA phase: the buckets of BS_WARP < items <= BS_LOCAL.
   uint64_t* sk = bs_smem;                              // NL arrays of BS_LOCAL limbs
   uint32_t* svl = (uint32_t*)(bs_smem + NL * BS_LOCAL);  // values
   for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
     const uint32_t m = size[b];
-    if (m == 0) continue;
+    if (m <= BS_WARP) continue;
     const uint32_t o = off[b];
     if (m > BS_LOCAL) {
       if (threadIdx.x == 0) {
@@ -413,7 +492,8 @@ static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* t
   if ((rc = scan_u32(st, off, nb, sums, launches))) return rc;
   SPK_CUDA(cudaMemcpyAsync(cur, off, (size_t)nb * 4, cudaMemcpyDeviceToDevice, st));
   k_bs_scatter<NL, HASV><<<g, BS_BLOCK, 0, st>>>(K, v, T, tv, n, limb, sh, nb, cur);
-  const size_t smem = BS_LOCAL * (NL * 8 + (HASV ? 4 : 0));
+  const size_t smem = std::max<size_t>(BS_LOCAL * (NL * 8 + (HASV ? 4 : 0)),
+                                       (size_t)(BS_BLOCK / 32) * BS_WARP * (NL + (HASV ? 1 : 0)) * 8);
   SPK_CUDA(cudaFuncSetAttribute(k_bs_local<NL, HASV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem));
   const unsigned gl = (unsigned)std::min<uint32_t>(nb, 148 * 4);
