@@ -166,6 +166,17 @@ typedef struct spk_count_opts {
   uint32_t flags;         /* SPK_F_* (default SPK_F_EDGES | SPK_F_KEEP_BLOOM) */
   uint32_t table_log2;    /* 0 = size the count table automatically; else start with
                              2^table_log2 slots (it still grows on overflow) */
+  /* Prior and trusted contigs (src/assemble.rs:244-284): ASCII sequences in
+   * host memory, contig i = prior_seqs[prior_offsets[i] .. + prior_lengths[i]),
+   * borrowed for the call (for spk_job: until the job completes).  Every
+   * k-window of a contig that Kmer256::from_bytes accepts (src/dna.rs:299-321)
+   * adds max(4 * (uint32_t)min_coverage, 50) to its canonical k-mer's count,
+   * after singleton admission and before the cutoff; a k-mer the table does
+   * not hold is inserted with that count.  n_prior = 0: none. */
+  const uint8_t* prior_seqs;
+  const uint64_t* prior_offsets;
+  const uint32_t* prior_lengths;
+  uint64_t n_prior;
 } spk_count_opts;
 
 void spk_count_opts_default(spk_count_opts* opts);

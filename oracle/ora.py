@@ -75,6 +75,9 @@ def lib():
         L.ora_count.argtypes = [u8p, C.c_size_t, u64p, u32p, C.c_size_t, C.c_uint, C.c_uint64,
                                 C.c_int, C.c_int, C.c_int]
         L.ora_count_free.argtypes = [C.c_void_p]
+        L.ora_count_inject_priors.restype = None
+        L.ora_count_inject_priors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_size_t, C.c_uint, C.c_uint32]
         L.ora_count_size.restype = C.c_size_t
         L.ora_count_size.argtypes = [C.c_void_p, C.c_uint32]
         L.ora_count_table.restype = C.c_size_t
@@ -272,6 +275,18 @@ class CountResult:
         if getattr(self, "h", None):
             lib().ora_count_free(self.h)
             self.h = None
+
+    def inject_priors(self, priors, boost: int):
+        """src/assemble.rs:267-283 on this table: every accepted k-window of every
+        prior contig (ASCII bytes) adds `boost` to its canonical k-mer."""
+        seqs = [bytes(p) for p in priors]
+        if not seqs:
+            return
+        buf = np.frombuffer(b"".join(seqs) or b"\0", dtype=np.uint8).copy()
+        lens = np.array([len(p) for p in seqs], dtype=np.uint32)
+        offs = np.concatenate([[0], np.cumsum(lens.astype(np.uint64))[:-1]]).astype(np.uint64)
+        lib().ora_count_inject_priors(self.h, buf.ctypes.data, offs.ctypes.data, lens.ctypes.data,
+                                      len(seqs), self.k, boost)
 
     def table(self, min_count: int = 1):
         n = lib().ora_count_size(self.h, min_count)

@@ -150,6 +150,13 @@ void* ora_count(const uint8_t* data, size_t data_len, const uint64_t* offsets,
   return r;
 }
 void ora_count_free(void* r) { delete (CountResult*)r; }
+// prior contigs (ASCII) concatenated in seqs, contig i = seqs[offs[i] .. offs[i] + lens[i])
+void ora_count_inject_priors(void* r, const uint8_t* seqs, const uint64_t* offs, const uint32_t* lens,
+                             size_t n, unsigned k, uint32_t boost) {
+  std::vector<std::vector<uint8_t>> pr(n);
+  for (size_t i = 0; i < n; i++) pr[i].assign(seqs + offs[i], seqs + offs[i] + lens[i]);
+  inject_priors((CountResult*)r, pr, k, boost);
+}
 size_t ora_count_size(void* r, uint32_t min_count) {
   size_t n = 0;
   for (auto& e : ((CountResult*)r)->table) n += e.count >= min_count;

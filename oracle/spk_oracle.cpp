@@ -7,6 +7,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <thread>
 
@@ -689,6 +690,24 @@ std::vector<Kmer256> edges(const std::vector<Kmer256>& solid_sorted, unsigned k)
   std::sort(out.begin(), out.end());
   out.erase(std::unique(out.begin(), out.end()), out.end());
   return out;
+}
+
+// src/assemble.rs:267-283
+void inject_priors(CountResult* r, const std::vector<std::vector<uint8_t>>& priors, unsigned k,
+                   uint32_t boost) {
+  std::map<Kmer256, uint32_t> m;  // ordered by Kmer256 (lexicographic on (lo, hi))
+  for (const auto& e : r->table) m[e.key] = e.count;
+  for (const auto& seq : priors) {
+    if (seq.size() < k) continue;                      // :273-275
+    for (size_t i = 0; i + k <= seq.size(); i++) {     // :276
+      Kmer256 x;
+      if (!k256_from_bytes(seq.data() + i, k, k, &x)) continue;  // :277
+      bool rc;
+      m[k256_canonical(x, k, &rc)] += boost;           // :278-279
+    }
+  }
+  r->table.clear();
+  for (const auto& kv : m) r->table.push_back(CountEntry{kv.first, kv.second});
 }
 
 }  // namespace ora

@@ -122,6 +122,13 @@ void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int 
 // assemble.rs:692-735
 uint32_t determine_solid_kmer_cutoff(const std::vector<uint32_t>& counts, double min_coverage);
 
+// src/assemble.rs:267-283: every k-window of every prior contig that
+// Kmer256::from_bytes accepts adds `boost` to its canonical k-mer's count,
+// inserting the k-mer when the table does not hold it.  The table stays
+// sorted by key.
+void inject_priors(CountResult* r, const std::vector<std::vector<uint8_t>>& priors, unsigned k,
+                   uint32_t boost);
+
 // graph.rs:78-102: the (k+1)-mer edge set implied by get_successors over the
 // solid set, as canonical (k+1)-mers, sorted.
 std::vector<Kmer256> edges(const std::vector<Kmer256>& solid_sorted, unsigned k);

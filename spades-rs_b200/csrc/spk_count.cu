@@ -1157,26 +1157,44 @@ __global__ void __launch_bounds__(kBlock, 4) k_admit_compact(TableView t, unsign
     for (int u = 0; u < U; u++) {
       const uint64_t s = chunk + 32 * u + lane;
       c[u] = s < t.capacity ? load_slot<NL>(t, s, C[u]) : 0u;
-      if (c[u] & kRejected) c[u] = 0;
+      if (c[u] & kRejected) {  // rejected by an earlier admission pass
+        c[u] = 0;
+        n_rej++;
+      }
     }
-    // Singletons: the three twice bits of every slot in flight together.
-    uint64_t pos[U][3], tw[U][3];
+    // Singletons: a k-mer seen once is admitted when its three twice bits are
+    // set.  Most fail on the first bit (the twice tier is sparse), so the
+    // first bits of every slot are loaded together and the other two only
+    // when needed.
+    HashPre hp[U];
+    uint64_t q0[U], tw0[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (c[u] == 1 && check_singletons) {
-        uint64_t raw[3];
-        bloom_positions<NL>(C[u], k, fm, raw, pos[u]);
-#pragma unroll
-        for (int j = 0; j < 3; j++) tw[u][j] = __ldg(twice + (pos[u][j] >> 6));
+        uint64_t w4[4];
+        kmer256_limbs<NL>(C[u], k, w4);
+        hp[u] = hash_pre(w4);
+        q0[u] = fastmod(fm, hash_seed(hp[u], kSeed1));
+        tw0[u] = __ldg(twice + (q0[u] >> 6));
       }
     }
     unsigned km[U];
     unsigned nkeep = 0;
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      if (c[u] == 1 && check_singletons &&
-          !((tw[u][0] >> (pos[u][0] & 63)) & (tw[u][1] >> (pos[u][1] & 63)) &
-            (tw[u][2] >> (pos[u][2] & 63)) & 1)) {
+      bool admit = true;
+      if (c[u] == 1 && check_singletons) {
+        admit = (tw0[u] >> (q0[u] & 63)) & 1;
+        if (admit) {
+          const uint64_t q = fastmod(fm, hash_seed(hp[u], kSeed2));
+          admit = (__ldg(twice + (q >> 6)) >> (q & 63)) & 1;
+        }
+        if (admit) {
+          const uint64_t q = fastmod(fm, hash_seed(hp[u], kSeed3));
+          admit = (__ldg(twice + (q >> 6)) >> (q & 63)) & 1;
+        }
+      }
+      if (!admit) {
         *slot_count<NL>(t, chunk + 32 * u + lane) = 1u | kRejected;
         c[u] = 0;
         n_rej++;
@@ -1483,6 +1501,84 @@ __global__ void __launch_bounds__(kBlock) k_edges(const uint64_t* l0, const uint
           if (NLE > 3) e3[p] = E.v[NLE > 3 ? 3 : 0];
         }
         p++;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Prior and trusted contigs (src/assemble.rs:267-283): every k-window of a
+// contig that Kmer256::from_bytes accepts (every byte A/C/G/T in either case,
+// src/dna.rs:11-37, 299-321) adds `boost` to its canonical k-mer.  Runs after
+// singleton admission: a singleton the Bloom rejected is not in the
+// reference's map, so its count restarts from the boost; a k-mer the table
+// lacks is inserted with it.  One warp per contig, lanes over its windows.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ascii_base(uint8_t c) {
+  switch (c) {
+    case 'A': case 'a': return 0;
+    case 'C': case 'c': return 1;
+    case 'G': case 'g': return 2;
+    case 'T': case 't': return 3;
+    default: return -1;
+  }
+}
+
+// The slot holding key C (probe sequence from home), or ~0 if absent.
+template <int NL>
+__device__ __forceinline__ uint64_t table_slot_of(const TableView& t, const Seq<NL>& C, uint64_t home) {
+  for (uint32_t i = 0; i < t.max_probe; i++) {
+    const uint64_t s = probe_slot(t, home, i);
+    const uint32_t c = *(volatile uint32_t*)slot_count<NL>(t, s);
+    if (c == 0) return ~0ULL;  // an empty slot ends the probe sequence
+    const volatile uint64_t* kp = slot_key<NL>(t, s);
+    bool eq = true;
+#pragma unroll
+    for (int j = 0; j < NL; j++) eq &= kp[j] == C.v[j];
+    if (eq) return s;
+  }
+  return ~0ULL;
+}
+
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_prior_inject(const uint8_t* __restrict__ seqs,
+                                                          const uint64_t* __restrict__ offs,
+                                                          const uint32_t* __restrict__ lens, uint64_t n,
+                                                          unsigned k, uint32_t boost, TableView t) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t c = warp; c < n; c += nwarps) {
+    const uint8_t* sq = seqs + offs[c];
+    const uint32_t L = lens[c];
+    if (L < k) continue;  // src/assemble.rs:273-275
+    for (uint32_t i = lane; i + k <= L; i += 32) {
+      Seq<NL> V;
+#pragma unroll
+      for (int j = 0; j < NL; j++) V.v[j] = 0;
+      bool ok = true;
+      for (unsigned j = 0; j < k && ok; j++) {
+        const int b = ascii_base(sq[i + j]);
+        if (b < 0) ok = false;
+        else V = shl_append<NL>(V, (unsigned)b, k);
+      }
+      if (!ok) continue;
+      const Seq<NL> C = canonical<NL>(V, k);
+      uint64_t w4[4];
+      kmer256_limbs<NL>(C, k, w4);
+      const uint64_t home = table_home(t, hash_seed(hash_pre(w4), kSeed1));
+      const uint64_t s = table_slot_of<NL>(t, C, home);
+      if (s == ~0ULL) {
+        table_add<NL>(t, C, home, boost);  // absent: inserted with the boost
+        continue;
+      }
+      uint32_t* cp = slot_count<NL>(t, s);
+      uint32_t cur = *(volatile uint32_t*)cp;
+      for (;;) {
+        const uint32_t nv = (cur & kRejected) ? boost : cur + boost;
+        const uint32_t old = atomicCAS(cp, cur, nv);
+        if (old == cur) break;
+        cur = old;
       }
     }
   }
@@ -1970,6 +2066,46 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   info.table_capacity = cap;
   SPK_CUDA(cudaEventRecord(e2.e, st));
 
+  // ---- prior contigs (src/assemble.rs:244-284), after singleton admission ----
+  const bool priors = o.n_prior > 0 && o.prior_seqs && o.prior_offsets && o.prior_lengths;
+  if (priors) {
+    // Mark the rejected singletons (nothing is listed), then inject.
+    DevBuf junk;
+    if ((rc = junk.alloc((kHistBins + 8) * 8, st))) return rc;
+    SPK_CUDA(cudaMemsetAsync(junk.p, 0, (kHistBins + 8) * 8, st));
+    unsigned long long* jw = junk.as<unsigned long long>();
+    uint64_t* none[4] = {nullptr, nullptr, nullptr, nullptr};
+    SPK_DISPATCH_NL(nl, launch_admit, ctx, st, kr.table, k, kr.fm, kr.twice.as<uint64_t>(),
+                    gated ? 0 : 1, 0xFFFFFFFFu, none, nullptr, 0, jw, jw + kHistBins,
+                    jw + kHistBins + 4);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < o.n_prior; i++) total = std::max(total, o.prior_offsets[i] + o.prior_lengths[i]);
+    DevBuf pseq, poff, plen;
+    if ((rc = pseq.alloc(std::max<uint64_t>(total, 1), st)) || (rc = poff.alloc(o.n_prior * 8, st)) ||
+        (rc = plen.alloc(o.n_prior * 4, st)))
+      return rc;
+    if (total) SPK_CUDA(cudaMemcpyAsync(pseq.p, o.prior_seqs, total, cudaMemcpyHostToDevice, st));
+    SPK_CUDA(cudaMemcpyAsync(poff.p, o.prior_offsets, o.n_prior * 8, cudaMemcpyHostToDevice, st));
+    SPK_CUDA(cudaMemcpyAsync(plen.p, o.prior_lengths, o.n_prior * 4, cudaMemcpyHostToDevice, st));
+    const uint32_t mc = o.min_coverage >= 4294967295.0 ? 0xFFFFFFFFu
+                        : o.min_coverage > 0 ? (uint32_t)o.min_coverage : 0u;
+    const uint32_t boost = std::max<uint32_t>(mc * 4u, 50u);  // src/assemble.rs:272
+    SPK_CUDA(cudaMemsetAsync(errp, 0, 4, st));
+    switch (nl) {
+      case 1: k_prior_inject<1><<<grid_for(ctx, 4), kBlock, 0, st>>>(pseq.as<uint8_t>(), poff.as<uint64_t>(), plen.as<uint32_t>(), o.n_prior, k, boost, kr.table); break;
+      case 2: k_prior_inject<2><<<grid_for(ctx, 4), kBlock, 0, st>>>(pseq.as<uint8_t>(), poff.as<uint64_t>(), plen.as<uint32_t>(), o.n_prior, k, boost, kr.table); break;
+      case 3: k_prior_inject<3><<<grid_for(ctx, 4), kBlock, 0, st>>>(pseq.as<uint8_t>(), poff.as<uint64_t>(), plen.as<uint32_t>(), o.n_prior, k, boost, kr.table); break;
+      default: k_prior_inject<4><<<grid_for(ctx, 4), kBlock, 0, st>>>(pseq.as<uint8_t>(), poff.as<uint64_t>(), plen.as<uint32_t>(), o.n_prior, k, boost, kr.table); break;
+    }
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    if ((rc = fetch(S_ERR + 1))) return rc;
+    if ((int)host[S_ERR] & 1)
+      return fail(SPK_E_TABLE_FULL, "count table: no free slot for a prior contig k-mer");
+  }
+
   // ---- admission of singletons, histogram, compaction, cutoff ----
   uint32_t fixed = o.min_count;
   if (!fixed && o.min_coverage > 5.0) {  // src/assemble.rs:693-694
@@ -2006,7 +2142,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     SPK_CUDA(cudaMemsetAsync(sw + S_REJ, 0, 8, st));
     SPK_CUDA(cudaMemsetAsync(sw + S_HIST, 0, kHistBins * 8, st));
     SPK_DISPATCH_NL(nl, launch_admit, ctx, st, kr.table, k, kr.fm, kr.twice.as<uint64_t>(),
-                    gated ? 0 : 1, lmin_pre, lp, kr.list[4].as<uint32_t>(), lcap, su + S_HIST,
+                    (gated || priors) ? 0 : 1, lmin_pre, lp, kr.list[4].as<uint32_t>(), lcap, su + S_HIST,
                     su + S_SUMS, su + S_REJ);
     SPK_CUDA(cudaGetLastError());
     launches++;

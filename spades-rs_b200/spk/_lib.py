@@ -43,7 +43,9 @@ class SpkError(RuntimeError):
 class CountOpts(C.Structure):
     _fields_ = [("bloom_bits", C.c_uint64), ("min_count", C.c_uint32),
                 ("list_min_count", C.c_uint32), ("min_coverage", C.c_double),
-                ("flags", C.c_uint32), ("table_log2", C.c_uint32)]
+                ("flags", C.c_uint32), ("table_log2", C.c_uint32),
+                ("prior_seqs", C.c_void_p), ("prior_offsets", C.c_void_p),
+                ("prior_lengths", C.c_void_p), ("n_prior", C.c_uint64)]
 
 
 class ResultInfo(C.Structure):

@@ -217,7 +217,9 @@ class PackedReads:
 # ---------------------------------------------------------------------------
 def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: int = 2,
               min_coverage: float = 5.0, flags: Optional[int] = None,
-              table_log2: int = 0) -> CountOpts:
+              table_log2: int = 0, priors: Optional[Sequence[bytes]] = None) -> CountOpts:
+    """spk_count_opts.  priors: prior/trusted contigs as ASCII byte strings
+    (src/assemble.rs:244-284); the returned options keep them alive."""
     o = CountOpts()
     lib().spk_count_opts_default(C.byref(o))
     o.bloom_bits = bloom_bits
@@ -227,6 +229,16 @@ def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: i
     o.table_log2 = table_log2
     if flags is not None:
         o.flags = flags
+    if priors:
+        seqs = [bytes(p) for p in priors]
+        buf = np.frombuffer(b"".join(seqs) + b"\0", dtype=np.uint8).copy()
+        lens = np.array([len(p) for p in seqs], dtype=np.uint32)
+        offs = np.concatenate([[0], np.cumsum(lens.astype(np.uint64))[:-1]]).astype(np.uint64)
+        o._prior_arrays = (buf, offs, lens)
+        o.prior_seqs = buf.ctypes.data
+        o.prior_offsets = offs.ctypes.data
+        o.prior_lengths = lens.ctypes.data
+        o.n_prior = len(seqs)
     return o
 
 
@@ -393,7 +405,8 @@ class Job:
         j.n_reads = self._len.size
         j.ks = self._ks.ctypes.data
         j.n_k = self._ks.size
-        j.opts = make_opts(**self.opts)
+        self._opts = make_opts(**self.opts)  # keeps any prior contig arrays alive
+        j.opts = self._opts
         return j
 
 

@@ -382,3 +382,34 @@ def test_large_lists_bucket_sort(spk, ora):
     np.testing.assert_array_equal(gc, tc)
     sk, _ = r.solid(0)
     np.testing.assert_array_equal(r.edges(0), ora.edges(sk, k))
+
+
+@pytest.mark.parametrize("k", [31, 55, 77])
+def test_prior_contigs(spk, ora, k):
+    """Prior and trusted contigs (src/assemble.rs:244-284) add their boost to
+    every accepted k-window after singleton admission and before the cutoff:
+    the table, the cutoff and the edges equal the oracle's count followed by
+    its prior injection."""
+    from oracle import pyref
+    data, offs, lens = synth_small_packed()
+    reads = [pyref.get_read(data, offs, lens, i) for i in range(0, 200, 7)]
+    rng = np.random.default_rng(k)
+    priors = [r[5:120].encode() for r in reads[:20]]                       # known k-mers, singletons
+    priors += ["".join("ACGT"[b] for b in rng.integers(0, 4, 300)).encode()]  # new k-mers
+    priors += [(reads[20][:60].lower() + "NN" + reads[20][60:]).encode()]   # case, ambiguous bases
+    priors += [b"ACGT" * 5]                                                  # shorter than k
+    bits = 1 << 20
+    ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE)
+    ref.inject_priors(priors, 50)  # max(4 * 5, 50) with the default min_coverage 5.0
+    tk, tc = ref.table(1)
+    for flags in (BASE, BASE | GATED):
+        r = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=flags,
+                      priors=priors)
+        gk, gc = r.kmers(0, 1)
+        np.testing.assert_array_equal(gk, tk)
+        np.testing.assert_array_equal(gc, tc)
+        info = r.info(0)
+        assert info["cutoff"] == ora.cutoff(tc, 5.0)
+        assert info["n_table"] == tk.shape[0]
+        sk, _ = r.solid(0)
+        np.testing.assert_array_equal(r.edges(0), ora.edges(sk, k))

@@ -188,3 +188,32 @@ def test_ecoli_packing_matches_oracle_ingest(ora):
     data, offs, lens, d = ecoli_packed()
     assert int(d["pe_count"][0]) > 0 and lens.size == offs.size
     assert int(d["n_raw"][0]) == 2054 and int(d["n_raw"][1]) == 2054
+
+
+def test_prior_injection_matches_python_restatement(ora):
+    """src/assemble.rs:267-283 on the C++ oracle against the Python
+    restatement: windows with a non-ACGT byte are skipped, either case is
+    accepted, contigs shorter than k add nothing, and absent k-mers are
+    inserted with the boost."""
+    data, offs, lens = synth_small_packed()
+    k, boost = 21, 50
+    r = ora.count(data, offs, lens, k, 1 << 20, mode=ora.MODE_TWICE)
+    before_k, before_c = r.table(1)
+    reads = [pyref.get_read(data, offs, lens, i) for i in (0, 5, 9)]
+    priors = [reads[0][10:90].encode(), reads[1][:40].lower().encode(),
+              (reads[2][:30] + "N" + reads[2][30:70]).encode(), b"ACGTACGT",
+              b"GATTACAGATTACATTTTGGGGCCCCAAAATTTT"]
+    r.inject_priors(priors, boost)
+    got_k, got_c = r.table(1)
+    want = {tuple(int(x) for x in row): int(c) for row, c in zip(before_k, before_c)}
+    for p in priors:
+        s = p.decode()
+        for i in range(len(s) - k + 1):
+            x = pyref.k256_from_str(s[i:i + k], k)
+            if x is None:
+                continue
+            key = tuple(int(v) for v in pyref.limbs(pyref.k256_canonical(x, k)[0]))[: nlimbs(k)]
+            want[key] = want.get(key, 0) + boost
+    keys = sorted(want)
+    np.testing.assert_array_equal(got_k, np.array(keys, dtype=np.uint64))
+    np.testing.assert_array_equal(got_c, np.array([want[t] for t in keys], dtype=np.uint32))
