@@ -1163,37 +1163,24 @@ __global__ void __launch_bounds__(kBlock, 4) k_admit_compact(TableView t, unsign
       }
     }
     // Singletons: a k-mer seen once is admitted when its three twice bits are
-    // set.  Most fail on the first bit (the twice tier is sparse), so the
-    // first bits of every slot are loaded together and the other two only
-    // when needed.
-    HashPre hp[U];
-    uint64_t q0[U], tw0[U];
+    // set; the twice words of every slot in flight are loaded together.
+    uint64_t pos[U][3], tw[U][3];
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (c[u] == 1 && check_singletons) {
-        uint64_t w4[4];
-        kmer256_limbs<NL>(C[u], k, w4);
-        hp[u] = hash_pre(w4);
-        q0[u] = fastmod(fm, hash_seed(hp[u], kSeed1));
-        tw0[u] = __ldg(twice + (q0[u] >> 6));
+        uint64_t raw[3];
+        bloom_positions<NL>(C[u], k, fm, raw, pos[u]);
+#pragma unroll
+        for (int j = 0; j < 3; j++) tw[u][j] = __ldg(twice + (pos[u][j] >> 6));
       }
     }
     unsigned km[U];
     unsigned nkeep = 0;
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      bool admit = true;
-      if (c[u] == 1 && check_singletons) {
-        admit = (tw0[u] >> (q0[u] & 63)) & 1;
-        if (admit) {
-          const uint64_t q = fastmod(fm, hash_seed(hp[u], kSeed2));
-          admit = (__ldg(twice + (q >> 6)) >> (q & 63)) & 1;
-        }
-        if (admit) {
-          const uint64_t q = fastmod(fm, hash_seed(hp[u], kSeed3));
-          admit = (__ldg(twice + (q >> 6)) >> (q & 63)) & 1;
-        }
-      }
+      const bool admit = !(c[u] == 1 && check_singletons) ||
+                         ((tw[u][0] >> (pos[u][0] & 63)) & (tw[u][1] >> (pos[u][1] & 63)) &
+                          (tw[u][2] >> (pos[u][2] & 63)) & 1);
       if (!admit) {
         *slot_count<NL>(t, chunk + 32 * u + lane) = 1u | kRejected;
         c[u] = 0;
