@@ -266,6 +266,26 @@ typedef struct spk_table_view {
 } spk_table_view;
 int spk_result_table_view(spk_result* res, int k_index, spk_table_view* view);
 
+/* Unitigs of the solid k-mers: the maximal non-branching paths of their de
+ * Bruijn graph, one per reverse-complement pair, as CompactedGraph::build
+ * (src/graph.rs:65-235) finds them.  An isolated cycle is cut at its smallest
+ * solid k-mer read forward, where the reference's walk in sorted order starts.
+ * Replaces the unitig list of CompactedGraph (src/graph.rs:44-62); the Rust
+ * side orders its unitigs by hash-set iteration, so here each unitig is
+ * given in the orientation not greater than its reverse complement and the
+ * list is sorted by sequence.  k must be odd (src/main.rs:10-23).
+ *
+ * seqs receives the concatenated ASCII sequences (no separators; lengths[i]
+ * bases each), mean_coverage[i] the mean count of unitig i's k-mers and
+ * kmers_count[i] their number.  With every output pointer null, *n_inout
+ * and *seq_bytes_inout receive the unitig count and the total bases; with
+ * outputs, they give the capacities (checked) and receive the sizes.  Any
+ * output pointer may be null.  Built on the device on the first call and
+ * cached in the result. */
+int spk_result_unitigs(spk_result* res, int k_index, char* seqs, uint64_t* seq_bytes_inout,
+                       uint64_t* lengths, double* mean_coverage, uint64_t* kmers_count,
+                       uint64_t* n_inout);
+
 int spk_result_free(spk_result* res);
 
 /* ---- batched and serving entry points ---------------------------------- */

@@ -75,6 +75,16 @@ def lib():
         L.ora_count.argtypes = [u8p, C.c_size_t, u64p, u32p, C.c_size_t, C.c_uint, C.c_uint64,
                                 C.c_int, C.c_int, C.c_int]
         L.ora_count_free.argtypes = [C.c_void_p]
+        L.ora_unitigs.restype = C.c_void_p
+        L.ora_unitigs.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint]
+        L.ora_unitigs_count.restype = C.c_size_t
+        L.ora_unitigs_count.argtypes = [C.c_void_p]
+        L.ora_unitigs_bases.restype = C.c_size_t
+        L.ora_unitigs_bases.argtypes = [C.c_void_p]
+        L.ora_unitigs_get.restype = None
+        L.ora_unitigs_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ora_unitigs_free.restype = None
+        L.ora_unitigs_free.argtypes = [C.c_void_p]
         L.ora_count_inject_priors.restype = None
         L.ora_count_inject_priors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_size_t, C.c_uint, C.c_uint32]
@@ -327,6 +337,31 @@ def cutoff(counts, min_coverage: float) -> int:
     c = np.ascontiguousarray(counts, dtype=np.uint32)
     cc = c if c.size else np.zeros(1, np.uint32)
     return int(lib().ora_cutoff(_p(cc, u32p), c.size, C.c_double(min_coverage)))
+
+
+def unitigs(solid_keys: np.ndarray, counts: np.ndarray, k: int):
+    """CompactedGraph::build (src/graph.rs:65-235) on a sorted solid list:
+    (sequences as a list of str, mean coverage float64[n], k-mer counts
+    uint64[n]), each unitig in the orientation not greater than its reverse
+    complement, sorted by sequence."""
+    keys = np.ascontiguousarray(solid_keys, dtype=np.uint64)
+    cnt = np.ascontiguousarray(counts, dtype=np.uint32)
+    h = lib().ora_unitigs(keys.ctypes.data, cnt.ctypes.data, cnt.size, k)
+    try:
+        n = lib().ora_unitigs_count(h)
+        nb = lib().ora_unitigs_bases(h)
+        buf = np.zeros(max(nb, 1), dtype=np.uint8)
+        lens = np.zeros(max(n, 1), dtype=np.uint64)
+        cov = np.zeros(max(n, 1), dtype=np.float64)
+        km = np.zeros(max(n, 1), dtype=np.uint64)
+        lib().ora_unitigs_get(h, buf.ctypes.data, lens.ctypes.data, cov.ctypes.data, km.ctypes.data)
+    finally:
+        lib().ora_unitigs_free(h)
+    seqs, o = [], 0
+    for ln in lens[:n]:
+        seqs.append(buf[o:o + int(ln)].tobytes().decode())
+        o += int(ln)
+    return seqs, cov[:n], km[:n]
 
 
 def edges(solid_keys: np.ndarray, k: int) -> np.ndarray:

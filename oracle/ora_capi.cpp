@@ -150,6 +150,32 @@ void* ora_count(const uint8_t* data, size_t data_len, const uint64_t* offsets,
   return r;
 }
 void ora_count_free(void* r) { delete (CountResult*)r; }
+// Unitigs of a sorted solid list (keys as ceil(k/32) limbs): returns a handle.
+void* ora_unitigs(const uint64_t* keys, const uint32_t* counts, size_t n, unsigned k) {
+  const unsigned L = nlimbs(k);
+  std::vector<Kmer256> s(n);
+  for (size_t i = 0; i < n; i++) s[i] = from_limbs(keys + i * L, L);
+  std::vector<uint32_t> c(counts, counts + n);
+  return new std::vector<Unitig>(unitigs(s, c, k));
+}
+size_t ora_unitigs_count(void* h) { return ((std::vector<Unitig>*)h)->size(); }
+size_t ora_unitigs_bases(void* h) {
+  size_t b = 0;
+  for (auto& u : *(std::vector<Unitig>*)h) b += u.sequence.size();
+  return b;
+}
+void ora_unitigs_get(void* h, char* seqs, uint64_t* lengths, double* cov, uint64_t* kmers) {
+  size_t o = 0, i = 0;
+  for (auto& u : *(std::vector<Unitig>*)h) {
+    memcpy(seqs + o, u.sequence.data(), u.sequence.size());
+    o += u.sequence.size();
+    lengths[i] = u.sequence.size();
+    cov[i] = u.mean_coverage;
+    kmers[i] = u.kmers_count;
+    i++;
+  }
+}
+void ora_unitigs_free(void* h) { delete (std::vector<Unitig>*)h; }
 // prior contigs (ASCII) concatenated in seqs, contig i = seqs[offs[i] .. offs[i] + lens[i])
 void ora_count_inject_priors(void* r, const uint8_t* seqs, const uint64_t* offs, const uint32_t* lens,
                              size_t n, unsigned k, uint32_t boost) {

@@ -294,6 +294,92 @@ def edges(solid, k: int):
     return sorted(out)
 
 
+def unitigs(solid_strs, counts, k: int):
+    """CompactedGraph::build (src/graph.rs:65-235) on string k-mers.
+
+    solid_strs: the canonical solid k-mers as strings, sorted (string order is
+    the 2-bit value order); counts: their counts.  The walk follows the
+    reference step by step on oriented k-mers (kmer, is_rc): pass 1 starts at
+    k-mers with an orientation that has no unique unvisited predecessor of
+    out-degree one (:183-216), pass 2 takes what is left, i.e. isolated cycles
+    (:219-231).  Returns (sequences, mean coverages, k-mer counts), each
+    sequence in the orientation not greater than its reverse complement, sorted
+    by sequence (the reference's own order follows its hash-set iteration)."""
+    idx = {s: i for i, s in enumerate(solid_strs)}
+
+    def explicit(o):  # :24-30
+        return revcomp_str(o[0]) if o[1] else o[0]
+
+    def canon(x):  # src/dna.rs:185-192
+        r = revcomp_str(x)
+        return (x, False) if x <= r else (r, True)
+
+    def succs(o):  # :78-90
+        e = explicit(o)
+        return [c for c in (canon(e[1:] + b) for b in BASES) if c[0] in idx]
+
+    def preds(o):  # :91-102
+        e = explicit(o)
+        return [c for c in (canon(a + e[:-1]) for a in BASES) if c[0] in idx]
+
+    visited = set()
+
+    def extract(start):  # :104-157
+        path, curr = [], start
+        while curr[0] not in visited:
+            visited.add(curr[0])
+            path.append(curr)
+            sc = succs(curr)
+            if len(sc) != 1:
+                break
+            nx = sc[0]
+            if nx[0] in visited or len(preds(nx)) != 1:
+                break
+            curr = nx
+        if not path:
+            return path
+        back, bc = [], path[0]
+        while True:
+            pr = preds(bc)
+            if len(pr) != 1:
+                break
+            pv = pr[0]
+            if pv[0] in visited or len(succs(pv)) != 1:
+                break
+            visited.add(pv[0])
+            back.append(pv)
+            bc = pv
+        return back[::-1] + path
+
+    out = []
+
+    def build(path):  # :159-177
+        seq = explicit(path[0]) + "".join(explicit(o)[-1] for o in path[1:])
+        cov = sum(int(counts[idx[o[0]]]) for o in path)
+        out.append((seq, cov / len(path), len(path)))
+
+    for km in solid_strs:  # pass 1
+        if km in visited:
+            continue
+        start = (km, False)
+        pf, pr = preds((km, False)), preds((km, True))
+        if len(pf) == 1 and len(succs(pf[0])) == 1 and pf[0][0] not in visited:
+            if len(pr) == 1 and len(succs(pr[0])) == 1 and pr[0][0] not in visited:
+                continue
+            start = (km, True)
+        p = extract(start)
+        if p:
+            build(p)
+    for km in solid_strs:  # pass 2
+        if km not in visited:
+            p = extract((km, False))
+            if p:
+                build(p)
+    norm = [(min(s, revcomp_str(s)), c, n) for s, c, n in out]
+    norm.sort(key=lambda t: t[0])
+    return [t[0] for t in norm], [t[1] for t in norm], [t[2] for t in norm]
+
+
 MIN_K = 21  # src/packed_reads.rs:38
 
 

@@ -710,4 +710,119 @@ void inject_priors(CountResult* r, const std::vector<std::vector<uint8_t>>& prio
   for (const auto& kv : m) r->table.push_back(CountEntry{kv.first, kv.second});
 }
 
+// src/graph.rs:14-40, 65-235
+namespace {
+struct OK {
+  Kmer256 kmer;
+  bool is_rc;
+};
+}  // namespace
+
+std::vector<Unitig> unitigs(const std::vector<Kmer256>& solid, const std::vector<uint32_t>& counts,
+                            unsigned k) {
+  std::vector<Unitig> out;
+  if (k == 0 || solid.empty()) return out;  // :70-75
+  auto index_of = [&](const Kmer256& x) -> long {
+    auto it = std::lower_bound(solid.begin(), solid.end(), x);
+    return (it != solid.end() && *it == x) ? (long)(it - solid.begin()) : -1;
+  };
+  auto explicit_seq = [&](const OK& o) { return o.is_rc ? k256_revcomp(o.kmer, k) : o.kmer; };  // :24-30
+  auto succs = [&](const OK& o) {  // :78-90
+    std::vector<OK> v;
+    const Kmer256 s = explicit_seq(o);
+    for (uint8_t b = 0; b < 4; b++) {
+      bool rc;
+      const Kmer256 can = k256_canonical(k256_extend_right(s, b, k), k, &rc);
+      if (index_of(can) >= 0) v.push_back(OK{can, rc});
+    }
+    return v;
+  };
+  auto preds = [&](const OK& o) {  // :91-102
+    std::vector<OK> v;
+    const Kmer256 s = explicit_seq(o);
+    for (uint8_t a = 0; a < 4; a++) {
+      bool rc;
+      const Kmer256 can = k256_canonical(k256_prepend_left(s, a, k), k, &rc);
+      if (index_of(can) >= 0) v.push_back(OK{can, rc});
+    }
+    return v;
+  };
+  std::vector<char> visited(solid.size(), 0);
+  auto vis = [&](const Kmer256& x) { return visited[index_of(x)] != 0; };
+  auto mark = [&](const Kmer256& x) { visited[index_of(x)] = 1; };
+  auto extract = [&](OK start) {  // :104-157
+    std::vector<OK> path;
+    OK curr = start;
+    while (!vis(curr.kmer)) {
+      mark(curr.kmer);
+      path.push_back(curr);
+      const auto sc = succs(curr);
+      if (sc.size() != 1) break;
+      const OK nx = sc[0];
+      if (vis(nx.kmer)) break;
+      if (preds(nx).size() != 1) break;
+      curr = nx;
+    }
+    if (path.empty()) return path;
+    std::vector<OK> back;
+    OK bc = path[0];
+    for (;;) {
+      const auto pr = preds(bc);
+      if (pr.size() != 1) break;
+      const OK pv = pr[0];
+      if (vis(pv.kmer)) break;
+      if (succs(pv).size() != 1) break;
+      mark(pv.kmer);
+      back.push_back(pv);
+      bc = pv;
+    }
+    std::reverse(back.begin(), back.end());
+    back.insert(back.end(), path.begin(), path.end());
+    return back;
+  };
+  auto build = [&](const std::vector<OK>& path) {  // :159-177
+    std::string seq = k256_to_string(explicit_seq(path[0]), k);
+    double cov = (double)counts[index_of(path[0].kmer)];
+    for (size_t i = 1; i < path.size(); i++) {
+      const Kmer256 e = explicit_seq(path[i]);
+      seq.push_back("ACGT"[k256_last_base(e, k)]);
+      cov += (double)counts[index_of(path[i].kmer)];
+    }
+    return Unitig{seq, cov / (double)path.size(), path.size()};
+  };
+  for (const Kmer256& km : solid) {  // pass 1, :183-216
+    if (vis(km)) continue;
+    OK start{km, false};
+    const auto pf = preds(start);
+    const auto pr = preds(OK{km, true});
+    if (pf.size() == 1) {
+      const OK pn = pf[0];
+      if (succs(pn).size() == 1 && !vis(pn.kmer)) {
+        if (pr.size() == 1) {
+          const OK prn = pr[0];
+          if (succs(prn).size() == 1 && !vis(prn.kmer)) continue;  // interior: deferred
+          start = OK{km, true};
+        } else {
+          start = OK{km, true};
+        }
+      }
+    }
+    const auto p = extract(start);
+    if (!p.empty()) out.push_back(build(p));
+  }
+  for (const Kmer256& km : solid) {  // pass 2, :219-231
+    if (vis(km)) continue;
+    const auto p = extract(OK{km, false});
+    if (!p.empty()) out.push_back(build(p));
+  }
+  // orientation not greater than the reverse complement; sorted by sequence
+  for (Unitig& u : out) {
+    std::string rc(u.sequence.rbegin(), u.sequence.rend());
+    for (char& c : rc) c = c == 'A' ? 'T' : c == 'C' ? 'G' : c == 'G' ? 'C' : 'A';
+    if (rc < u.sequence) u.sequence = rc;
+  }
+  std::sort(out.begin(), out.end(), [](const Unitig& a, const Unitig& b) { return a.sequence < b.sequence; });
+  return out;
+}
+
 }  // namespace ora

@@ -129,6 +129,22 @@ uint32_t determine_solid_kmer_cutoff(const std::vector<uint32_t>& counts, double
 void inject_priors(CountResult* r, const std::vector<std::vector<uint8_t>>& priors, unsigned k,
                    uint32_t boost);
 
+// CompactedGraph::build (src/graph.rs:65-235): maximal non-branching paths
+// of the solid k-mers.  The reference walks a HashSet, whose order (and so
+// each unitig's orientation, its position in the output and where an
+// isolated cycle is cut) depends on the hasher; here the solid k-mers are
+// walked in sorted order.  Each unitig is then put in the orientation that
+// is not greater than its reverse complement and the list is sorted by
+// sequence, which is the same for every walk order except the cut of a
+// cycle (taken at the cycle's smallest k-mer, as the sorted walk does).
+struct Unitig {
+  std::string sequence;
+  double mean_coverage;
+  size_t kmers_count;
+};
+std::vector<Unitig> unitigs(const std::vector<Kmer256>& solid_sorted,
+                            const std::vector<uint32_t>& counts, unsigned k);
+
 // graph.rs:78-102: the (k+1)-mer edge set implied by get_successors over the
 // solid set, as canonical (k+1)-mers, sorted.
 std::vector<Kmer256> edges(const std::vector<Kmer256>& solid_sorted, unsigned k);

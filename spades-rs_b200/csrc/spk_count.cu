@@ -1285,16 +1285,6 @@ __global__ void k_cutoff(const unsigned long long* __restrict__ hist, uint32_t f
 // so only the copy that is its own canonical form is emitted: every
 // canonical (k+1)-mer comes out exactly once without a dedup pass.
 // ---------------------------------------------------------------------------
-template <int NL>
-__device__ __forceinline__ Seq<NL> shl_append(const Seq<NL>& X, unsigned b, unsigned k) {
-  Seq<NL> R;
-#pragma unroll
-  for (int i = NL - 1; i >= 1; i--) R.v[i] = shl2(X.v[i], X.v[i - 1], 2);
-  R.v[0] = (X.v[0] << 2) | b;
-  const unsigned topbits = 2u * k - 64u * (NL - 1);  // bits used in the top limb (1..64)
-  if (topbits < 64) R.v[NL - 1] &= (1ULL << topbits) - 1;
-  return R;
-}
 template <int NL, int NLE>
 __device__ __forceinline__ Seq<NLE> widen_append(const Seq<NL>& X, unsigned b) {
   Seq<NLE> R;
@@ -1304,20 +1294,6 @@ __device__ __forceinline__ Seq<NLE> widen_append(const Seq<NL>& X, unsigned b) {
     R.v[i] = shl2(hi, X.v[i - 1], 2);
   }
   R.v[0] = (X.v[0] << 2) | b;
-  return R;
-}
-// The reverse complement of X.extend_right(b), from RC = revcomp(X): the
-// complement of b enters at the front (the top two of the 2k bits) and the
-// last base of RC drops out.
-template <int NL>
-__device__ __forceinline__ Seq<NL> shr_prepend(const Seq<NL>& RC, unsigned c, unsigned k) {
-  Seq<NL> R;
-#pragma unroll
-  for (int i = 0; i < NL; i++) R.v[i] = (i + 1 < NL) ? shr2(RC.v[i + 1], RC.v[i], 2) : (RC.v[i] >> 2);
-  const unsigned top = 2u * k - 2u;  // bit of the first base
-#pragma unroll
-  for (int i = 0; i < NL; i++)
-    if ((unsigned)i == (top >> 6)) R.v[i] |= (uint64_t)c << (top & 63);
   return R;
 }
 // rc(X.extend_right(b)) as a (k+1)-mer: comp(b) in front of RC = revcomp(X).

@@ -85,6 +85,17 @@ struct TableView {
 };
 
 // ---- per-k result ---------------------------------------------------------------
+// Unitigs of the solid k-mers (spk_graph.cu), built on first request.
+struct UnitigSet {
+  bool ready = false;
+  std::string seq;                // concatenated sequences
+  std::vector<uint64_t> lengths;  // bases per unitig
+  std::vector<double> cov;        // mean k-mer count
+  std::vector<uint64_t> kmers;    // k-mers per unitig
+  uint32_t launches = 0;          // kernels the build launched
+  float ms_device = 0.f;          // device time of the build (kernels and copies)
+};
+
 struct KResult {
   uint32_t k = 0;
   int nl = 0;
@@ -110,6 +121,7 @@ struct KResult {
     uint64_t n = 0;
     DevBuf keys, cnt;
   } conv;
+  UnitigSet unitigs;
 };
 
 struct spk_result_impl;

@@ -109,6 +109,8 @@ _SIGS = [
     ("spk_result_edges", C.c_int, [vp, C.c_int, u64p, C.POINTER(C.c_size_t)]),
     ("spk_result_bloom", C.c_int, [vp, C.c_int, u64p, u64p, u64p]),
     ("spk_result_table_view", C.c_int, [vp, C.c_int, C.POINTER(TableView)]),
+    ("spk_result_unitigs", C.c_int, [vp, C.c_int, C.c_char_p, u64p, u64p, C.POINTER(C.c_double), u64p,
+                                     u64p]),
     ("spk_result_free", C.c_int, [vp]),
     ("spk_count_batch", C.c_int, [vp, C.POINTER(JobC), C.c_int, C.POINTER(vp)]),
     ("spk_serve_start", C.c_int, [vp, C.c_uint64, C.c_int]),

@@ -312,6 +312,29 @@ class CountResult:
         check(lib().spk_result_edges(self.h, ki, _ptr(e, u64p), C.byref(n)))
         return e[: n.value]
 
+    def unitigs(self, ki: int = 0):
+        """Unitigs of the solid k-mers (CompactedGraph::build, src/graph.rs:65-235):
+        (sequences, mean_coverage float64[n], kmers_count uint64[n]), each
+        sequence in the orientation not greater than its reverse complement,
+        sorted by sequence.  k must be odd."""
+        n = C.c_uint64(0)
+        nb = C.c_uint64(0)
+        check(lib().spk_result_unitigs(self.h, ki, None, C.byref(nb), None, None, None, C.byref(n)))
+        m, b = n.value, nb.value
+        buf = C.create_string_buffer(max(b, 1))
+        lengths = np.zeros(max(m, 1), dtype=np.uint64)
+        cov = np.zeros(max(m, 1), dtype=np.float64)
+        kmers = np.zeros(max(m, 1), dtype=np.uint64)
+        check(lib().spk_result_unitigs(self.h, ki, buf, C.byref(nb), _ptr(lengths, u64p),
+                                       cov.ctypes.data_as(C.POINTER(C.c_double)), _ptr(kmers, u64p),
+                                       C.byref(n)))
+        raw = buf.raw[: nb.value].decode("ascii")
+        seqs, o = [], 0
+        for L in lengths[: n.value].tolist():
+            seqs.append(raw[o : o + L])
+            o += L
+        return seqs, cov[: n.value], kmers[: n.value]
+
     def bloom(self, ki: int = 0, ref_solid: bool = False):
         """(seen, twice[, ref_solid]) Bloom word arrays of this k."""
         n = self.info(ki)["bloom_size_bits"] // 64

@@ -48,3 +48,75 @@ def kmer_strings(data, offsets, lengths, k):
         s = "".join("ACGT"[c] for c in codes)
         out.extend(s[i:i + k] for i in range(n - k + 1))
     return out
+
+
+# ---- unitig cases -------------------------------------------------------------
+_COMP = str.maketrans("ACGT", "TGCA")
+
+
+def revcomp(s):
+    return s.translate(_COMP)[::-1]
+
+
+def rand_seq(rng, n):
+    return "".join("ACGT"[c] for c in rng.integers(0, 4, n))
+
+
+def key_rows(strs, k):
+    """Canonical k-mer strings -> (n, nlimbs(k)) u64 keys in Kmer256 limb order."""
+    from oracle import pyref
+    L = nlimbs(k)
+    out = np.zeros((len(strs), L), dtype=np.uint64)
+    for i, s in enumerate(strs):
+        out[i] = pyref.limbs(pyref.k256_from_str(s, k))[:L]
+    return out
+
+
+def graph_sequences(rng, k):
+    """Sequences whose k-mers make a graph with every shape the unitig walk
+    meets: a genome with a repeat (two branch points each side), a tip (an
+    error-like side branch), a bubble, a circle (an isolated cycle), a
+    hairpin (a sequence followed by its own reverse complement) and a short
+    isolated piece."""
+    rep = rand_seq(rng, 2 * k)
+    g = rand_seq(rng, 700) + rep + rand_seq(rng, 500) + rep + rand_seq(rng, 600)
+    tip = g[300:300 + k + 5] + rand_seq(rng, 12)
+    bub = g[900:900 + 3 * k]
+    bub = bub[:k + 10] + ("A" if bub[k + 10] != "A" else "C") + bub[k + 11:]
+    circle = rand_seq(rng, 400)
+    circ_seq = circle + circle[:k - 1]
+    h = rand_seq(rng, 90)
+    hairpin = h + revcomp(h)
+    piece = rand_seq(rng, k + 3)
+    return [g, tip, bub, circ_seq, hairpin, piece], circle
+
+
+def solid_from_sequences(seqs, k, rng):
+    """Sorted canonical k-mer strings of the sequences with counts 2..60."""
+    ks = set()
+    for s in seqs:
+        for i in range(len(s) - k + 1):
+            w = s[i:i + k]
+            ks.add(min(w, revcomp(w)))
+    strs = sorted(ks)
+    counts = rng.integers(2, 61, len(strs)).astype(np.uint32)
+    return strs, counts
+
+
+def reads_from(seqs, circle, rng, cov=30, rl=(90, 150)):
+    """Error-free reads tiling every sequence, and the circle with reads that
+    wrap around its end, at about cov-fold coverage; half of them reverse
+    complemented."""
+    out = []
+
+    def take(s, n_start):
+        for _ in range(max(1, cov * n_start // 120)):
+            L = min(int(rng.integers(rl[0], rl[1] + 1)), len(s))
+            st = int(rng.integers(0, min(n_start, len(s) - L + 1)))
+            r = s[st:st + L]
+            out.append(revcomp(r) if rng.integers(0, 2) else r)
+
+    for s in seqs:
+        take(s, len(s))
+    take(circle + circle[:rl[1]], len(circle))
+    return out
