@@ -113,6 +113,184 @@ def replica_throughput(occ_per_rank, world, ms):
 
 # ---------------------------------------------------------------------------
 # reference CPU arm
+def run_unitigs(args, ctx, log_rank0):
+    """Unitig compaction (CompactedGraph::build, src/graph.rs:65-235) of the
+    solid k-mers of the 5 Mb x 100x reads (scaled by --scale) at k=55.  Each
+    step counts the reads on the device (untimed) and then builds the unitigs
+    (timed): the device time of the build from its events, the host's
+    orientation and sort, and the host clock around spk_result_unitigs with
+    the unitigs copied into host buffers.  CPU baseline: the oracle's
+    restatement of the reference walk on the same solid list, one thread."""
+    import numpy as np
+    import torch
+    import spk
+    from spk import synth
+    from oracle import ora
+    p = synth.c2(args.scale).packed
+    dev = torch.device("cuda", 0)
+    d_data = torch.zeros(p.data.size + 64, dtype=torch.uint8, device=dev)
+    d_data[: p.data.size] = torch.from_numpy(p.data).to(dev)
+    d_off = torch.from_numpy(p.offsets.view(np.int64)).to(dev)
+    d_len = torch.from_numpy(p.lengths.view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+    opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
+
+    def count():
+        return spk.count_device(d_data.data_ptr(), p.data.size, d_off.data_ptr(), d_len.data_ptr(),
+                                p.lengths.size, [K], ctx=ctx, **opts)
+
+    dev_ms, host_ms, wall_ms = [], [], []
+    n_solid = n_unitigs = launches = 0
+    out_bytes = 0
+    for i in range(args.warmup + args.steps):
+        r = count()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        seqs, cov, kmers = r.unitigs(0)
+        t1 = time.perf_counter()
+        info = r.info(0)
+        if i >= args.warmup:
+            dev_ms.append(info["ms_unitigs"])
+            host_ms.append(info["ms_unitigs_host"])
+            wall_ms.append((t1 - t0) * 1e3)
+        n_solid, n_unitigs, launches = info["n_solid"], info["n_unitigs"], info["unitig_launches"]
+        out_bytes = sum(len(x) for x in seqs) + 16 * len(seqs)
+        if i == args.warmup + args.steps - 1:
+            keys, counts = r.solid(0)
+        r.close()
+    med = lambda a: float(np.median(a))
+    t_build = med(dev_ms) + med(host_ms)
+    line = {"metric": "unitig compaction throughput (solid k-mers per second)",
+            "value": n_solid / (t_build / 1e3) / 1e6, "unit": "M solid k-mers/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_build,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": f"unitigs of the k=55 solid k-mers of the 5 Mb x 100x reads at "
+                                   f"scale {args.scale}", "n_solid": n_solid, "n_unitigs": n_unitigs,
+                       "timing": "CUDA events around the device build (through the copy of the "
+                                 "unitigs to the host) plus the host's orientation and sort; "
+                                 "median over steps"},
+            "device_ms": med(dev_ms), "host_ms": med(host_ms), "gpu_launches": launches,
+            "e2e": {"value": n_solid / (med(wall_ms) / 1e3) / 1e6, "unit": "M solid k-mers/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": out_bytes,
+                    "what": "host clock around spk_result_unitigs through the Python binding, "
+                            "results in host buffers"}}
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        ref = ora.unitigs(keys, counts, K)
+        sec = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n_solid / sec / 1e6, "unit": "M solid k-mers/s", "cores": 1,
+                                "kind": "port", "seconds": sec,
+                                "sample": "the whole solid list of the workload; the oracle's C++ "
+                                          "restatement of the reference walk, one thread"}
+        line["parity"] = bool(ref[0] == seqs and np.array_equal(ref[2], kmers)
+                              and np.array_equal(ref[1], cov))
+    return line
+
+
+def run_correct(args, ctx, log_rank0):
+    """Stage 3 with error correction (config.error_correct,
+    src/assemble.rs:183-191; ErrorCorrector, src/hammer.rs:34-121) on the
+    5 Mb x 100x reads (scaled by --scale) at k=55: each step is one counting
+    job with SPK_F_CORRECT (Bloom pass, correction of every read into a
+    device copy, gated count of the corrected reads, cutoff, sort, edges),
+    reads resident in HBM; host clock around the synchronised call.  Also:
+    the correction kernel alone (its device time), the same job without
+    correction, and the job end to end from host reads.  CPU baseline: the
+    threaded restatement of the same Stage 2 + corrected Stage 3 on a sample
+    of the reads, all host threads."""
+    import numpy as np
+    import torch
+    import spk
+    from spk import synth
+    from oracle import ora
+    p = synth.c2(args.scale).packed
+    occ = synth.occurrences(p, K)
+    dev = torch.device("cuda", 0)
+    d_data = torch.zeros(p.data.size + 64, dtype=torch.uint8, device=dev)
+    d_data[: p.data.size] = torch.from_numpy(p.data).to(dev)
+    d_off = torch.from_numpy(p.offsets.view(np.int64)).to(dev)
+    d_len = torch.from_numpy(p.lengths.view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+    corr = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES | spk.SPK_F_CORRECT)
+    gated = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES | spk.SPK_F_GATED)
+
+    def run(opts):
+        return spk.count_device(d_data.data_ptr(), p.data.size, d_off.data_ptr(), d_len.data_ptr(),
+                                p.lengths.size, [K], ctx=ctx, **opts)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ms, infos = [], []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            info = fn()
+            torch.cuda.synchronize()
+            ms.append((time.perf_counter() - t0) * 1e3)
+            infos.append(info)
+        return float(np.median(ms)), infos
+
+    def job(opts):
+        r = run(opts)
+        info = r.info(0)
+        r.close()
+        return info
+
+    t_corr, infos = timed(lambda: job(corr))
+    t_plain, _ = timed(lambda: job(gated))
+    ms_kernel = float(np.median([i["ms_correct"] for i in infos]))
+    n_corr = infos[-1]["n_corrected_reads"]
+    e2e_ms, _ = timed(lambda: spk.count(p, [K], ctx=ctx, **corr).close())
+    line = {"metric": "k-mer counting with error correction (k-mer occurrences per second)",
+            "value": occ / (t_corr / 1e3) / 1e9, "unit": "Gk-mers/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_corr,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": f"c2 reads at scale {args.scale}, k={K}, SPK_F_CORRECT (Stage 3 "
+                                   "corrects every read against the twice tier, then counts)",
+                       "occurrences": occ, "reads": int(p.lengths.size), "bloom_bits": args.bloom_bits,
+                       "timing": "host clock around synchronised calls, median"},
+            "correct_kernel": {"ms": ms_kernel, "reads_per_s": p.lengths.size / (ms_kernel / 1e3),
+                               "corrected_reads": n_corr},
+            "without_correction": {"ms_per_step": t_plain,
+                                   "value": occ / (t_plain / 1e3) / 1e9, "schedule": "gated"},
+            "gpu_launches": infos[-1]["kernel_launches"],
+            "e2e": {"value": occ / (e2e_ms / 1e3) / 1e9, "unit": "Gk-mers/s",
+                    "h2d_bytes_per_step": int(p.data.size + p.offsets.nbytes + p.lengths.nbytes),
+                    "d2h_bytes_per_step": 0,
+                    "what": "spk.count on host reads (H2D of the reads inside the call); the solid "
+                            "list stays on the device"}}
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        n = min(p.lengths.size, 4000)
+        for _ in range(4):
+            d, o, ln, socc = cpu_sample_reads(p, n)
+            t0 = time.perf_counter()
+            r = ora.count(d, o, ln, K, args.bloom_bits, mode=ora.MODE_REF, threads=threads,
+                          keep_bloom=False, correct=True)
+            sec = time.perf_counter() - t0
+            if sec > 8 or n == p.lengths.size:
+                break
+            n = min(p.lengths.size, int(n * min(20.0, 15.0 / max(sec, 1e-3))))
+        line["cpu_baseline"] = {"value": socc / sec / 1e9, "unit": "Gk-mers/s", "cores": threads,
+                                "kind": "port", "seconds": sec,
+                                "sample": f"first {ln.size} reads ({socc} k-mer occurrences); threaded "
+                                          f"C++ restatement of Stage 2 and the correcting Stage 3, "
+                                          f"{threads} threads, full-size Bloom",
+                                "corrected_reads": r.stats()["corrected_reads"]}
+    return line
+
+
+def cpu_sample_reads(packed, n):
+    """The first n reads of the workload and their k-mer occurrences."""
+    import numpy as np
+    end = int(packed.offsets[n - 1]) + (int(packed.lengths[n - 1]) + 3) // 4
+    per = np.clip(packed.lengths[:n].astype(np.int64) - K + 1, 0, None)
+    return packed.data[:end], packed.offsets[:n], packed.lengths[:n], int(per.sum())
+
+
 # ---------------------------------------------------------------------------
 def cpu_sample(packed, target_occ):
     """The first reads of the workload holding about target_occ k-mer occurrences."""
@@ -328,13 +506,15 @@ def main():
                     help="k-mer occurrences in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "unitigs", "correct"],
                     help="c2 (default): k=55 on the 5 Mb x 100x reads; c3: multi-k; "
-                         "c4: 64 batched samples; c5: serving")
+                         "c4: 64 batched samples; c5: serving; unitigs: unitig compaction "
+                         "of the c2 solid k-mers; correct: c2 with error correction")
     args = ap.parse_args()
     assert args.warmup >= 1
     if args.scale is None:
-        args.scale = {"c2": 1.0, "c3": 1.0, "c4": 0.05, "c5": 0.02}[args.workload]
+        args.scale = {"c2": 1.0, "c3": 1.0, "c4": 0.05, "c5": 0.02, "unitigs": 1.0,
+                      "correct": 1.0}[args.workload]
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -369,7 +549,8 @@ def main():
             return
         torch.cuda.set_device(local_rank)
         ctx = spk.Context(local_rank)
-        fn = {"c3": run_c3, "c4": run_c4, "c5": run_c5}[args.workload]
+        fn = {"c3": run_c3, "c4": run_c4, "c5": run_c5, "unitigs": run_unitigs,
+              "correct": run_correct}[args.workload]
         print(json.dumps(fn(args, ctx, log)), flush=True)
         ctx.close()
         return

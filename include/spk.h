@@ -135,6 +135,24 @@ int spk_bloom_insert_k256_noalloc(uint64_t* d_seen, uint64_t* d_solid, uint64_t 
                                   const uint64_t* d_keys4, size_t n, uint8_t* d_out_promoted,
                                   void* cuda_stream);
 
+/* ErrorCorrector::correct_read_in_place (src/hammer.rs:34-121) on every read
+ * of a packed read set, against this filter's solid tier, as Stage 3 applies
+ * it before counting (src/assemble.rs:183-191).  data_out (data_len bytes;
+ * may equal data) receives the packed data with the corrected bases in place;
+ * reads shorter than k are unchanged.  corrected (nullable, n_reads bytes)
+ * gets 1 for every read with a changed base, *n_corrected (nullable) their
+ * number.  k: 0 corrects nothing (as the reference); 1..127; reads of at most
+ * 8192 bases (longer ones: SPK_E_INVALID_ARG).  The result equals calling the
+ * reference once per read in any order (reads are independent). */
+int spk_bloom_correct_reads(spk_bloom* bloom, uint32_t k, const uint8_t* data, size_t data_len,
+                            const uint64_t* offsets, const uint32_t* lengths, size_t n_reads,
+                            uint8_t* data_out, uint8_t* corrected, uint64_t* n_corrected);
+/* The same on device-resident reads: every pointer except n_corrected is a
+ * device pointer on the filter's device. */
+int spk_bloom_correct_reads_device(spk_bloom* bloom, uint32_t k, const uint8_t* d_data, size_t data_len,
+                                   const uint64_t* d_offsets, const uint32_t* d_lengths, size_t n_reads,
+                                   uint8_t* d_data_out, uint8_t* d_corrected, uint64_t* n_corrected);
+
 /* ---- counting (src/assemble.rs:129-292, src/graph.rs:78-102) ------------ */
 #define SPK_F_EDGES      0x1u  /* build the (k+1)-mer edge list */
 #define SPK_F_REF_SOLID  0x2u  /* also build the reference-semantics solid tier */
@@ -146,6 +164,11 @@ int spk_bloom_insert_k256_noalloc(uint64_t* d_seen, uint64_t* d_solid, uint64_t 
                                   only admitted k-mers, for read sets too large for that */
 #define SPK_F_DIRECT     0x10u /* count-first with one global-table atomic per occurrence
                                   instead of the partitioned passes (k <= 64) */
+#define SPK_F_CORRECT    0x20u /* Stage 3 with error correction (config.error_correct,
+                                  src/assemble.rs:183-191): after the Bloom pass every read
+                                  is corrected against the twice tier (src/hammer.rs:34-121)
+                                  into a device copy, and the count pass reads the
+                                  corrected copy.  Implies SPK_F_GATED. */
 
 /* spk_result_info.schedule */
 #define SPK_SCHEDULE_GATED       0u  /* SPK_F_GATED: Bloom pass, then the gated count pass */
@@ -221,7 +244,14 @@ typedef struct spk_result_info {
   uint64_t n_distinct;           /* distinct k-mers in the table before singleton admission
                                     (n_table plus the rejected singletons) */
   float ms_scatter_kernel;       /* partitioned: the read pass that scatters keys by span */
-  float reserved_f;
+  float ms_unitigs;              /* spk_result_unitigs: device time of the build, through the
+                                    copy of the unitigs to the host (0 until built) */
+  float ms_unitigs_host;         /* ... and the host's orientation and sort of the unitigs */
+  uint32_t unitig_launches;      /* kernels the unitig build launched */
+  uint64_t n_unitigs;
+  uint64_t n_corrected_reads;    /* SPK_F_CORRECT: reads with a corrected base */
+  float ms_correct;              /* SPK_F_CORRECT: device time of the correction */
+  uint32_t reserved2;
 } spk_result_info;
 
 int spk_result_count(const spk_result* res, int* n_k);

@@ -85,6 +85,17 @@ def lib():
         L.ora_unitigs_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ora_unitigs_free.restype = None
         L.ora_unitigs_free.argtypes = [C.c_void_p]
+        L.ora_packed_from_texts.restype = C.c_void_p
+        L.ora_packed_from_texts.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_char_p]
+        L.ora_packed_sidecar_get.restype = C.c_size_t
+        L.ora_packed_sidecar_get.argtypes = [C.c_void_p, C.c_size_t, C.c_char_p]
+        L.ora_bloom_load.restype = None
+        L.ora_bloom_load.argtypes = [C.c_void_p, u64p, u64p]
+        L.ora_correct_ascii.restype = C.c_int
+        L.ora_correct_ascii.argtypes = [C.c_void_p, C.c_uint, C.c_char_p, C.c_size_t]
+        L.ora_correct_packed.restype = C.c_size_t
+        L.ora_correct_packed.argtypes = [C.c_void_p, C.c_uint, C.c_void_p, C.c_size_t, C.c_void_p,
+                                         C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]
         L.ora_count_inject_priors.restype = None
         L.ora_count_inject_priors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_size_t, C.c_uint, C.c_uint32]
@@ -223,6 +234,31 @@ class Bloom:
         lib().ora_bloom_download(self.h, _p(seen, u64p), _p(solid, u64p))
         return seen, solid
 
+    def load(self, seen=None, solid=None):
+        """Overwrite the tiers with word arrays of num_words u64 each."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.uint64) for a in (seen, solid)]
+        for a in arrs:
+            assert a is None or a.size == self.num_words
+        lib().ora_bloom_load(self.h, *[None if a is None else _p(a, u64p) for a in arrs])
+
+    def correct_read(self, k: int, seq: str):
+        """ErrorCorrector::correct_read_in_place (hammer.rs:34-121): (read, changed)."""
+        b = C.create_string_buffer(seq.encode(), len(seq))
+        m = lib().ora_correct_ascii(self.h, k, b, len(seq))
+        return b.raw[: len(seq)].decode(), bool(m)
+
+    def correct_packed(self, k: int, data, offsets, lengths):
+        """Every packed read corrected as Stage 3 does (assemble.rs:183-191):
+        (corrected packed data, per-read flags uint8, number corrected)."""
+        d = np.ascontiguousarray(data, dtype=np.uint8)
+        o = np.ascontiguousarray(offsets, dtype=np.uint64)
+        ln = np.ascontiguousarray(lengths, dtype=np.uint32)
+        out = np.zeros(max(d.size, 1), dtype=np.uint8)
+        fl = np.zeros(max(ln.size, 1), dtype=np.uint8)
+        nc = lib().ora_correct_packed(self.h, k, d.ctypes.data, d.size, o.ctypes.data, ln.ctypes.data,
+                                      ln.size, out.ctypes.data, fl.ctypes.data)
+        return out[: d.size], fl[: ln.size], int(nc)
+
 
 class Packed:
     """PackedReads (packed_reads.rs:42-59) built by the oracle's ingest restatement."""
@@ -246,6 +282,26 @@ class Packed:
         la = la if la.size else np.zeros(1, np.uint64)
         lb = lb if lb.size else np.zeros(1, np.uint64)
         return Packed(lib().ora_packed_from_paired(a, _p(la, u64p), len(r1), b, _p(lb, u64p), len(r2)))
+
+    @staticmethod
+    def from_texts(t1: bytes, t2: bytes = None):
+        """FASTQ/FASTA texts (decompressed) as from_paired_files (two texts) or
+        append_from_file on an empty store (one text), packed_reads.rs:300-504.
+        Raises ValueError for a malformed text."""
+        err = C.create_string_buffer(256)
+        h = lib().ora_packed_from_texts(t1, len(t1), t2, len(t2) if t2 is not None else 0, err)
+        if not h:
+            raise ValueError(err.value.decode())
+        return Packed(h)
+
+    def sidecar(self):
+        out = []
+        for i in range(self.sizes()["n_sidecar"]):
+            n = lib().ora_packed_sidecar_get(self.h, i, None)
+            buf = C.create_string_buffer(max(n, 1))
+            lib().ora_packed_sidecar_get(self.h, i, buf)
+            out.append(buf.raw[:n])
+        return out
 
     def pack_clean(self, s):
         s = s.encode() if isinstance(s, str) else bytes(s)
@@ -314,14 +370,19 @@ class CountResult:
         return seen[:n], solid[:n]
 
     def stats(self):
-        o = (C.c_double * 5)()
+        o = (C.c_double * 6)()
         lib().ora_count_stats(self.h, o)
         return dict(occurrences=int(o[0]), admitted_occurrences=int(o[1]),
-                    seconds_stage2=o[2], seconds_stage3=o[3], seconds_total=o[4])
+                    seconds_stage2=o[2], seconds_stage3=o[3], seconds_total=o[4],
+                    corrected_reads=int(o[5]))
 
 
 def count(data, offsets, lengths, k: int, bloom_bits: int, mode: int = MODE_TWICE,
-          threads: int = 0, keep_bloom: bool = True) -> CountResult:
+          threads: int = 0, keep_bloom: bool = True, correct: bool = False) -> CountResult:
+    """assemble.rs:129-242.  correct: the error-correcting Stage 3
+    (config.error_correct, :183-191)."""
+    if correct:
+        mode |= 0x100
     data = np.ascontiguousarray(data, dtype=np.uint8)
     offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
     lengths = np.ascontiguousarray(lengths, dtype=np.uint32)

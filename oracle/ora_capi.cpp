@@ -7,6 +7,7 @@
 // limb 2 = hi bits 0..63, limb 3 = hi bits 64..127.  A k-mer list uses
 // ceil(k/32) limbs per key.
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -124,6 +125,25 @@ void ora_packed_copy(void* p, uint8_t* data, uint64_t* offsets, uint32_t* length
   if (offsets) memcpy(offsets, r->offsets.data(), r->offsets.size() * 8);
   if (lengths) memcpy(lengths, r->lengths.data(), r->lengths.size() * 4);
 }
+// FASTQ / FASTA texts (decompressed) ingested as from_paired_files (t2 != null)
+// or append_from_file on an empty store; null on a malformed text (*err_out
+// gets the message, up to 255 bytes).
+void* ora_packed_from_texts(const uint8_t* t1, size_t l1, const uint8_t* t2, size_t l2, char* err_out) {
+  PackedReads* r = new PackedReads();
+  std::string err;
+  const bool ok = t2 ? from_paired_texts(t1, l1, t2, l2, r, &err) : from_single_text(t1, l1, r, &err);
+  if (!ok) {
+    delete r;
+    if (err_out) snprintf(err_out, 256, "%s", err.c_str());
+    return nullptr;
+  }
+  return r;
+}
+size_t ora_packed_sidecar_get(void* p, size_t i, uint8_t* out) {
+  const std::string& s = ((PackedReads*)p)->ambiguous_sidecar[i];
+  if (out) memcpy(out, s.data(), s.size());
+  return s.size();
+}
 size_t ora_packed_get_read(void* p, size_t idx, uint8_t* out) {
   std::vector<uint8_t> buf;
   ((PackedReads*)p)->get_read(idx, buf);
@@ -142,10 +162,11 @@ void* ora_count(const uint8_t* data, size_t data_len, const uint64_t* offsets,
   pr.lengths.assign(lengths, lengths + n_reads);
   CountResult* r = new CountResult();
   if (threads <= 0) {
-    count_serial(pr, k, bloom_bits, (Mode)mode, r);
+    // mode bit 8: the error-correcting Stage 3 (assemble.rs:183-191)
+    count_serial(pr, k, bloom_bits, (Mode)(mode & 0xFF), r, (mode & 0x100) != 0);
     if (!keep_bloom) { r->seen.clear(); r->solid.clear(); }
   } else {
-    count_threaded(pr, k, bloom_bits, threads, (Mode)mode, keep_bloom != 0, r);
+    count_threaded(pr, k, bloom_bits, threads, (Mode)(mode & 0xFF), keep_bloom != 0, r, (mode & 0x100) != 0);
   }
   return r;
 }
@@ -176,6 +197,46 @@ void ora_unitigs_get(void* h, char* seqs, uint64_t* lengths, double* cov, uint64
   }
 }
 void ora_unitigs_free(void* h) { delete (std::vector<Unitig>*)h; }
+// Overwrites the filter's tiers (num_words words each; either may be null).
+void ora_bloom_load(void* f, const uint64_t* seen, const uint64_t* solid) {
+  auto* b = (TwoTierFilter*)f;
+  if (seen) memcpy(b->seen.data(), seen, b->num_words * 8);
+  if (solid) memcpy(b->solid.data(), solid, b->num_words * 8);
+}
+// ErrorCorrector::correct_read_in_place on one ASCII read, in place.
+int ora_correct_ascii(void* f, unsigned k, uint8_t* seq, size_t len) {
+  std::vector<uint8_t> v(seq, seq + len);
+  const bool m = correct_read_in_place(k, v, *(TwoTierFilter*)f);
+  memcpy(seq, v.data(), len);
+  return m ? 1 : 0;
+}
+// The Stage 3 use (src/assemble.rs:183-191): every packed read decoded,
+// corrected and its changed bases written back into a copy of the packed data
+// (out_data, data_len bytes); corrected[i] = 1 if read i changed.  Returns the
+// number of corrected reads.
+size_t ora_correct_packed(void* f, unsigned k, const uint8_t* data, size_t data_len, const uint64_t* offs,
+                          const uint32_t* lens, size_t n, uint8_t* out_data, uint8_t* corrected) {
+  memcpy(out_data, data, data_len);
+  size_t nc = 0;
+  std::vector<uint8_t> buf;
+  for (size_t r = 0; r < n; r++) {
+    const uint32_t L = lens[r];
+    buf.resize(L);
+    for (uint32_t j = 0; j < L; j++)
+      buf[j] = "ACGT"[(data[offs[r] + j / 4] >> (6 - 2 * (j % 4))) & 3];
+    const std::vector<uint8_t> before(buf);
+    const bool m = L >= k && correct_read_in_place(k, buf, *(TwoTierFilter*)f);
+    corrected[r] = m ? 1 : 0;
+    nc += m;
+    for (uint32_t j = 0; j < L; j++) {
+      if (buf[j] == before[j]) continue;
+      uint8_t& byte = out_data[offs[r] + j / 4];
+      const unsigned sh = 6 - 2 * (j % 4);
+      byte = (uint8_t)((byte & ~(3u << sh)) | ((unsigned)base_to_2bit(buf[j]) << sh));
+    }
+  }
+  return nc;
+}
 // prior contigs (ASCII) concatenated in seqs, contig i = seqs[offs[i] .. offs[i] + lens[i])
 void ora_count_inject_priors(void* r, const uint8_t* seqs, const uint64_t* offs, const uint32_t* lens,
                              size_t n, unsigned k, uint32_t boost) {
@@ -205,7 +266,7 @@ void ora_count_bloom(void* r, uint64_t* seen, uint64_t* solid) {
   if (seen) memcpy(seen, c->seen.data(), c->seen.size() * 8);
   if (solid) memcpy(solid, c->solid.data(), c->solid.size() * 8);
 }
-// out: occurrences, admitted_occurrences, stage2 s, stage3 s, total s
+// out: occurrences, admitted_occurrences, stage2 s, stage3 s, total s, corrected reads
 void ora_count_stats(void* r, double* out) {
   CountResult* c = (CountResult*)r;
   out[0] = (double)c->occurrences;
@@ -213,6 +274,7 @@ void ora_count_stats(void* r, double* out) {
   out[2] = c->seconds_stage2;
   out[3] = c->seconds_stage3;
   out[4] = c->seconds_total;
+  out[5] = (double)c->corrected_reads;
 }
 
 uint32_t ora_cutoff(const uint32_t* counts, size_t n, double min_coverage) {

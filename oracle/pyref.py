@@ -192,6 +192,50 @@ class TwoTierFilter:
         return self.num_words * 8 * 2
 
 
+def correct_read(seq: str, k: int, filt: TwoTierFilter):
+    """src/hammer.rs:34-121 on a string read against filt's solid tier:
+    (corrected read, changed).  Written over strings with a memo of window
+    solidity (the filter does not change during a correction)."""
+    if k == 0 or k > 128 or len(seq) < k:
+        return seq, False
+    memo = {}
+
+    def solid(w: str) -> bool:
+        if w not in memo:
+            x = k256_from_str(w, k)
+            memo[w] = x is not None and filt.is_solid_kmer256(k256_canonical(x, k)[0])
+        return memo[w]
+
+    cur = list(seq)
+    changed = False
+    n = len(cur)
+    for i in range(n - k + 1):
+        win = "".join(cur[i:i + k])
+        if k256_from_str(win, k) is None or solid(win):
+            continue
+        best, best_gain = None, 0
+        for off in range(k):
+            pos = i + off
+            lo, hi = max(pos - (k - 1), 0), min(pos, n - k)
+            others = [s for s in range(lo, hi + 1) if s != i]
+            base = sum(solid("".join(cur[s:s + k])) for s in others)
+            orig = cur[pos]
+            for c in "ACGT":
+                if c == orig.upper():
+                    continue
+                cur[pos] = c
+                if solid("".join(cur[i:i + k])):
+                    cnt = 1 + sum(solid("".join(cur[s:s + k])) for s in others)
+                    gain = max(cnt - base, 0)
+                    if gain > best_gain:
+                        best, best_gain = (pos, c), gain
+                cur[pos] = orig
+        if best is not None:
+            cur[best[0]] = best[1]
+            changed = True
+    return "".join(cur), changed
+
+
 def pack_reads(reads):
     """src/packed_reads.rs:547-578 for a list of clean ACGT strings -> (data, offsets, lengths)."""
     data = bytearray()

@@ -374,6 +374,106 @@ PackedReads from_paired_slices(const std::vector<std::string>& r1,
   return b1;
 }
 
+// packed_reads.rs:69-234 on a memory buffer.  Lines end at '\n' (the last one
+// may lack it); next_seq strips every trailing '\n' / '\r' of a line.
+bool fastx_records(const uint8_t* text, size_t len, std::vector<std::string>* out, std::string* err) {
+  size_t pos = 0;
+  // read_until(b'\n'): the next line with its terminator; false at EOF
+  auto next_line = [&](size_t* a, size_t* b) {
+    if (pos >= len) return false;
+    size_t e = pos;
+    while (e < len && text[e] != '\n') e++;
+    *a = pos;
+    *b = e < len ? e + 1 : e;
+    pos = *b;
+    return true;
+  };
+  auto strip = [&](size_t a, size_t b) {  // pop trailing \n and \r
+    while (b > a && (text[b - 1] == '\n' || text[b - 1] == '\r')) b--;
+    return b;
+  };
+  // open(): skip blank / whitespace-only leading lines (:87-112)
+  for (;;) {
+    if (pos >= len) return true;  // empty: no records
+    const uint8_t c0 = text[pos];
+    if (c0 == '\n' || c0 == '\r') {
+      size_t a, b;
+      next_line(&a, &b);
+      continue;
+    }
+    size_t e = pos;
+    while (e < len && text[e] != '\n') e++;
+    bool ws = true;
+    for (size_t i = pos; i < e; i++) ws &= (text[i] == ' ' || text[i] == '\t' || text[i] == '\r' ||
+                                           text[i] == '\x0c');  // u8::is_ascii_whitespace
+    if (ws) {
+      size_t a, b;
+      next_line(&a, &b);
+      continue;
+    }
+    break;
+  }
+  const bool fastq = text[pos] == '@';
+  if (!fastq && text[pos] != '>') {
+    *err = "expected '@' or '>' header";
+    return false;
+  }
+  size_t a, b;
+  if (!fastq) next_line(&a, &b);  // consume the first '>' header (:118-124)
+  for (;;) {
+    std::string seq;
+    if (fastq) {  // :146-212
+      size_t h0, h1;
+      for (;;) {
+        if (!next_line(&h0, &h1)) return true;
+        h1 = strip(h0, h1);
+        if (h1 > h0) break;  // blank lines between records are skipped
+      }
+      if (text[h0] != '@') { *err = "expected '@' header"; return false; }
+      size_t s0, s1;
+      if (!next_line(&s0, &s1)) { *err = "unexpected EOF waiting for sequence line"; return false; }
+      s1 = strip(s0, s1);
+      seq.assign((const char*)text + s0, s1 - s0);
+      size_t p0, p1;
+      if (!next_line(&p0, &p1)) { *err = "unexpected EOF waiting for '+' separator"; return false; }
+      if (p1 == p0 || text[p0] != '+') { *err = "expected '+' separator line"; return false; }
+      size_t q0, q1;
+      if (!next_line(&q0, &q1)) { *err = "unexpected EOF waiting for quality scores"; return false; }
+      q1 = strip(q0, q1);
+      if (q1 - q0 != seq.size()) { *err = "sequence length != quality length"; return false; }
+      out->push_back(std::move(seq));
+    } else {  // :214-231
+      for (;;) {
+        size_t l0, l1;
+        if (!next_line(&l0, &l1)) {
+          if (!seq.empty()) out->push_back(std::move(seq));
+          return true;
+        }
+        l1 = strip(l0, l1);
+        if (l1 > l0 && text[l0] == '>') break;
+        seq.append((const char*)text + l0, l1 - l0);
+      }
+      out->push_back(std::move(seq));
+    }
+  }
+}
+
+bool from_paired_texts(const uint8_t* t1, size_t l1, const uint8_t* t2, size_t l2, PackedReads* out,
+                       std::string* err) {
+  std::vector<std::string> a, b;
+  if (!fastx_records(t1, l1, &a, err) || !fastx_records(t2, l2, &b, err)) return false;
+  *out = from_paired_slices(a, b);  // pairs, then the longer file's tail into Block 3
+  return true;
+}
+
+bool from_single_text(const uint8_t* t, size_t l, PackedReads* out, std::string* err) {
+  std::vector<std::string> a;
+  if (!fastx_records(t, l, &a, err)) return false;
+  *out = PackedReads();
+  for (auto& r : a) out->ingest_read((const uint8_t*)r.data(), r.size());
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // Count map: open addressing with linear probing, grown at 7/8 load like
 // hashbrown's maximum load factor.  Storage only: its hash never reaches any
@@ -431,7 +531,7 @@ static void sort_entries(std::vector<CountEntry>& v) {
 
 // assemble.rs:129-161 (Stage 2) and 166-242 (Stage 3), serial order.
 void count_serial(const PackedReads& pr, unsigned k, uint64_t bloom_bits, Mode mode,
-                  CountResult* out) {
+                  CountResult* out, bool correct) {
   double t0 = now_s();
   TwoTierFilter f(bloom_bits);
   std::vector<uint8_t> buf;
@@ -450,10 +550,11 @@ void count_serial(const PackedReads& pr, unsigned k, uint64_t bloom_bits, Mode m
   }
   double t1 = now_s();
   KmerMap map(1024);
-  uint64_t adm = 0;
+  uint64_t adm = 0, ncorr = 0;
   for (size_t idx = 0; idx < pr.size(); idx++) {
     pr.get_read(idx, buf);
     if (buf.size() < k) continue;
+    if (correct && correct_read_in_place(k, buf, f)) ncorr++;  // assemble.rs:188-191
     for (size_t i = 0; i + k <= buf.size(); i++) {
       Kmer256 km;
       if (k256_from_bytes(buf.data() + i, k, k, &km)) {
@@ -470,6 +571,7 @@ void count_serial(const PackedReads& pr, unsigned k, uint64_t bloom_bits, Mode m
   out->solid = f.solid;
   out->occurrences = occ;
   out->admitted_occurrences = adm;
+  out->corrected_reads = ncorr;
   out->seconds_stage2 = t1 - t0;
   out->seconds_stage3 = t2 - t1;
   out->seconds_total = now_s() - t0;
@@ -478,7 +580,7 @@ void count_serial(const PackedReads& pr, unsigned k, uint64_t bloom_bits, Mode m
 // Threaded restatement (CPU baseline).  Chunking assemble.rs:137-139; rayon's
 // dynamic chunk scheduling is modelled by an atomic chunk cursor.
 void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int threads,
-                    Mode mode, bool keep_bloom, CountResult* out) {
+                    Mode mode, bool keep_bloom, CountResult* out, bool correct) {
   double t0 = now_s();
   if (threads < 1) threads = 1;
   uint64_t num_words = (bloom_bits + 63) / 64;
@@ -553,6 +655,12 @@ void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int 
   while (num_shards < size_t(threads) * 4) num_shards <<= 1;
   num_shards = std::min<size_t>(std::max<size_t>(num_shards, 8), 64);  // assemble.rs:167
   size_t shard_mask = num_shards - 1;
+  // config.error_correct (assemble.rs:183-191): the corrector reads the
+  // filter through a plain snapshot of the finished tiers.
+  TwoTierFilter snap(correct ? size_bits : 64);
+  if (correct)
+    for (uint64_t i = 0; i < num_words; i++) snap.solid[i] = solid[i].load(std::memory_order_relaxed);
+  std::atomic<uint64_t> corr_total{0};
   std::vector<std::mutex> locks(num_shards);
   std::vector<KmerMap> shards;
   for (size_t s = 0; s < num_shards; s++) shards.emplace_back(75000);  // assemble.rs:170
@@ -571,6 +679,7 @@ void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int 
       for (size_t idx = start; idx < end; idx++) {
         pr.get_read(idx, buf);
         if (buf.size() < k) continue;
+        if (correct && correct_read_in_place(k, buf, snap)) corr_total.fetch_add(1);
         for (size_t i = 0; i + k <= buf.size(); i++) {
           Kmer256 km;
           if (!k256_from_bytes(buf.data() + i, k, k, &km)) continue;
@@ -624,6 +733,7 @@ void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int 
   }
   out->occurrences = occ_total.load();
   out->admitted_occurrences = adm_total.load();
+  out->corrected_reads = corr_total.load();
   out->seconds_stage2 = t1 - t0;
   out->seconds_stage3 = t2 - t1;
   out->seconds_total = now_s() - t0;
@@ -823,6 +933,64 @@ std::vector<Unitig> unitigs(const std::vector<Kmer256>& solid, const std::vector
   }
   std::sort(out.begin(), out.end(), [](const Unitig& a, const Unitig& b) { return a.sequence < b.sequence; });
   return out;
+}
+
+// ---------------------------------------------------------------------------
+// src/hammer.rs
+// ---------------------------------------------------------------------------
+bool correct_read_in_place(unsigned k, std::vector<uint8_t>& seq, const TwoTierFilter& filter) {
+  if (k == 0 || k > 128 || seq.size() < k) return false;  // :41-43
+  std::vector<uint8_t> scratch(seq);                      // :45-46
+  bool modified = false;
+  const size_t n = scratch.size();
+  // from_bytes + canonical + is_solid_kmer256 of the window at s; None is not solid
+  auto solid_at = [&](size_t s) {
+    Kmer256 km;
+    if (!k256_from_bytes(scratch.data() + s, k, k, &km)) return false;
+    return filter.is_solid_kmer256(k256_canonical(km, k, nullptr));
+  };
+  for (size_t i = 0; i + k <= n; i++) {  // :49
+    Kmer256 km;
+    if (!k256_from_bytes(scratch.data() + i, k, k, &km)) continue;  // :50
+    if (filter.is_solid_kmer256(k256_canonical(km, k, nullptr))) continue;  // :51-52
+    bool have = false;
+    size_t best_off = 0;
+    uint8_t best_base = 0;
+    size_t max_gain = 0;
+    for (size_t offset = 0; offset < k; offset++) {  // :56
+      const size_t pos = i + offset;
+      const uint8_t orig = scratch[pos];
+      const uint8_t orig_upper = (orig >= 'a' && orig <= 'z') ? (uint8_t)(orig - 32) : orig;
+      const size_t start_scan = pos >= k - 1 ? pos - (k - 1) : 0;  // :60
+      const size_t end_scan = std::min(pos, n - k);                 // :61
+      size_t base_solid = 0;  // :63-74
+      for (size_t s = start_scan; s <= end_scan; s++)
+        if (s != i && solid_at(s)) base_solid++;
+      for (uint8_t cand : {(uint8_t)'A', (uint8_t)'C', (uint8_t)'G', (uint8_t)'T'}) {  // :76
+        if (cand == orig_upper) continue;
+        scratch[pos] = cand;
+        if (solid_at(i)) {  // :81-84
+          size_t solid_count = 1;
+          for (size_t s = start_scan; s <= end_scan; s++)
+            if (s != i && solid_at(s)) solid_count++;
+          const size_t gain = solid_count > base_solid ? solid_count - base_solid : 0;  // :99
+          if (gain > max_gain) {  // :100-103
+            max_gain = gain;
+            have = true;
+            best_off = offset;
+            best_base = cand;
+          }
+        }
+        scratch[pos] = orig;  // :106
+      }
+    }
+    if (have) {  // :111-115
+      seq[i + best_off] = best_base;
+      scratch[i + best_off] = best_base;
+      modified = true;
+    }
+  }
+  return modified;
 }
 
 }  // namespace ora

@@ -96,6 +96,15 @@ struct PackedReads {
 // packed_reads.rs:438-461 + 481-489 + 668-690
 PackedReads from_paired_slices(const std::vector<std::string>& r1,
                                const std::vector<std::string>& r2);
+// FastxReader::open + next_seq (packed_reads.rs:69-234) over an in-memory
+// (decompressed) FASTQ or FASTA text: the sequence of every record, in order.
+// false with *err set for a malformed text.
+bool fastx_records(const uint8_t* text, size_t len, std::vector<std::string>* out, std::string* err);
+// from_paired_files (packed_reads.rs:324-381) and append_from_file on an
+// empty store (packed_reads.rs:493-504) over in-memory texts.
+bool from_paired_texts(const uint8_t* t1, size_t l1, const uint8_t* t2, size_t l2, PackedReads* out,
+                       std::string* err);
+bool from_single_text(const uint8_t* t, size_t l, PackedReads* out, std::string* err);
 
 // ---- src/assemble.rs Stages 2-3 -------------------------------------------
 struct CountEntry { Kmer256 key; uint32_t count; };
@@ -106,18 +115,20 @@ struct CountResult {
   std::vector<uint64_t> solid;      // solid tier (REF) or twice tier (TWICE)
   uint64_t occurrences = 0;         // k-mer positions visited per pass
   uint64_t admitted_occurrences = 0;
+  uint64_t corrected_reads = 0;     // reads the Stage 3 error correction changed
   double seconds_stage2 = 0, seconds_stage3 = 0, seconds_total = 0;
 };
 
-// Serial restatement of assemble.rs:129-242 (no error correction): reads in
-// index order, positions left to right.
+// Serial restatement of assemble.rs:129-242: reads in index order, positions
+// left to right.  correct: the config.error_correct branch (:183-191), every
+// read corrected against the filter before its k-mers are counted.
 void count_serial(const PackedReads& pr, unsigned k, uint64_t bloom_bits, Mode mode,
-                  CountResult* out);
+                  CountResult* out, bool correct = false);
 // Threaded restatement used as the CPU baseline: same chunking
 // (assemble.rs:137-139), sharded maps behind mutexes with 256-entry local
 // buffers (assemble.rs:167-218), shard merge (assemble.rs:238-242).
 void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int threads,
-                    Mode mode, bool keep_bloom, CountResult* out);
+                    Mode mode, bool keep_bloom, CountResult* out, bool correct = false);
 
 // assemble.rs:692-735
 uint32_t determine_solid_kmer_cutoff(const std::vector<uint32_t>& counts, double min_coverage);
@@ -148,5 +159,9 @@ std::vector<Unitig> unitigs(const std::vector<Kmer256>& solid_sorted,
 // graph.rs:78-102: the (k+1)-mer edge set implied by get_successors over the
 // solid set, as canonical (k+1)-mers, sorted.
 std::vector<Kmer256> edges(const std::vector<Kmer256>& solid_sorted, unsigned k);
+
+// hammer.rs:34-121: ErrorCorrector::correct_read_in_place, single-base
+// substitutions against the filter's solid tier; true if a base changed.
+bool correct_read_in_place(unsigned k, std::vector<uint8_t>& seq, const TwoTierFilter& filter);
 
 }  // namespace ora

@@ -396,6 +396,13 @@ int spk_result_info_get(const spk_result* res, int ki, spk_result_info* info) {
   if ((rc = get_k(res, ki))) return rc;
   if (!info) return fail(SPK_E_INVALID_ARG, "null info");
   *info = res->ks[ki]->info;
+  const UnitigSet& u = res->ks[ki]->unitigs;
+  if (u.ready) {
+    info->ms_unitigs = u.ms_device;
+    info->ms_unitigs_host = u.ms_host;
+    info->unitig_launches = u.launches;
+    info->n_unitigs = u.lengths.size();
+  }
   return SPK_OK;
 }
 int spk_result_solid(spk_result* res, int ki, uint64_t* keys, uint32_t* counts, size_t* n) {

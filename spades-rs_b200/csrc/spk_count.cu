@@ -1792,13 +1792,14 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   ReadsView rv = rv_in;
   rv.err = errp;
   const bool ref = (o.flags & SPK_F_REF_SOLID) != 0;
-  const bool gated = (o.flags & SPK_F_GATED) != 0;
+  const bool correct = (o.flags & SPK_F_CORRECT) != 0;
+  const bool gated = (o.flags & SPK_F_GATED) != 0 || correct;
   // The reference-semantics solid tier depends on the order of the inserts,
   // so it needs the per-occurrence Bloom of the fused pass.
   const bool count_first = !gated && !ref;
   bool partitioned = count_first && nl <= 2 && !(o.flags & SPK_F_DIRECT);
 
-  Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1;
+  Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1, ec0, ec1;
   uint32_t launches = 0;
   SPK_CUDA(cudaEventRecord(e0.e, st));
 
@@ -2006,6 +2007,22 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   info.seen_popcount = host[S_POPS];
   info.twice_popcount = host[S_POPS + 1];
 
+  DevBuf cdata;  // SPK_F_CORRECT: the corrected copy of the packed reads
+  if (correct) {
+    // ---- Stage 3 error correction (src/assemble.rs:183-191) into a copy ----
+    if ((rc = cdata.alloc(rv.data_len + 128, st))) return rc;
+    SPK_CUDA(cudaMemsetAsync(cdata.as<uint8_t>() + rv.data_len, 0, 128, st));
+    SPK_CUDA(cudaEventRecord(ec0.e, st));
+    uint64_t nc = 0;
+    if ((rc = correct_reads(ctx, st, k, (const unsigned long long*)kr.twice.as<uint64_t>(), kr.fm,
+                            (const uint8_t*)rv.words + rv.byte_base, rv.data_len, rv.offsets, rv.lengths,
+                            rv.n_reads, cdata.as<uint8_t>(), nullptr, &nc, &launches)))
+      return rc;
+    SPK_CUDA(cudaEventRecord(ec1.e, st));
+    info.n_corrected_reads = nc;
+    rv.words = cdata.as<uint64_t>();
+    rv.byte_base = 0;
+  }
   if (gated) {
     // ---- gated: Stage 3 over admitted occurrences ----
     cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40))
@@ -2204,6 +2221,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   SPK_CUDA(cudaEventRecord(e6.e, st));
   SPK_CUDA(cudaStreamSynchronize(st));
   info.ms_bloom = ms_between(e0, e1);
+  info.ms_correct = correct ? ms_between(ec0, ec1) : 0.f;
   info.ms_count = ms_between(e1, e2);
   info.ms_finish = ms_between(e2, e3);
   info.ms_sort = ms_between(e3, e4);

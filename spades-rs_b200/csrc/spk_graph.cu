@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -164,69 +165,62 @@ __global__ void k_ug_links(const uint8_t* __restrict__ nsucc, const uint32_t* __
   }
 }
 
-// List ranking by pointer jumping.  J: jump pointer towards the head, D:
-// distance covered, R: the farthest node reached (the head once J is kNil).
-__global__ void k_ug_rank_init(const uint32_t* __restrict__ prev, uint64_t n2, uint32_t* __restrict__ J,
-                               uint32_t* __restrict__ D, uint32_t* __restrict__ R) {
+// List ranking by pointer jumping.  One 16-byte record per node (x: jump
+// pointer towards the head, y: distance covered, z: the farthest node
+// reached, which is the head once x is kNil), so a round gathers one record.
+__global__ void k_ug_rank_init(const uint32_t* __restrict__ prev, uint64_t n2, uint4* __restrict__ A) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n2;
        v += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t p = prev[v];
-    J[v] = p;
-    D[v] = p != kNil ? 1u : 0u;
-    R[v] = p != kNil ? p : (uint32_t)v;
+    A[v] = make_uint4(p, p != kNil ? 1u : 0u, p != kNil ? p : (uint32_t)v, 0u);
   }
 }
-__global__ void k_ug_rank_step(const uint32_t* __restrict__ J, const uint32_t* __restrict__ D,
-                               const uint32_t* __restrict__ R, uint64_t n2, uint32_t* __restrict__ J2,
-                               uint32_t* __restrict__ D2, uint32_t* __restrict__ R2) {
+__global__ void k_ug_rank_step(const uint4* __restrict__ A, uint64_t n2, uint4* __restrict__ B) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n2;
        v += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t j = J[v];
-    if (j != kNil) {
-      J2[v] = J[j];
-      D2[v] = D[v] + D[j];
-      R2[v] = R[j];
-    } else {
-      J2[v] = kNil;
-      D2[v] = D[v];
-      R2[v] = R[v];
+    uint4 r = A[v];
+    if (r.x != kNil) {
+      const uint4 q = A[r.x];
+      r = make_uint4(q.x, r.y + q.y, q.z, 0u);
     }
+    B[v] = r;
   }
 }
 
-// Cycles: nodes whose jump pointer is still set after enough rounds.  M: the
-// smallest node of the cycle, by pointer jumping along next.
-__global__ void k_ug_cyc_init(const uint32_t* __restrict__ J, const uint32_t* __restrict__ next, uint64_t n2,
-                              uint32_t* __restrict__ M, uint32_t* __restrict__ C) {
+// Cycles: nodes whose jump pointer is still set after enough rounds.  Per
+// node (x: the smallest node seen so far, y: the node 2^r steps ahead along
+// next), by pointer jumping along next; *ncyc counts the nodes on cycles.
+__global__ void k_ug_cyc_init(const uint4* __restrict__ A, const uint32_t* __restrict__ next, uint64_t n2,
+                              uint2* __restrict__ MC, unsigned long long* __restrict__ ncyc) {
+  uint32_t c = 0;
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n2;
        v += (uint64_t)gridDim.x * blockDim.x) {
-    const bool cyc = J[v] != kNil;
-    M[v] = cyc ? (uint32_t)v : kNil;
-    C[v] = cyc ? next[v] : kNil;
+    const bool cyc = A[v].x != kNil;
+    MC[v] = cyc ? make_uint2((uint32_t)v, next[v]) : make_uint2(kNil, kNil);
+    c += cyc;
   }
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(ncyc, (unsigned long long)c);
 }
-__global__ void k_ug_cyc_step(const uint32_t* __restrict__ M, const uint32_t* __restrict__ C, uint64_t n2,
-                              uint32_t* __restrict__ M2, uint32_t* __restrict__ C2) {
+__global__ void k_ug_cyc_step(const uint2* __restrict__ MC, uint64_t n2, uint2* __restrict__ MC2) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n2;
        v += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t c = C[v];
-    if (c != kNil) {
-      M2[v] = min(M[v], M[c]);
-      C2[v] = C[c];
-    } else {
-      M2[v] = M[v];
-      C2[v] = kNil;
+    uint2 m = MC[v];
+    if (m.y != kNil) {
+      const uint2 q = MC[m.y];
+      m = make_uint2(min(m.x, q.x), q.y);
     }
+    MC2[v] = m;
   }
 }
 // Cut every cycle before its smallest node; a cycle whose smallest node is a
 // reverse orientation is the twin of the cycle holding the forward one and is
 // dropped.  flags bit 0: on a cycle, bit 1: dropped.
-__global__ void k_ug_cut(const uint32_t* __restrict__ M, uint64_t n2, uint32_t* __restrict__ next,
+__global__ void k_ug_cut(const uint2* __restrict__ MC, uint64_t n2, uint32_t* __restrict__ next,
                          uint32_t* __restrict__ prev, uint8_t* __restrict__ flags) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n2;
        v += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t m = M[v];
+    const uint32_t m = MC[v].x;
     if (m == kNil) {
       flags[v] = 0;
       continue;
@@ -242,20 +236,21 @@ __global__ void k_ug_cut(const uint32_t* __restrict__ M, uint64_t n2, uint32_t* 
 // Tails: the kept chains (one per twin pair: the chain whose head is not
 // greater than the twin of its tail; cut cycles that were not dropped) and
 // their lengths, recorded at their heads.
-__global__ void k_ug_tails(const uint32_t* __restrict__ next, const uint32_t* __restrict__ R,
-                           const uint32_t* __restrict__ D, const uint8_t* __restrict__ flags, uint64_t n2,
-                           unsigned k, uint32_t* __restrict__ bytes, uint32_t* __restrict__ keep,
+__global__ void k_ug_tails(const uint32_t* __restrict__ next, const uint4* __restrict__ A,
+                           const uint8_t* __restrict__ flags, uint64_t n2, unsigned k,
+                           uint32_t* __restrict__ bytes, uint32_t* __restrict__ keep,
                            uint32_t* __restrict__ len) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n2;
        v += (uint64_t)gridDim.x * blockDim.x) {
     if (next[v] != kNil) continue;
-    const uint32_t h = R[v];
+    const uint4 a = A[v];
+    const uint32_t h = a.z;
     const bool cyc = flags[v] & 1u;
     const bool kept = cyc ? !(flags[v] & 2u) : h <= ((uint32_t)v ^ 1u);
     if (!kept) continue;
     keep[h] = 1;
-    len[h] = D[v] + 1;
-    bytes[h] = D[v] + k;
+    len[h] = a.y + 1;
+    bytes[h] = a.y + k;
   }
 }
 
@@ -264,8 +259,7 @@ __global__ void k_ug_tails(const uint32_t* __restrict__ next, const uint32_t* __
 // first k - 1 bases (build_unitig, src/graph.rs:159-177).  Coverage sums per
 // unitig (kmer_cov of each k-mer, src/graph.rs:162-168).
 template <int NL>
-__global__ void __launch_bounds__(kUgBlock) k_ug_spell(SolidView S, unsigned k, const uint32_t* __restrict__ R,
-                                                        const uint32_t* __restrict__ D,
+__global__ void __launch_bounds__(kUgBlock) k_ug_spell(SolidView S, unsigned k, const uint4* __restrict__ A,
                                                         const uint32_t* __restrict__ keep,
                                                         const uint32_t* __restrict__ off,
                                                         const uint32_t* __restrict__ uidx,
@@ -275,13 +269,14 @@ __global__ void __launch_bounds__(kUgBlock) k_ug_spell(SolidView S, unsigned k, 
                                                         uint32_t* __restrict__ ulen) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n2;
        v += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t h = R[v];
+    const uint4 a = A[v];
+    const uint32_t h = a.z;
     if (!keep[h]) continue;
     const uint32_t i = (uint32_t)(v >> 1);
     const Seq<NL> K = ug_key<NL>(S, i);
     const Seq<NL> X = (v & 1) ? revcomp<NL>(K, k) : K;
     const uint32_t o = off[h];
-    seq[o + k - 1 + D[v]] = "ACGT"[X.v[0] & 3];
+    seq[o + k - 1 + a.y] = "ACGT"[X.v[0] & 3];
     if (h == (uint32_t)v) {
       ulen[uidx[h]] = len[h];
       for (unsigned p = 0; p + 1 < k; p++) {
@@ -300,7 +295,8 @@ __global__ void __launch_bounds__(kUgBlock) k_ug_spell(SolidView S, unsigned k, 
 static unsigned ug_grid(spk_ctx* ctx) { return (unsigned)ctx->sm_count * 8; }
 
 template <int NL>
-static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches, UnitigSet& out) {
+static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches, UnitigSet& out,
+                  cudaEvent_t e_end) {
   const unsigned k = kr.k;
   const uint32_t cutoff = kr.info.cutoff;
   const uint64_t nl_list = kr.list_len;
@@ -316,7 +312,10 @@ static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches
   SPK_CUDA(cudaMemcpyAsync(&hn, pos.as<uint32_t>() + nl_list, 4, cudaMemcpyDeviceToHost, st));
   SPK_CUDA(cudaStreamSynchronize(st));
   const uint64_t n = hn;
-  if (n == 0) return SPK_OK;
+  if (n == 0) {
+    SPK_CUDA(cudaEventRecord(e_end, st));
+    return SPK_OK;
+  }
   if (2 * n >= kNil) return fail(SPK_E_INVALID_ARG, "unitigs: more than 2^31 solid k-mers");
   DevBuf sl[4], scnt;
   for (int j = 0; j < NL; j++)
@@ -354,22 +353,18 @@ static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches
   succ.release();
   if (launches) *launches += 6;
   // ---- list ranking; cycles found, cut and ranked again ----
-  DevBuf J[2], Dd[2], R[2];
+  DevBuf A[2];
   for (int b = 0; b < 2; b++)
-    if ((rc = J[b].alloc(n2 * 4, st)) || (rc = Dd[b].alloc(n2 * 4, st)) || (rc = R[b].alloc(n2 * 4, st)))
-      return rc;
+    if ((rc = A[b].alloc(n2 * 16, st))) return rc;
   int rounds = 1;
   while ((1ull << rounds) < n2) rounds++;
   rounds += 1;
   int cur = 0;
   auto rank = [&]() {
-    k_ug_rank_init<<<g, kUgBlock, 0, st>>>(prev.as<uint32_t>(), n2, J[0].as<uint32_t>(), Dd[0].as<uint32_t>(),
-                                           R[0].as<uint32_t>());
+    k_ug_rank_init<<<g, kUgBlock, 0, st>>>(prev.as<uint32_t>(), n2, A[0].as<uint4>());
     cur = 0;
     for (int r = 0; r < rounds; r++) {
-      k_ug_rank_step<<<g, kUgBlock, 0, st>>>(J[cur].as<uint32_t>(), Dd[cur].as<uint32_t>(), R[cur].as<uint32_t>(),
-                                             n2, J[cur ^ 1].as<uint32_t>(), Dd[cur ^ 1].as<uint32_t>(),
-                                             R[cur ^ 1].as<uint32_t>());
+      k_ug_rank_step<<<g, kUgBlock, 0, st>>>(A[cur].as<uint4>(), n2, A[cur ^ 1].as<uint4>());
       cur ^= 1;
     }
     if (launches) *launches += 1 + rounds;
@@ -378,23 +373,32 @@ static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches
   DevBuf flags;
   if ((rc = flags.alloc(n2, st))) return rc;
   {
-    // J[cur] != kNil marks the nodes on cycles; find each cycle's smallest node.
-    DevBuf M[2], Cc[2];
+    // A[cur].x != kNil marks the nodes on cycles; find each cycle's smallest node.
+    DevBuf MC[2], ncyc;
     for (int b = 0; b < 2; b++)
-      if ((rc = M[b].alloc(n2 * 4, st)) || (rc = Cc[b].alloc(n2 * 4, st))) return rc;
-    k_ug_cyc_init<<<g, kUgBlock, 0, st>>>(J[cur].as<uint32_t>(), next.as<uint32_t>(), n2, M[0].as<uint32_t>(),
-                                          Cc[0].as<uint32_t>());
-    int c = 0;
-    for (int r = 0; r < rounds; r++) {
-      k_ug_cyc_step<<<g, kUgBlock, 0, st>>>(M[c].as<uint32_t>(), Cc[c].as<uint32_t>(), n2,
-                                            M[c ^ 1].as<uint32_t>(), Cc[c ^ 1].as<uint32_t>());
-      c ^= 1;
+      if ((rc = MC[b].alloc(n2 * 8, st))) return rc;
+    if ((rc = ncyc.alloc(8, st))) return rc;
+    SPK_CUDA(cudaMemsetAsync(ncyc.p, 0, 8, st));
+    k_ug_cyc_init<<<g, kUgBlock, 0, st>>>(A[cur].as<uint4>(), next.as<uint32_t>(), n2, MC[0].as<uint2>(),
+                                          ncyc.as<unsigned long long>());
+    unsigned long long hc = 0;
+    SPK_CUDA(cudaMemcpyAsync(&hc, ncyc.p, 8, cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    if (launches) *launches += 1;
+    if (hc == 0) {
+      SPK_CUDA(cudaMemsetAsync(flags.p, 0, n2, st));  // no cycles: the ranking stands
+    } else {
+      int c = 0;
+      for (int r = 0; r < rounds; r++) {
+        k_ug_cyc_step<<<g, kUgBlock, 0, st>>>(MC[c].as<uint2>(), n2, MC[c ^ 1].as<uint2>());
+        c ^= 1;
+      }
+      k_ug_cut<<<g, kUgBlock, 0, st>>>(MC[c].as<uint2>(), n2, next.as<uint32_t>(), prev.as<uint32_t>(),
+                                       flags.as<uint8_t>());
+      if (launches) *launches += 1 + rounds;
+      rank();
     }
-    k_ug_cut<<<g, kUgBlock, 0, st>>>(M[c].as<uint32_t>(), n2, next.as<uint32_t>(), prev.as<uint32_t>(),
-                                     flags.as<uint8_t>());
-    if (launches) *launches += 2 + rounds;
   }
-  rank();
   // ---- kept chains, offsets, spelling ----
   DevBuf bytes, keep, len, uidx;
   if ((rc = bytes.alloc(n2 * 4 + 4, st)) || (rc = keep.alloc(n2 * 4 + 4, st)) || (rc = len.alloc(n2 * 4, st)) ||
@@ -402,9 +406,8 @@ static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches
     return rc;
   SPK_CUDA(cudaMemsetAsync(bytes.p, 0, n2 * 4 + 4, st));
   SPK_CUDA(cudaMemsetAsync(keep.p, 0, n2 * 4 + 4, st));
-  k_ug_tails<<<g, kUgBlock, 0, st>>>(next.as<uint32_t>(), R[cur].as<uint32_t>(), Dd[cur].as<uint32_t>(),
-                                     flags.as<uint8_t>(), n2, k, bytes.as<uint32_t>(), keep.as<uint32_t>(),
-                                     len.as<uint32_t>());
+  k_ug_tails<<<g, kUgBlock, 0, st>>>(next.as<uint32_t>(), A[cur].as<uint4>(), flags.as<uint8_t>(), n2, k,
+                                     bytes.as<uint32_t>(), keep.as<uint32_t>(), len.as<uint32_t>());
   SPK_CUDA(cudaMemcpyAsync(uidx.p, keep.p, n2 * 4 + 4, cudaMemcpyDeviceToDevice, st));
   if ((rc = scan_u32(st, uidx.as<uint32_t>(), n2 + 1, sums, launches))) return rc;
   uint32_t hv[2] = {0, 0};
@@ -420,8 +423,7 @@ static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches
       (rc = ulen.alloc(std::max<uint64_t>(nu, 1) * 4, st)))
     return rc;
   SPK_CUDA(cudaMemsetAsync(cov.p, 0, std::max<uint64_t>(nu, 1) * 8, st));
-  k_ug_spell<NL><<<g, kUgBlock, 0, st>>>(S, k, R[cur].as<uint32_t>(), Dd[cur].as<uint32_t>(),
-                                        keep.as<uint32_t>(), bytes.as<uint32_t>(), uidx.as<uint32_t>(),
+  k_ug_spell<NL><<<g, kUgBlock, 0, st>>>(S, k, A[cur].as<uint4>(), keep.as<uint32_t>(), bytes.as<uint32_t>(), uidx.as<uint32_t>(),
                                         len.as<uint32_t>(), n2, seq.as<char>(), cov.as<unsigned long long>(),
                                         ulen.as<uint32_t>());
   SPK_CUDA(cudaGetLastError());
@@ -436,7 +438,9 @@ static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches
     SPK_CUDA(cudaMemcpyAsync(&h_seq[0], seq.p, total, cudaMemcpyDeviceToHost, st));
     SPK_CUDA(cudaMemcpyAsync(h_cov.data(), cov.p, nu * 8, cudaMemcpyDeviceToHost, st));
   }
+  SPK_CUDA(cudaEventRecord(e_end, st));
   SPK_CUDA(cudaStreamSynchronize(st));
+  const auto t0 = std::chrono::steady_clock::now();
   std::vector<uint64_t> off(nu + 1, 0);
   for (uint64_t u = 0; u < nu; u++) off[u + 1] = off[u] + h_len[u] + k - 1;
   if (off[nu] != total) return fail(SPK_E_CUDA, "unitigs: spelled length mismatch");
@@ -477,6 +481,7 @@ static int ug_run(spk_ctx* ctx, cudaStream_t st, KResult& kr, uint32_t* launches
     out.kmers[r] = h_len[u];
     out.cov[r] = (double)h_cov[u] / (double)h_len[u];
   }
+  out.ms_host = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return SPK_OK;
 }
 
@@ -493,14 +498,13 @@ int build_unitigs(spk_result* res, int ki) {
   if (cudaEventRecord(e0, st) != cudaSuccess) rc = fail(SPK_E_CUDA, "event record");
   if (!rc) {
     switch (kr.nl) {
-      case 1: rc = ug_run<1>(res->ctx, st, kr, &u.launches, u); break;
-      case 2: rc = ug_run<2>(res->ctx, st, kr, &u.launches, u); break;
-      case 3: rc = ug_run<3>(res->ctx, st, kr, &u.launches, u); break;
-      default: rc = ug_run<4>(res->ctx, st, kr, &u.launches, u); break;
+      case 1: rc = ug_run<1>(res->ctx, st, kr, &u.launches, u, e1); break;
+      case 2: rc = ug_run<2>(res->ctx, st, kr, &u.launches, u, e1); break;
+      case 3: rc = ug_run<3>(res->ctx, st, kr, &u.launches, u, e1); break;
+      default: rc = ug_run<4>(res->ctx, st, kr, &u.launches, u, e1); break;
     }
   }
-  if (!rc && cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess)
-    cudaEventElapsedTime(&u.ms_device, e0, e1);
+  if (!rc && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&u.ms_device, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;

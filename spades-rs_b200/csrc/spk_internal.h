@@ -94,6 +94,7 @@ struct UnitigSet {
   std::vector<uint64_t> kmers;    // k-mers per unitig
   uint32_t launches = 0;          // kernels the build launched
   float ms_device = 0.f;          // device time of the build (kernels and copies)
+  float ms_host = 0.f;            // host time of the orientation and sort
 };
 
 struct KResult {
@@ -194,6 +195,13 @@ int radix_sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf*
 // a pinned host staging block (kStagingBytes).
 int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys, DevBuf* vals,
               uint64_t* h_staging, uint32_t* launches = nullptr);
+// ErrorCorrector::correct_read_in_place on every read (spk_correct.cu), against
+// a solid tier of size fm.d bits: d_out (data_len bytes, may equal d_data)
+// gets the packed data with the corrected bases; d_corr (nullable) a flag per
+// read; *nc the number of corrected reads.  Synchronises st.
+int correct_reads(spk_ctx* ctx, cudaStream_t st, unsigned k, const unsigned long long* tier, const FastMod& fm,
+                  const uint8_t* d_data, uint64_t data_len, const uint64_t* d_off, const uint32_t* d_len,
+                  uint64_t n, uint8_t* d_out, uint8_t* d_corr, uint64_t* nc, uint32_t* launches = nullptr);
 // Exclusive scan of u32 in place (spk_sort.cu).
 int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches = nullptr);
 // Ordered compaction of a sorted SoA list into AoS Kmer256 limbs; *m is the

@@ -13,6 +13,7 @@ SPK_F_REF_SOLID = 0x2
 SPK_F_KEEP_BLOOM = 0x4
 SPK_F_GATED = 0x8
 SPK_F_DIRECT = 0x10
+SPK_F_CORRECT = 0x20
 SPK_NOALLOC_MAX_KEYS = 65536
 SPK_SCHEDULE_GATED = 0
 SPK_SCHEDULE_FUSED = 1
@@ -60,7 +61,10 @@ class ResultInfo(C.Structure):
                 ("ms_total", C.c_float), ("ms_bloom_kernel", C.c_float),
                 ("ms_count_kernel", C.c_float), ("schedule", C.c_uint32),
                 ("part_rescatters", C.c_uint32), ("n_distinct", C.c_uint64),
-                ("ms_scatter_kernel", C.c_float), ("reserved_f", C.c_float)]
+                ("ms_scatter_kernel", C.c_float), ("ms_unitigs", C.c_float),
+                ("ms_unitigs_host", C.c_float), ("unitig_launches", C.c_uint32),
+                ("n_unitigs", C.c_uint64), ("n_corrected_reads", C.c_uint64),
+                ("ms_correct", C.c_float), ("reserved2", C.c_uint32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -97,6 +101,10 @@ _SIGS = [
     ("spk_bloom_is_solid_k256", C.c_int, [vp, u64p, C.c_size_t, u8p]),
     ("spk_bloom_download", C.c_int, [vp, u64p, u64p]),
     ("spk_bloom_insert_k256_noalloc", C.c_int, [vp, vp, C.c_uint64, vp, C.c_size_t, vp, vp]),
+    ("spk_bloom_correct_reads", C.c_int, [vp, C.c_uint32, vp, C.c_size_t, vp, vp, C.c_size_t, vp, vp,
+                                          u64p]),
+    ("spk_bloom_correct_reads_device", C.c_int, [vp, C.c_uint32, vp, C.c_size_t, vp, vp, C.c_size_t, vp,
+                                                 vp, u64p]),
     ("spk_count_opts_default", None, [C.POINTER(CountOpts)]),
     ("spk_count", C.c_int, [vp, vp, C.c_size_t, vp, vp, C.c_size_t, u32p, C.c_int,
                             C.POINTER(CountOpts), C.POINTER(vp)]),

@@ -152,6 +152,32 @@ class TwoTierFilter:
     def is_solid_kmer256(self, kmer: Kmer256) -> bool:
         return bool(self.is_solid_kmer256_batch(np.array([limbs_from_kmer256(kmer)], dtype=np.uint64))[0])
 
+    def correct_reads(self, packed, k: int):
+        """ErrorCorrector::correct_read_in_place (src/hammer.rs:34-121) on every
+        read, against this filter's solid tier, as Stage 3 does before counting
+        (src/assemble.rs:183-191).  Returns (PackedReads with the corrected
+        bases, per-read bool flags, number of corrected reads)."""
+        data, offsets, lengths = _as_arrays(packed)
+        d = np.ascontiguousarray(data, dtype=np.uint8)
+        o = np.ascontiguousarray(offsets, dtype=np.uint64)
+        ln = np.ascontiguousarray(lengths, dtype=np.uint32)
+        out = np.empty(max(d.size, 1), dtype=np.uint8)
+        flags = np.zeros(max(ln.size, 1), dtype=np.uint8)
+        nc = C.c_uint64(0)
+        check(lib().spk_bloom_correct_reads(self.h, k, d.ctypes.data, d.size, o.ctypes.data, ln.ctypes.data,
+                                            ln.size, out.ctypes.data, flags.ctypes.data, C.byref(nc)))
+        pe = getattr(packed, "pe_count", 0)
+        return (PackedReads(out[: d.size], o.copy(), ln.copy(), pe), flags[: ln.size].astype(bool),
+                int(nc.value))
+
+    def correct_read(self, seq: str, k: int) -> Tuple[str, bool]:
+        """One ACGT read, as correct_read_in_place on it: (read, changed)."""
+        pr = PackedReads.from_clean_reads([seq])
+        if len(pr.lengths) != 1 or int(pr.lengths[0]) != len(seq):
+            raise SpkError(1, "correct_read takes a read of A, C, G and T only")
+        out, flags, _ = self.correct_reads(pr, k)
+        return out.get_read(0), bool(flags[0])
+
     def download(self) -> Tuple[np.ndarray, np.ndarray]:
         """(seen_bits, solid_bits) word arrays of src/bloom.rs:19-21."""
         n = self.size_bits // 64

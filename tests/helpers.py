@@ -120,3 +120,43 @@ def reads_from(seqs, circle, rng, cov=30, rl=(90, 150)):
         take(s, len(s))
     take(circle + circle[:rl[1]], len(circle))
     return out
+
+
+# ---- error-correction cases -------------------------------------------------
+def correction_case(k, seed, genome_len=3000, n_reads=60, filter_bits=1 << 20):
+    """A genome whose canonical k-mers are inserted twice (solid), plus reads
+    drawn from it (either strand) with 0-4 substitutions, some of them
+    adjacent or at the read ends; a few reads shorter than k and a few longer
+    than 256 bases.  Returns (key list in insertion order as 4-limb rows,
+    reads as strings)."""
+    from oracle import pyref
+    rng = np.random.default_rng(seed)
+    g = rand_seq(rng, genome_len)
+    keys = []
+    for _ in range(2):
+        for i in range(len(g) - k + 1):
+            x = pyref.k256_canonical(pyref.k256_from_str(g[i:i + k], k), k)[0]
+            keys.append(pyref.limbs(x))
+    reads = []
+    for j in range(n_reads):
+        if j % 20 == 7:
+            L = int(rng.integers(max(1, k - 10), k))          # shorter than k
+        elif j % 20 == 11:
+            L = int(rng.integers(300, 900))                   # several words
+        else:
+            L = int(rng.integers(k + 5, 200))
+        L = min(L, len(g))
+        st = int(rng.integers(0, len(g) - L + 1))
+        r = list(g[st:st + L])
+        ne = int(rng.integers(0, 5))
+        for e in range(ne):
+            if e == 1 and rng.integers(0, 3) == 0:
+                p = min(L - 1, int(rng.integers(0, L)) + 1)  # may sit next to another error
+            elif rng.integers(0, 6) == 0:
+                p = int(rng.choice([0, L - 1]))               # read ends
+            else:
+                p = int(rng.integers(0, L))
+            r[p] = "ACGT"[("ACGT".index(r[p]) + int(rng.integers(1, 4))) % 4]
+        s = "".join(r)
+        reads.append(revcomp(s) if rng.integers(0, 2) else s)
+    return np.array(keys, dtype=np.uint64), reads
