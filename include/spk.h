@@ -153,6 +153,37 @@ int spk_bloom_correct_reads_device(spk_bloom* bloom, uint32_t k, const uint8_t* 
                                    const uint64_t* d_offsets, const uint32_t* d_lengths, size_t n_reads,
                                    uint8_t* d_data_out, uint8_t* d_corrected, uint64_t* n_corrected);
 
+/* ---- FASTQ / FASTA ingest (src/packed_reads.rs:69-690) ------------------
+ * PackedReads::from_paired_files (text2 != NULL) or append_from_file into an
+ * empty store (text2 == NULL) over decompressed FASTQ or FASTA texts (each
+ * text is detected on its own, as FastxReader::open does; gzip stays with the
+ * caller, as flate2 does in the reference).  The three gates and the
+ * three-block layout (src/packed_reads.rs:8-27): terminal N trim, pairs
+ * whose trimmed mates both have no internal N and MIN_K (21) bases or more
+ * go to Block 1 (R1) and Block 2 (R2), the N-split sub-reads of MIN_K bases
+ * or more of every other record go to Block 3, and records with no such
+ * sub-read go to the ambiguous sidecar.  The store stays on the device
+ * (spk_packed_device gives pointers for spk_count_device).  Malformed texts
+ * return SPK_E_INVALID_ARG with the reference's message.  Each text must be
+ * shorter than 4 GiB. */
+typedef struct spk_packed spk_packed;
+int spk_ingest(spk_ctx* ctx, const uint8_t* text1, size_t len1, const uint8_t* text2, size_t len2,
+               spk_packed** out);
+int spk_packed_info(const spk_packed* p, uint64_t* n_reads, uint64_t* data_len, uint64_t* pe_count,
+                    uint64_t* n_sidecar, uint64_t* sidecar_bytes);
+/* Device time of the ingest (text upload included) and its kernel launches. */
+int spk_packed_stats(const spk_packed* p, float* ms_device, uint32_t* kernel_launches);
+/* Host copies: data (data_len bytes), offsets / lengths (n_reads each), the
+ * sidecar reads concatenated (sidecar_bytes) and their lengths (n_sidecar).
+ * Any pointer may be NULL. */
+int spk_packed_download(spk_packed* p, uint8_t* data, uint64_t* offsets, uint32_t* lengths,
+                        uint8_t* sidecar, uint64_t* sidecar_lengths);
+/* Device pointers of the store (valid until spk_packed_free); data is padded
+ * for spk_count_device. */
+int spk_packed_device(spk_packed* p, const uint8_t** d_data, const uint64_t** d_offsets,
+                      const uint32_t** d_lengths);
+int spk_packed_free(spk_packed* p);
+
 /* ---- counting (src/assemble.rs:129-292, src/graph.rs:78-102) ------------ */
 #define SPK_F_EDGES      0x1u  /* build the (k+1)-mer edge list */
 #define SPK_F_REF_SOLID  0x2u  /* also build the reference-semantics solid tier */

@@ -89,6 +89,9 @@ def lib():
         L.ora_packed_from_texts.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_char_p]
         L.ora_packed_sidecar_get.restype = C.c_size_t
         L.ora_packed_sidecar_get.argtypes = [C.c_void_p, C.c_size_t, C.c_char_p]
+        L.ora_count_sample3.restype = C.c_void_p
+        L.ora_count_sample3.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t, C.c_uint,
+                                        C.c_uint64, C.c_int, C.c_int, C.c_size_t]
         L.ora_bloom_load.restype = None
         L.ora_bloom_load.argtypes = [C.c_void_p, u64p, u64p]
         L.ora_correct_ascii.restype = C.c_int
@@ -391,6 +394,18 @@ def count(data, offsets, lengths, k: int, bloom_bits: int, mode: int = MODE_TWIC
     ln = lengths if lengths.size else np.zeros(1, np.uint32)
     h = lib().ora_count(_p(d, u8p), data.size, _p(o, u64p), _p(ln, u32p), lengths.size, k,
                         C.c_uint64(bloom_bits), mode, threads, 1 if keep_bloom else 0)
+    return CountResult(h, k)
+
+
+def count_sample3(data, offsets, lengths, k: int, bloom_bits: int, threads: int, stage3_reads: int,
+                  mode: int = MODE_REF, correct: bool = True) -> CountResult:
+    """The threaded count (Stage 2 over every read) with Stage 3 over the first
+    stage3_reads reads only; stats() times both stages."""
+    d = np.ascontiguousarray(data, dtype=np.uint8)
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    ln = np.ascontiguousarray(lengths, dtype=np.uint32)
+    h = lib().ora_count_sample3(d.ctypes.data, d.size, o.ctypes.data, ln.ctypes.data, ln.size, k,
+                                bloom_bits, mode | (0x100 if correct else 0), threads, stage3_reads)
     return CountResult(h, k)
 
 

@@ -171,6 +171,18 @@ void* ora_count(const uint8_t* data, size_t data_len, const uint64_t* offsets,
   return r;
 }
 void ora_count_free(void* r) { delete (CountResult*)r; }
+// The threaded count with Stage 3 restricted to the first stage3_reads reads
+// (Stage 2 over all of them): a bounded sample of a full-size job's Stage 3.
+void* ora_count_sample3(const uint8_t* data, size_t data_len, const uint64_t* offsets, const uint32_t* lengths,
+                        size_t n_reads, unsigned k, uint64_t bloom_bits, int mode, int threads, size_t stage3_reads) {
+  PackedReads pr;
+  pr.data.assign(data, data + data_len);
+  pr.offsets.assign(offsets, offsets + n_reads);
+  pr.lengths.assign(lengths, lengths + n_reads);
+  CountResult* r = new CountResult();
+  count_threaded(pr, k, bloom_bits, threads, (Mode)(mode & 0xFF), false, r, (mode & 0x100) != 0, stage3_reads);
+  return r;
+}
 // Unitigs of a sorted solid list (keys as ceil(k/32) limbs): returns a handle.
 void* ora_unitigs(const uint64_t* keys, const uint32_t* counts, size_t n, unsigned k) {
   const unsigned L = nlimbs(k);

@@ -479,6 +479,60 @@ def from_paired_slices(r1, r2):
     return b1 + b2 + b3, len(b1), side
 
 
+def fastx_records(text: bytes):
+    """FastxReader::open + next_seq (src/packed_reads.rs:69-234) on a
+    decompressed text: the record sequences as bytes.  Raises ValueError on a
+    malformed text.  Written over a list of lines (the Rust reader streams)."""
+    raw = text.split(b"\n")
+    if raw and raw[-1] == b"":
+        raw.pop()  # a final '\n' ends the last line; it does not start another
+    lines = [(r, r.rstrip(b"\r\n")) for r in raw]
+    i = 0
+    ws = b" \t\r\x0c"
+    while i < len(lines) and all(c in ws for c in lines[i][0]):
+        i += 1  # open(): blank or whitespace-only leading lines
+    if i == len(lines):
+        return []
+    first = lines[i][0][:1]
+    out = []
+    if first == b"@":
+        while i < len(lines):
+            if lines[i][1] == b"":
+                i += 1
+                continue
+            if not lines[i][1].startswith(b"@"):
+                raise ValueError("expected '@' header")
+            if i + 1 >= len(lines):
+                raise ValueError("unexpected EOF waiting for sequence line")
+            seq = lines[i + 1][1]
+            if i + 2 >= len(lines):
+                raise ValueError("unexpected EOF waiting for '+' separator")
+            if not lines[i + 2][0].startswith(b"+"):
+                raise ValueError("expected '+' separator line")
+            if i + 3 >= len(lines):
+                raise ValueError("unexpected EOF waiting for quality scores")
+            if len(lines[i + 3][1]) != len(seq):
+                raise ValueError("sequence length != quality length")
+            out.append(seq)
+            i += 4
+        return out
+    if first != b">":
+        raise ValueError("expected '@' or '>' header")
+    i += 1
+    cur = b""
+    while i < len(lines):
+        c = lines[i][1]
+        if c.startswith(b">"):
+            out.append(cur)
+            cur = b""
+        else:
+            cur += c
+        i += 1
+    if cur:
+        out.append(cur)
+    return out
+
+
 def read_fastq_gz(path):
     """Sequence lines of a (gzipped) FASTQ file (src/packed_reads.rs:141-216, no validation)."""
     import gzip

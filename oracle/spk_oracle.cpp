@@ -580,7 +580,7 @@ void count_serial(const PackedReads& pr, unsigned k, uint64_t bloom_bits, Mode m
 // Threaded restatement (CPU baseline).  Chunking assemble.rs:137-139; rayon's
 // dynamic chunk scheduling is modelled by an atomic chunk cursor.
 void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int threads,
-                    Mode mode, bool keep_bloom, CountResult* out, bool correct) {
+                    Mode mode, bool keep_bloom, CountResult* out, bool correct, size_t stage3_reads) {
   double t0 = now_s();
   if (threads < 1) threads = 1;
   uint64_t num_words = (bloom_bits + 63) / 64;
@@ -666,14 +666,19 @@ void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int 
   for (size_t s = 0; s < num_shards; s++) shards.emplace_back(75000);  // assemble.rs:170
   std::atomic<uint64_t> adm_total{0};
   cursor.store(0);
+  // stage3_reads < n: Stage 3 over the first stage3_reads reads only (a timed
+  // sample of the full Stage 3 against the full filter)
+  const size_t n3 = std::min(n, stage3_reads);
+  const size_t chunk3 = std::min(chunk, std::max<size_t>(n3 / size_t(threads), 1));
+  const size_t num_chunks3 = n3 ? (n3 + chunk3 - 1) / chunk3 : 0;
   auto stage3 = [&]() {
     std::vector<uint8_t> buf;
     buf.reserve(512);
     uint64_t adm = 0;
     for (;;) {
       size_t c = cursor.fetch_add(1);
-      if (c >= num_chunks) break;
-      size_t start = c * chunk, end = std::min(start + chunk, n);
+      if (c >= num_chunks3) break;
+      size_t start = c * chunk3, end = std::min(start + chunk3, n3);
       std::vector<std::vector<Kmer256>> tb(num_shards);
       for (auto& v : tb) v.reserve(256);
       for (size_t idx = start; idx < end; idx++) {

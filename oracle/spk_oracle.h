@@ -12,6 +12,7 @@
 // algorithm, not a binding.
 #pragma once
 #include <cstddef>
+#include <climits>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -128,7 +129,8 @@ void count_serial(const PackedReads& pr, unsigned k, uint64_t bloom_bits, Mode m
 // (assemble.rs:137-139), sharded maps behind mutexes with 256-entry local
 // buffers (assemble.rs:167-218), shard merge (assemble.rs:238-242).
 void count_threaded(const PackedReads& pr, unsigned k, uint64_t bloom_bits, int threads,
-                    Mode mode, bool keep_bloom, CountResult* out, bool correct = false);
+                    Mode mode, bool keep_bloom, CountResult* out, bool correct = false,
+                    size_t stage3_reads = SIZE_MAX);
 
 // assemble.rs:692-735
 uint32_t determine_solid_kmer_cutoff(const std::vector<uint32_t>& counts, double min_coverage);

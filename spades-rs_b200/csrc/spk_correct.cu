@@ -161,24 +161,36 @@ __global__ void __launch_bounds__(kCorrWarps * 32) k_correct(const uint8_t* __re
         }
         if (next >= nw) break;
         i = next;
-        // trials t = 4 * offset + base, base != the current one
+        // trials t = 4 * offset + base, base != the current one: the lanes
+        // split the trials; the trials that make window i solid are then
+        // scored one by one, the lanes splitting the windows that cover the
+        // substituted base
         const Seq<NL> Vi = corr_window<NL>(W, i, k);
         uint32_t best = 0;
-        for (uint32_t t = lane; t < 4u * k; t += 32) {
-          const uint32_t o = t >> 2, c = t & 3u, pos = i + o;
-          if (c == corr_base(W, pos)) continue;
-          if (!corr_solid<NL>(T, corr_patch<NL>(Vi, o, c, k), k)) continue;
-          const uint32_t a = pos >= k - 1 ? pos - (k - 1) : 0;
-          const uint32_t b = min(pos, nw - 1);
-          uint32_t cnt = 1;
-          for (uint32_t s = a; s <= b; s++) {
-            if (s == i) continue;
-            cnt += corr_solid<NL>(T, corr_patch<NL>(corr_window<NL>(W, s, k), pos - s, c, k), k) ? 1u : 0u;
+        for (uint32_t t0 = 0; t0 < 4u * k; t0 += 32) {
+          const uint32_t t = t0 + lane;
+          bool hit = false;
+          if (t < 4u * k) {
+            const uint32_t o = t >> 2, c = t & 3u;
+            hit = c != corr_base(W, i + o) && corr_solid<NL>(T, corr_patch<NL>(Vi, o, c, k), k);
           }
-          const uint32_t base = corr_count(F, a, b);  // window i is unsolid: not counted
-          if (cnt > base) best = max(best, ((cnt - base) << 12) | (4095u - t));
+          uint32_t hits = __ballot_sync(0xffffffffu, hit);
+          while (hits) {
+            const uint32_t tt = t0 + (__ffs(hits) - 1);
+            hits &= hits - 1;
+            const uint32_t pos = i + (tt >> 2), c = tt & 3u;
+            const uint32_t a = pos >= k - 1 ? pos - (k - 1) : 0;
+            const uint32_t b = min(pos, nw - 1);
+            uint32_t cnt = 0;
+            for (uint32_t s = a + lane; s <= b; s += 32) {
+              if (s == i) continue;
+              cnt += corr_solid<NL>(T, corr_patch<NL>(corr_window<NL>(W, s, k), pos - s, c, k), k) ? 1u : 0u;
+            }
+            cnt = __reduce_add_sync(0xffffffffu, cnt) + 1u;  // + window i, solid by the trial
+            const uint32_t base = corr_count(F, a, b);       // window i is unsolid: not counted
+            if (cnt > base) best = max(best, ((cnt - base) << 12) | (4095u - tt));
+          }
         }
-        best = __reduce_max_sync(0xffffffffu, best);
         if (best) {
           const uint32_t t = 4095u - (best & 4095u);
           const uint32_t pos = i + (t >> 2), c = t & 3u;

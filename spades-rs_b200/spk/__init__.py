@@ -19,15 +19,15 @@ missing.
 from ._lib import (SPK_F_CORRECT, SPK_F_DIRECT, SPK_F_EDGES, SPK_F_GATED, SPK_F_KEEP_BLOOM, SPK_F_REF_SOLID,
                    SPK_SCHEDULE_COUNT_FIRST, SPK_SCHEDULE_FUSED, SPK_SCHEDULE_GATED,
                    SPK_SCHEDULE_PARTITIONED, SpkError, lib, lib_path, validate_k)
-from .api import (Context, CountResult, Job, PackedReads, Server, TwoTierFilter, count,
-                  count_batch, count_device, count_solid_kmers, default_context, kmer256_from_limbs,
+from .api import (Context, CountResult, DevicePackedReads, Job, PackedReads, Server, TwoTierFilter, count,
+                  count_batch, count_device, count_solid_kmers, default_context, ingest, kmer256_from_limbs,
                   limbs_from_kmer256, nlimbs)
 
 __all__ = [
     "SPK_F_CORRECT", "SPK_F_DIRECT", "SPK_F_EDGES", "SPK_F_GATED", "SPK_F_KEEP_BLOOM", "SPK_F_REF_SOLID",
     "SPK_SCHEDULE_COUNT_FIRST", "SPK_SCHEDULE_FUSED", "SPK_SCHEDULE_GATED", "SPK_SCHEDULE_PARTITIONED",
     "SpkError", "lib", "lib_path",
-    "validate_k", "Context", "CountResult", "Job", "PackedReads", "Server", "TwoTierFilter",
-    "count", "count_batch", "count_device", "count_solid_kmers", "default_context",
+    "validate_k", "Context", "CountResult", "DevicePackedReads", "Job", "PackedReads", "Server",
+    "TwoTierFilter", "count", "count_batch", "count_device", "count_solid_kmers", "default_context", "ingest",
     "kmer256_from_limbs", "limbs_from_kmer256", "nlimbs",
 ]

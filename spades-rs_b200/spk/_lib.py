@@ -105,6 +105,12 @@ _SIGS = [
                                           u64p]),
     ("spk_bloom_correct_reads_device", C.c_int, [vp, C.c_uint32, vp, C.c_size_t, vp, vp, C.c_size_t, vp,
                                                  vp, u64p]),
+    ("spk_ingest", C.c_int, [vp, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.POINTER(vp)]),
+    ("spk_packed_info", C.c_int, [vp, u64p, u64p, u64p, u64p, u64p]),
+    ("spk_packed_stats", C.c_int, [vp, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
+    ("spk_packed_download", C.c_int, [vp, vp, vp, vp, vp, vp]),
+    ("spk_packed_device", C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    ("spk_packed_free", C.c_int, [vp]),
     ("spk_count_opts_default", None, [C.POINTER(CountOpts)]),
     ("spk_count", C.c_int, [vp, vp, C.c_size_t, vp, vp, C.c_size_t, u32p, C.c_int,
                             C.POINTER(CountOpts), C.POINTER(vp)]),
@@ -133,7 +139,9 @@ EXPORTED = [s[0] for s in _SIGS]
 
 
 def lib_path() -> str:
-    return os.path.join(_PKG_ROOT, "libspk.so")
+    """The in-tree libspk.so, or the build named by $SPK_LIBRARY (for example a
+    build with other values of the launch-shape macros)."""
+    return os.environ.get("SPK_LIBRARY") or os.path.join(_PKG_ROOT, "libspk.so")
 
 
 def build(quiet: bool = True) -> str:

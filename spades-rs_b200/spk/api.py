@@ -415,6 +415,72 @@ def count_device(d_data: int, data_len: int, d_offsets: int, d_lengths: int, n_r
     return CountResult(h.value, ctx)
 
 
+class DevicePackedReads:
+    """A PackedReads store built on the device by spk_ingest from FASTQ/FASTA
+    texts (PackedReads::from_paired_files / append_from_file,
+    src/packed_reads.rs:300-504)."""
+
+    def __init__(self, text1: bytes, text2: Optional[bytes] = None, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        h = vp()
+        t1 = bytes(text1)
+        t2 = None if text2 is None else bytes(text2)
+        check(lib().spk_ingest(self.ctx.h, t1, len(t1), t2, 0 if t2 is None else len(t2), C.byref(h)))
+        self.h = h.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().spk_packed_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        v = [C.c_uint64() for _ in range(5)]
+        check(lib().spk_packed_info(self.h, *[C.byref(x) for x in v]))
+        ms, nl = C.c_float(), C.c_uint32()
+        check(lib().spk_packed_stats(self.h, C.byref(ms), C.byref(nl)))
+        return dict(n_reads=v[0].value, data_len=v[1].value, pe_count=v[2].value, n_sidecar=v[3].value,
+                    sidecar_bytes=v[4].value, ms_device=ms.value, kernel_launches=nl.value)
+
+    def download(self) -> Tuple[PackedReads, list]:
+        """(PackedReads on the host, sidecar reads as bytes)."""
+        i = self.info()
+        data = np.zeros(max(i["data_len"], 1), np.uint8)
+        offs = np.zeros(max(i["n_reads"], 1), np.uint64)
+        lens = np.zeros(max(i["n_reads"], 1), np.uint32)
+        sc = np.zeros(max(i["sidecar_bytes"], 1), np.uint8)
+        scl = np.zeros(max(i["n_sidecar"], 1), np.uint64)
+        check(lib().spk_packed_download(self.h, data.ctypes.data, offs.ctypes.data, lens.ctypes.data,
+                                        sc.ctypes.data, scl.ctypes.data))
+        side, o = [], 0
+        for n in scl[: i["n_sidecar"]].tolist():
+            side.append(sc[o:o + n].tobytes())
+            o += n
+        pr = PackedReads(data[: i["data_len"]], offs[: i["n_reads"]], lens[: i["n_reads"]], i["pe_count"])
+        return pr, side
+
+    def device(self) -> Tuple[int, int, int]:
+        d, o, ln = vp(), vp(), vp()
+        check(lib().spk_packed_device(self.h, C.byref(d), C.byref(o), C.byref(ln)))
+        return d.value or 0, o.value or 0, ln.value or 0
+
+    def count(self, ks, **opt_kw) -> "CountResult":
+        """spk_count_device on the resident store."""
+        i = self.info()
+        d, o, ln = self.device()
+        return count_device(d, i["data_len"], o, ln, i["n_reads"], ks, ctx=self.ctx, **opt_kw)
+
+
+def ingest(text1: bytes, text2: Optional[bytes] = None, ctx: Optional[Context] = None) -> DevicePackedReads:
+    """spk_ingest: FASTQ/FASTA text(s) to a device-resident PackedReads store."""
+    return DevicePackedReads(text1, text2, ctx)
+
+
 def count_solid_kmers(packed, k: int, bloom_bits: int = 512 << 20,
                       ctx: Optional[Context] = None) -> Dict[Kmer256, int]:
     """The Stage 2-3 seam: HashMap<Kmer256, u32> of the admitted k-mers with count >= 2.

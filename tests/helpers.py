@@ -160,3 +160,55 @@ def correction_case(k, seed, genome_len=3000, n_reads=60, filter_bits=1 << 20):
         s = "".join(r)
         reads.append(revcomp(s) if rng.integers(0, 2) else s)
     return np.array(keys, dtype=np.uint64), reads
+
+
+# ---- FASTQ / FASTA texts ---------------------------------------------------------
+def fastq_text(seqs, rng, crlf=False, blank_between=False, plus_name=False):
+    """A FASTQ text of the given sequences (bytes or str) with random qualities."""
+    nl = b"\r\n" if crlf else b"\n"
+    out = []
+    for i, s in enumerate(seqs):
+        s = s.encode() if isinstance(s, str) else bytes(s)
+        q = bytes(rng.integers(35, 75, len(s)).astype(np.uint8).tolist())
+        out.append(b"@read_%d/1" % i + nl + s + nl + (b"+read_%d" % i if plus_name else b"+") + nl + q + nl)
+        if blank_between and i % 3 == 0:
+            out.append(nl)
+    return b"".join(out)
+
+
+def fasta_text(seqs, width=60):
+    out = []
+    for i, s in enumerate(seqs):
+        s = s.encode() if isinstance(s, str) else bytes(s)
+        out.append(b">contig_%d some description\n" % i)
+        for j in range(0, len(s), width):
+            out.append(s[j:j + width] + b"\n")
+    return b"".join(out)
+
+
+def messy_reads(rng, n, genome=None):
+    """Reads with every case the ingest gates meet: leading/trailing N runs,
+    internal N (one or several, sub-reads short and long), all-N, lowercase,
+    other IUPAC letters, lengths 0..400 (and a few of 2000)."""
+    g = genome if genome is not None else rand_seq(rng, 20000)
+    out = []
+    for i in range(n):
+        kind = i % 10
+        L = int(rng.integers(0, 400)) if kind != 9 else 2000
+        st = int(rng.integers(0, max(1, len(g) - L)))
+        r = list(g[st:st + L])
+        if kind == 1 and L:
+            r[: int(rng.integers(1, 6))] = "N" * min(L, int(rng.integers(1, 6)))
+        if kind == 2 and L:
+            r[-int(rng.integers(1, 6)):] = "n" * min(L, int(rng.integers(1, 6)))
+        if kind in (3, 4) and L > 2:
+            for _ in range(1 if kind == 3 else int(rng.integers(2, 6))):
+                r[int(rng.integers(0, L))] = "N"
+        if kind == 5:
+            r = ["N"] * L
+        if kind == 6:
+            r = [c.lower() if rng.integers(0, 2) else c for c in r]
+        if kind == 7 and L:
+            r[int(rng.integers(0, L))] = "RYKMSWBDHV"[int(rng.integers(0, 10))]
+        out.append("".join(r))
+    return out
