@@ -709,6 +709,295 @@ __global__ void __launch_bounds__(kBlock) k_part_scatter(ReadsView R, unsigned k
   warp_add_u64(occ_out, occ);
 }
 
+// Two-level form of the read pass (k <= 64).  k_part_scatter appends every
+// key to its span's region with a 16-byte store of its own, and those
+// scattered stores, not the claims, bound it.  Here the keys are partitioned
+// twice, each time through shared memory, so every global store is part of a
+// contiguous run:
+//   k_part_coarse  one read per thread; per round each thread rolls
+//                  kCoarseW windows into a shared-memory tile, the tile is
+//                  counting-sorted by coarse bucket (the top kCoarseBits bits
+//                  of the span index), each bucket's run is reserved with one
+//                  atomic and written out contiguously.
+//   k_part_fine    chunks of a coarse bucket's keys are sorted the same way
+//                  by span and written to the span regions k_part_count reads.
+// The keys, and the home bits packed into them, are those k_part_scatter
+// writes; only the order inside a region differs, and k_part_count is
+// order-free.
+constexpr uint32_t kCoarseBits = 6;
+constexpr uint32_t kCoarse = 1u << kCoarseBits;
+constexpr int kCoarseBlock = 512;
+constexpr int kCoarseW = 4;                              // windows per thread per round
+constexpr uint32_t kCoarseSlots = kCoarseBlock * kCoarseW;
+constexpr int kFineBlock = 512;
+constexpr uint32_t kFineChunk = 2048;                    // keys per chunk
+constexpr uint32_t kFineMaxBits = 12;                    // spans per coarse bucket <= 2^12
+
+struct CoarseView {
+  uint64_t* keys;        // NL u64 per entry
+  const uint64_t* base;  // bucket b = entries [base[b], base[b + 1]) when uniform == 0
+  unsigned int* fill;    // entries appended to bucket b: fill[b * kFillStride]
+  uint64_t uniform;      // > 0: base[b] = b * uniform
+  int* err;              // bit 3: a bucket overflowed
+};
+__device__ __forceinline__ uint64_t coarse_base(const CoarseView& cv, uint32_t b) {
+  return cv.uniform ? (uint64_t)b * cv.uniform : cv.base[b];
+}
+__device__ __forceinline__ uint64_t region_base(const PartView& pv, uint32_t p) {
+  return pv.uniform ? (uint64_t)p * pv.uniform : pv.base[p];
+}
+
+template <int NL>
+size_t coarse_smem() {
+  return (size_t)kCoarseSlots * NL * 8 * 2 + kCoarseSlots * (1 + 1 + 2) + kCoarse * (4 + 4 + 8);
+}
+
+template <int NL>
+__global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, unsigned k, PartView pv,
+                                                                 CoarseView cv,
+                                                                 unsigned long long* __restrict__ occ_out) {
+  extern __shared__ __align__(16) unsigned char cs_smem[];
+  uint64_t* ks = (uint64_t*)cs_smem;                       // keys by slot
+  uint64_t* ss = ks + kCoarseSlots * NL;                   // keys sorted by bucket
+  unsigned long long* gbase = (unsigned long long*)(ss + kCoarseSlots * NL);
+  uint32_t* hist = (uint32_t*)(gbase + kCoarse);
+  uint32_t* start = hist + kCoarse;
+  uint16_t* rk = (uint16_t*)(start + kCoarse);             // rank of a slot in its bucket
+  uint8_t* bk = (uint8_t*)(rk + kCoarseSlots);             // bucket of a slot (0xFF: none)
+  uint8_t* sb = bk + kCoarseSlots;                         // bucket of a sorted position
+  const unsigned topsh = 2 * k - 2 - 64 * (NL - 1);
+  const uint64_t topmask = (2 * k - 64 * (NL - 1)) >= 64 ? ~0ULL : ((1ULL << (2 * k - 64 * (NL - 1))) - 1);
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t fshift = pv.log2parts - kCoarseBits;      // span index -> bucket
+  if (threadIdx.x < kCoarse) hist[threadIdx.x] = 0;
+  uint64_t occ = 0;
+  const uint64_t ntiles = (R.n_reads + blockDim.x - 1) / blockDim.x;
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint64_t r = tile * blockDim.x + threadIdx.x;
+    uint32_t np = 0;
+    uint64_t bit0 = 0;
+    if (r < R.n_reads) {
+      const uint32_t len = __ldg(R.lengths + r);
+      const uint64_t off = __ldg(R.offsets + r);
+      if (off + ((uint64_t)len + 3) / 4 > R.data_len) {  // src/packed_reads.rs:600-602
+        atomicOr(R.err, 4);
+      } else if (len >= k) {
+        np = len - k + 1;
+        bit0 = 8ull * (R.byte_base + off);
+      }
+    }
+    Seq<NL> V, Rc;
+    if (np) {
+      V = extract<NL>(R.words, bit0, k);
+      Rc = revcomp<NL>(V, k);
+    }
+    uint64_t buf = 0, nextbit = bit0 + 2ull * k;
+    unsigned bleft = 0;
+    uint32_t i = 0;
+    while (__syncthreads_or(i < np)) {
+      // ---- roll up to kCoarseW windows into the tile ----
+#pragma unroll
+      for (int w = 0; w < kCoarseW; w++) {
+        const uint32_t slot = threadIdx.x * kCoarseW + w;
+        uint8_t b = 0xFF;
+        if (i < np) {
+          if (i > 0) {
+            if (bleft == 0) {
+              buf = extract<1>(R.words, nextbit, 32).v[0];
+              bleft = 32;
+            }
+            const uint64_t bb = buf >> 62;
+            buf <<= 2;
+            bleft--;
+            nextbit += 2;
+            if (NL == 1) {
+              V.v[0] = ((V.v[0] << 2) | bb) & topmask;
+              Rc.v[0] = (Rc.v[0] >> 2) | ((3 - bb) << topsh);
+            } else {
+              V.v[NL - 1] = ((V.v[NL - 1] << 2) | (V.v[0] >> 62)) & topmask;
+              V.v[0] = (V.v[0] << 2) | bb;
+              Rc.v[0] = (Rc.v[0] >> 2) | (Rc.v[NL - 1] << 62);
+              Rc.v[NL - 1] = (Rc.v[NL - 1] >> 2) | ((3 - bb) << topsh);
+            }
+          }
+          Seq<NL> C = seq_le<NL>(V, Rc) ? V : Rc;  // canonical, src/dna.rs:185-192
+          i++;
+          occ++;
+          uint64_t w4[4];
+          kmer256_limbs<NL>(C, k, w4);
+          const uint64_t raw0 = hash_seed(hash_pre(w4), kSeed1);
+          const uint32_t p = (uint32_t)(raw0 >> (64 - pv.log2parts));  // log2parts > kCoarseBits
+          if (pv.packed_home)
+            C.v[NL - 1] |= (raw0 << pv.log2parts) >> (64 - kHomeBits) << (64 - kHomeBits);
+          b = (uint8_t)(p >> fshift);
+#pragma unroll
+          for (int j = 0; j < NL; j++) ks[slot * NL + j] = C.v[j];
+          rk[slot] = (uint16_t)atomicAdd(&hist[b], 1u);
+        }
+        bk[slot] = b;
+      }
+      __syncthreads();
+      // ---- bucket starts in the tile, and one reservation per bucket ----
+      if (threadIdx.x < 32) {
+        const uint32_t h0 = hist[2 * lane], h1 = hist[2 * lane + 1];
+        uint32_t x = h0 + h1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+          if ((int)lane >= d) x += y;
+        }
+        const uint32_t ex = x - h0 - h1;
+        start[2 * lane] = ex;
+        start[2 * lane + 1] = ex + h0;
+        gbase[2 * lane] = h0 ? coarse_base(cv, 2 * lane) + atomicAdd(cv.fill + (uint64_t)(2 * lane) * kFillStride, h0) : 0;
+        gbase[2 * lane + 1] =
+            h1 ? coarse_base(cv, 2 * lane + 1) + atomicAdd(cv.fill + (uint64_t)(2 * lane + 1) * kFillStride, h1) : 0;
+      }
+      __syncthreads();
+      for (uint32_t slot = threadIdx.x; slot < kCoarseSlots; slot += blockDim.x) {
+        const uint8_t b = bk[slot];
+        if (b == 0xFF) continue;
+        const uint32_t pos = start[b] + rk[slot];
+#pragma unroll
+        for (int j = 0; j < NL; j++) ss[pos * NL + j] = ks[slot * NL + j];
+        sb[pos] = b;
+      }
+      __syncthreads();
+      // ---- contiguous runs out ----
+      const uint32_t total = start[kCoarse - 1] + hist[kCoarse - 1];
+      for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+        const uint32_t b = sb[j];
+        const uint64_t gi = gbase[b] + (j - start[b]);
+        const uint64_t end = cv.uniform ? (uint64_t)(b + 1) * cv.uniform : cv.base[b + 1];
+        if (gi < end) {
+          if (NL == 1) cv.keys[gi] = ss[j];
+          else *(ulonglong2*)(cv.keys + 2 * gi) = make_ulonglong2(ss[2 * j], ss[2 * j + 1]);
+        } else {
+          atomicOr(cv.err, (int)kErrRegion);
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x < kCoarse) hist[threadIdx.x] = 0;
+    }
+  }
+  warp_add_u64(occ_out, occ);
+}
+
+// cfirst[b] = the first chunk of bucket b (kFineChunk keys per chunk);
+// cfirst[kCoarse] = the number of chunks.  One warp.
+__global__ void k_coarse_chunks(const unsigned int* __restrict__ fill, uint32_t* __restrict__ cfirst) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t c0 = (fill[(2 * lane) * kFillStride] + kFineChunk - 1) / kFineChunk;
+  const uint32_t c1 = (fill[(2 * lane + 1) * kFillStride] + kFineChunk - 1) / kFineChunk;
+  uint32_t x = c0 + c1;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if ((int)lane >= d) x += y;
+  }
+  cfirst[2 * lane] = x - c0 - c1;
+  cfirst[2 * lane + 1] = x - c1;
+  if (lane == 31) cfirst[kCoarse] = x;
+}
+
+template <int NL>
+size_t fine_smem(uint32_t nfine) {
+  return (size_t)kFineChunk * NL * 8 * 2 + (size_t)kFineChunk * (2 + 2 + 2) + (size_t)nfine * (8 + 4 + 4) + 64;
+}
+
+template <int NL>
+__global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, const uint32_t* __restrict__ cfirst,
+                                                             PartView pv, unsigned k) {
+  extern __shared__ __align__(16) unsigned char fs_smem[];
+  const uint32_t fbits = pv.log2parts - kCoarseBits, nfine = 1u << fbits;
+  uint64_t* ks = (uint64_t*)fs_smem;
+  uint64_t* ss = ks + kFineChunk * NL;
+  unsigned long long* gbase = (unsigned long long*)(ss + kFineChunk * NL);
+  uint32_t* hist = (uint32_t*)(gbase + nfine);
+  uint32_t* start = hist + nfine;
+  uint16_t* fb = (uint16_t*)(start + nfine);  // span (in the bucket) of a loaded key
+  uint16_t* rk = fb + kFineChunk;             // its rank in that span
+  uint16_t* sf = rk + kFineChunk;             // span of a sorted position
+  __shared__ uint32_t wsum[kFineBlock / 32];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t nchunks = cfirst[kCoarse];
+  for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    uint32_t b = 0;  // cfirst[b] <= c < cfirst[b + 1]
+    for (uint32_t step = kCoarse >> 1; step; step >>= 1)
+      if (cfirst[b + step] <= c) b += step;
+    const uint64_t bb = coarse_base(cv, b);
+    const uint64_t bend = bb + cv.fill[(uint64_t)b * kFillStride];
+    const uint64_t s0 = bb + (uint64_t)(c - cfirst[b]) * kFineChunk;
+    const uint32_t n = (uint32_t)min((uint64_t)kFineChunk, bend - s0);
+    for (uint32_t f = threadIdx.x; f < nfine; f += blockDim.x) hist[f] = 0;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+      Seq<NL> C;
+      if (NL == 1) {
+        C.v[0] = __ldcs(cv.keys + s0 + j);
+      } else {
+        const ulonglong2 v = __ldcs((const ulonglong2*)(cv.keys + 2 * (s0 + j)));
+        C.v[0] = v.x;
+        C.v[NL - 1] = v.y;
+      }
+#pragma unroll
+      for (int q = 0; q < NL; q++) ks[j * NL + q] = C.v[q];
+      if (pv.packed_home) C.v[NL - 1] &= ~0ULL >> kHomeBits;
+      uint64_t w4[4];
+      kmer256_limbs<NL>(C, k, w4);
+      const uint32_t p = (uint32_t)(hash_seed(hash_pre(w4), kSeed1) >> (64 - pv.log2parts));
+      const uint32_t f = p & (nfine - 1);
+      fb[j] = (uint16_t)f;
+      rk[j] = (uint16_t)atomicAdd(&hist[f], 1u);
+    }
+    __syncthreads();
+    // exclusive scan of hist (each thread a run of consecutive spans)
+    const uint32_t per = (nfine + blockDim.x - 1) / blockDim.x;
+    const uint32_t f0 = min(nfine, threadIdx.x * per), f1 = min(nfine, f0 + per);
+    uint32_t run = 0;
+    for (uint32_t f = f0; f < f1; f++) run += hist[f];
+    uint32_t x = run;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+      if ((int)lane >= d) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    uint32_t before = x - run;
+    for (unsigned w = 0; w < warp; w++) before += wsum[w];
+    for (uint32_t f = f0; f < f1; f++) {
+      const uint32_t h = hist[f];
+      start[f] = before;
+      before += h;
+      const uint32_t pg = (b << fbits) | f;
+      gbase[f] = h ? region_base(pv, pg) + atomicAdd(pv.fill + (uint64_t)pg * kFillStride, h) : 0ULL;
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+      const uint32_t f = fb[j];
+      const uint32_t pos = start[f] + rk[j];
+#pragma unroll
+      for (int q = 0; q < NL; q++) ss[pos * NL + q] = ks[j * NL + q];
+      sf[pos] = (uint16_t)f;
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+      const uint32_t f = sf[j];
+      const uint32_t pg = (b << fbits) | f;
+      const uint64_t gi = gbase[f] + (j - start[f]);
+      const uint64_t end = pv.uniform ? (uint64_t)(pg + 1) * pv.uniform : pv.base[pg + 1];
+      if (gi < end) {
+        if (NL == 1) pv.keys[gi] = ss[j];
+        else *(ulonglong2*)(pv.keys + 2 * gi) = make_ulonglong2(ss[2 * j], ss[2 * j + 1]);
+      } else {
+        atomicOr(pv.err, (int)kErrRegion);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Shared-memory slots of one span: keys (8 or 16 bytes) then u32 counts.
 template <int NL>
 struct SpanKey;
@@ -1595,6 +1884,25 @@ static void launch_part_scatter(spk_ctx* ctx, cudaStream_t st, const ReadsView& 
                                 const PartView& pv, unsigned long long* occ) {
   k_part_scatter<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(rv, k, pv, occ);
 }
+#ifndef SPK_TWO_LEVEL
+#define SPK_TWO_LEVEL 1
+#endif
+template <int NL>
+static int launch_part_coarse(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
+                              const PartView& pv, const CoarseView& cv, unsigned long long* occ) {
+  const size_t smem = coarse_smem<NL>();
+  SPK_CUDA(cudaFuncSetAttribute(k_part_coarse<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_part_coarse<NL><<<grid_for(ctx, 2), kCoarseBlock, smem, st>>>(rv, k, pv, cv, occ);
+  return SPK_OK;
+}
+template <int NL>
+static int launch_part_fine(spk_ctx* ctx, cudaStream_t st, const CoarseView& cv, const uint32_t* cfirst,
+                            const PartView& pv, unsigned k) {
+  const size_t smem = fine_smem<NL>(1u << (pv.log2parts - kCoarseBits));
+  SPK_CUDA(cudaFuncSetAttribute(k_part_fine<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_part_fine<NL><<<grid_for(ctx, 2), kFineBlock, smem, st>>>(cv, cfirst, pv, k);
+  return SPK_OK;
+}
 // rv.ops == nullptr: apply the Bloom operations to the interleaved tiers
 // directly; else bin them by range into rv.
 template <int NL>
@@ -1840,12 +2148,15 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     if ((rc = fetch(S_OCC0 + 1))) return rc;
     const uint64_t occ0 = host[S_OCC0];
     cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(occ0);
+    bool two_level_fits = false;
     if (partitioned) {
       // Regions hold 1.5x the mean share of occurrences per span: keep them
       // within a quarter of the device memory, else count with global atomics.
+      // The two-level pass also holds the coarse buckets (1.125x) meanwhile.
       size_t fr = 0, tot = 0;
       SPK_CUDA(cudaMemGetInfo(&fr, &tot));
       partitioned = (occ0 + (occ0 >> 1) + (1u << 20)) * (uint64_t)nl * 8 <= tot / 4;
+      two_level_fits = (occ0 * 3 + (1u << 22)) * (uint64_t)nl * 8 <= tot / 4;
     }
     for (int attempt = 0; partitioned; attempt++) {
       if (!use_ops && (rc = reset_tiers())) return rc;
@@ -1867,6 +2178,71 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
       PartView pv{region.as<uint64_t>(), base.as<uint64_t>(), fill.as<unsigned int>(), capu, log2parts,
                   home_fits(k, nl) ? 1u : 0u, errp};
       SPK_CUDA(cudaEventRecord(ks0.e, st));
+      const bool two_level = SPK_TWO_LEVEL && two_level_fits && log2parts > kCoarseBits &&
+                             log2parts - kCoarseBits <= kFineMaxBits;
+      if (two_level) {
+        // ---- coarse buckets, then spans (k_part_coarse, k_part_fine) ----
+        DevBuf cbase, cfill, cregion, cfirst;
+        const uint64_t cper = occ0 / kCoarse;
+        const uint64_t ccap = cper + (cper >> 3) + 8192;
+        if ((rc = cbase.alloc((kCoarse + 1) * 8, st)) || (rc = cfill.alloc(kCoarse * 4 * kFillStride, st)) ||
+            (rc = cregion.alloc(kCoarse * ccap * nl * 8, st)) || (rc = cfirst.alloc((kCoarse + 1) * 4, st)))
+          return rc;
+        k_part_uniform<<<1, 128, 0, st>>>(kCoarse, ccap, cbase.as<uint64_t>());
+        SPK_CUDA(cudaMemsetAsync(cfill.p, 0, kCoarse * 4 * kFillStride, st));
+        CoarseView cv{cregion.as<uint64_t>(), cbase.as<uint64_t>(), cfill.as<unsigned int>(), ccap, errp};
+        if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rv, k, pv, cv, su + S_OCC);
+        else rc = launch_part_coarse<2>(ctx, st, rv, k, pv, cv, su + S_OCC);
+        if (rc) return rc;
+        SPK_CUDA(cudaGetLastError());
+        launches += 2;  // k_part_uniform, k_part_coarse
+        if ((rc = fetch(S_ERR + 1))) return rc;
+        if ((int)host[S_ERR] & kErrRegion) {
+          // A bucket outgrew its share: exact buckets from the fill counts.
+          k_part_bases<<<1, 1024, 0, st>>>(cfill.as<unsigned int>(), kCoarse, cbase.as<uint64_t>());
+          SPK_CUDA(cudaMemcpyAsync(host + S_WORDS, cbase.as<uint64_t>() + kCoarse, 8, cudaMemcpyDeviceToHost, st));
+          SPK_CUDA(cudaStreamSynchronize(st));
+          if ((rc = cregion.alloc(std::max<uint64_t>(host[S_WORDS], 1) * nl * 8, st))) return rc;
+          cv.keys = cregion.as<uint64_t>();
+          cv.uniform = 0;
+          SPK_CUDA(cudaMemsetAsync(cfill.p, 0, kCoarse * 4 * kFillStride, st));
+          SPK_CUDA(cudaMemsetAsync(sw, 0, (S_ERR + 1) * 8, st));
+          if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rv, k, pv, cv, su + S_OCC);
+          else rc = launch_part_coarse<2>(ctx, st, rv, k, pv, cv, su + S_OCC);
+          if (rc) return rc;
+          SPK_CUDA(cudaGetLastError());
+          launches += 2;
+          info.part_rescatters++;
+          if ((rc = fetch(S_ERR + 1))) return rc;
+          if ((int)host[S_ERR] & kErrRegion) return fail(SPK_E_CUDA, "coarse bucket overflow after resizing");
+        }
+        k_coarse_chunks<<<1, 32, 0, st>>>(cfill.as<unsigned int>(), cfirst.as<uint32_t>());
+        if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
+        else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
+        if (rc) return rc;
+        SPK_CUDA(cudaGetLastError());
+        launches += 2;  // k_coarse_chunks, k_part_fine
+        if ((rc = fetch(S_ERR + 1))) return rc;
+        if ((int)host[S_ERR] & kErrRegion) {
+          // Skewed spans: exact regions from the span fill counts, fine pass again.
+          k_part_bases<<<1, 1024, 0, st>>>(fill.as<unsigned int>(), (uint32_t)nparts, base.as<uint64_t>());
+          SPK_CUDA(cudaMemcpyAsync(host + S_WORDS, base.as<uint64_t>() + nparts, 8, cudaMemcpyDeviceToHost, st));
+          SPK_CUDA(cudaStreamSynchronize(st));
+          if ((rc = region.alloc(std::max<uint64_t>(host[S_WORDS], 1) * nl * 8, st))) return rc;
+          pv.keys = region.as<uint64_t>();
+          pv.uniform = 0;
+          SPK_CUDA(cudaMemsetAsync(fill.p, 0, nparts * 4 * kFillStride, st));
+          SPK_CUDA(cudaMemsetAsync(errp, 0, 4, st));
+          if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
+          else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
+          if (rc) return rc;
+          SPK_CUDA(cudaGetLastError());
+          launches += 2;
+          info.part_rescatters++;
+          if ((rc = fetch(S_ERR + 1))) return rc;
+          if ((int)host[S_ERR] & kErrRegion) return fail(SPK_E_CUDA, "span region overflow after resizing");
+        }
+      } else {
       if (nl == 1) launch_part_scatter<1>(ctx, st, rv, k, pv, su + S_OCC);
       else launch_part_scatter<2>(ctx, st, rv, k, pv, su + S_OCC);
       SPK_CUDA(cudaGetLastError());
@@ -1889,6 +2265,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
         SPK_CUDA(cudaGetLastError());
         launches += 2;  // k_part_bases, k_part_scatter
         info.part_rescatters++;
+      }
       }
       SPK_CUDA(cudaEventRecord(ks1.e, st));
       if (use_ops) {
