@@ -787,9 +787,13 @@ def main():
         # algorithmic bytes.
         scatter_ms = sum(i["ms_scatter_kernel"] for i in infos) / len(infos)
         ops = 3 * info["n_distinct"]
+        # the read pass that leaves every key in its span's region: one kernel,
+        # or two (coarse buckets, then spans) timed together
+        sname = "k_part_coarse+k_part_fine" if info.get("part_passes") == 2 else "k_part_scatter"
         cands = [
-            # read stream and one streamed key write per occurrence
-            ("k_part_scatter", scatter_ms, occ * (sb + 16)),
+            # read stream and one streamed key write per occurrence (the
+            # algorithm's need; the two-level form moves the keys twice more)
+            (sname, scatter_ms, occ * (sb + 16)),
             # keys read back, every table slot written, 4-byte Bloom ops written
             ("k_part_count", count_ms, occ * 16 + info["table_capacity"] * 32 + ops * 4),
             # Bloom ops read, both tiers written

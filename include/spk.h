@@ -282,7 +282,9 @@ typedef struct spk_result_info {
   uint64_t n_unitigs;
   uint64_t n_corrected_reads;    /* SPK_F_CORRECT: reads with a corrected base */
   float ms_correct;              /* SPK_F_CORRECT: device time of the correction */
-  uint32_t reserved2;
+  uint32_t part_passes;          /* partitioned: 1 = the keys went to their spans in one pass,
+                                    2 = through coarse buckets first (ms_scatter_kernel covers
+                                    both passes) */
 } spk_result_info;
 
 int spk_result_count(const spk_result* res, int* n_k);

@@ -732,6 +732,7 @@ constexpr uint32_t kCoarseSlots = kCoarseBlock * kCoarseW;
 constexpr int kFineBlock = 512;
 constexpr uint32_t kFineChunk = 2048;                    // keys per chunk
 constexpr uint32_t kFineMaxBits = 12;                    // spans per coarse bucket <= 2^12
+static_assert(kFineChunk % kFineBlock == 0, "k_part_fine loads whole rounds of keys");
 
 struct CoarseView {
   uint64_t* keys;        // NL u64 per entry
@@ -798,7 +799,7 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
       // ---- roll up to kCoarseW windows into the tile ----
 #pragma unroll
       for (int w = 0; w < kCoarseW; w++) {
-        const uint32_t slot = threadIdx.x * kCoarseW + w;
+        const uint32_t slot = w * kCoarseBlock + threadIdx.x;  // consecutive lanes, consecutive slots
         uint8_t b = 0xFF;
         if (i < np) {
           if (i > 0) {
@@ -830,8 +831,8 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
           if (pv.packed_home)
             C.v[NL - 1] |= (raw0 << pv.log2parts) >> (64 - kHomeBits) << (64 - kHomeBits);
           b = (uint8_t)(p >> fshift);
-#pragma unroll
-          for (int j = 0; j < NL; j++) ks[slot * NL + j] = C.v[j];
+          if (NL == 1) ks[slot] = C.v[0];
+          else ((ulonglong2*)ks)[slot] = make_ulonglong2(C.v[0], C.v[NL - 1]);
           rk[slot] = (uint16_t)atomicAdd(&hist[b], 1u);
         }
         bk[slot] = b;
@@ -858,8 +859,8 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
         const uint8_t b = bk[slot];
         if (b == 0xFF) continue;
         const uint32_t pos = start[b] + rk[slot];
-#pragma unroll
-        for (int j = 0; j < NL; j++) ss[pos * NL + j] = ks[slot * NL + j];
+        if (NL == 1) ss[pos] = ks[slot];
+        else ((ulonglong2*)ss)[pos] = ((const ulonglong2*)ks)[slot];
         sb[pos] = b;
       }
       __syncthreads();
@@ -871,7 +872,7 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
         const uint64_t end = cv.uniform ? (uint64_t)(b + 1) * cv.uniform : cv.base[b + 1];
         if (gi < end) {
           if (NL == 1) cv.keys[gi] = ss[j];
-          else *(ulonglong2*)(cv.keys + 2 * gi) = make_ulonglong2(ss[2 * j], ss[2 * j + 1]);
+          else *(ulonglong2*)(cv.keys + 2 * gi) = ((const ulonglong2*)ss)[j];
         } else {
           atomicOr(cv.err, (int)kErrRegion);
         }
@@ -931,24 +932,36 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
     const uint32_t n = (uint32_t)min((uint64_t)kFineChunk, bend - s0);
     for (uint32_t f = threadIdx.x; f < nfine; f += blockDim.x) hist[f] = 0;
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
-      Seq<NL> C;
-      if (NL == 1) {
-        C.v[0] = __ldcs(cv.keys + s0 + j);
-      } else {
-        const ulonglong2 v = __ldcs((const ulonglong2*)(cv.keys + 2 * (s0 + j)));
-        C.v[0] = v.x;
-        C.v[NL - 1] = v.y;
+    {
+      // every key of this thread loaded before any is processed
+      constexpr int PER = kFineChunk / kFineBlock;
+      Seq<NL> C[PER];
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const uint32_t j = threadIdx.x + q * kFineBlock;
+        if (j >= n) continue;
+        if (NL == 1) {
+          C[q].v[0] = __ldcs(cv.keys + s0 + j);
+        } else {
+          const ulonglong2 v = __ldcs((const ulonglong2*)(cv.keys + 2 * (s0 + j)));
+          C[q].v[0] = v.x;
+          C[q].v[NL - 1] = v.y;
+        }
       }
 #pragma unroll
-      for (int q = 0; q < NL; q++) ks[j * NL + q] = C.v[q];
-      if (pv.packed_home) C.v[NL - 1] &= ~0ULL >> kHomeBits;
-      uint64_t w4[4];
-      kmer256_limbs<NL>(C, k, w4);
-      const uint32_t p = (uint32_t)(hash_seed(hash_pre(w4), kSeed1) >> (64 - pv.log2parts));
-      const uint32_t f = p & (nfine - 1);
-      fb[j] = (uint16_t)f;
-      rk[j] = (uint16_t)atomicAdd(&hist[f], 1u);
+      for (int q = 0; q < PER; q++) {
+        const uint32_t j = threadIdx.x + q * kFineBlock;
+        if (j >= n) continue;
+        if (NL == 1) ks[j] = C[q].v[0];
+        else ((ulonglong2*)ks)[j] = make_ulonglong2(C[q].v[0], C[q].v[NL - 1]);
+        if (pv.packed_home) C[q].v[NL - 1] &= ~0ULL >> kHomeBits;
+        uint64_t w4[4];
+        kmer256_limbs<NL>(C[q], k, w4);
+        const uint32_t p = (uint32_t)(hash_seed(hash_pre(w4), kSeed1) >> (64 - pv.log2parts));
+        const uint32_t f = p & (nfine - 1);
+        fb[j] = (uint16_t)f;
+        rk[j] = (uint16_t)atomicAdd(&hist[f], 1u);
+      }
     }
     __syncthreads();
     // exclusive scan of hist (each thread a run of consecutive spans)
@@ -977,8 +990,8 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
       const uint32_t f = fb[j];
       const uint32_t pos = start[f] + rk[j];
-#pragma unroll
-      for (int q = 0; q < NL; q++) ss[pos * NL + q] = ks[j * NL + q];
+      if (NL == 1) ss[pos] = ks[j];
+      else ((ulonglong2*)ss)[pos] = ((const ulonglong2*)ks)[j];
       sf[pos] = (uint16_t)f;
     }
     __syncthreads();
@@ -989,7 +1002,7 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
       const uint64_t end = pv.uniform ? (uint64_t)(pg + 1) * pv.uniform : pv.base[pg + 1];
       if (gi < end) {
         if (NL == 1) pv.keys[gi] = ss[j];
-        else *(ulonglong2*)(pv.keys + 2 * gi) = make_ulonglong2(ss[2 * j], ss[2 * j + 1]);
+        else *(ulonglong2*)(pv.keys + 2 * gi) = ((const ulonglong2*)ss)[j];
       } else {
         atomicOr(pv.err, (int)kErrRegion);
       }
@@ -2180,6 +2193,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
       SPK_CUDA(cudaEventRecord(ks0.e, st));
       const bool two_level = SPK_TWO_LEVEL && two_level_fits && log2parts > kCoarseBits &&
                              log2parts - kCoarseBits <= kFineMaxBits;
+      info.part_passes = two_level ? 2 : 1;
       if (two_level) {
         // ---- coarse buckets, then spans (k_part_coarse, k_part_fine) ----
         DevBuf cbase, cfill, cregion, cfirst;

@@ -64,7 +64,7 @@ class ResultInfo(C.Structure):
                 ("ms_scatter_kernel", C.c_float), ("ms_unitigs", C.c_float),
                 ("ms_unitigs_host", C.c_float), ("unitig_launches", C.c_uint32),
                 ("n_unitigs", C.c_uint64), ("n_corrected_reads", C.c_uint64),
-                ("ms_correct", C.c_float), ("reserved2", C.c_uint32)]
+                ("ms_correct", C.c_float), ("part_passes", C.c_uint32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
