@@ -1075,6 +1075,131 @@ __device__ __forceinline__ uint64_t range_base(const RangeView& rv, uint32_t r) 
   return rv.uniform ? (uint64_t)r * rv.uniform : rv.base[r];
 }
 
+// Sorted emission of a span's Bloom operations (k <= 64).  Written one by
+// one, the ~3 operations per distinct k-mer are 4-byte stores scattered over
+// all ranges, and they cost the span pass about a third of its time.  Here
+// they are sorted by range in shared memory first: the per-range counts become
+// starts (an exclusive scan), and the operations are placed in groups of
+// ranges whose operations fit the span's count array (free once the span is
+// written out), then each group goes out in contiguous runs.  A group holds
+// the ranges whose first operation falls in a window of S minus the largest
+// range count, so its operations fit the S entries; a span whose largest
+// range count exceeds S/2 is emitted directly instead.
+#ifndef SPK_SORTED_OPS
+#define SPK_SORTED_OPS 1
+#endif
+constexpr bool kSortedOps = SPK_SORTED_OPS;
+
+template <int NL>
+__device__ __forceinline__ void span_emit_sorted(const typename SpanKey<NL>::T* keys, uint32_t* buf, uint32_t S,
+                                                 uint32_t* rs, uint32_t* rcur,
+                                                 const unsigned long long* rbase, const RangeView& rv) {
+  __shared__ uint32_t wpart[32], wmax[32], bnd[8];
+  __shared__ uint32_t s_total, s_maxc;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t nr = rv.nranges;
+  const uint32_t mask = (1u << kLog2Range) - 1u;
+  // counts -> starts (exclusive scan in place), their total and largest count
+  const uint32_t per = (nr + blockDim.x - 1) / blockDim.x;
+  const uint32_t r0 = min(nr, threadIdx.x * per), r1 = min(nr, r0 + per);
+  uint32_t sum = 0, mx = 0;
+  for (uint32_t r = r0; r < r1; r++) {
+    const uint32_t c = rs[r];
+    sum += c;
+    mx = max(mx, c);
+  }
+  uint32_t x = sum;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if ((int)lane >= d) x += y;
+  }
+  const uint32_t wm = __reduce_max_sync(0xffffffffu, mx);
+  if (lane == 31) wpart[warp] = x;
+  if (lane == 0) wmax[warp] = wm;
+  __syncthreads();
+  uint32_t before = x - sum;
+  for (unsigned w = 0; w < warp; w++) before += wpart[w];
+  for (uint32_t r = r0; r < r1; r++) {
+    const uint32_t c = rs[r];
+    rs[r] = before;
+    before += c;
+  }
+  if (threadIdx.x == 0) {
+    uint32_t tt = 0, mm = 0;
+    for (unsigned w = 0; w < nwarps; w++) {
+      tt += wpart[w];
+      mm = max(mm, wmax[w]);
+    }
+    s_total = tt;
+    s_maxc = mm;
+  }
+  __syncthreads();
+  // groups of ranges starting within a window of H positions span at most
+  // H + (largest count) <= S positions of the buffer
+  const uint32_t total = s_total, H = s_maxc <= (S >> 1) ? S - s_maxc : 0u;
+  if (H == 0) {
+    // direct emission (a range holds more than half a span's worth)
+    for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+      const uint32_t* st = (const uint32_t*)&keys[s];
+      if (st[1] == 0xFFFFFFFFu) continue;  // empty slot
+      const uint32_t flag = st[0] >> 31;
+      const uint32_t pk[3] = {st[0] & 0x7FFFFFFFu, st[1], st[2]};
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const uint32_t r = pk[j] >> kLog2Range;
+        const uint64_t i = rbase[r] + atomicAdd(rcur + r, 1u);
+        const uint64_t end = rv.uniform ? (uint64_t)(r + 1) * rv.uniform : rv.base[r + 1];
+        if (i < end) rv.ops[i] = ((pk[j] & mask) << 1) | flag;
+        else atomicOr(rv.err, (int)kErrRange);
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  const uint32_t G = (total + H - 1) / H;  // <= 6: at most 3 S operations, H >= S / 2
+  if (threadIdx.x <= G) {
+    // bnd[g] = the first range start at or after g H (total if none)
+    const uint32_t xv = threadIdx.x * H;
+    uint32_t lo = 0, hi = nr;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (rs[mid] < xv) lo = mid + 1;
+      else hi = mid;
+    }
+    bnd[threadIdx.x] = (xv >= total || lo == nr) ? total : rs[lo];
+  }
+  __syncthreads();
+  for (uint32_t g = 0; g < G; g++) {
+    const uint32_t gb = g * H;
+    for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+      const uint32_t* st = (const uint32_t*)&keys[s];
+      if (st[1] == 0xFFFFFFFFu) continue;  // empty slot
+      const uint32_t flag = st[0] >> 31;
+      const uint32_t pk[3] = {st[0] & 0x7FFFFFFFu, st[1], st[2]};
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const uint32_t r = pk[j] >> kLog2Range;
+        const uint32_t a = rs[r];
+        if (a < gb || a - gb >= H) continue;  // another group's range
+        const uint32_t pos = a + atomicAdd(rcur + r, 1u);
+        buf[pos - gb] = (r << 20) | ((pk[j] & mask) << 1) | flag;
+      }
+    }
+    __syncthreads();
+    const uint32_t lo = bnd[g], hi = bnd[g + 1];
+    for (uint32_t q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+      const uint32_t v = buf[q - gb];
+      const uint32_t r = v >> 20;
+      const uint64_t i = rbase[r] + (q - rs[r]);
+      const uint64_t end = rv.uniform ? (uint64_t)(r + 1) * rv.uniform : rv.base[r + 1];
+      if (i < end) rv.ops[i] = v & 0xFFFFFu;
+      else atomicOr(rv.err, (int)kErrRange);
+    }
+    __syncthreads();
+  }
+}
+
 template <int NL, bool OPS>
 __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartView pv, TableView t, unsigned k,
                                                             FastMod fm, U128* __restrict__ tiers,
@@ -1087,7 +1212,10 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
   // OPS: per-range op counts (then the ops emitted so far), and the global
   // index reserved for each range's ops of this span
   uint32_t* rhist = cnt + S;
-  unsigned long long* rbase = (unsigned long long*)(rhist + ((rv.nranges + 1) & ~1u));
+  // k <= 64 with sorted emission: a cursor per range (the ops placed so far)
+  uint32_t* rcur = rhist + ((rv.nranges + 1) & ~1u);
+  unsigned long long* rbase =
+      (unsigned long long*)(rcur + ((NL == 2 && kSortedOps) ? ((rv.nranges + 1) & ~1u) : 0u));
   const uint32_t nparts = 1u << pv.log2parts;
   for (uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
     for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
@@ -1096,7 +1224,10 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
       cnt[s] = 0;
     }
     if (OPS)
-      for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) rhist[r] = 0;
+      for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) {
+        rhist[r] = 0;
+        if (NL == 2 && kSortedOps) rcur[r] = 0;
+      }
     __syncthreads();
     const uint64_t b = pv.base[p];
     const uint64_t e = min(pv.base[p + 1], b + (uint64_t)pv.fill[(uint64_t)p * kFillStride]);
@@ -1170,6 +1301,11 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
           // (range << kLog2Range | offset), at most 31 bits each
           if (NL == 2) ((uint32_t*)&keys[s])[j] = (uint32_t)pos[j];
         }
+        // with the sorted emission the count array is reused: the slot's
+        // stash keeps "count >= 2" in bit 31 of its first position (positions
+        // are below 2^31 since there are at most 2^12 ranges); an empty
+        // slot's stash stays all ones
+        if (NL == 2 && kSortedOps && c >= 2) ((uint32_t*)&keys[s])[0] |= 0x80000000u;
       }
       __syncthreads();
       // One reservation per non-empty range; rhist then counts the span's
@@ -1177,9 +1313,12 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
       for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) {
         const uint32_t n = rhist[r];
         rbase[r] = n ? range_base(rv, r) + atomicAdd(rv.fill + (uint64_t)r * kFillStride, n) : 0ULL;
-        rhist[r] = 0;
+        if (!(NL == 2 && kSortedOps)) rhist[r] = 0;
       }
       __syncthreads();
+      if (NL == 2 && kSortedOps) {
+        span_emit_sorted<NL>(keys, cnt, S, rhist, rcur, rbase, rv);
+      } else {
       // Emit the operations.
       for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
         const uint32_t c = cnt[s];
@@ -1208,6 +1347,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
         }
       }
       __syncthreads();
+      }
       continue;
     }
     constexpr int U = kSpanBatch;
@@ -1926,6 +2066,7 @@ static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, 
   const int grid = (int)std::min<uint64_t>(nparts, (uint64_t)ctx->sm_count * kPartCtasPerSm);
   if (rv.ops) {
     smem += ((rv.nranges + 1) & ~1u) * 4 + (size_t)rv.nranges * 8;
+    if (NL == 2 && kSortedOps) smem += ((rv.nranges + 1) & ~1u) * 4;  // range cursors
     SPK_CUDA(cudaFuncSetAttribute(k_part_count<NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
     k_part_count<NL, true><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv);
