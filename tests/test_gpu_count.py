@@ -322,9 +322,50 @@ def test_partition_rescatter_on_skew(spk, ora, table_log2):
                   table_log2=table_log2)
     ri = r.info(0)
     assert ri["schedule"] == 3 and ri["part_rescatters"] >= 1
+    assert ri["part_passes"] == (2 if table_log2 == 21 else 1)  # 256 spans: two-level partition
     assert ri["n_table"] == info["n_table"]
     v = r.table_view(0)
     assert v["log2span"] == 13 and v["capacity"] == 1 << table_log2  # 8192-slot spans for k <= 32
+
+
+def test_two_level_rescatter_on_skew_k55(spk, ora):
+    """The two-level read partition (16-byte keys) with one k-mer making up
+    most occurrences: its coarse bucket and its span both overflow, both
+    passes are repeated with exact sizes, and the result equals the oracle's."""
+    data, offs, lens = synth_small_packed()
+    extra = np.zeros(38 * 400, dtype=np.uint8)  # 400 poly-A reads of 150 bases
+    d2 = np.concatenate([data[: int(offs[-1]) + (int(lens[-1]) + 3) // 4], extra])
+    o2 = np.concatenate([offs, int(offs[-1]) + (int(lens[-1]) + 3) // 4 + 38 * np.arange(400, dtype=np.uint64)])
+    l2 = np.concatenate([lens, np.full(400, 150, dtype=np.uint32)])
+    o2, l2 = o2.astype(np.uint64), l2.astype(np.uint32)
+    info = check_against_oracle(spk, ora, d2, o2, l2, 55, 1 << 20, table_log2=21)
+    r = spk.count((d2, o2, l2), [55], bloom_bits=1 << 20, table_log2=21)
+    ri = r.info(0)
+    assert ri["schedule"] == 3 and ri["part_passes"] == 2 and ri["part_rescatters"] >= 1
+    assert ri["n_table"] == info["n_table"]
+
+
+def test_one_bloom_range_direct_emission(spk, ora):
+    """A 2^19-bit Bloom is a single range, so a span's Bloom operations all
+    fall into it; with 64 spans of ~790 distinct k-mers each they exceed half
+    a span (2,048), and the span pass emits them directly instead of sorting
+    them.  The tiers and the table equal the oracle's.  (The order-dependent
+    reference solid tier is left out: a Bloom this small is saturated.)"""
+    data, offs, lens = synth_small_packed()
+    bits = 1 << 19
+    tw = ora.count(data, offs, lens, 55, bits, mode=ora.MODE_TWICE)
+    tk, tc = tw.table(1)
+    oseen, otwice = tw.bloom()
+    r = spk.count((data, offs, lens), [55], bloom_bits=bits, list_min_count=1, flags=BASE, table_log2=18)
+    assert r.info(0)["schedule"] == 3
+    gk, gc = r.kmers(0, 1)
+    np.testing.assert_array_equal(gk, tk)
+    np.testing.assert_array_equal(gc, tc)
+    seen, twice = r.bloom(0)
+    np.testing.assert_array_equal(seen, oseen)
+    np.testing.assert_array_equal(twice, otwice)
+    sk, _ = r.solid(0)
+    np.testing.assert_array_equal(r.edges(0), ora.edges(sk, 55))
 
 
 @pytest.mark.parametrize("k,table_log2", [(21, 22), (55, 22), (55, 20), (64, 23)])
