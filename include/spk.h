@@ -8,7 +8,13 @@
  *   - Stage 3 solid k-mer count table (src/assemble.rs:166-242),
  *   - the solid-k-mer cutoff and set  (src/assemble.rs:286-292, 692-735),
  *   - (k+1)-mer edges implied by      (src/graph.rs:78-102),
- *   - the per-k loop of multi-k runs  (src/multik.rs:109-178).
+ *   - the per-k loop of multi-k runs  (src/multik.rs:109-178),
+ * and the steps either side of it:
+ *   - FASTQ / FASTA ingest into the PackedReads store (src/packed_reads.rs:69-690),
+ *   - single-base read error correction (src/hammer.rs:34-121) and the
+ *     correcting Stage 3 (src/assemble.rs:183-191),
+ *   - the prior-contig boost          (src/assemble.rs:244-284),
+ *   - unitig compaction               (src/graph.rs:65-235).
  * The reference computes all of this on host threads; here everything runs on
  * one GPU and the host only moves buffers across this boundary.
  *
