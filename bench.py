@@ -840,6 +840,11 @@ def main():
             traffic = json.load(f).get(kname)
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                # the captured DRAM bytes of the kernel over its live time: what
+                # it really moves (the two-level partition moves every key three
+                # times against the algorithm's once)
+                "traffic_achieved": (traffic / (kms / 1e3) / 1e9) if traffic else None,
+                "traffic_frac": (traffic / (kms / 1e3) / 1e9 / peak) if traffic else None,
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes,
                 "kernel_ms": kms, "kernel_share": kms / ms,
                 "job": {"bytes_per_occurrence": job_bytes_per_occ,
