@@ -531,32 +531,46 @@ def run_c4(args, ctx, log_rank0):
     log_rank0(f"c4: {len(packs)} samples, {occ} occurrences, generated in {time.time() - t0:.1f}s")
     opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
 
-    def plain():
+    # job latency: from the start of the step's work on that job (plain) or
+    # of the batch (batched) to the job's solid list on the host
+    lat_plain, lat_batch = [], []
+
+    def plain(lat=None):
         for p in packs:
+            a = time.perf_counter()
             r = spk.count(p, [33], ctx=ctx, **opts)
             r.solid(0)
             r.close()
+            if lat is not None:
+                lat.append((time.perf_counter() - a) * 1e3)
 
-    def batched():
+    def batched(lat=None):
+        a = time.perf_counter()
         rs = spk.count_batch([spk.Job(p, [33], dict(opts)) for p in packs], ctx=ctx)
         for r in rs:
             r.solid(0)
             r.close()
+            if lat is not None:
+                lat.append((time.perf_counter() - a) * 1e3)
 
-    def timed(fn):
+    def timed(fn, lat):
         for _ in range(args.warmup):
             fn()
         out = []
         for _ in range(args.steps):
             torch.cuda.synchronize()
             a = time.perf_counter()
-            fn()
+            fn(lat)
             torch.cuda.synchronize()
             out.append(time.perf_counter() - a)
         return sum(out) / len(out)
 
-    t_plain = timed(plain)
-    t_batch = timed(batched)
+    t_plain = timed(plain, lat_plain)
+    t_batch = timed(batched, lat_batch)
+
+    def pct(v):
+        v = sorted(v)
+        return {"p50": v[len(v) // 2], "p99": v[min(len(v) - 1, int(0.99 * len(v)))]} if v else None
     return {"metric": METRIC, "value": _gk(occ, t_batch), "unit": "Gk-mers/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
@@ -566,7 +580,8 @@ def run_c4(args, ctx, log_rank0):
                        "occurrences": occ, "bloom_bits": args.bloom_bits,
                        "timing": "host clock around synchronised calls"},
             "plain": {"what": "spk_count on one sample after another", "value": _gk(occ, t_plain),
-                      "ms_per_step": t_plain * 1e3},
+                      "ms_per_step": t_plain * 1e3, "job_latency_ms": pct(lat_plain)},
+            "job_latency_ms": pct(lat_batch),
             "speedup_vs_plain": t_plain / t_batch}
 
 

@@ -23,6 +23,19 @@ int cuda_fail(cudaError_t e, const char* what) {
   return SPK_E_CUDA;
 }
 
+int raise_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> limits;
+  int dev = 0;
+  SPK_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limits[{kernel, dev}];
+  if (bytes <= cur) return SPK_OK;
+  SPK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+  return SPK_OK;
+}
+
 // ---- FastMod constants (Granlund & Montgomery 1994, Fig. 4.1, N = 64) ---------
 FastMod make_fastmod(uint64_t d) {
   FastMod f{};

@@ -2044,7 +2044,8 @@ template <int NL>
 static int launch_part_coarse(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
                               const PartView& pv, const CoarseView& cv, unsigned long long* occ) {
   const size_t smem = coarse_smem<NL>();
-  SPK_CUDA(cudaFuncSetAttribute(k_part_coarse<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int rc;
+  if ((rc = raise_smem_limit((const void*)k_part_coarse<NL>, smem))) return rc;
   k_part_coarse<NL><<<grid_for(ctx, 2), kCoarseBlock, smem, st>>>(rv, k, pv, cv, occ);
   return SPK_OK;
 }
@@ -2052,7 +2053,8 @@ template <int NL>
 static int launch_part_fine(spk_ctx* ctx, cudaStream_t st, const CoarseView& cv, const uint32_t* cfirst,
                             const PartView& pv, unsigned k) {
   const size_t smem = fine_smem<NL>(1u << (pv.log2parts - kCoarseBits));
-  SPK_CUDA(cudaFuncSetAttribute(k_part_fine<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int rc;
+  if ((rc = raise_smem_limit((const void*)k_part_fine<NL>, smem))) return rc;
   k_part_fine<NL><<<grid_for(ctx, 2), kFineBlock, smem, st>>>(cv, cfirst, pv, k);
   return SPK_OK;
 }
@@ -2067,12 +2069,12 @@ static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, 
   if (rv.ops) {
     smem += ((rv.nranges + 1) & ~1u) * 4 + (size_t)rv.nranges * 8;
     if (NL == 2 && kSortedOps) smem += ((rv.nranges + 1) & ~1u) * 4;  // range cursors
-    SPK_CUDA(cudaFuncSetAttribute(k_part_count<NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    int rc;
+    if ((rc = raise_smem_limit((const void*)k_part_count<NL, true>, smem))) return rc;
     k_part_count<NL, true><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv);
   } else {
-    SPK_CUDA(cudaFuncSetAttribute(k_part_count<NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    int rc;
+    if ((rc = raise_smem_limit((const void*)k_part_count<NL, false>, smem))) return rc;
     k_part_count<NL, false><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv);
   }
   return SPK_OK;
@@ -2080,7 +2082,8 @@ static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, 
 static int launch_bloom_apply(spk_ctx* ctx, cudaStream_t st, const RangeView& rv, uint64_t num_words,
                               uint64_t* seen, uint64_t* twice, unsigned long long* pops) {
   const size_t smem = (size_t)2 * ((1u << kLog2Range) / 32) * 4;
-  SPK_CUDA(cudaFuncSetAttribute(k_bloom_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int rc;
+  if ((rc = raise_smem_limit((const void*)k_bloom_apply, smem))) return rc;
   const int grid = (int)std::min<uint64_t>(rv.nranges, (uint64_t)ctx->sm_count);
   k_bloom_apply<<<grid, kApplyBlock, smem, st>>>(rv, num_words, seen, twice, pops);
   return SPK_OK;

@@ -202,6 +202,12 @@ int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
 int correct_reads(spk_ctx* ctx, cudaStream_t st, unsigned k, const unsigned long long* tier, const FastMod& fm,
                   const uint8_t* d_data, uint64_t data_len, const uint64_t* d_off, const uint32_t* d_len,
                   uint64_t n, uint8_t* d_out, uint8_t* d_corr, uint64_t* nc, uint32_t* launches = nullptr);
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`, and never lowers it (spk_api.cu).  Jobs on other host threads
+// (batches, serving, multi-k) launch the same kernels with other sizes; a
+// limit lowered between another thread's raise and its launch would make that
+// launch fail.
+int raise_smem_limit(const void* kernel, size_t bytes);
 // Exclusive scan of u32 in place (spk_sort.cu).
 int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches = nullptr);
 // Ordered compaction of a sorted SoA list into AoS Kmer256 limbs; *m is the

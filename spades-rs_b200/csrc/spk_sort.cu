@@ -494,8 +494,7 @@ static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* t
   k_bs_scatter<NL, HASV><<<g, BS_BLOCK, 0, st>>>(K, v, T, tv, n, limb, sh, nb, cur);
   const size_t smem = std::max<size_t>(BS_LOCAL * (NL * 8 + (HASV ? 4 : 0)),
                                        (size_t)(BS_BLOCK / 32) * BS_WARP * (NL + (HASV ? 1 : 0)) * 8);
-  SPK_CUDA(cudaFuncSetAttribute(k_bs_local<NL, HASV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+  if ((rc = raise_smem_limit((const void*)k_bs_local<NL, HASV>, smem))) return rc;
   const unsigned gl = (unsigned)std::min<uint32_t>(nb, 148 * 4);
   k_bs_local<NL, HASV><<<gl, BS_BLOCK, smem, st>>>(T, tv, K, v, off, hist, nb, big, nbig);
   SPK_CUDA(cudaGetLastError());
