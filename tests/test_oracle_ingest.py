@@ -100,3 +100,59 @@ def test_reference_ecoli_reads_match_golden(ora):
     np.testing.assert_array_equal(d, g["data"])
     np.testing.assert_array_equal(o, g["offsets"])
     np.testing.assert_array_equal(ln, g["lengths"])
+
+
+def test_fuzzed_texts_agree(ora):
+    """Random texts built from FASTQ/FASTA line fragments (headers, bases with
+    N and lowercase, '+' lines, qualities of matching or wrong length, blank,
+    whitespace and CR-terminated lines): the C++ and Python restatements of
+    the reader accept the same texts, refuse the same ones, and ingest the
+    same store."""
+    rng = np.random.default_rng(2024)
+    nl_choices = [b"\n", b"\r\n", b"\r\r\n"]
+
+    def seq():
+        n = int(rng.integers(0, 60))
+        return bytes(rng.choice(list(b"ACGTacgtN"), n).tolist())
+
+    def fastq_record():
+        s = seq()
+        q = b"I" * (len(s) if rng.random() < 0.9 else len(s) + 1)
+        nl = nl_choices[int(rng.integers(0, 3))]
+        plus = b"+" if rng.random() < 0.95 else b"-"
+        head = b"@r" if rng.random() < 0.97 else b"r"
+        rec = head + nl + s + nl + plus + nl + q
+        if rng.random() < 0.95:
+            rec += nl
+        return rec
+
+    def fasta_record():
+        out = b">h\n"
+        for _ in range(int(rng.integers(0, 4))):
+            out += seq() + nl_choices[int(rng.integers(0, 3))]
+        return out
+
+    agree = refused = 0
+    for case in range(300):
+        lead = b"".join([b"\n", b" \t\n", b"\r\n"][int(rng.integers(0, 3))] for _ in range(int(rng.integers(0, 3))))
+        if case % 2:
+            body = b"".join(fastq_record() + (b"\n" if rng.random() < 0.2 else b"") for _ in range(int(rng.integers(0, 6))))
+        else:
+            body = b"".join(fasta_record() for _ in range(int(rng.integers(0, 6))))
+        text = lead + body
+        try:
+            want = pyref.fastx_records(text)
+        except ValueError:
+            with pytest.raises(ValueError):
+                ora.Packed.from_texts(text)
+            refused += 1
+            continue
+        p = ora.Packed.from_texts(text)
+        q = ora.Packed()
+        for r in want:
+            q.ingest_read(r)
+        for x, y in zip(p.arrays(), q.arrays()):
+            np.testing.assert_array_equal(x, y)
+        assert p.sidecar() == q.sidecar()
+        agree += 1
+    assert agree > 100 and refused > 20
