@@ -410,19 +410,13 @@ def run_ingest(args, ctx, log_rank0):
     return line
 
 
-def cpu_sample_reads(packed, n):
-    """The first n reads of the workload and their k-mer occurrences."""
-    import numpy as np
-    end = int(packed.offsets[n - 1]) + (int(packed.lengths[n - 1]) + 3) // 4
-    per = np.clip(packed.lengths[:n].astype(np.int64) - K + 1, 0, None)
-    return packed.data[:end], packed.offsets[:n], packed.lengths[:n], int(per.sum())
-
-
-# ---------------------------------------------------------------------------
 def cpu_sample(packed, target_occ):
-    """The first reads of the workload holding about target_occ k-mer occurrences."""
+    """The first reads of the workload holding about target_occ k-mer
+    occurrences (target_occ <= 0: the whole workload)."""
     import numpy as np
     per = np.clip(packed.lengths.astype(np.int64) - K + 1, 0, None)
+    if target_occ <= 0:
+        return packed.data, packed.offsets, packed.lengths, int(per.sum())
     n = int(np.searchsorted(np.cumsum(per), target_occ)) + 1
     n = min(n, packed.lengths.size)
     end = int(packed.offsets[n - 1]) + (int(packed.lengths[n - 1]) + 3) // 4
@@ -432,8 +426,10 @@ def cpu_sample(packed, target_occ):
 def run_cpu_baseline(packed, steps, warmup, target_occ, bloom_bits):
     """The reference algorithm (C++ restatement of src/assemble.rs:129-242 with
     the rayon chunking and sharded maps) on all host cores."""
+    import numpy as np
     from oracle import ora
     data, offs, lens, occ = cpu_sample(packed, target_occ)
+    total = int(np.clip(packed.lengths.astype(np.int64) - K + 1, 0, None).sum())
     threads = os.cpu_count() or 1
     times = []
     for i in range(warmup + steps):
@@ -444,12 +440,70 @@ def run_cpu_baseline(packed, steps, warmup, target_occ, bloom_bits):
             times.append(st["seconds_total"])
         r.table(2)
     sec = sum(times) / len(times)
+    what = ("the whole workload" if occ == total else
+            f"the first {lens.size} reads of the workload ({occ / total:.1%} of its occurrences)")
     return {"value": occ / sec / 1e9, "unit": "Gk-mers/s", "cores": threads, "kind": "port",
             "seconds_per_step": sec,
-            "sample": f"first {lens.size} reads of the workload ({occ} k-mer occurrences, "
-                      f"{occ / 320_000_064:.1%} of it), full-size Bloom ({bloom_bits} bits/tier); "
-                      f"C++ restatement of spades-rs Stages 2-3, {threads} threads, timed from "
-                      f"packed reads in RAM to the sorted count>=2 list"}
+            "sample": f"{what}: {lens.size} reads, {occ} k-mer occurrences, Bloom {bloom_bits} "
+                      f"bits/tier; C++ restatement of spades-rs Stages 2-3, {threads} threads, timed "
+                      f"from packed reads in RAM to the sorted count>=2 list"}
+
+
+def c2_config(p, occ, args, world):
+    """config of the k=55 line (both arms print the same one)."""
+    return {"workload": "c2: 5 Mb genome (50% GC, 20 repeats of 1-5 kb at 99% identity), "
+                        "2x150 bp pairs at 100x, substitution errors 0.1%->1.0% along the "
+                        "read; canonical k=55; Bloom 512 Mi bits/tier; adaptive cutoff; "
+                        "sorted solid list + (k+1)-mer edges",
+            "k": K, "reads": int(len(p)), "occurrences_per_gpu": occ,
+            "bloom_bits": args.bloom_bits, "scale": args.scale,
+            "l2": "flushed between steps (512 MiB write)",
+            "parallelism": f"replicas x{world} (one read set per GPU, no collective)"}
+
+
+def run_parity(p, run_job, bloom_bits, timed_info):
+    """The full result of one more (untimed) job against the oracle's
+    twice-tier count of the same reads (threaded; order-free, so equal to the
+    serial restatement): the whole admitted table with its counts, both Bloom
+    tiers, the cutoff and the edge list, bit for bit; and the timed steps'
+    result sizes against this job's."""
+    import hashlib
+    import numpy as np
+    import spk
+    from oracle import ora
+    t0 = time.time()
+    r = run_job(flags=spk.SPK_F_EDGES | spk.SPK_F_KEEP_BLOOM, list_min_count=1)
+    info = r.info(0)
+    gk, gc = r.kmers(0, 1)
+    seen, twice = r.bloom(0)
+    ge = r.edges(0)
+    r.close()
+    t1 = time.time()
+    threads = os.cpu_count() or 1
+    o = ora.count(p.data, p.offsets, p.lengths, K, bloom_bits, mode=ora.MODE_TWICE, threads=threads)
+    tk, tc = o.table(1)
+    oseen, otwice = o.bloom()
+    cut = ora.cutoff(tc, 5.0)
+    solid = tc >= cut
+    oe = ora.edges(tk[solid], K)
+    checks = {
+        "table": bool(np.array_equal(gk, tk) and np.array_equal(gc, tc)),
+        "count_ge2_list": bool(np.array_equal(gk[gc >= 2], tk[tc >= 2]) and np.array_equal(gc[gc >= 2], tc[tc >= 2])),
+        "seen_tier": bool(np.array_equal(seen, oseen)),
+        "twice_tier": bool(np.array_equal(twice, otwice)),
+        "cutoff": int(info["cutoff"]) == cut,
+        "edges": bool(np.array_equal(ge, oe)),
+        "singletons": int(info["n_singletons"]) == int((tc == 1).sum()),
+        "timed_steps_same_sizes": all(
+            ti[key] == info[key] for ti in timed_info
+            for key in ("n_solid", "n_edges", "cutoff", "n_table", "admitted_occurrences")),
+    }
+    sha = hashlib.sha256(tk[solid].tobytes() + tc[solid].tobytes()).hexdigest()[:16]
+    return bool(all(checks.values())), {
+        "checks": checks, "oracle": f"C++ restatement, twice-tier mode, {threads} threads",
+        "n_table": int(tk.shape[0]), "n_count_ge2": int((tc >= 2).sum()), "n_solid": int(solid.sum()),
+        "n_edges": int(oe.shape[0]), "cutoff": cut, "solid_sha256_16": sha,
+        "gpu_seconds": round(t1 - t0, 2), "oracle_seconds": round(time.time() - t1, 2)}
 
 
 # ---------------------------------------------------------------------------
@@ -644,8 +698,10 @@ def main():
     ap.add_argument("--scale", type=float, default=None,
                     help="genome scale (default 1.0 for c2/c3, 0.05 for c4, 0.02 for c5)")
     ap.add_argument("--bloom-bits", type=int, default=512 << 20)
-    ap.add_argument("--cpu-occ", type=int, default=96_000_000,
-                    help="k-mer occurrences in the CPU baseline sample")
+    ap.add_argument("--cpu-occ", type=int, default=0,
+                    help="k-mer occurrences in the CPU baseline sample (0: the whole workload)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the full-size check of one job's result against the oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "unitigs", "correct", "ingest"],
@@ -670,14 +726,14 @@ def main():
         if rank != 0:
             return
         s = synth.c2(args.scale)
+        occ = synth.occurrences(s.packed, K)
         cb = run_cpu_baseline(s.packed, args.steps, args.warmup, args.cpu_occ, args.bloom_bits)
         line = {"metric": METRIC, "value": cb["value"], "unit": "Gk-mers/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": cb["seconds_per_step"] * 1e3, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-                "impl": "reference",
-                "config": {"workload": "c2 sample: " + cb["sample"], "k": K,
-                           "bloom_bits": args.bloom_bits},
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic (seeded; no public dataset)", "impl": "reference",
+                "config": c2_config(s.packed, occ, args, world),
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": "Gk-mers/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
@@ -872,7 +928,15 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = run_cpu_baseline(p, 1, 1, args.cpu_occ, args.bloom_bits)
+        cpu = run_cpu_baseline(p, 1, 0, args.cpu_occ, args.bloom_bits)
+
+    # full-size parity of one more job against the oracle (rank 0 alone; every
+    # rank counts the same reads)
+    parity, parity_detail = None, None
+    if rank == 0 and not args.no_parity:
+        parity, parity_detail = run_parity(p, lambda **kw: spk.count_device(
+            d_data.data_ptr(), p.data.size, d_off.data_ptr(), d_len.data_ptr(), p.lengths.size, [K],
+            ctx=ctx, bloom_bits=args.bloom_bits, **kw), args.bloom_bits, infos)
 
     if rank == 0:
         line = {
@@ -881,13 +945,8 @@ def main():
             "step_ms": [round(x, 3) for x in step_ms],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded; no public dataset)",
-            "config": {"workload": "c2: 5 Mb genome (50% GC, 20 repeats of 1-5 kb at 99% identity), "
-                                   "2x150 bp pairs at 100x, substitution errors 0.1%->1.0% along the "
-                                   "read; canonical k=55; Bloom 512 Mi bits/tier; adaptive cutoff; "
-                                   "sorted solid list + (k+1)-mer edges",
-                       "k": K, "reads": int(len(p)), "occurrences_per_gpu": occ,
-                       "bloom_bits": args.bloom_bits, "l2": "flushed between steps (512 MiB write)",
-                       "parallelism": f"replicas x{world} (one read set per GPU, no collective)"},
+            "config": c2_config(p, occ, args, world),
+            "parity": parity, "parity_detail": parity_detail,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks,
             "result": {"n_solid": info["n_solid"], "n_list": info["n_list"],

@@ -391,6 +391,18 @@ int spk_poll(spk_ctx* ctx, uint64_t ticket, int* done);
  * the job's own status if it failed.  latency_ms (nullable) = submit->done. */
 int spk_wait(spk_ctx* ctx, uint64_t ticket, int timeout_ms, spk_result** out, double* latency_ms);
 
+/* ---- diagnostics --------------------------------------------------------- */
+/* The count table's bounded wait for keys of k = 65..127.  The reference's
+ * table is a mutex-guarded HashMap (src/assemble.rs:166-242) whose waits have
+ * no bound; here a writer claims a slot, publishes its key and marks the slot
+ * ready, and a reader that finds a slot claimed waits a bounded time for it.
+ * This call counts one k-mer into a small table whose home slot for that
+ * k-mer was left claimed and never published (what a writer gone mid-claim
+ * would leave): the wait runs out after a fraction of a second and the call
+ * returns SPK_E_TIMEOUT, with the context still usable.  No counterpart in the
+ * reference. */
+int spk_diag_stuck_claim(spk_ctx* ctx, uint32_t k);
+
 #ifdef __cplusplus
 }
 #endif

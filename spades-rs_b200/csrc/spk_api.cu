@@ -36,6 +36,26 @@ int raise_smem_limit(const void* kernel, size_t bytes) {
   return SPK_OK;
 }
 
+int current_sm_count() {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 148;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    n = 148;
+  }
+  cache[dev] = n;
+  return n;
+}
+
 // ---- FastMod constants (Granlund & Montgomery 1994, Fig. 4.1, N = 64) ---------
 FastMod make_fastmod(uint64_t d) {
   FastMod f{};
@@ -169,6 +189,8 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
   return SPK_OK;
 }
 
+int stuck_claim(spk_ctx* ctx, uint32_t k);
+
 }  // namespace spk
 
 using namespace spk;
@@ -176,6 +198,12 @@ using namespace spk;
 extern "C" {
 
 const char* spk_last_error(void) { return g_err.c_str(); }
+
+int spk_diag_stuck_claim(spk_ctx* ctx, uint32_t k) {
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  return stuck_claim(ctx, k);
+}
 int spk_version(void) { return SPK_VERSION; }
 
 // src/main.rs:11-30

@@ -44,15 +44,14 @@ extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, sp
   for (int i = 0; i < n_jobs; i++) budget = std::max<uint64_t>(budget, job_estimate(jobs[i]));
   int status = SPK_OK;
   std::string msg;
-  std::vector<std::string> errs(n_jobs);  // a worker thread's error message
+  std::vector<std::string> errs(n_jobs);  // the error message of a failed job
   {
     Scheduler sched(budget, kBatchInflight);
     std::vector<uint64_t> tickets(n_jobs);
     for (int i = 0; i < n_jobs; i++) {
       spk_job j = jobs[i];
       std::vector<uint32_t> ks(j.ks, j.ks + j.n_k);
-      std::string* err = &errs[i];
-      tickets[i] = sched.submit(job_estimate(j), [ctx, j, ks, err](void** out) {
+      tickets[i] = sched.submit(job_estimate(j), [ctx, j, ks](void** out, std::string* err) {
         const int rc = run_job(ctx, j, ks, out);
         if (rc) *err = spk_last_error();
         return rc;
@@ -61,7 +60,7 @@ extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, sp
     for (int i = 0; i < n_jobs; i++) {
       int st = 0;
       void* r = nullptr;
-      sched.wait(tickets[i], -1, &st, &r, nullptr);
+      sched.wait(tickets[i], -1, &st, &r, nullptr, &errs[i]);
       results[i] = (spk_result*)r;
       if (st && status == SPK_OK) {
         status = st;

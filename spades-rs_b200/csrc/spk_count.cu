@@ -2901,4 +2901,54 @@ int download_bloom(spk_result* res, int ki, uint64_t* seen, uint64_t* twice, uin
   return SPK_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Diagnostic of the bounded claim wait of wide keys (table_add, NL >= 3).
+// A writer that claims a slot publishes its key and marks the slot ready
+// right after; a slot that stays claimed (a writer gone mid-claim) would stall
+// every reader of it.  Here one thread leaves the home slot of a k-mer
+// claimed and then counts that k-mer: its wait runs out after kSpinLimit
+// polls (a fraction of a second), sets error bit 1 and returns.
+// ---------------------------------------------------------------------------
+template <int NL>
+__global__ void k_stuck_claim(TableView t, Seq<NL> C, unsigned k) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint64_t w4[4];
+  kmer256_limbs<NL>(C, k, w4);
+  const uint64_t home = table_home(t, hash_seed(hash_pre(w4), kSeed1));
+  atomicExch(slot_state<NL>(t, home), 1u);  // claimed, never published
+  __threadfence();
+  table_add<NL>(t, C, home, 1);
+}
+
+int stuck_claim(spk_ctx* ctx, uint32_t k) {
+  if (k < 65 || k > 127) return fail(SPK_E_INVALID_K, "the claim wait serves keys of k = 65..127");
+  cudaStream_t st = ctx->stream;
+  KResult kr;
+  kr.nl = (int)((k + 31) / 32);
+  int rc;
+  DevBuf errw;
+  if ((rc = errw.alloc(8, st))) return rc;
+  SPK_CUDA(cudaMemsetAsync(errw.p, 0, 8, st));
+  if ((rc = alloc_table(ctx, kr, st, 1024))) return rc;
+  kr.table.err = errw.as<int>();
+  // any k-mer of k bases: limb j holds bases 32j.. in its low bits
+  Seq<4> C4{};
+  for (int j = 0; j < 4; j++) C4.v[j] = 0x9e3779b97f4a7c15ULL * (j + 1);
+  const unsigned top = 2 * k - 64 * (kr.nl - 1);
+  if (top < 64) C4.v[kr.nl - 1] &= (1ULL << top) - 1;
+  if (kr.nl == 3) {
+    Seq<3> C;
+    for (int j = 0; j < 3; j++) C.v[j] = C4.v[j];
+    k_stuck_claim<3><<<1, 32, 0, st>>>(kr.table, C, k);
+  } else {
+    k_stuck_claim<4><<<1, 32, 0, st>>>(kr.table, C4, k);
+  }
+  SPK_CUDA(cudaGetLastError());
+  int host_err = 0;
+  SPK_CUDA(cudaMemcpyAsync(&host_err, errw.p, 4, cudaMemcpyDeviceToHost, st));
+  SPK_CUDA(cudaStreamSynchronize(st));
+  if (host_err & 2) return fail(SPK_E_TIMEOUT, "count table: claim wait timed out (slot left claimed)");
+  return fail(SPK_E_CUDA, "the claim wait ended without its timeout");
+}
+
 }  // namespace spk

@@ -208,6 +208,9 @@ int correct_reads(spk_ctx* ctx, cudaStream_t st, unsigned k, const unsigned long
 // limit lowered between another thread's raise and its launch would make that
 // launch fail.
 int raise_smem_limit(const void* kernel, size_t bytes);
+// Streaming multiprocessors of the current device (cached per device), for
+// grid sizing in code that has no context at hand.
+int current_sm_count();
 // Exclusive scan of u32 in place (spk_sort.cu).
 int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches = nullptr);
 // Ordered compaction of a sorted SoA list into AoS Kmer256 limbs; *m is the

@@ -7,7 +7,13 @@
 // callback executes one job (on its own CUDA stream in libspk; a fake in the
 // CPU tests) on a worker thread; when it returns, its memory and slot are
 // released and the next jobs are admitted.  No CUDA here, so the policy is
-// tested on machines without a GPU.
+// tested on machines without a GPU (tests/sched_test.cpp).
+//
+// Lifetime.  A caller blocked in wait() holds the scheduler through a
+// shared_ptr of its own, so stop() followed by the owner dropping its pointer
+// never destroys the mutex or condition variables under a waiter.  stop()
+// frees (with the deleter given at construction) the results of finished jobs
+// nobody waits for, so tickets never collected do not leak their results.
 #pragma once
 #include <chrono>
 #include <condition_variable>
@@ -17,6 +23,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -25,22 +32,34 @@ namespace spk {
 struct SchedJob {
   uint64_t ticket = 0;
   uint64_t need = 0;                 // estimated device bytes
-  std::function<int(void**)> run;    // returns status, sets an opaque result
+  // returns status, sets an opaque result and, on failure, the error message
+  std::function<int(void**, std::string*)> run;
   std::chrono::steady_clock::time_point t_submit, t_start, t_done;
   bool done = false;
   int status = 0;
   void* result = nullptr;
+  std::string msg;                   // error message of a failed job
+  int waiters = 0;                   // callers inside wait() for this job
 };
 
 class Scheduler {
  public:
   enum { kAdmissionError = 8 /* SPK_E_ADMISSION */ };
 
-  Scheduler(uint64_t budget, int max_inflight)
-      : budget_(budget), max_inflight_(max_inflight < 1 ? 1 : max_inflight) {
+  // free_result: how to free the result of a job nobody collected (may be empty).
+  Scheduler(uint64_t budget, int max_inflight, std::function<void(void*)> free_result = nullptr)
+      : budget_(budget), max_inflight_(max_inflight < 1 ? 1 : max_inflight),
+        free_result_(std::move(free_result)) {
     thread_ = std::thread([this] { loop(); });
   }
-  ~Scheduler() { stop(); }
+  ~Scheduler() {
+    stop();
+    // No waiter is left (each holds the scheduler): free what nobody took.
+    std::unique_lock<std::mutex> l(mu_);
+    for (auto& kv : jobs_)
+      if (kv.second->result && free_result_) free_result_(kv.second->result);
+    jobs_.clear();
+  }
 
   void stop() {
     {
@@ -61,9 +80,20 @@ class Scheduler {
     done_cv_.notify_all();
     // Running jobs finish on their own worker threads.
     done_cv_.wait(l, [&] { return inflight_ == 0; });
+    // Results of finished jobs that no caller is waiting for are freed; a
+    // waiter already inside wait() still collects its own.
+    for (auto it = jobs_.begin(); it != jobs_.end();) {
+      auto& j = it->second;
+      if (j->waiters == 0) {
+        if (j->result && free_result_) free_result_(j->result);
+        it = jobs_.erase(it);
+      } else {
+        ++it;
+      }
+    }
   }
 
-  uint64_t submit(uint64_t need, std::function<int(void**)> run) {
+  uint64_t submit(uint64_t need, std::function<int(void**, std::string*)> run) {
     std::unique_lock<std::mutex> l(mu_);
     auto j = std::make_shared<SchedJob>();
     j->ticket = ++next_ticket_;
@@ -71,7 +101,7 @@ class Scheduler {
     j->run = std::move(run);
     j->t_submit = std::chrono::steady_clock::now();
     jobs_[j->ticket] = j;
-    if (need > budget_) {  // can never fit: fail now rather than block the queue
+    if (stopping_ || need > budget_) {  // stopped, or can never fit: fail now
       j->done = true;
       j->status = kAdmissionError;
       j->t_start = j->t_done = j->t_submit;
@@ -91,17 +121,25 @@ class Scheduler {
   }
 
   // Waits up to timeout_ms (< 0: forever).  Returns -1 unknown ticket, 0 not
-  // ready, 1 done (the job is removed and its fields copied out).
-  int wait(uint64_t ticket, int timeout_ms, int* status, void** result, double* latency_ms) {
+  // ready, 1 done (the job is removed and its fields copied out; msg gets the
+  // error message of a failed job).
+  int wait(uint64_t ticket, int timeout_ms, int* status, void** result, double* latency_ms,
+           std::string* msg = nullptr) {
     std::unique_lock<std::mutex> l(mu_);
     auto it = jobs_.find(ticket);
     if (it == jobs_.end()) return -1;
     auto j = it->second;
     auto pred = [&] { return j->done; };
+    j->waiters++;
+    bool ready = true;
     if (timeout_ms < 0) done_cv_.wait(l, pred);
-    else if (!done_cv_.wait_for(l, std::chrono::milliseconds(timeout_ms), pred)) return 0;
+    else ready = done_cv_.wait_for(l, std::chrono::milliseconds(timeout_ms), pred);
+    j->waiters--;
+    if (!ready) return 0;
+    if (jobs_.find(ticket) == jobs_.end()) return -1;  // another waiter took it
     if (status) *status = j->status;
     if (result) *result = j->result;
+    if (msg) *msg = j->msg;
     if (latency_ms)
       *latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
     jobs_.erase(ticket);
@@ -138,10 +176,12 @@ class Scheduler {
       j->t_start = std::chrono::steady_clock::now();
       std::thread([this, j] {
         void* r = nullptr;
-        int st = j->run(&r);
+        std::string msg;
+        int st = j->run(&r, &msg);
         std::unique_lock<std::mutex> l2(mu_);
         j->status = st;
         j->result = r;
+        j->msg = std::move(msg);
         j->t_done = std::chrono::steady_clock::now();
         j->done = true;
         in_use_ -= j->need;
@@ -164,6 +204,7 @@ class Scheduler {
   int inflight_ = 0;
   int peak_inflight_ = 0;
   bool stopping_ = false;
+  std::function<void(void*)> free_result_;
 };
 
 }  // namespace spk

@@ -16,7 +16,9 @@
 #include "spk_sched.h"
 
 struct Server {
-  spk::Scheduler* sched = nullptr;
+  // Shared with every caller inside spk_wait, so that a concurrent stop never
+  // destroys the scheduler under a waiter.
+  std::shared_ptr<spk::Scheduler> sched;
   uint64_t budget = 0;
 };
 
@@ -95,8 +97,10 @@ int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, voi
 void serve_shutdown(spk_ctx* ctx) {
   std::unique_lock<std::mutex> l(ctx->serve_mu);
   if (!ctx->server) return;
+  // Queued jobs end cancelled, running ones finish, and the results nobody
+  // waits for are freed; a caller already in spk_wait keeps the scheduler
+  // alive until it returns.
   ctx->server->sched->stop();
-  delete ctx->server->sched;
   delete ctx->server;
   ctx->server = nullptr;
 }
@@ -125,7 +129,8 @@ int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight) {
   }
   auto* s = new Server();
   s->budget = hbm_budget_bytes;
-  s->sched = new Scheduler(hbm_budget_bytes, max_inflight > 0 ? max_inflight : 4);
+  s->sched = std::make_shared<Scheduler>(hbm_budget_bytes, max_inflight > 0 ? max_inflight : 4,
+                                         [](void* r) { spk_result_free((spk_result*)r); });
   ctx->server = s;
   return SPK_OK;
 }
@@ -146,7 +151,13 @@ int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket) {
   spk_job j = *job;
   std::vector<uint32_t> ks(job->ks, job->ks + job->n_k);
   const uint64_t need = job_estimate(j);
-  *ticket = ctx->server->sched->submit(need, [ctx, j, ks](void** out) { return run_job(ctx, j, ks, out); });
+  // The job runs on a worker thread: its error message is taken there and
+  // handed to the caller of spk_wait with the status.
+  *ticket = ctx->server->sched->submit(need, [ctx, j, ks](void** out, std::string* msg) {
+    const int rc = run_job(ctx, j, ks, out);
+    if (rc) *msg = spk_last_error();
+    return rc;
+  });
   return SPK_OK;
 }
 
@@ -163,7 +174,7 @@ int spk_poll(spk_ctx* ctx, uint64_t ticket, int* done) {
 int spk_wait(spk_ctx* ctx, uint64_t ticket, int timeout_ms, spk_result** out, double* latency_ms) {
   if (!ctx || !out) return fail(SPK_E_INVALID_ARG, "null argument");
   *out = nullptr;
-  Scheduler* sched;
+  std::shared_ptr<Scheduler> sched;
   {
     std::unique_lock<std::mutex> l(ctx->serve_mu);
     if (!ctx->server) return fail(SPK_E_INVALID_ARG, "serving loop not started");
@@ -171,12 +182,14 @@ int spk_wait(spk_ctx* ctx, uint64_t ticket, int timeout_ms, spk_result** out, do
   }
   int status = 0;
   void* r = nullptr;
-  int w = sched->wait(ticket, timeout_ms, &status, &r, latency_ms);
+  std::string msg;
+  int w = sched->wait(ticket, timeout_ms, &status, &r, latency_ms, &msg);
   if (w < 0) return fail(SPK_E_NOT_FOUND, "unknown ticket");
   if (w == 0) return fail(SPK_E_NOT_READY, "job not finished");
   if (status == SPK_E_ADMISSION)
-    return fail(SPK_E_ADMISSION, "job needs more device memory than the serving budget");
-  if (status) return status;
+    return fail(SPK_E_ADMISSION, "job needs more device memory than the serving budget, "
+                                 "or the serving loop stopped before admitting it");
+  if (status) return fail(status, msg);
   *out = (spk_result*)r;
   return SPK_OK;
 }

@@ -484,7 +484,8 @@ template <int NL, bool HASV>
 static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* tv, uint64_t n,
                      unsigned limb, unsigned sh, uint32_t nb, uint32_t* hist, uint32_t* off,
                      uint32_t* cur, uint32_t* big, unsigned* nbig, uint32_t* launches) {
-  const unsigned g = (unsigned)std::min<uint64_t>((n + BS_BLOCK - 1) / BS_BLOCK, 148 * 16);
+  const int sms = current_sm_count();
+  const unsigned g = (unsigned)std::min<uint64_t>((n + BS_BLOCK - 1) / BS_BLOCK, (uint64_t)sms * 16);
   k_bs_hist<NL><<<g, BS_BLOCK, 0, st>>>(K, n, limb, sh, nb, hist);
   SPK_CUDA(cudaMemcpyAsync(off, hist, (size_t)nb * 4, cudaMemcpyDeviceToDevice, st));
   DevBuf sums;
@@ -495,7 +496,7 @@ static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* t
   const size_t smem = std::max<size_t>(BS_LOCAL * (NL * 8 + (HASV ? 4 : 0)),
                                        (size_t)(BS_BLOCK / 32) * BS_WARP * (NL + (HASV ? 1 : 0)) * 8);
   if ((rc = raise_smem_limit((const void*)k_bs_local<NL, HASV>, smem))) return rc;
-  const unsigned gl = (unsigned)std::min<uint32_t>(nb, 148 * 4);
+  const unsigned gl = (unsigned)std::min<uint32_t>(nb, (uint32_t)sms * 4);
   k_bs_local<NL, HASV><<<gl, BS_BLOCK, smem, st>>>(T, tv, K, v, off, hist, nb, big, nbig);
   SPK_CUDA(cudaGetLastError());
   if (launches) *launches += 3;

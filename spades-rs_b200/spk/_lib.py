@@ -133,6 +133,7 @@ _SIGS = [
     ("spk_submit", C.c_int, [vp, C.POINTER(JobC), u64p]),
     ("spk_poll", C.c_int, [vp, C.c_uint64, C.POINTER(C.c_int)]),
     ("spk_wait", C.c_int, [vp, C.c_uint64, C.c_int, C.POINTER(vp), C.POINTER(C.c_double)]),
+    ("spk_diag_stuck_claim", C.c_int, [vp, C.c_uint32]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]

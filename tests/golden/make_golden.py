@@ -1,6 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from the Python restatement.
 
-Run once in a checkout that has the spades-rs sources next to it:
+Run once with a spades-rs checkout at hand, named on the command line or by
+the SPK_REFERENCE_ROOT environment variable:
 
     python tests/golden/make_golden.py /path/to/spades-rs
 
@@ -195,4 +196,7 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPK_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py /path/to/spades-rs (or set SPK_REFERENCE_ROOT)")
+    main(root)

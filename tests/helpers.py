@@ -58,6 +58,26 @@ def revcomp(s):
     return s.translate(_COMP)[::-1]
 
 
+def spelled_path(unitigs, ref, k):
+    """The unitigs that lie inside ref (either strand), ordered along it,
+    when consecutive ones overlap by k - 1 bases and together cover ref from
+    its first base to its last; else None."""
+    placed = []
+    for s in unitigs:
+        for t in (s, revcomp(s)):
+            i = ref.find(t)
+            if i >= 0:
+                placed.append((i, i + len(t)))
+                break
+    placed.sort()
+    if not placed or placed[0][0] != 0 or placed[-1][1] != len(ref):
+        return None
+    for (a0, a1), (b0, b1) in zip(placed, placed[1:]):
+        if b0 != a1 - (k - 1):
+            return None
+    return placed
+
+
 def rand_seq(rng, n):
     return "".join("ACGT"[c] for c in rng.integers(0, 4, n))
 

@@ -454,3 +454,28 @@ def test_prior_contigs(spk, ora, k):
         assert info["n_table"] == tk.shape[0]
         sk, _ = r.solid(0)
         np.testing.assert_array_equal(r.edges(0), ora.edges(sk, k))
+
+
+@pytest.mark.parametrize("k", [77, 127])
+def test_claim_wait_times_out(spk, ora, k):
+    """A wide-key table slot left claimed and never published (a writer gone
+    mid-claim): the reader's bounded wait gives up after a fraction of a
+    second, the call returns SPK_E_TIMEOUT (5), and the context still counts."""
+    import time
+    from spk._lib import lib
+    ctx = spk.Context(0)
+    t0 = time.time()
+    rc = lib().spk_diag_stuck_claim(ctx.h, k)
+    assert rc == 5, spk._lib.last_error()
+    assert "claim wait timed out" in spk._lib.last_error()
+    assert time.time() - t0 < 30
+    data, offs, lens = synth_small_packed()
+    r = spk.count((data, offs, lens), [k], ctx=ctx, bloom_bits=1 << 20, list_min_count=1)
+    tw = ora.count(data, offs, lens, k, 1 << 20, mode=ora.MODE_TWICE)
+    gk, gc = r.kmers(0, 1)
+    tk, tc = tw.table(1)
+    np.testing.assert_array_equal(gk, tk)
+    np.testing.assert_array_equal(gc, tc)
+    r.close()
+    with pytest.raises(spk.SpkError):
+        spk._lib.check(lib().spk_diag_stuck_claim(ctx.h, 55))

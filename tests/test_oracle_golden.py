@@ -183,6 +183,47 @@ def test_ecoli_reference_kmers_are_solid(ora):
             assert tuple(pyref.limbs(can)[: nlimbs(k)]) in solid
 
 
+def test_ecoli_pipeline_spells_reference(ora):
+    """The reference's integration test (tests/test_pipeline.rs:33-91) on the
+    oracle: k = 31, a 16 Mi-bit Bloom, error correction, the adaptive cutoff
+    at min_coverage 5, then CompactedGraph::build.  The unitigs spell
+    data/reference_1K.fa.gz as one path; the only others are error tips,
+    which the reference's simplifier (outside the counting path) clips."""
+    from helpers import revcomp, spelled_path
+    data, offs, lens, d = ecoli_packed()
+    ref = str(d["reference_1K"][0])
+    k = 31
+    res = ora.count(data, offs, lens, k, 16 * 1024 * 1024, mode=ora.MODE_TWICE, correct=True)
+    tk, tc = res.table(1)
+    keep = tc >= ora.cutoff(tc, 5.0)
+    seqs, _, _ = ora.unitigs(tk[keep], tc[keep], k)
+    path = spelled_path(seqs, ref, k)
+    assert path is not None
+    assert len(path) < len(seqs)  # the tips split the contig at their branch points
+    off = [s for s in seqs if s not in {ref[a:b] for a, b in path} and revcomp(s) not in {ref[a:b] for a, b in path}]
+    assert all(len(s) < 2 * k for s in off)
+
+
+def test_threaded_twice_count_equals_serial(ora):
+    """The twice tier is order-free, so the threaded oracle (the checker of the
+    full-size GPU tests and of the benchmark's parity check) gives the serial
+    table and tiers exactly, whatever its thread count."""
+    from spk import synth
+    p = synth.c2(0.004).packed
+    for k in (21, 55, 77):
+        s = ora.count(p.data, p.offsets, p.lengths, k, 1 << 22, mode=ora.MODE_TWICE)
+        sk, sc = s.table(1)
+        ss, st = s.bloom()
+        for threads in (2, 7):
+            t = ora.count(p.data, p.offsets, p.lengths, k, 1 << 22, mode=ora.MODE_TWICE, threads=threads)
+            tk, tc = t.table(1)
+            ts, tt = t.bloom()
+            np.testing.assert_array_equal(tk, sk)
+            np.testing.assert_array_equal(tc, sc)
+            np.testing.assert_array_equal(ts, ss)
+            np.testing.assert_array_equal(tt, st)
+
+
 def test_ecoli_packing_matches_oracle_ingest(ora):
     """The committed ecoli_1K packing equals the C++ oracle's ingest of the same reads."""
     data, offs, lens, d = ecoli_packed()

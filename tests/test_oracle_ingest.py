@@ -12,7 +12,10 @@ import pytest
 from helpers import fasta_text, fastq_text, load_npz, messy_reads, rand_seq
 from oracle import pyref
 
-REF_DATA = "/root/reference/data"
+# The spades-rs checkout whose data/ holds the reference's own test reads, if
+# the caller points at one (SPK_REFERENCE_ROOT); the test that reads them is
+# skipped otherwise.
+REF_DATA = os.path.join(os.environ.get("SPK_REFERENCE_ROOT", ""), "data")
 
 
 def py_paired(t1, t2):
@@ -87,8 +90,9 @@ def test_edge_texts(ora):
         assert p.sizes()["n_reads"] == 0
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DATA, "ecoli_1K_1.fq.gz")),
-                    reason="the reference's test data is not on this machine")
+@pytest.mark.skipif(not os.environ.get("SPK_REFERENCE_ROOT")
+                    or not os.path.exists(os.path.join(REF_DATA, "ecoli_1K_1.fq.gz")),
+                    reason="SPK_REFERENCE_ROOT does not name a spades-rs checkout with its test data")
 def test_reference_ecoli_reads_match_golden(ora):
     """The reference's data/ecoli_1K_{1,2}.fq.gz parsed by the oracle equal the
     golden packed store (made from the same files by the Python restatement)."""
