@@ -115,6 +115,12 @@ def lib():
         L.ora_edges.restype = C.c_size_t
         L.ora_edges.argtypes = [u64p, C.c_size_t, C.c_uint, C.POINTER(u64p)]
         L.ora_free.argtypes = [C.c_void_p]
+        L.ora_shard_bloom.restype = None
+        L.ora_shard_bloom.argtypes = [u8p, C.c_size_t, u64p, u32p, C.c_size_t, C.c_uint, C.c_uint64,
+                                      C.c_uint64, C.c_uint64, u64p, u64p]
+        L.ora_shard_count.restype = C.c_void_p
+        L.ora_shard_count.argtypes = [u8p, C.c_size_t, u64p, u32p, C.c_size_t, C.c_uint, C.c_uint64, u64p,
+                                      C.c_uint, C.c_uint]
         _LIB = L
     return _LIB
 
@@ -450,3 +456,34 @@ def edges(solid_keys: np.ndarray, k: int) -> np.ndarray:
     arr = np.ctypeslib.as_array(out, shape=(max(n, 1) * Le,)).copy()[: n * Le].reshape(n, Le)
     lib().ora_free(out)
     return arr
+
+
+def shard_words(num_words: int, rank: int, world: int):
+    """Bloom words [lo, hi) of one rank in the sharded design."""
+    return num_words * rank // world, num_words * (rank + 1) // world
+
+
+def shard_bloom(data, offsets, lengths, k: int, bloom_bits: int, rank: int, world: int):
+    """Phase 1 of one rank: the seen and twice words of its word range."""
+    num_words = max((bloom_bits + 63) // 64, 1)
+    lo, hi = shard_words(num_words, rank, world)
+    d = np.ascontiguousarray(data, dtype=np.uint8)
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    ln = np.ascontiguousarray(lengths, dtype=np.uint32)
+    seen = np.zeros(max(hi - lo, 1), dtype=np.uint64)
+    twice = np.zeros(max(hi - lo, 1), dtype=np.uint64)
+    lib().ora_shard_bloom(_p(d, u8p), d.size, _p(o, u64p), _p(ln, u32p), ln.size, k, C.c_uint64(bloom_bits),
+                          lo, hi, _p(seen, u64p), _p(twice, u64p))
+    return seen[: hi - lo], twice[: hi - lo]
+
+
+def shard_count(data, offsets, lengths, k: int, bloom_bits: int, twice, rank: int, world: int):
+    """Phase 2 of one rank: its own k-mers counted and admitted against the
+    gathered twice tier; (keys, counts) sorted."""
+    d = np.ascontiguousarray(data, dtype=np.uint8)
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    ln = np.ascontiguousarray(lengths, dtype=np.uint32)
+    tw = np.ascontiguousarray(twice, dtype=np.uint64)
+    h = lib().ora_shard_count(_p(d, u8p), d.size, _p(o, u64p), _p(ln, u32p), ln.size, k, C.c_uint64(bloom_bits),
+                              _p(tw, u64p), rank, world)
+    return CountResult(h, k).table(1)

@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <map>
+
 #include "spk_oracle.h"
 
 using namespace ora;
@@ -308,5 +310,82 @@ size_t ora_edges(const uint64_t* solid_keys, size_t n, unsigned k, uint64_t** ou
   return e.size();
 }
 void ora_free(void* p) { free(p); }
+
+// ---- one rank's share of the sharded design (several GPUs) ----------------
+// Rank r of G owns the Bloom words [r W / G, (r + 1) W / G) and the k-mers
+// whose hash_kmer256(seed 1) falls in the r-th of G equal ranges of 2^64.
+// Phase 1: the rank applies the twice-tier inserts (bloom.rs:95-97 with the
+// twice tier) of every k-mer occurrence whose position lies in its words;
+// the tiers are order-free, so the ranks' word ranges side by side are the
+// single filter.  Phase 2, with the gathered twice tier: the rank counts
+// every occurrence of its own k-mers (assemble.rs:175-219 without the gate)
+// and admits a k-mer seen once when its three twice bits are set.  The
+// ranks' tables are disjoint; merged and sorted they are the single table.
+// Test infrastructure: the restatement the multi-rank tests check the
+// partition and the exchange against.
+static uint32_t owner_of(const Kmer256& c, unsigned world) {
+  return (uint32_t)(((unsigned __int128)hash_kmer256(c, SEED1) * world) >> 64);
+}
+void ora_shard_bloom(const uint8_t* data, size_t data_len, const uint64_t* offsets, const uint32_t* lengths,
+                     size_t n_reads, unsigned k, uint64_t bloom_bits, uint64_t word_lo, uint64_t word_hi,
+                     uint64_t* seen, uint64_t* twice) {
+  PackedReads pr;
+  pr.data.assign(data, data + data_len);
+  pr.offsets.assign(offsets, offsets + n_reads);
+  pr.lengths.assign(lengths, lengths + n_reads);
+  uint64_t num_words = std::max<uint64_t>((bloom_bits + 63) / 64, 1), size_bits = num_words * 64;
+  memset(seen, 0, (word_hi - word_lo) * 8);
+  memset(twice, 0, (word_hi - word_lo) * 8);
+  std::vector<uint8_t> buf;
+  for (size_t idx = 0; idx < pr.size(); idx++) {
+    pr.get_read(idx, buf);
+    for (size_t i = 0; i + k <= buf.size(); i++) {
+      Kmer256 km;
+      if (!k256_from_bytes(buf.data() + i, k, k, &km)) continue;
+      const Kmer256 can = k256_canonical(km, k, nullptr);
+      const uint64_t h[3] = {hash_kmer256(can, SEED1) % size_bits, hash_kmer256(can, SEED2) % size_bits,
+                             hash_kmer256(can, SEED3) % size_bits};
+      for (int j = 0; j < 3; j++) {
+        const uint64_t w = h[j] / 64, b = 1ULL << (h[j] % 64);
+        if (w < word_lo || w >= word_hi) continue;
+        if (seen[w - word_lo] & b) twice[w - word_lo] |= b;
+        seen[w - word_lo] |= b;
+      }
+    }
+  }
+}
+void* ora_shard_count(const uint8_t* data, size_t data_len, const uint64_t* offsets, const uint32_t* lengths,
+                      size_t n_reads, unsigned k, uint64_t bloom_bits, const uint64_t* twice, unsigned rank,
+                      unsigned world) {
+  PackedReads pr;
+  pr.data.assign(data, data + data_len);
+  pr.offsets.assign(offsets, offsets + n_reads);
+  pr.lengths.assign(lengths, lengths + n_reads);
+  uint64_t num_words = std::max<uint64_t>((bloom_bits + 63) / 64, 1), size_bits = num_words * 64;
+  std::map<Kmer256, uint32_t> cnt;
+  std::vector<uint8_t> buf;
+  for (size_t idx = 0; idx < pr.size(); idx++) {
+    pr.get_read(idx, buf);
+    for (size_t i = 0; i + k <= buf.size(); i++) {
+      Kmer256 km;
+      if (!k256_from_bytes(buf.data() + i, k, k, &km)) continue;
+      const Kmer256 can = k256_canonical(km, k, nullptr);
+      if (owner_of(can, world) == rank) cnt[can]++;
+    }
+  }
+  CountResult* r = new CountResult();
+  for (auto& kv : cnt) {
+    bool admit = kv.second >= 2;
+    if (!admit) {
+      admit = true;
+      for (uint64_t seed : {SEED1, SEED2, SEED3}) {
+        const uint64_t h = hash_kmer256(kv.first, seed) % size_bits;
+        admit = admit && ((twice[h / 64] >> (h % 64)) & 1);
+      }
+    }
+    if (admit) r->table.push_back(CountEntry{kv.first, kv.second});
+  }
+  return r;  // sorted: std::map order is Kmer256 order
+}
 
 }  // extern "C"

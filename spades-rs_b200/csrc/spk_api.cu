@@ -475,6 +475,8 @@ int spk_result_table_view(spk_result* res, int ki, spk_table_view* v) {
   if ((rc = get_k(res, ki))) return rc;
   if (!v) return fail(SPK_E_INVALID_ARG, "null view");
   KResult& kr = *res->ks[ki];
+  if (!kr.tslots.p)
+    return fail(SPK_E_INVALID_ARG, "the count table was not kept (SPK_F_KEEP_TABLE)");
   v->slots = kr.table.slots;
   v->capacity = kr.table.capacity;
   v->key_limbs = (uint32_t)kr.nl;

@@ -884,12 +884,19 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
   warp_add_u64(occ_out, occ);
 }
 
+// Keys in coarse bucket b: its fill, at most its capacity (a bucket that
+// overflowed holds only what fits; the overflow flag sends the job back).
+__device__ __forceinline__ uint64_t coarse_len(const CoarseView& cv, uint32_t b) {
+  const uint64_t capb = cv.uniform ? cv.uniform : cv.base[b + 1] - cv.base[b];
+  return min((uint64_t)cv.fill[(uint64_t)b * kFillStride], capb);
+}
+
 // cfirst[b] = the first chunk of bucket b (kFineChunk keys per chunk);
 // cfirst[kCoarse] = the number of chunks.  One warp.
-__global__ void k_coarse_chunks(const unsigned int* __restrict__ fill, uint32_t* __restrict__ cfirst) {
+__global__ void k_coarse_chunks(CoarseView cv, uint32_t* __restrict__ cfirst) {
   const unsigned lane = threadIdx.x & 31;
-  const uint32_t c0 = (fill[(2 * lane) * kFillStride] + kFineChunk - 1) / kFineChunk;
-  const uint32_t c1 = (fill[(2 * lane + 1) * kFillStride] + kFineChunk - 1) / kFineChunk;
+  const uint32_t c0 = (uint32_t)((coarse_len(cv, 2 * lane) + kFineChunk - 1) / kFineChunk);
+  const uint32_t c1 = (uint32_t)((coarse_len(cv, 2 * lane + 1) + kFineChunk - 1) / kFineChunk);
   uint32_t x = c0 + c1;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
@@ -927,7 +934,7 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
     for (uint32_t step = kCoarse >> 1; step; step >>= 1)
       if (cfirst[b + step] <= c) b += step;
     const uint64_t bb = coarse_base(cv, b);
-    const uint64_t bend = bb + cv.fill[(uint64_t)b * kFillStride];
+    const uint64_t bend = bb + coarse_len(cv, b);
     const uint64_t s0 = bb + (uint64_t)(c - cfirst[b]) * kFineChunk;
     const uint32_t n = (uint32_t)min((uint64_t)kFineChunk, bend - s0);
     for (uint32_t f = threadIdx.x; f < nfine; f += blockDim.x) hist[f] = 0;
@@ -1200,12 +1207,44 @@ __device__ __forceinline__ void span_emit_sorted(const typename SpanKey<NL>::T* 
   }
 }
 
+// Output of the span count when the count table is not kept: the span's
+// k-mers counted at least lmin times (at least twice) go straight to the
+// k-mer list, and those counted once to a buffer of keys that singleton
+// admission reads after the Bloom tiers are built.  Both hold every distinct
+// k-mer at most once, so cap (the table's slot count) bounds each.
+constexpr int kHistBins = 256;  // counts >= 255 share the last bin
+struct ListOut {
+  uint64_t* l0;                 // list: limb 0 (SoA)
+  uint64_t* l1;                 // list: limb 1 (k > 32)
+  uint32_t* cnt;                // list: counts (nullptr: the table is written instead)
+  uint64_t* s0;                 // singletons: limb 0
+  uint64_t* s1;                 // singletons: limb 1
+  uint64_t cap;
+  uint32_t lmin;                // smallest count listed (>= 2 here; singletons are listed
+                                // by admission when lmin is 1)
+  unsigned long long* fill;     // [0] list entries, [1] singletons
+  unsigned long long* hist;     // kHistBins counts of the k-mers counted >= 2 times
+  unsigned long long* occ2;     // occurrences of the k-mers counted >= 2 times
+};
+
 template <int NL, bool OPS>
 __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartView pv, TableView t, unsigned k,
                                                             FastMod fm, U128* __restrict__ tiers,
-                                                            RangeView rv) {
+                                                            RangeView rv, ListOut lo) {
   typedef typename SpanKey<NL>::T KeyT;
   extern __shared__ __align__(16) unsigned char span_smem[];
+  // list output: per (write-out round, warp) entry counts of the list and of
+  // the singletons, their exclusive prefixes, and the span's two reservations
+  constexpr int kWarps = kPartBlock / 32;
+  constexpr int kRounds = (1 << kHomeBits) / kPartBlock > 0 ? (1 << kHomeBits) / kPartBlock : 1;
+  __shared__ uint32_t lw[2][kRounds * kWarps];
+  __shared__ unsigned long long lbase[2];
+  __shared__ unsigned s_hist[kHistBins];
+  const bool to_list = lo.cnt != nullptr;
+  const uint32_t lmin = lo.lmin < 2 ? 2u : lo.lmin;
+  uint64_t occ2 = 0;
+  if (to_list)
+    for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) s_hist[i] = 0;
   const uint32_t S = 1u << t.log2span;
   KeyT* keys = (KeyT*)span_smem;
   uint32_t* cnt = (uint32_t*)(span_smem + (size_t)S * sizeof(KeyT));
@@ -1274,22 +1313,89 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
     if (full) atomicOr(t.err, 1);  // span full: the host regrows the table
     __syncthreads();
     const uint64_t g0 = (uint64_t)p << t.log2span;
+    if (OPS && to_list) {
+      // Entries of each (round, warp) of the write-out loop below: a ballot
+      // per round, then one reservation per span for the list and one for
+      // the singletons, so that each warp's entries of a round are
+      // contiguous in both.
+      const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      const uint32_t rounds = (S + blockDim.x - 1) / blockDim.x;
+      for (uint32_t r = 0; r < rounds; r++) {
+        const uint32_t s = r * blockDim.x + threadIdx.x;
+        const uint32_t c = s < S ? cnt[s] : 0u;
+        const unsigned bl = __ballot_sync(FULL, c >= lmin), bs = __ballot_sync(FULL, c == 1);
+        if (lane == 0) {
+          lw[0][r * kWarps + warp] = __popc(bl);
+          lw[1][r * kWarps + warp] = __popc(bs);
+        }
+        if (c >= 2) {
+          atomicAdd(&s_hist[c < kHistBins - 1 ? c : kHistBins - 1], 1u);
+          occ2 += c;
+        }
+      }
+      __syncthreads();
+      if (warp < 2) {
+        // exclusive scan of the (round, warp) counts of list `warp`
+        const uint32_t n = ((S + blockDim.x - 1) / blockDim.x) * kWarps;
+        uint32_t carry = 0;
+        for (uint32_t b = 0; b < n; b += 32) {
+          const uint32_t v = b + lane < n ? lw[warp][b + lane] : 0u;
+          uint32_t x = v;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, x, d);
+            if ((int)lane >= d) x += y;
+          }
+          if (b + lane < n) lw[warp][b + lane] = carry + x - v;
+          carry += __shfl_sync(FULL, x, 31);
+        }
+        if (lane == 0) lbase[warp] = carry ? atomicAdd(lo.fill + warp, (unsigned long long)carry) : 0ULL;
+      }
+      __syncthreads();
+    }
     if (OPS) {
-      // Write the span out and count its Bloom operations per range.
-      for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
-        const uint32_t c = cnt[s];
+      // Write the span out (to the table, or to the list and the singleton
+      // keys) and count its Bloom operations per range.
+      const unsigned warp = threadIdx.x >> 5;
+      const uint32_t rounds = (S + blockDim.x - 1) / blockDim.x;
+      for (uint32_t r = 0; r < rounds; r++) {
+        const uint32_t s = r * blockDim.x + threadIdx.x;
+        if (!to_list && s >= S) continue;
+        const uint32_t c = s < S ? cnt[s] : 0u;
         Seq<NL> C;
         if (NL == 1) {
           C.v[0] = c ? ((unsigned long long*)keys)[s] : kEmpty;
-          ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
-          *gp = make_ulonglong2(C.v[0], (unsigned long long)c);
+          if (!to_list) {
+            ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
+            *gp = make_ulonglong2(C.v[0], (unsigned long long)c);
+          }
         } else {
           const U128 kv = c ? ((U128*)keys)[s] : U128{kEmpty, kEmpty};
           C.v[0] = kv.x;
           C.v[NL - 1] = kv.y;
-          ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
-          gp[0] = make_ulonglong2(kv.x, kv.y);
-          gp[1] = make_ulonglong2((unsigned long long)c, 0ULL);
+          if (!to_list) {
+            ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
+            gp[0] = make_ulonglong2(kv.x, kv.y);
+            gp[1] = make_ulonglong2((unsigned long long)c, 0ULL);
+          }
+        }
+        if (to_list) {
+          // (lanes past the span's end have c == 0 and take part in the ballots only)
+          const unsigned bl = __ballot_sync(FULL, c >= lmin), bs = __ballot_sync(FULL, c == 1);
+          if (c >= lmin) {
+            const uint64_t q = lbase[0] + lw[0][r * kWarps + warp] + __popc(bl & lanemask_lt());
+            if (q < lo.cap) {
+              lo.l0[q] = C.v[0];
+              if (NL == 2) lo.l1[q] = C.v[NL - 1];
+              lo.cnt[q] = c;
+            }
+          } else if (c == 1) {
+            const uint64_t q = lbase[1] + lw[1][r * kWarps + warp] + __popc(bs & lanemask_lt());
+            if (q < lo.cap) {
+              lo.s0[q] = C.v[0];
+              if (NL == 2) lo.s1[q] = C.v[NL - 1];
+            }
+          }
         }
         if (!c) continue;
         uint64_t raw[3], pos[3];
@@ -1383,6 +1489,12 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
       bloom_ops_distinct<U>(tiers, pos, c);
     }
     __syncthreads();
+  }
+  if (to_list) {
+    warp_add_u64(lo.occ2, occ2);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
+      if (s_hist[i]) atomicAdd(lo.hist + i, (unsigned long long)s_hist[i]);
   }
 }
 
@@ -1543,8 +1655,6 @@ __global__ void __launch_bounds__(kBlock) k_tier_finish(const U128* __restrict__
 // sums: [0] admitted k-mers, [1] admitted count-1 k-mers, [2] admitted
 // occurrences (sum of counts), [3] list length.
 // ---------------------------------------------------------------------------
-constexpr int kHistBins = 256;  // counts >= 255 share the last bin
-
 // A table slot: its count, and its key in C (keys of empty slots are junk).
 template <int NL>
 __device__ __forceinline__ uint32_t load_slot(const TableView& t, uint64_t s, Seq<NL>& C) {
@@ -1668,6 +1778,52 @@ __global__ void __launch_bounds__(kBlock, 4) k_admit_compact(TableView t, unsign
   __syncthreads();
   for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
     if (sh[i]) atomicAdd(hist + i, (unsigned long long)sh[i]);
+}
+
+// Singleton admission when the span count wrote the list instead of the
+// table: a k-mer counted once is admitted when its three twice bits are set
+// (a k-mer counted twice always has them).  Admitted singletons add to the
+// count histogram's bin 1 and, when the list keeps count-1 k-mers (lmin 1),
+// are appended to the list after the span count's entries, one reservation
+// per warp.  sums: [0] admitted singletons.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_admit_singletons(ListOut lo, unsigned k, FastMod fm,
+                                                              const uint64_t* __restrict__ twice,
+                                                              unsigned long long* __restrict__ sums) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t n = min((uint64_t)lo.fill[1], lo.cap);
+  uint64_t adm = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    bool admit = false;
+    Seq<NL> C;
+    if (i < n) {
+      C.v[0] = __ldcs(lo.s0 + i);
+      if (NL == 2) C.v[NL - 1] = __ldcs(lo.s1 + i);
+      uint64_t raw[3], pos[3];
+      bloom_positions<NL>(C, k, fm, raw, pos);
+      const uint64_t a = __ldg(twice + (pos[0] >> 6)), b = __ldg(twice + (pos[1] >> 6)),
+                     c = __ldg(twice + (pos[2] >> 6));
+      admit = (a >> (pos[0] & 63)) & (b >> (pos[1] & 63)) & (c >> (pos[2] & 63)) & 1;
+    }
+    adm += admit;
+    if (lo.lmin <= 1) {
+      const unsigned m = __ballot_sync(FULL, admit);
+      if (m) {
+        unsigned long long wb = 0;
+        if (lane == 0) wb = atomicAdd(lo.fill, (unsigned long long)__popc(m));
+        const uint64_t q = __shfl_sync(FULL, wb, 0) + __popc(m & lanemask_lt());
+        if (admit && q < lo.cap) {
+          lo.l0[q] = C.v[0];
+          if (NL == 2) lo.l1[q] = C.v[NL - 1];
+          lo.cnt[q] = 1;
+        }
+      }
+    }
+  }
+  warp_add_u64(sums, adm);
+  warp_add_u64(lo.hist + 1, adm);
 }
 
 // Solid k-mers of the list (count >= cutoff), for cutoffs the histogram cannot resolve.
@@ -2062,7 +2218,8 @@ static int launch_part_fine(spk_ctx* ctx, cudaStream_t st, const CoarseView& cv,
 // directly; else bin them by range into rv.
 template <int NL>
 static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, const TableView& t,
-                             unsigned k, const FastMod& fm, U128* tiers, const RangeView& rv) {
+                             unsigned k, const FastMod& fm, U128* tiers, const RangeView& rv,
+                             const ListOut& lo) {
   size_t smem = ((size_t)1 << t.log2span) * (sizeof(typename SpanKey<NL>::T) + 4);
   const uint64_t nparts = 1ULL << pv.log2parts;
   const int grid = (int)std::min<uint64_t>(nparts, (uint64_t)ctx->sm_count * kPartCtasPerSm);
@@ -2071,11 +2228,12 @@ static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, 
     if (NL == 2 && kSortedOps) smem += ((rv.nranges + 1) & ~1u) * 4;  // range cursors
     int rc;
     if ((rc = raise_smem_limit((const void*)k_part_count<NL, true>, smem))) return rc;
-    k_part_count<NL, true><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv);
+    k_part_count<NL, true><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv, lo);
   } else {
     int rc;
     if ((rc = raise_smem_limit((const void*)k_part_count<NL, false>, smem))) return rc;
-    k_part_count<NL, false><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv);
+    ListOut none{};  // the in-place Bloom form writes the table
+    k_part_count<NL, false><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv, none);
   }
   return SPK_OK;
 }
@@ -2200,11 +2358,12 @@ static float ms_between(const Ev& a, const Ev& b) {
 // slots (0: the whole table).  init = false leaves the slots unwritten for a
 // pass that writes every slot itself.
 static int alloc_table(spk_ctx* ctx, KResult& kr, cudaStream_t st, uint64_t cap,
-                       uint32_t log2span = 0, bool init = true) {
+                       uint32_t log2span = 0, bool init = true, bool with_slots = true) {
   const uint32_t sb = slot_bytes(kr.nl);
   int rc;
-  if ((rc = kr.tslots.alloc(cap * sb, st))) return rc;
-  if (init) {
+  if (!with_slots) kr.tslots.release();
+  else if ((rc = kr.tslots.alloc(cap * sb, st))) return rc;
+  if (init && with_slots) {
     SPK_DISPATCH_NL(kr.nl, launch_init, ctx, st, kr.tslots.as<uint8_t>(), cap);
     SPK_CUDA(cudaGetLastError());
   }
@@ -2229,6 +2388,8 @@ enum {
   S_EDGES = 10,
   S_OCC0 = 11,           /* occurrences before the pass */
   S_REJ = 12,            /* singletons the twice tier rejected */
+  S_LFILL = 13,          /* 2 words: list entries, singletons (span count to the list) */
+  S_OCC2 = 15,           /* occurrences of the k-mers counted at least twice */
   S_HIST = 16,           /* 256 words */
   S_WORDS = 16 + kHistBins
 };
@@ -2263,6 +2424,21 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   // so it needs the per-occurrence Bloom of the fused pass.
   const bool count_first = !gated && !ref;
   bool partitioned = count_first && nl <= 2 && !(o.flags & SPK_F_DIRECT);
+  const bool priors = o.n_prior > 0 && o.prior_seqs && o.prior_offsets && o.prior_lengths;
+  // The partitioned span count writes the k-mer list itself unless the count
+  // table is asked for (its view, or prior contigs that update it).
+  const bool table_wanted = priors || (o.flags & SPK_F_KEEP_TABLE);
+  // Thresholds of the list (src/assemble.rs:286-292, 693-694).
+  uint32_t fixed = o.min_count;
+  if (!fixed && o.min_coverage > 5.0) {
+    double v = std::max(o.min_coverage * 0.35, 2.0);
+    fixed = v >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v;
+  }
+  const uint32_t list_min = o.list_min_count ? o.list_min_count : 2;
+  // The list keeps counts >= min(cutoff, list_min).  The adaptive cutoff is
+  // never below 2, so compacting counts >= min(2 or the fixed cutoff,
+  // list_min) keeps a superset; the exact threshold filters downloads.
+  const uint32_t lmin_pre = std::max(1u, std::min(fixed ? fixed : 2u, list_min));
 
   Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1, ec0, ec1;
   uint32_t launches = 0;
@@ -2297,6 +2473,9 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   const bool use_ops = nranges <= kMaxRanges;
   DevBuf rbase, rfill, ops;
   RangeView bv{nullptr, nullptr, nullptr, 0, (uint32_t)nranges, errp};
+  bool list_mode = false;  // the span count wrote the list (no table)
+  ListOut lo{};
+  DevBuf sgl[2];           // list mode: keys of the k-mers counted once
   if (!gated) {
     // ---- fused: Bloom and the count of every k-mer in one pass ----
     k_occ<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv.lengths, rv.n_reads, k, su + S_OCC0);
@@ -2317,8 +2496,24 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     }
     for (int attempt = 0; partitioned; attempt++) {
       if (!use_ops && (rc = reset_tiers())) return rc;
-      if ((rc = alloc_table(ctx, kr, st, cap, nl == 1 ? kPartLog2Span1 : kPartLog2Span2, false)))
+      list_mode = use_ops && !table_wanted;
+      if ((rc = alloc_table(ctx, kr, st, cap, nl == 1 ? kPartLog2Span1 : kPartLog2Span2, false,
+                            !list_mode)))
         return rc;
+      lo = ListOut{};
+      if (list_mode) {
+        // the list (entries counted >= lmin times) and the singleton keys,
+        // each at most one entry per table slot
+        for (int j = 0; j < nl; j++)
+          if ((rc = kr.list[j].alloc(cap * 8, st)) || (rc = sgl[j].alloc(cap * 8, st))) return rc;
+        if ((rc = kr.list[4].alloc(cap * 4, st))) return rc;
+        SPK_CUDA(cudaMemsetAsync(sw + S_LFILL, 0, 3 * 8, st));  // fills and S_OCC2
+        SPK_CUDA(cudaMemsetAsync(sw + S_HIST, 0, kHistBins * 8, st));
+        lo = ListOut{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
+                     kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(),
+                     nl == 2 ? sgl[1].as<uint64_t>() : nullptr, cap, lmin_pre, su + S_LFILL,
+                     su + S_HIST, su + S_OCC2};
+      }
       TableView& t = kr.table;
       t.err = errp;
       SPK_CUDA(cudaMemsetAsync(sw, 0, (S_ERR + 1) * 8, st));
@@ -2374,7 +2569,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
           if ((rc = fetch(S_ERR + 1))) return rc;
           if ((int)host[S_ERR] & kErrRegion) return fail(SPK_E_CUDA, "coarse bucket overflow after resizing");
         }
-        k_coarse_chunks<<<1, 32, 0, st>>>(cfill.as<unsigned int>(), cfirst.as<uint32_t>());
+        k_coarse_chunks<<<1, 32, 0, st>>>(cv, cfirst.as<uint32_t>());
         if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
         else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
         if (rc) return rc;
@@ -2439,8 +2634,8 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
                        (uint32_t)nranges, errp};
       }
       SPK_CUDA(cudaEventRecord(kc0.e, st));
-      if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, tiers, bv);
-      else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, tiers, bv);
+      if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, tiers, bv, lo);
+      else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, tiers, bv, lo);
       if (rc) return rc;
       SPK_CUDA(cudaGetLastError());
       SPK_CUDA(cudaEventRecord(kc1.e, st));
@@ -2466,8 +2661,12 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
         SPK_CUDA(cudaMemsetAsync(errp, 0, 4, st));
         bv = RangeView{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), 0,
                        (uint32_t)nranges, errp};
-        if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, tiers, bv);
-        else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, tiers, bv);
+        if (list_mode) {
+          SPK_CUDA(cudaMemsetAsync(sw + S_LFILL, 0, 3 * 8, st));
+          SPK_CUDA(cudaMemsetAsync(sw + S_HIST, 0, kHistBins * 8, st));
+        }
+        if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, tiers, bv, lo);
+        else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, tiers, bv, lo);
         if (rc) return rc;
         SPK_CUDA(cudaGetLastError());
         launches += 2;  // k_part_bases, k_part_count
@@ -2582,7 +2781,6 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   SPK_CUDA(cudaEventRecord(e2.e, st));
 
   // ---- prior contigs (src/assemble.rs:244-284), after singleton admission ----
-  const bool priors = o.n_prior > 0 && o.prior_seqs && o.prior_offsets && o.prior_lengths;
   if (priors) {
     // Mark the rejected singletons (nothing is listed), then inject.
     DevBuf junk;
@@ -2622,21 +2820,27 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   }
 
   // ---- admission of singletons, histogram, compaction, cutoff ----
-  uint32_t fixed = o.min_count;
-  if (!fixed && o.min_coverage > 5.0) {  // src/assemble.rs:693-694
-    double v = std::max(o.min_coverage * 0.35, 2.0);
-    fixed = v >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v;
-  }
-  const uint32_t list_min = o.list_min_count ? o.list_min_count : 2;
-  // The list keeps counts >= min(cutoff, list_min).  The adaptive cutoff is
-  // never below 2, so compacting counts >= min(2 or the fixed cutoff,
-  // list_min) keeps a superset; the exact threshold filters downloads.
-  const uint32_t lmin_pre = std::max(1u, std::min(fixed ? fixed : 2u, list_min));
   kr.list_min = lmin_pre;
+  uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (list_mode) {
+    // The span count listed the k-mers counted >= lmin times and histogrammed
+    // those counted twice or more; admission adds the singletons.
+    SPK_CUDA(cudaMemsetAsync(sw + S_SUMS, 0, 4 * 8, st));
+    SPK_CUDA(cudaMemsetAsync(sw + S_REJ, 0, 8, st));
+    if (nl == 1)
+      k_admit_singletons<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lo, k, kr.fm, kr.twice.as<uint64_t>(),
+                                                                 su + S_SUMS + 1);
+    else
+      k_admit_singletons<2><<<grid_for(ctx, 8), kBlock, 0, st>>>(lo, k, kr.fm, kr.twice.as<uint64_t>(),
+                                                                 su + S_SUMS + 1);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    for (int j = 0; j < nl; j++) lp[j] = kr.list[j].as<uint64_t>();
+  }
   // List capacity from the Bloom: k-mers seen at least twice (twice-tier
   // estimate, an overestimate), plus admitted singletons if they are listed.
-  uint64_t lcap;
-  {
+  uint64_t lcap = 0;
+  if (!list_mode) {
     const double md = (double)size_bits;
     const double fs = std::min((double)info.seen_popcount / md, 0.999999);
     const double ft = std::min((double)info.twice_popcount / md, 0.999999);
@@ -2646,8 +2850,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     if (kr.list_min <= 1) est += std::max(n_all - n2, 0.0) * ft * ft * ft * 1.5 + 65536;
     lcap = std::min<uint64_t>((uint64_t)est, cap);
   }
-  uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
-  for (int pass = 0;; pass++) {
+  for (int pass = 0; !list_mode; pass++) {
     for (int j = 0; j < nl; j++) {
       if ((rc = kr.list[j].alloc(std::max<uint64_t>(lcap, 1) * 8, st))) return rc;
       lp[j] = kr.list[j].as<uint64_t>();
@@ -2676,11 +2879,24 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   const uint32_t* hthr = (const uint32_t*)(host + S_THR);
   info.cutoff = hthr[0];
   kr.list_min = hthr[1];
-  info.n_table = host[S_SUMS + 0];
-  info.n_singletons = host[S_SUMS + 1];
-  info.n_distinct = host[S_SUMS + 0] + host[S_REJ];
-  info.admitted_occurrences = host[S_SUMS + 2];
-  kr.list_len = host[S_SUMS + 3];
+  if (list_mode) {
+    uint64_t n2 = 0;
+    for (int c = 2; c < kHistBins; c++) n2 += host[S_HIST + c];
+    const uint64_t adm1 = host[S_SUMS + 1];
+    info.n_table = n2 + adm1;
+    info.n_singletons = adm1;
+    info.n_distinct = n2 + host[S_LFILL + 1];
+    info.admitted_occurrences = host[S_OCC2] + adm1;
+    kr.list_len = host[S_LFILL];
+    if (kr.list_len > cap || host[S_LFILL + 1] > cap)
+      return fail(SPK_E_CUDA, "k-mer list larger than the table it came from");
+  } else {
+    info.n_table = host[S_SUMS + 0];
+    info.n_singletons = host[S_SUMS + 1];
+    info.n_distinct = host[S_SUMS + 0] + host[S_REJ];
+    info.admitted_occurrences = host[S_SUMS + 2];
+    kr.list_len = host[S_SUMS + 3];
+  }
   auto hist_from = [&](uint32_t c0) {
     uint64_t ns = 0;
     for (int c = (int)c0; c < kHistBins; c++) ns += host[S_HIST + c];
@@ -2773,6 +2989,295 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   return SPK_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The default job for 12 <= k <= 64 with few host round trips.  It runs the
+// partitioned schedule with the two-level read partition and the span count
+// writing the k-mer list (no table), and reads device values back three
+// times: the occurrence count that sizes the table, one block of counters
+// after the cutoff (sizes of the lists, the histogram, the overflow flags),
+// and the edge count at the end.  Region, bucket and range overflows (skewed
+// inputs) and full spans are only checked at the mid-job readback: the
+// kernels keep every access inside its buffer, and on any overflow the job is
+// counted again by count_one_k, which lays the buffers out exactly.
+// Returns kNotThisPath when the inputs need another layout (count_one_k
+// handles them), kRedo after an overflow, else the status.
+// ---------------------------------------------------------------------------
+constexpr int kNotThisPath = -100, kRedo = -101;
+
+int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv_in, unsigned k,
+                     const spk_count_opts& o, KResult& kr) {
+  const int nl = (int)((k + 31) / 32);
+  if (k < 12 || nl > 2) return kNotThisPath;
+  if (o.flags & (SPK_F_GATED | SPK_F_CORRECT | SPK_F_REF_SOLID | SPK_F_DIRECT | SPK_F_KEEP_TABLE))
+    return kNotThisPath;
+  if (o.n_prior > 0 && o.prior_seqs && o.prior_offsets && o.prior_lengths) return kNotThisPath;
+  const uint64_t bloom_bits = o.bloom_bits ? o.bloom_bits : (512ULL << 20);
+  const uint64_t num_words = std::max<uint64_t>((bloom_bits + 63) / 64, 1);  // src/bloom.rs:27
+  const uint64_t size_bits = num_words * 64;                                  // src/bloom.rs:28
+  const uint64_t nranges = (size_bits + (1ULL << kLog2Range) - 1) >> kLog2Range;
+  if (nranges > kMaxRanges) return kNotThisPath;
+  int rc;
+  DevBuf scratch;
+  if ((rc = scratch.alloc(S_WORDS * 8, st))) return rc;
+  uint64_t* sw = scratch.as<uint64_t>();
+  SPK_CUDA(cudaMemsetAsync(sw, 0, S_WORDS * 8, st));
+  unsigned long long* su = (unsigned long long*)sw;
+  // ---- the first readback: occurrences, which size the table ----
+  Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1;
+  SPK_CUDA(cudaEventRecord(e0.e, st));
+  k_occ<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv_in.lengths, rv_in.n_reads, k, su + S_OCC0);
+  SPK_CUDA(cudaGetLastError());
+  SPK_CUDA(cudaMemcpyAsync(host + S_OCC0, sw + S_OCC0, 8, cudaMemcpyDeviceToHost, st));
+  SPK_CUDA(cudaStreamSynchronize(st));
+  const uint64_t occ0 = host[S_OCC0];
+  uint64_t cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(occ0);
+  const uint32_t log2span = nl == 1 ? kPartLog2Span1 : kPartLog2Span2;
+  uint32_t log2cap = 0;
+  while ((1ULL << log2cap) < cap) log2cap++;
+  if (log2cap <= log2span) return kNotThisPath;
+  const uint32_t log2parts = log2cap - log2span;
+  if (!SPK_TWO_LEVEL || log2parts <= kCoarseBits || log2parts - kCoarseBits > kFineMaxBits) return kNotThisPath;
+  {
+    size_t fr = 0, tot = 0;
+    SPK_CUDA(cudaMemGetInfo(&fr, &tot));
+    if ((occ0 * 3 + (1u << 22)) * (uint64_t)nl * 8 > tot / 4) return kNotThisPath;
+  }
+
+  kr.k = k;
+  kr.nl = nl;
+  kr.num_words = num_words;
+  kr.fm = make_fastmod(size_bits);
+  spk_result_info& info = kr.info;
+  memset(&info, 0, sizeof info);
+  info.k = k;
+  info.bloom_size_bits = size_bits;
+  int* errp = (int*)(sw + S_ERR);
+  ReadsView rv = rv_in;
+  rv.err = errp;
+  uint32_t fixed = o.min_count;
+  if (!fixed && o.min_coverage > 5.0) {  // src/assemble.rs:693-694
+    double v = std::max(o.min_coverage * 0.35, 2.0);
+    fixed = v >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v;
+  }
+  const uint32_t list_min = o.list_min_count ? o.list_min_count : 2;
+  const uint32_t lmin_pre = std::max(1u, std::min(fixed ? fixed : 2u, list_min));
+  kr.list_min = lmin_pre;
+
+  uint32_t launches = 1;  // k_occ
+  if ((rc = alloc_table(ctx, kr, st, cap, log2span, false, false))) return rc;
+  TableView& t = kr.table;
+  t.err = errp;
+  const uint64_t nparts = 1ULL << log2parts;
+
+  // ---- two-level read partition (k_part_coarse, k_part_fine) ----
+  DevBuf base, fill, region;
+  const uint64_t per = occ0 / nparts;
+  const uint64_t capu = per + (per >> 1) + 256;
+  if ((rc = base.alloc((nparts + 1) * 8, st)) || (rc = fill.alloc(nparts * 4 * kFillStride, st)) ||
+      (rc = region.alloc(nparts * capu * nl * 8, st)))
+    return rc;
+  k_part_uniform<<<64, kBlock, 0, st>>>((uint32_t)nparts, capu, base.as<uint64_t>());
+  SPK_CUDA(cudaMemsetAsync(fill.p, 0, nparts * 4 * kFillStride, st));
+  PartView pv{region.as<uint64_t>(), base.as<uint64_t>(), fill.as<unsigned int>(), capu, log2parts,
+              home_fits(k, nl) ? 1u : 0u, errp};
+  info.part_passes = 2;
+  SPK_CUDA(cudaEventRecord(ks0.e, st));
+  {
+    DevBuf cbase, cfill, cregion, cfirst;
+    const uint64_t cper = occ0 / kCoarse;
+    const uint64_t ccap = cper + (cper >> 3) + 8192;
+    if ((rc = cbase.alloc((kCoarse + 1) * 8, st)) || (rc = cfill.alloc(kCoarse * 4 * kFillStride, st)) ||
+        (rc = cregion.alloc(kCoarse * ccap * nl * 8, st)) || (rc = cfirst.alloc((kCoarse + 1) * 4, st)))
+      return rc;
+    k_part_uniform<<<1, 128, 0, st>>>(kCoarse, ccap, cbase.as<uint64_t>());
+    SPK_CUDA(cudaMemsetAsync(cfill.p, 0, kCoarse * 4 * kFillStride, st));
+    CoarseView cv{cregion.as<uint64_t>(), cbase.as<uint64_t>(), cfill.as<unsigned int>(), ccap, errp};
+    if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rv, k, pv, cv, su + S_OCC);
+    else rc = launch_part_coarse<2>(ctx, st, rv, k, pv, cv, su + S_OCC);
+    if (rc) return rc;
+    k_coarse_chunks<<<1, 32, 0, st>>>(cv, cfirst.as<uint32_t>());
+    if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
+    else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
+    if (rc) return rc;
+    SPK_CUDA(cudaGetLastError());
+    launches += 5;  // 2 x k_part_uniform, k_part_coarse, k_coarse_chunks, k_part_fine
+  }
+  SPK_CUDA(cudaEventRecord(ks1.e, st));
+
+  // ---- span count: the list, the singleton keys and the binned Bloom ops ----
+  DevBuf rbase, rfill, ops, sgl[2];
+  {
+    const uint64_t share = 3 * cap / nranges + 1;
+    const uint64_t rcap = share + (share >> 2) + 1024;
+    if ((rc = rbase.alloc((nranges + 1) * 8, st)) || (rc = rfill.alloc(nranges * 4 * kFillStride, st)) ||
+        (rc = ops.alloc(nranges * rcap * 4, st)))
+      return rc;
+    SPK_CUDA(cudaMemsetAsync(rfill.p, 0, nranges * 4 * kFillStride, st));
+    RangeView bv{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), rcap, (uint32_t)nranges,
+                 errp};
+    for (int j = 0; j < nl; j++)
+      if ((rc = kr.list[j].alloc(cap * 8, st)) || (rc = sgl[j].alloc(cap * 8, st))) return rc;
+    if ((rc = kr.list[4].alloc(cap * 4, st))) return rc;
+    ListOut lo{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
+               kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(), nl == 2 ? sgl[1].as<uint64_t>() : nullptr,
+               cap, lmin_pre, su + S_LFILL, su + S_HIST, su + S_OCC2};
+    SPK_CUDA(cudaEventRecord(kc0.e, st));
+    if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
+    else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
+    if (rc) return rc;
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaEventRecord(kc1.e, st));
+    region.release();
+    base.release();
+    fill.release();
+    // ---- Bloom tiers from the binned operations ----
+    if ((rc = kr.seen.alloc(num_words * 8, st)) || (rc = kr.twice.alloc(num_words * 8, st))) return rc;
+    SPK_CUDA(cudaEventRecord(kb0.e, st));
+    if ((rc = launch_bloom_apply(ctx, st, bv, num_words, kr.seen.as<uint64_t>(), kr.twice.as<uint64_t>(),
+                                 su + S_POPS)))
+      return rc;
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaEventRecord(kb1.e, st));
+    ops.release();
+    rbase.release();
+    rfill.release();
+    launches += 2;
+    SPK_CUDA(cudaEventRecord(e1.e, st));
+    SPK_CUDA(cudaEventRecord(e2.e, st));
+    // ---- singleton admission, histogram, cutoff ----
+    if (nl == 1)
+      k_admit_singletons<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lo, k, kr.fm, kr.twice.as<uint64_t>(),
+                                                                 su + S_SUMS + 1);
+    else
+      k_admit_singletons<2><<<grid_for(ctx, 8), kBlock, 0, st>>>(lo, k, kr.fm, kr.twice.as<uint64_t>(),
+                                                                 su + S_SUMS + 1);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+  }
+  uint32_t* thr = (uint32_t*)(sw + S_THR);
+  k_cutoff<<<1, 32, 0, st>>>(su + S_HIST, fixed, list_min, thr);
+  SPK_CUDA(cudaGetLastError());
+  launches++;
+  // ---- the one mid-job readback ----
+  SPK_CUDA(cudaMemcpyAsync(host, sw, S_WORDS * 8, cudaMemcpyDeviceToHost, st));
+  SPK_CUDA(cudaStreamSynchronize(st));
+  const int err = (int)host[S_ERR];
+  if (err & 4) return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
+  if (err & (1 | kErrRegion | kErrRange)) return kRedo;  // a full span or an overflowed region
+  info.occurrences = host[S_OCC];
+  info.seen_popcount = host[S_POPS];
+  info.twice_popcount = host[S_POPS + 1];
+  info.table_capacity = cap;
+  const uint32_t* hthr = (const uint32_t*)(host + S_THR);
+  info.cutoff = hthr[0];
+  kr.list_min = hthr[1];
+  uint64_t n2 = 0;
+  for (int c = 2; c < kHistBins; c++) n2 += host[S_HIST + c];
+  const uint64_t adm1 = host[S_SUMS + 1];
+  info.n_table = n2 + adm1;
+  info.n_singletons = adm1;
+  info.n_distinct = n2 + host[S_LFILL + 1];
+  info.admitted_occurrences = host[S_OCC2] + adm1;
+  kr.list_len = host[S_LFILL];
+  if (kr.list_len > cap || host[S_LFILL + 1] > cap)
+    return fail(SPK_E_CUDA, "k-mer list larger than the table it came from");
+  auto hist_from = [&](uint32_t c0) {
+    uint64_t ns = 0;
+    for (int c = (int)c0; c < kHistBins; c++) ns += host[S_HIST + c];
+    return ns;
+  };
+  info.n_list = kr.list_min == lmin_pre ? kr.list_len : hist_from(kr.list_min);
+  if (kr.list_min != lmin_pre && kr.list_min >= (uint32_t)(kHistBins - 1))
+    return fail(SPK_E_INVALID_ARG, "list_min_count above 254 needs a fixed min_count");
+  if (info.cutoff < (uint32_t)(kHistBins - 1)) {
+    info.n_solid = hist_from(info.cutoff);
+  } else {
+    SPK_CUDA(cudaMemsetAsync(sw + S_CNT, 0, 8, st));
+    k_count_solid<<<grid_for(ctx, 2), 256, 0, st>>>(kr.list[4].as<uint32_t>(), kr.list_len, thr, su + S_CNT);
+    SPK_CUDA(cudaGetLastError());
+    launches++;
+    SPK_CUDA(cudaMemcpyAsync(host + S_CNT, sw + S_CNT, 8, cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    info.n_solid = host[S_CNT];
+  }
+  SPK_CUDA(cudaEventRecord(e3.e, st));
+
+  // ---- sort of the list (the singleton buffers are its temporaries) ----
+  DevSort lsort, esort;
+  if ((rc = sort_dev_enqueue(st, nl, kr.list_len, nullptr, 2 * k, kr.list, &kr.list[4], sgl, lsort, &launches)))
+    return rc;
+  uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int j = 0; j < nl; j++) lp[j] = kr.list[j].as<uint64_t>();
+  SPK_CUDA(cudaEventRecord(e4.e, st));
+
+  // ---- edges ----
+  kr.nle = (int)((k + 1 + 31) / 32);
+  uint64_t ecap = 0;
+  DevBuf set, filt;
+  if ((o.flags & SPK_F_EDGES) && info.n_solid > 0) {
+    uint64_t* ep[4] = {nullptr, nullptr, nullptr, nullptr};
+    ecap = info.n_solid * 8;  // at most 8 canonical edges per solid k-mer
+    for (int j = 0; j < kr.nle; j++) {
+      if ((rc = kr.edges[j].alloc(ecap * 8, st))) return rc;
+      ep[j] = kr.edges[j].as<uint64_t>();
+    }
+    uint32_t lg = 10, lf = 20;
+    while ((1ULL << lg) < info.n_solid + (info.n_solid >> 1) + 1) lg++;
+    while (lf < 30 && (1ULL << lf) < info.n_solid * 16) lf++;  // ~1/16 false positives
+    if ((rc = set.alloc((1ULL << lg) * nl * 8, st)) || (rc = filt.alloc((1ULL << lf) / 8, st))) return rc;
+    SPK_CUDA(cudaMemsetAsync(set.p, 0xFF, (1ULL << lg) * nl * 8, st));
+    SPK_CUDA(cudaMemsetAsync(filt.p, 0, (1ULL << lf) / 8, st));
+    SetView sv{set.as<uint64_t>(), lg, lf, filt.as<uint32_t>()};
+    if (nl == 1)
+      k_solid_set<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[0], kr.list[4].as<uint32_t>(),
+                                                         kr.list_len, thr, k, sv);
+    else
+      k_solid_set<2><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[1], kr.list[4].as<uint32_t>(),
+                                                         kr.list_len, thr, k, sv);
+    SPK_CUDA(cudaGetLastError());
+    launch_edges(ctx, st, nl, kr.nle, lp, kr.list[4].as<uint32_t>(), kr.list_len, thr, kr.table, &sv, k, ep,
+                 ecap, su + S_EDGES);
+    SPK_CUDA(cudaGetLastError());
+    launches += 2;
+    set.release();
+    filt.release();
+    if ((rc = sort_dev_enqueue(st, kr.nle, ecap, su + S_EDGES, 2 * (k + 1), kr.edges, nullptr, nullptr, esort,
+                               &launches)))
+      return rc;
+  }
+  SPK_CUDA(cudaEventRecord(e5.e, st));
+  if (!(o.flags & SPK_F_KEEP_BLOOM)) {
+    kr.seen.release();
+    kr.twice.release();
+  }
+  // ---- the final readback: edge count and the buckets left to sort ----
+  SPK_CUDA(cudaMemcpyAsync(host + S_EDGES, sw + S_EDGES, 8, cudaMemcpyDeviceToHost, st));
+  uint32_t* hb = (uint32_t*)(host + S_WORDS);
+  SPK_CUDA(cudaMemcpyAsync(hb, sort_dev_nbig(lsort), 4, cudaMemcpyDeviceToHost, st));
+  if (esort.pending) SPK_CUDA(cudaMemcpyAsync(hb + 1, sort_dev_nbig(esort), 4, cudaMemcpyDeviceToHost, st));
+  else hb[1] = 0;
+  SPK_CUDA(cudaStreamSynchronize(st));
+  info.n_edges = ecap ? host[S_EDGES] : 0;
+  if (info.n_edges > ecap) return fail(SPK_E_CUDA, "edge list larger than its bound");
+  const unsigned nbig_l = hb[0], nbig_e = hb[1];
+  if ((rc = sort_dev_finish(st, lsort, kr.list, &kr.list[4], kr.list_len, nbig_l, host, &launches))) return rc;
+  if ((rc = sort_dev_finish(st, esort, kr.edges, nullptr, info.n_edges, nbig_e, host, &launches))) return rc;
+  SPK_CUDA(cudaEventRecord(e6.e, st));
+  SPK_CUDA(cudaStreamSynchronize(st));
+  info.ms_bloom = ms_between(e0, e1);
+  info.ms_count = ms_between(e1, e2);
+  info.ms_finish = ms_between(e2, e3);
+  info.ms_sort = ms_between(e3, e4);
+  info.ms_edges = ms_between(e4, e5);
+  info.ms_total = ms_between(e0, e6);
+  info.ms_bloom_kernel = ms_between(kb0, kb1);
+  info.ms_count_kernel = ms_between(kc0, kc1);
+  info.ms_scatter_kernel = ms_between(ks0, ks1);
+  info.kernel_launches = launches;
+  info.schedule = SPK_SCHEDULE_PARTITIONED;
+  return SPK_OK;
+}
+
 // Device buffers of a k allocated on another stream: stream-ordered frees
 // go to `s` from now on (the allocating stream has been synchronised).
 static void rehome(KResult& kr, cudaStream_t s) {
@@ -2783,12 +3288,25 @@ static void rehome(KResult& kr, cudaStream_t s) {
   for (DevBuf& b : kr.edges) b.st = s;
 }
 
+// One k: the job with few round trips where it applies, else (or after an
+// overflow there) the general one.
+static int count_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv, unsigned k,
+                   const spk_count_opts& o, KResult& kr) {
+  const int rc = count_one_k_list(ctx, st, host, rv, k, o, kr);
+  if (rc != kNotThisPath && rc != kRedo) return rc;
+  SPK_CUDA(cudaStreamSynchronize(st));  // the abandoned job's buffers are freed in stream order
+  kr = KResult();
+  const int rc2 = count_one_k(ctx, st, host, rv, k, o, kr);
+  if (!rc2 && rc == kRedo) kr.info.part_rescatters++;  // the first layout overflowed
+  return rc2;
+}
+
 int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t max_len,
                    const uint32_t* ks, int n_k, const spk_count_opts& o, spk_result* res) {
   (void)max_len;
   if (n_k == 1) {
     auto kr = std::make_unique<KResult>();
-    int rc = count_one_k(ctx, st, res->h_staging, rv, ks[0], o, *kr);
+    int rc = count_k(ctx, st, res->h_staging, rv, ks[0], o, *kr);
     if (rc) return rc;
     res->ks.push_back(std::move(kr));
     return SPK_OK;
@@ -2815,7 +3333,7 @@ int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t 
         rc = cuda_fail(cudaGetLastError(), "per-k stream");
       auto kr = std::make_unique<KResult>();
       if (!rc && cudaStreamWaitEvent(s2, ready, 0) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "wait");
-      if (!rc) rc = count_one_k(ctx, s2, h, rv, ks[i], o, *kr);
+      if (!rc) rc = count_k(ctx, s2, h, rv, ks[i], o, *kr);
       if (s2) {
         cudaStreamSynchronize(s2);
         rehome(*kr, st);

@@ -211,6 +211,33 @@ int raise_smem_limit(const void* kernel, size_t bytes);
 // Streaming multiprocessors of the current device (cached per device), for
 // grid sizing in code that has no context at hand.
 int current_sm_count();
+// Bucket sort of a list whose length is in device memory (spk_sort.cu): the
+// bucketed copy, offsets and the list of buckets too large for shared
+// memory stay here between sort_dev_enqueue and sort_dev_finish.
+struct DevSort {
+  int nl = 0;
+  unsigned nbits = 0;
+  uint32_t bbits = 0;
+  uint64_t n_cap = 0;
+  bool has_vals = false;
+  bool pending = false;
+  DevBuf tk[4], tv, hist, off, cur, big;
+  void release() {
+    for (DevBuf& b : tk) b.release();
+    tv.release();
+    hist.release();
+    off.release();
+    cur.release();
+    big.release();
+  }
+};
+int sort_dev_enqueue(cudaStream_t st, int nl, uint64_t n_cap, const unsigned long long* n_dev,
+                     unsigned nbits, DevBuf* keys, DevBuf* vals, DevBuf* tmp_keys, DevSort& ds,
+                     uint32_t* launches = nullptr);
+// Device word counting the buckets left for sort_dev_finish.
+const unsigned* sort_dev_nbig(const DevSort& ds);
+int sort_dev_finish(cudaStream_t st, DevSort& ds, DevBuf* keys, DevBuf* vals, uint64_t n_host,
+                    unsigned nbig_host, uint64_t* h_staging, uint32_t* launches = nullptr);
 // Exclusive scan of u32 in place (spk_sort.cu).
 int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches = nullptr);
 // Ordered compaction of a sorted SoA list into AoS Kmer256 limbs; *m is the

@@ -301,9 +301,12 @@ __device__ __forceinline__ uint32_t bs_digit(const Limbs& L, uint64_t i, unsigne
   return (uint32_t)(((lo >> sh) | ((hi << 1) << (63 - sh))) & (nb - 1));
 }
 
+// n_dev (nullable): the item count in device memory, at most n.
 template <int NL>
-__global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(Limbs L, uint64_t n, unsigned limb, unsigned sh,
-                                                       uint32_t nb, uint32_t* __restrict__ hist) {
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(Limbs L, uint64_t n, const unsigned long long* n_dev,
+                                                       unsigned limb, unsigned sh, uint32_t nb,
+                                                       uint32_t* __restrict__ hist) {
+  if (n_dev) n = min(n, (uint64_t)*n_dev);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
     atomicAdd(hist + bs_digit<NL>(L, i, limb, sh, nb), 1u);
@@ -312,8 +315,10 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(Limbs L, uint64_t n, unsig
 template <int NL, bool HASV>
 __global__ void __launch_bounds__(BS_BLOCK) k_bs_scatter(Limbs S, const uint32_t* __restrict__ sv, Limbs D,
                                                           uint32_t* __restrict__ dv, uint64_t n,
+                                                          const unsigned long long* n_dev,
                                                           unsigned limb, unsigned sh, uint32_t nb,
                                                           uint32_t* __restrict__ cur) {
+  if (n_dev) n = min(n, (uint64_t)*n_dev);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t p = atomicAdd(cur + bs_digit<NL>(S, i, limb, sh, nb), 1u);
@@ -482,17 +487,19 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* 
 
 template <int NL, bool HASV>
 static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* tv, uint64_t n,
-                     unsigned limb, unsigned sh, uint32_t nb, uint32_t* hist, uint32_t* off,
-                     uint32_t* cur, uint32_t* big, unsigned* nbig, uint32_t* launches) {
+                     const unsigned long long* n_dev, unsigned limb, unsigned sh, uint32_t nb,
+                     uint32_t* hist, uint32_t* off, uint32_t* cur, uint32_t* big, unsigned* nbig,
+                     uint32_t* launches) {
   const int sms = current_sm_count();
-  const unsigned g = (unsigned)std::min<uint64_t>((n + BS_BLOCK - 1) / BS_BLOCK, (uint64_t)sms * 16);
-  k_bs_hist<NL><<<g, BS_BLOCK, 0, st>>>(K, n, limb, sh, nb, hist);
+  const unsigned g = (unsigned)std::max<uint64_t>(
+      std::min<uint64_t>((n + BS_BLOCK - 1) / BS_BLOCK, (uint64_t)sms * 16), 1);
+  k_bs_hist<NL><<<g, BS_BLOCK, 0, st>>>(K, n, n_dev, limb, sh, nb, hist);
   SPK_CUDA(cudaMemcpyAsync(off, hist, (size_t)nb * 4, cudaMemcpyDeviceToDevice, st));
   DevBuf sums;
   int rc;
   if ((rc = scan_u32(st, off, nb, sums, launches))) return rc;
   SPK_CUDA(cudaMemcpyAsync(cur, off, (size_t)nb * 4, cudaMemcpyDeviceToDevice, st));
-  k_bs_scatter<NL, HASV><<<g, BS_BLOCK, 0, st>>>(K, v, T, tv, n, limb, sh, nb, cur);
+  k_bs_scatter<NL, HASV><<<g, BS_BLOCK, 0, st>>>(K, v, T, tv, n, n_dev, limb, sh, nb, cur);
   const size_t smem = std::max<size_t>(BS_LOCAL * (NL * 8 + (HASV ? 4 : 0)),
                                        (size_t)(BS_BLOCK / 32) * BS_WARP * (NL + (HASV ? 1 : 0)) * 8);
   if ((rc = raise_smem_limit((const void*)k_bs_local<NL, HASV>, smem))) return rc;
@@ -535,14 +542,14 @@ int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
   uint32_t* Cu = cur.as<uint32_t>();
   uint32_t* B = big.as<uint32_t>();
   switch (nl * 2 + (vals ? 1 : 0)) {
-    case 2: rc = bs_launch<1, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
-    case 3: rc = bs_launch<1, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
-    case 4: rc = bs_launch<2, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
-    case 5: rc = bs_launch<2, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
-    case 6: rc = bs_launch<3, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
-    case 7: rc = bs_launch<3, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
-    case 8: rc = bs_launch<4, false>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
-    default: rc = bs_launch<4, true>(st, K, v, T, tvp, n, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 2: rc = bs_launch<1, false>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 3: rc = bs_launch<1, true>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 4: rc = bs_launch<2, false>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 5: rc = bs_launch<2, true>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 6: rc = bs_launch<3, false>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 7: rc = bs_launch<3, true>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 8: rc = bs_launch<4, false>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    default: rc = bs_launch<4, true>(st, K, v, T, tvp, n, nullptr, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
   }
   if (rc) return rc;
   uint64_t* hs = h_staging + BS_STAGE_WORDS;
@@ -577,6 +584,112 @@ int sort_bufs(cudaStream_t st, int nl, uint64_t n, unsigned nbits, DevBuf* keys,
     if (vals) SPK_CUDA(cudaMemcpyAsync(v + o, bvv.p, m * 4, cudaMemcpyDeviceToDevice, st));
   }
   return SPK_OK;
+}
+
+// Bucket sort of a list whose length is known only on the device (*n_dev, at
+// most n_cap): the same split and shared-memory sorts, enqueued without
+// reading anything back.  Buckets over BS_LOCAL items stay in the bucketed
+// copy and are listed on the device; sort_dev_finish sorts them once the
+// host has the counts.  Temporaries: tmp_keys (nullable, NL limb arrays of
+// n_cap items that the caller no longer needs) or new allocations.
+int sort_dev_enqueue(cudaStream_t st, int nl, uint64_t n_cap, const unsigned long long* n_dev,
+                     unsigned nbits, DevBuf* keys, DevBuf* vals, DevBuf* tmp_keys, DevSort& ds,
+                     uint32_t* launches) {
+  uint32_t bbits = 8;
+  while (bbits < BS_MAX_BITS && (n_cap >> (bbits + 1)) >= 128) bbits++;
+  if (nbits < bbits + 8) return fail(SPK_E_INVALID_ARG, "device-count sort: keys too short");
+  if (n_cap >= (1ULL << 32)) return fail(SPK_E_INVALID_ARG, "sort: more than 2^32 items");
+  const uint32_t nb = 1u << bbits;
+  ds.nl = nl;
+  ds.nbits = nbits;
+  ds.bbits = bbits;
+  ds.n_cap = n_cap;
+  ds.has_vals = vals != nullptr;
+  int rc;
+  Limbs K{}, T{};
+  for (int j = 0; j < nl; j++) {
+    if (tmp_keys) ds.tk[j] = std::move(tmp_keys[j]);
+    else if ((rc = ds.tk[j].alloc(std::max<uint64_t>(n_cap, 1) * 8, st))) return rc;
+    K.p[j] = keys[j].as<uint64_t>();
+    T.p[j] = ds.tk[j].as<uint64_t>();
+  }
+  if (vals && (rc = ds.tv.alloc(std::max<uint64_t>(n_cap, 1) * 4, st))) return rc;
+  if ((rc = ds.hist.alloc(nb * 4, st)) || (rc = ds.off.alloc(nb * 4, st)) || (rc = ds.cur.alloc(nb * 4, st)) ||
+      (rc = ds.big.alloc((3 * BS_MAX_BIG + 1) * 4, st)))
+    return rc;
+  SPK_CUDA(cudaMemsetAsync(ds.hist.p, 0, nb * 4, st));
+  unsigned* nbig = (unsigned*)(ds.big.as<uint32_t>() + 3 * BS_MAX_BIG);
+  SPK_CUDA(cudaMemsetAsync(nbig, 0, 4, st));
+  const unsigned hi_bit = nbits - bbits, limb = hi_bit / 64, sh = hi_bit % 64;
+  uint32_t* v = vals ? vals->as<uint32_t>() : nullptr;
+  uint32_t* tvp = vals ? ds.tv.as<uint32_t>() : nullptr;
+  uint32_t* H = ds.hist.as<uint32_t>();
+  uint32_t* O = ds.off.as<uint32_t>();
+  uint32_t* Cu = ds.cur.as<uint32_t>();
+  uint32_t* B = ds.big.as<uint32_t>();
+  switch (nl * 2 + (vals ? 1 : 0)) {
+    case 2: rc = bs_launch<1, false>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 3: rc = bs_launch<1, true>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 4: rc = bs_launch<2, false>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 5: rc = bs_launch<2, true>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 6: rc = bs_launch<3, false>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 7: rc = bs_launch<3, true>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    case 8: rc = bs_launch<4, false>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+    default: rc = bs_launch<4, true>(st, K, v, T, tvp, n_cap, n_dev, limb, sh, nb, H, O, Cu, B, nbig, launches); break;
+  }
+  if (rc) return rc;
+  ds.pending = true;
+  return SPK_OK;
+}
+
+const unsigned* sort_dev_nbig(const DevSort& ds) {
+  return (const unsigned*)(ds.big.as<uint32_t>() + 3 * BS_MAX_BIG);
+}
+
+// Sorts the buckets sort_dev_enqueue left over (nbig_host of them, read
+// back by the caller; n_host = the list length) and frees the temporaries.
+int sort_dev_finish(cudaStream_t st, DevSort& ds, DevBuf* keys, DevBuf* vals, uint64_t n_host,
+                    unsigned nbig_host, uint64_t* h_staging, uint32_t* launches) {
+  if (!ds.pending) return SPK_OK;
+  ds.pending = false;
+  const int nl = ds.nl;
+  int rc;
+  uint32_t* v = vals ? vals->as<uint32_t>() : nullptr;
+  uint32_t* tvp = vals ? ds.tv.as<uint32_t>() : nullptr;
+  if (nbig_host > BS_MAX_BIG) {
+    // Too many large buckets: sort the bucketed copy as a whole instead.
+    for (int j = 0; j < nl; j++)
+      SPK_CUDA(cudaMemcpyAsync(keys[j].p, ds.tk[j].p, n_host * 8, cudaMemcpyDeviceToDevice, st));
+    if (vals) SPK_CUDA(cudaMemcpyAsync(v, tvp, n_host * 4, cudaMemcpyDeviceToDevice, st));
+    rc = radix_sort_bufs(st, nl, n_host, ds.nbits, keys, vals, launches);
+  } else if (nbig_host > 0) {
+    uint64_t* hs = h_staging + BS_STAGE_WORDS;
+    SPK_CUDA(cudaMemcpyAsync(hs, ds.big.p, (size_t)nbig_host * 12, cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint32_t> bl((const uint32_t*)hs, (const uint32_t*)hs + 3 * nbig_host);
+    const unsigned hi_bit = ds.nbits - ds.bbits;
+    rc = SPK_OK;
+    for (unsigned q = 0; q < nbig_host && !rc; q++) {
+      const uint64_t o = bl[3 * q + 1], m = bl[3 * q + 2];
+      DevBuf bk[4], bvv;
+      for (int j = 0; j < nl; j++) {
+        if ((rc = bk[j].alloc(m * 8, st))) return rc;
+        SPK_CUDA(cudaMemcpyAsync(bk[j].p, ds.tk[j].as<uint64_t>() + o, m * 8, cudaMemcpyDeviceToDevice, st));
+      }
+      if (vals) {
+        if ((rc = bvv.alloc(m * 4, st))) return rc;
+        SPK_CUDA(cudaMemcpyAsync(bvv.p, tvp + o, m * 4, cudaMemcpyDeviceToDevice, st));
+      }
+      if ((rc = radix_sort_bufs(st, nl, m, hi_bit, bk, vals ? &bvv : nullptr, launches))) return rc;
+      for (int j = 0; j < nl; j++)
+        SPK_CUDA(cudaMemcpyAsync(keys[j].as<uint64_t>() + o, bk[j].p, m * 8, cudaMemcpyDeviceToDevice, st));
+      if (vals) SPK_CUDA(cudaMemcpyAsync(v + o, bvv.p, m * 4, cudaMemcpyDeviceToDevice, st));
+    }
+  } else {
+    rc = SPK_OK;
+  }
+  ds.release();
+  return rc;
 }
 
 // ---------------------------------------------------------------------------

@@ -16,7 +16,8 @@ There is no CPU fallback: importing works anywhere, but every call that
 needs the GPU raises :class:`SpkError` when ``libspk.so`` or the device is
 missing.
 """
-from ._lib import (SPK_F_CORRECT, SPK_F_DIRECT, SPK_F_EDGES, SPK_F_GATED, SPK_F_KEEP_BLOOM, SPK_F_REF_SOLID,
+from ._lib import (SPK_F_CORRECT, SPK_F_DIRECT, SPK_F_EDGES, SPK_F_GATED, SPK_F_KEEP_BLOOM,
+                   SPK_F_KEEP_TABLE, SPK_F_REF_SOLID,
                    SPK_SCHEDULE_COUNT_FIRST, SPK_SCHEDULE_FUSED, SPK_SCHEDULE_GATED,
                    SPK_SCHEDULE_PARTITIONED, SpkError, lib, lib_path, validate_k)
 from .api import (Context, CountResult, DevicePackedReads, Job, PackedReads, Server, TwoTierFilter, count,
@@ -24,7 +25,8 @@ from .api import (Context, CountResult, DevicePackedReads, Job, PackedReads, Ser
                   limbs_from_kmer256, nlimbs)
 
 __all__ = [
-    "SPK_F_CORRECT", "SPK_F_DIRECT", "SPK_F_EDGES", "SPK_F_GATED", "SPK_F_KEEP_BLOOM", "SPK_F_REF_SOLID",
+    "SPK_F_CORRECT", "SPK_F_DIRECT", "SPK_F_EDGES", "SPK_F_GATED", "SPK_F_KEEP_BLOOM", "SPK_F_KEEP_TABLE",
+    "SPK_F_REF_SOLID",
     "SPK_SCHEDULE_COUNT_FIRST", "SPK_SCHEDULE_FUSED", "SPK_SCHEDULE_GATED", "SPK_SCHEDULE_PARTITIONED",
     "SpkError", "lib", "lib_path",
     "validate_k", "Context", "CountResult", "DevicePackedReads", "Job", "PackedReads", "Server",

@@ -14,6 +14,7 @@ SPK_F_KEEP_BLOOM = 0x4
 SPK_F_GATED = 0x8
 SPK_F_DIRECT = 0x10
 SPK_F_CORRECT = 0x20
+SPK_F_KEEP_TABLE = 0x40
 SPK_NOALLOC_MAX_KEYS = 65536
 SPK_SCHEDULE_GATED = 0
 SPK_SCHEDULE_FUSED = 1

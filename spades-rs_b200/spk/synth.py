@@ -264,6 +264,111 @@ def c5_job(i: int, scale: float = 1.0) -> Sample:
                   gc=float(rng.uniform(0.3, 0.7)), ks=(55,), name=f"c5_iso_{i}")
 
 
+# ---------------------------------------------------------------------------
+# Native generator (spk/libspksynth.so, synth_native.cpp): the batched and
+# serving workloads at their full sizes (tens of Gbp), seeded per sample and
+# independent of the thread count.  Reads are 2x150 N-free pairs, so every
+# pair is clean (blocks 1 and 2 of src/packed_reads.rs:9-27).
+# ---------------------------------------------------------------------------
+_NATIVE = None
+
+
+def _native():
+    global _NATIVE
+    if _NATIVE is None:
+        import ctypes as C
+        import os
+        here = os.path.dirname(os.path.abspath(__file__))
+        path = os.path.join(here, "libspksynth.so")
+        if not os.path.exists(path):
+            import subprocess
+            subprocess.run(["make", "-s", "-C", os.path.dirname(here), "spk/libspksynth.so"], check=True)
+        L = C.CDLL(path)
+        L.spk_synth_genome.restype = None
+        L.spk_synth_genome.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_int]
+        L.spk_synth_pairs.restype = None
+        L.spk_synth_pairs.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_double, C.c_double,
+                                      C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int]
+        _NATIVE = L
+    return _NATIVE
+
+
+def _threads() -> int:
+    import os
+    return os.cpu_count() or 1
+
+
+def native_genome(length: int, gc: float, seed: int, stream: int) -> np.ndarray:
+    g = np.empty(max(length, 1), dtype=np.uint8)
+    _native().spk_synth_genome(g.ctypes.data, length, gc, seed, stream, _threads())
+    return g[:length]
+
+
+def native_pairs(genomes: Sequence[np.ndarray], pairs: Sequence[int], seed: int, stream: int,
+                 err: float = 0.005, read_len: int = 150, frag_mean: float = 300.0,
+                 frag_sd: float = 30.0) -> PackedReads:
+    """pairs[g] read pairs from genomes[g] (stream stream + g), as one store:
+    every mate 1 in genome and pair order, then every mate 2."""
+    total = int(sum(pairs))
+    nb = (read_len + 3) // 4
+    data = np.empty(max(2 * total * nb, 1), dtype=np.uint8)
+    offsets = np.empty(max(2 * total, 1), dtype=np.uint64)
+    lengths = np.empty(max(2 * total, 1), dtype=np.uint32)
+    first = 0
+    for gi, (g, n) in enumerate(zip(genomes, pairs)):
+        if n:
+            _native().spk_synth_pairs(g.ctypes.data, g.size, int(n), read_len, frag_mean, frag_sd, err, seed,
+                                      stream + gi, first, total + first, data.ctypes.data,
+                                      offsets.ctypes.data, lengths.ctypes.data, _threads())
+        first += int(n)
+    return PackedReads(data[: 2 * total * nb], offsets[: 2 * total], lengths[: 2 * total], total)
+
+
+def native_sample(genome_len: int, coverage: float, seed: int, stream: int, gc: float = 0.5,
+                  err: float = 0.005, ks=(33,), name: str = "sample") -> Sample:
+    g = native_genome(genome_len, gc, seed, 2 * stream)
+    n_pairs = max(1, int(round(genome_len * coverage / 300)))
+    return Sample(name, native_pairs([g], [n_pairs], seed, 2 * stream + 1, err), genome_len, coverage,
+                  tuple(ks))
+
+
+def c4_native(n_samples: int = 64, scale: float = 1.0) -> List[Sample]:
+    """The 64-sample batch with the plan of c4_plan, made by the native generator."""
+    return [native_sample(p["genome_len"], p["coverage"], seed=3, stream=1 + p["index"], gc=p["gc"],
+                          err=0.005, ks=(33,), name=f"c4_{p['index']}")
+            for p in c4_plan(n_samples, scale)]
+
+
+def c5_plan(i: int, scale: float = 1.0) -> dict:
+    """The i-th serving request (seed 4): 1 in 4 is metagenome-like (20
+    genomes of 1-5 Mb, log-normal abundances with sigma 1.5, 20-100x in
+    total), the rest isolates (1-8 Mb, 30-100x).  scale multiplies the genome
+    sizes."""
+    rng = rng_for(4, 10_000 + i)
+    if rng.random() < 0.25:
+        sizes = (rng.uniform(1e6, 5e6, 20) * scale).astype(np.int64).clip(2000)
+        ab = rng.lognormal(0.0, 1.5, 20)
+        total_cov = float(rng.uniform(20, 100))
+        gcs = rng.uniform(0.3, 0.7, 20)
+        cov = total_cov * ab / ab.mean()
+        return dict(kind="meta", sizes=[int(x) for x in sizes], gcs=[float(x) for x in gcs],
+                    covs=[float(x) for x in cov], coverage=total_cov)
+    G = max(int(rng.uniform(1e6, 8e6) * scale), 2000)
+    return dict(kind="iso", sizes=[G], gcs=[float(rng.uniform(0.3, 0.7))], covs=[float(rng.uniform(30, 100))],
+                coverage=None)
+
+
+def c5_native(i: int, scale: float = 1.0) -> Sample:
+    """The i-th serving request of c5_plan, made by the native generator."""
+    p = c5_plan(i, scale)
+    genomes = [native_genome(sz, gc, 4, 40_000 + 64 * i + j) for j, (sz, gc) in enumerate(zip(p["sizes"], p["gcs"]))]
+    pairs = [max(1, int(sz * c / 300)) for sz, c in zip(p["sizes"], p["covs"])]
+    packed = native_pairs(genomes, pairs, 4, 80_000 + 64 * i)
+    cov = p["coverage"] if p["coverage"] is not None else p["covs"][0]
+    return Sample(f"c5_{p['kind']}_{i}", packed, int(sum(p["sizes"])), float(cov), (55,))
+
+
 def occurrences(p: PackedReads, k: int) -> int:
     L = p.lengths.astype(np.int64)
     return int(np.clip(L - k + 1, 0, None).sum())

@@ -22,6 +22,7 @@ BASE = 0x1 | 0x4        # SPK_F_EDGES | SPK_F_KEEP_BLOOM
 ALL = BASE | 0x2        # ... | SPK_F_REF_SOLID
 GATED = 0x8             # SPK_F_GATED: the two-pass schedule
 DIRECT = 0x10           # SPK_F_DIRECT: count-first with global-table atomics
+KEEP_TABLE = 0x40       # SPK_F_KEEP_TABLE: the partitioned schedule also writes the table
 
 
 def sha(words):
@@ -59,6 +60,14 @@ def check_against_oracle(spk, ora, data, offs, lens, k, bits, edges=True, **kw):
     dk, dc = d.kmers(0, 1)
     np.testing.assert_array_equal(dk, tk)
     np.testing.assert_array_equal(dc, tc)
+    # the default schedule with the table kept (its admission scans the table)
+    t = spk.count((data, offs, lens), [k], bloom_bits=bits, list_min_count=1, flags=BASE | KEEP_TABLE, **kw)
+    tkk, tcc = t.kmers(0, 1)
+    np.testing.assert_array_equal(tkk, tk)
+    np.testing.assert_array_equal(tcc, tc)
+    assert t.info(0)["cutoff"] == d.info(0)["cutoff"]
+    np.testing.assert_array_equal(t.edges(0), d.edges(0))
+    t.close()
     ds, dt = d.bloom(0)
     np.testing.assert_array_equal(ds, oseen)
     np.testing.assert_array_equal(dt, otwice)
@@ -319,7 +328,7 @@ def test_partition_rescatter_on_skew(spk, ora, table_log2):
     info = check_against_oracle(spk, ora, d2, o2.astype(np.uint64), l2.astype(np.uint32), 31,
                                 1 << 20, table_log2=table_log2)
     r = spk.count((d2, o2.astype(np.uint64), l2.astype(np.uint32)), [31], bloom_bits=1 << 20,
-                  table_log2=table_log2)
+                  table_log2=table_log2, flags=BASE | KEEP_TABLE)
     ri = r.info(0)
     assert ri["schedule"] == 3 and ri["part_rescatters"] >= 1
     assert ri["part_passes"] == (2 if table_log2 == 21 else 1)  # 256 spans: two-level partition
@@ -373,7 +382,8 @@ def test_many_spans(spk, ora, k, table_log2):
     """Tables of hundreds of spans: the result equals the oracle's."""
     data, offs, lens = synth_small_packed()
     check_against_oracle(spk, ora, data, offs, lens, k, 1 << 20, table_log2=table_log2)
-    r = spk.count((data, offs, lens), [k], bloom_bits=1 << 20, table_log2=table_log2)
+    r = spk.count((data, offs, lens), [k], bloom_bits=1 << 20, table_log2=table_log2,
+                  flags=BASE | KEEP_TABLE)
     v = r.table_view(0)
     assert r.info(0)["schedule"] == 3 and v["capacity"] == 1 << table_log2
     assert (table_log2 - v["log2span"]) >= 8
@@ -479,3 +489,21 @@ def test_claim_wait_times_out(spk, ora, k):
     r.close()
     with pytest.raises(spk.SpkError):
         spk._lib.check(lib().spk_diag_stuck_claim(ctx.h, 55))
+
+
+def test_table_view_needs_keep_table(spk):
+    """Without SPK_F_KEEP_TABLE the partitioned schedule writes the list from
+    its spans and keeps no table: the view is refused; with it, the view
+    describes the table; the lists are the same either way."""
+    data, offs, lens = synth_small_packed()
+    a = spk.count((data, offs, lens), [55], bloom_bits=1 << 20)
+    assert a.info(0)["schedule"] == 3
+    with pytest.raises(spk.SpkError) as e:
+        a.table_view(0)
+    assert e.value.code == 1 and "SPK_F_KEEP_TABLE" in str(e.value)
+    b = spk.count((data, offs, lens), [55], bloom_bits=1 << 20, flags=BASE | KEEP_TABLE)
+    v = b.table_view(0)
+    assert v["slots"] and v["capacity"] == b.info(0)["table_capacity"]
+    for x, y in zip(a.kmers(0), b.kmers(0)):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(a.edges(0), b.edges(0))
