@@ -3004,6 +3004,23 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
 // ---------------------------------------------------------------------------
 constexpr int kNotThisPath = -100, kRedo = -101;
 
+// A second stream of one job, joined back to the job's stream by events.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int open() {
+    SPK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    SPK_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    SPK_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    return SPK_OK;
+  }
+  ~SideStream() {
+    if (s) cudaStreamDestroy(s);  // pending work still completes
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+  }
+};
+
 int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv_in, unsigned k,
                      const spk_count_opts& o, KResult& kr) {
   const int nl = (int)((k + 31) / 32);
@@ -3105,6 +3122,10 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   SPK_CUDA(cudaEventRecord(ks1.e, st));
 
   // ---- span count: the list, the singleton keys and the binned Bloom ops ----
+  const bool early_sort = lmin_pre >= 2;
+  SideStream side;
+  if (early_sort && (rc = side.open())) return rc;
+  DevSort lsort, esort;  // after `side`: its buffers are freed on that stream first
   DevBuf rbase, rfill, ops, sgl[2];
   {
     const uint64_t share = 3 * cap / nranges + 1;
@@ -3127,6 +3148,17 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
     if (rc) return rc;
     SPK_CUDA(cudaGetLastError());
     SPK_CUDA(cudaEventRecord(kc1.e, st));
+    if (early_sort) {
+      // The list is final once the spans are counted (singletons are not
+      // listed): sort it on the side stream while the job's stream builds
+      // the Bloom tiers, admits the singletons and finds the cutoff.
+      SPK_CUDA(cudaEventRecord(side.fork, st));
+      SPK_CUDA(cudaStreamWaitEvent(side.s, side.fork, 0));
+      if ((rc = sort_dev_enqueue(side.s, nl, cap, su + S_LFILL, 2 * k, kr.list, &kr.list[4], nullptr, lsort,
+                                 &launches)))
+        return rc;
+      SPK_CUDA(cudaEventRecord(side.join, side.s));
+    }
     region.release();
     base.release();
     fill.release();
@@ -3159,6 +3191,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   SPK_CUDA(cudaGetLastError());
   launches++;
   // ---- the one mid-job readback ----
+  if (early_sort) SPK_CUDA(cudaStreamWaitEvent(st, side.join, 0));
   SPK_CUDA(cudaMemcpyAsync(host, sw, S_WORDS * 8, cudaMemcpyDeviceToHost, st));
   SPK_CUDA(cudaStreamSynchronize(st));
   const int err = (int)host[S_ERR];
@@ -3202,9 +3235,10 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   }
   SPK_CUDA(cudaEventRecord(e3.e, st));
 
-  // ---- sort of the list (the singleton buffers are its temporaries) ----
-  DevSort lsort, esort;
-  if ((rc = sort_dev_enqueue(st, nl, kr.list_len, nullptr, 2 * k, kr.list, &kr.list[4], sgl, lsort, &launches)))
+  // ---- sort of the list, unless it ran early (the singleton buffers, read by
+  // admission, are its temporaries here) ----
+  if (!early_sort &&
+      (rc = sort_dev_enqueue(st, nl, kr.list_len, nullptr, 2 * k, kr.list, &kr.list[4], sgl, lsort, &launches)))
     return rc;
   uint64_t* lp[4] = {nullptr, nullptr, nullptr, nullptr};
   for (int j = 0; j < nl; j++) lp[j] = kr.list[j].as<uint64_t>();

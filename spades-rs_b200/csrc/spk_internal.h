@@ -222,6 +222,10 @@ struct DevSort {
   bool has_vals = false;
   bool pending = false;
   DevBuf tk[4], tv, hist, off, cur, big;
+  void rehome(cudaStream_t s) {
+    for (DevBuf& b : tk) b.st = s;
+    tv.st = hist.st = off.st = cur.st = big.st = s;
+  }
   void release() {
     for (DevBuf& b : tk) b.release();
     tv.release();

@@ -652,6 +652,9 @@ int sort_dev_finish(cudaStream_t st, DevSort& ds, DevBuf* keys, DevBuf* vals, ui
                     unsigned nbig_host, uint64_t* h_staging, uint32_t* launches) {
   if (!ds.pending) return SPK_OK;
   ds.pending = false;
+  // The temporaries may come from another stream that `st` has joined; their
+  // frees follow the work enqueued here.
+  ds.rehome(st);
   const int nl = ds.nl;
   int rc;
   uint32_t* v = vals ? vals->as<uint32_t>() : nullptr;
