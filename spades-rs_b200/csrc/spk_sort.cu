@@ -369,7 +369,8 @@ __device__ __forceinline__ void warp_bitonic(uint64_t* sk, uint32_t* svl, uint32
 
 // Sorts every bucket of at most BS_LOCAL items from T into D: buckets of at
 // most BS_WARP items one per warp, the others one per CTA.  Larger buckets
-// are listed in big[3i..3i+2] = (bucket, offset, size) for the host.
+// are copied to D unsorted and listed in big[3i..3i+2] = (bucket, offset,
+// size) for the host, which sorts them from T.
 template <int NL, bool HASV>
 __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* __restrict__ tv, Limbs D,
                                                         uint32_t* __restrict__ dv,
@@ -431,6 +432,13 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* 
           big[3 * q + 1] = o;
           big[3 * q + 2] = m;
         }
+      }
+      // The bucket goes to its place unsorted, so that D holds the whole
+      // list (in every bucket's range) before the host sorts this range.
+      for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < NL; j++) D.p[j][o + i] = T.p[j][o + i];
+        if (HASV) dv[o + i] = tv[o + i];
       }
       continue;
     }

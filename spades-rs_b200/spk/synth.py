@@ -340,11 +340,11 @@ def c4_native(n_samples: int = 64, scale: float = 1.0) -> List[Sample]:
             for p in c4_plan(n_samples, scale)]
 
 
-def c5_plan(i: int, scale: float = 1.0) -> dict:
+def c5_plan(i: int, scale: float = 1.0, iso_scale: float = 1.0) -> dict:
     """The i-th serving request (seed 4): 1 in 4 is metagenome-like (20
     genomes of 1-5 Mb, log-normal abundances with sigma 1.5, 20-100x in
-    total), the rest isolates (1-8 Mb, 30-100x).  scale multiplies the genome
-    sizes."""
+    total), the rest isolates (1-8 Mb, 30-100x).  scale multiplies the
+    metagenomes' genome sizes, iso_scale the isolates'."""
     rng = rng_for(4, 10_000 + i)
     if rng.random() < 0.25:
         sizes = (rng.uniform(1e6, 5e6, 20) * scale).astype(np.int64).clip(2000)
@@ -354,14 +354,14 @@ def c5_plan(i: int, scale: float = 1.0) -> dict:
         cov = total_cov * ab / ab.mean()
         return dict(kind="meta", sizes=[int(x) for x in sizes], gcs=[float(x) for x in gcs],
                     covs=[float(x) for x in cov], coverage=total_cov)
-    G = max(int(rng.uniform(1e6, 8e6) * scale), 2000)
+    G = max(int(rng.uniform(1e6, 8e6) * iso_scale), 2000)
     return dict(kind="iso", sizes=[G], gcs=[float(rng.uniform(0.3, 0.7))], covs=[float(rng.uniform(30, 100))],
                 coverage=None)
 
 
-def c5_native(i: int, scale: float = 1.0) -> Sample:
+def c5_native(i: int, scale: float = 1.0, iso_scale: float = 1.0) -> Sample:
     """The i-th serving request of c5_plan, made by the native generator."""
-    p = c5_plan(i, scale)
+    p = c5_plan(i, scale, iso_scale)
     genomes = [native_genome(sz, gc, 4, 40_000 + 64 * i + j) for j, (sz, gc) in enumerate(zip(p["sizes"], p["gcs"]))]
     pairs = [max(1, int(sz * c / 300)) for sz, c in zip(p["sizes"], p["covs"])]
     packed = native_pairs(genomes, pairs, 4, 80_000 + 64 * i)
