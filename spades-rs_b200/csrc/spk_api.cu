@@ -56,6 +56,70 @@ int current_sm_count() {
   return n;
 }
 
+namespace {
+struct Pools {
+  std::mutex mu;
+  std::map<int, std::vector<cudaStream_t>> streams;
+  std::map<int, std::vector<cudaEvent_t>> events[2];  // [timing]
+};
+Pools& pools() {
+  static Pools* p = new Pools();  // kept to process exit: handles outlive contexts
+  return *p;
+}
+int cur_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) cudaGetLastError();
+  return d;
+}
+}  // namespace
+
+cudaStream_t pooled_stream() {
+  const int d = cur_device();
+  {
+    std::lock_guard<std::mutex> l(pools().mu);
+    auto& v = pools().streams[d];
+    if (!v.empty()) {
+      cudaStream_t s = v.back();
+      v.pop_back();
+      return s;
+    }
+  }
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return s;
+}
+void pooled_stream_put(cudaStream_t s) {
+  if (!s) return;
+  std::lock_guard<std::mutex> l(pools().mu);
+  pools().streams[cur_device()].push_back(s);
+}
+cudaEvent_t pooled_event(bool timing) {
+  const int d = cur_device();
+  {
+    std::lock_guard<std::mutex> l(pools().mu);
+    auto& v = pools().events[timing ? 1 : 0][d];
+    if (!v.empty()) {
+      cudaEvent_t e = v.back();
+      v.pop_back();
+      return e;
+    }
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreateWithFlags(&e, timing ? cudaEventDefault : cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return e;
+}
+void pooled_event_put(cudaEvent_t e, bool timing) {
+  if (!e) return;
+  std::lock_guard<std::mutex> l(pools().mu);
+  pools().events[timing ? 1 : 0][cur_device()].push_back(e);
+}
+
 // ---- FastMod constants (Granlund & Montgomery 1994, Fig. 4.1, N = 64) ---------
 FastMod make_fastmod(uint64_t d) {
   FastMod f{};
@@ -164,6 +228,9 @@ static int check_ks(const uint32_t* ks, int n_k) {
 
 // Copies packed reads to the device (data padded so that k-mer windows may
 // read whole 64-bit words past the last byte).
+constexpr uint64_t kChunkedUploadMin = 32ull << 20;  // bytes of packed data
+constexpr int kUploadChunks = 4;
+
 int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t data_len,
                  const uint64_t* offsets, const uint32_t* lengths, size_t n_reads, ReadsView* rv) {
   int rc;
@@ -174,7 +241,6 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
   // Zero the tail from the last whole word of data to the end of the padding.
   const size_t tail = data_len & ~(size_t)7;
   SPK_CUDA(cudaMemsetAsync(res->reads.as<uint8_t>() + tail, 0, padded - tail, st));
-  if (data_len) SPK_CUDA(cudaMemcpyAsync(res->reads.p, data, data_len, cudaMemcpyHostToDevice, st));
   if (n_reads) {
     SPK_CUDA(cudaMemcpyAsync(res->offs.p, offsets, n_reads * 8, cudaMemcpyHostToDevice, st));
     SPK_CUDA(cudaMemcpyAsync(res->lens.p, lengths, n_reads * 4, cudaMemcpyHostToDevice, st));
@@ -186,6 +252,48 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
   rv->byte_base = 0;
   rv->data_len = data_len;
   rv->err = nullptr;
+  rv->chunks = nullptr;
+  if (data_len < kChunkedUploadMin || n_reads < 2) {
+    if (data_len) SPK_CUDA(cudaMemcpyAsync(res->reads.p, data, data_len, cudaMemcpyHostToDevice, st));
+    return SPK_OK;
+  }
+  // Large read sets: the data go up in kUploadChunks pieces on a copy stream,
+  // so that the count's first pass works on the reads of a piece while the
+  // next one is copied.  Reads [0, read_end[c]) end at least 64 bytes before
+  // byte_end[c] (the word loads of a read reach past its last byte) if the
+  // reads lie in order; the count checks that on the device and otherwise
+  // waits for the last piece.
+  ReadChunks& ch = res->chunks;
+  res->copy_stream = pooled_stream();
+  cudaEvent_t alloc_done = pooled_event(false);
+  if (!res->copy_stream || !alloc_done) return fail(SPK_E_CUDA, "upload stream or event");
+  cudaError_t e = cudaEventRecord(alloc_done, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(res->copy_stream, alloc_done, 0);
+  pooled_event_put(alloc_done, false);
+  if (e != cudaSuccess) return cuda_fail(e, "upload stream");
+  ch.n = kUploadChunks;
+  uint64_t b0 = 0;
+  for (int c = 0; c < ch.n; c++) {
+    uint64_t b1 = c + 1 == ch.n ? data_len : (data_len * (c + 1) / ch.n) & ~(uint64_t)7;
+    if (b1 < b0) b1 = b0;
+    ch.byte_end[c] = b1;
+    if (c + 1 == ch.n) {
+      ch.read_end[c] = n_reads;
+    } else {
+      // reads i with offsets[i + 1] <= b1 - 64 (offsets ascending when in order)
+      const uint64_t lim = b1 >= 64 ? b1 - 64 : 0;
+      const uint64_t j = (uint64_t)(std::upper_bound(offsets, offsets + n_reads, lim) - offsets);
+      ch.read_end[c] = j > 0 ? j - 1 : 0;
+    }
+    ch.ready[c] = pooled_event(false);
+    if (!ch.ready[c]) return fail(SPK_E_CUDA, "upload event");
+    if (b1 > b0)
+      SPK_CUDA(cudaMemcpyAsync(res->reads.as<uint8_t>() + b0, data + b0, b1 - b0, cudaMemcpyHostToDevice,
+                               res->copy_stream));
+    SPK_CUDA(cudaEventRecord(ch.ready[c], res->copy_stream));
+    b0 = b1;
+  }
+  rv->chunks = &ch;
   return SPK_OK;
 }
 
@@ -235,6 +343,7 @@ int spk_ctx_create(int device, spk_ctx** out) {
   c->device = device;
   c->sm_count = prop.multiProcessorCount;
   c->l2_bytes = prop.l2CacheSize;
+  c->total_mem = prop.totalGlobalMem;
   e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   c->stream = c->own_stream;
   if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&c->pool, device);
@@ -378,6 +487,8 @@ int spk_count(spk_ctx* ctx, const uint8_t* data, size_t data_len, const uint64_t
   ReadsView rv;
   rc = upload_reads(res, ctx->stream, data, data_len, offsets, lengths, n_reads, &rv);
   if (!rc) rc = count_pipeline(ctx, ctx->stream, rv, 0, ks, n_k, res->opts, res);
+  if (res->chunks.n)  // the reads' buffer is freed after every piece has landed
+    cudaStreamWaitEvent(ctx->stream, res->chunks.ready[res->chunks.n - 1], 0);
   if (rc) {
     spk_result_free(res);
     return rc;
@@ -412,6 +523,7 @@ int spk_count_device(spk_ctx* ctx, const uint8_t* d_data, size_t data_len,
   rv.n_reads = n_reads;
   rv.data_len = data_len;
   rv.err = nullptr;
+  rv.chunks = nullptr;
   rc = count_pipeline(ctx, ctx->stream, rv, 0, ks, n_k, res->opts, res);
   if (rc) {
     spk_result_free(res);

@@ -18,7 +18,8 @@
 
 namespace spk {
 int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out);
-uint64_t job_estimate(const spk_job& j);
+uint64_t job_estimate(const spk_job& j, uint64_t total_mem);
+uint64_t usable_device_memory(spk_ctx* ctx);
 constexpr int kBatchInflight = 4;
 }  // namespace spk
 
@@ -37,21 +38,24 @@ extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, sp
     if (j.data_len && !j.data) return fail(SPK_E_INVALID_ARG, "null data");
   }
   SPK_CUDA(cudaSetDevice(ctx->device));
-  size_t fr = 0, tot = 0;
-  SPK_CUDA(cudaMemGetInfo(&fr, &tot));
   // A job larger than the whole budget still runs, alone.
-  uint64_t budget = (uint64_t)(fr * 0.9);
-  for (int i = 0; i < n_jobs; i++) budget = std::max<uint64_t>(budget, job_estimate(jobs[i]));
+  std::vector<uint64_t> need(n_jobs);
+  uint64_t budget = (uint64_t)(usable_device_memory(ctx) * 0.9);
+  for (int i = 0; i < n_jobs; i++) {
+    need[i] = job_estimate(jobs[i], ctx->total_mem);
+    budget = std::max<uint64_t>(budget, need[i]);
+  }
   int status = SPK_OK;
   std::string msg;
   std::vector<std::string> errs(n_jobs);  // the error message of a failed job
+  std::vector<int> sts(n_jobs, SPK_OK);
   {
     Scheduler sched(budget, kBatchInflight);
     std::vector<uint64_t> tickets(n_jobs);
     for (int i = 0; i < n_jobs; i++) {
       spk_job j = jobs[i];
       std::vector<uint32_t> ks(j.ks, j.ks + j.n_k);
-      tickets[i] = sched.submit(job_estimate(j), [ctx, j, ks](void** out, std::string* err) {
+      tickets[i] = sched.submit(need[i], [ctx, j, ks](void** out, std::string* err) {
         const int rc = run_job(ctx, j, ks, out);
         if (rc) *err = spk_last_error();
         return rc;
@@ -62,10 +66,22 @@ extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, sp
       void* r = nullptr;
       sched.wait(tickets[i], -1, &st, &r, nullptr, &errs[i]);
       results[i] = (spk_result*)r;
-      if (st && status == SPK_OK) {
-        status = st;
-        msg = "job " + std::to_string(i) + " of the batch failed: " + errs[i];
-      }
+      sts[i] = st;
+    }
+  }
+  // A job that ran out of device memory next to the others runs again alone.
+  for (int i = 0; i < n_jobs; i++) {
+    if (sts[i] == SPK_E_OOM) {
+      const spk_job& j = jobs[i];
+      std::vector<uint32_t> ks(j.ks, j.ks + j.n_k);
+      void* r = nullptr;
+      sts[i] = run_job(ctx, j, ks, &r);
+      if (sts[i]) errs[i] = spk_last_error();
+      else results[i] = (spk_result*)r;
+    }
+    if (sts[i] && status == SPK_OK) {
+      status = sts[i];
+      msg = "job " + std::to_string(i) + " of the batch failed: " + errs[i];
     }
   }
   if (status != SPK_OK) {

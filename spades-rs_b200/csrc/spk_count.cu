@@ -654,6 +654,9 @@ constexpr int kPartBlock = SPK_PART_BLOCK;
 constexpr int kPartCtasPerSm = SPK_PART_CTAS_PER_SM;
 constexpr int kScatterBatch = SPK_SCATTER_BATCH;  // positions per lane in flight in k_part_scatter
 constexpr int kSpanBatch = 2;      // slots per thread in flight in k_part_count's write-out
+#ifndef SPK_COUNT_PREFETCH
+#define SPK_COUNT_PREFETCH 0
+#endif
 constexpr uint32_t kErrRegion = 8;
 
 template <int NL>
@@ -1290,6 +1293,10 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
             C.v[NL - 1] = v.y;
           }
           i += blockDim.x;
+#if SPK_COUNT_PREFETCH
+          // the key this lane takes next, on its way to L1 while this one is placed
+          if (i < e) asm volatile("prefetch.global.L1 [%0];" ::"l"(pv.keys + (uint64_t)NL * i));
+#endif
           if (pv.packed_home) {
             const uint64_t top = C.v[NL - 1];
             home = (uint32_t)(top >> (64 - kHomeBits)) >> (kHomeBits - t.log2span);
@@ -2157,6 +2164,18 @@ __global__ void __launch_bounds__(kBlock) k_occ(const uint32_t* __restrict__ len
   warp_add_u64(out, s);
 }
 
+// flag = 1 if some read starts before the end of the read before it (the
+// chunked upload then cannot hand reads to the first pass piece by piece).
+__global__ void __launch_bounds__(kBlock) k_read_order(const uint64_t* __restrict__ offsets,
+                                                      const uint32_t* __restrict__ lengths, uint64_t n,
+                                                      unsigned long long* __restrict__ flag) {
+  bool bad = false;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i + 1 < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    bad |= offsets[i] + (lengths[i] + 3ull) / 4 > offsets[i + 1];
+  if (__any_sync(FULL, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1ull);
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -2340,8 +2359,8 @@ static uint64_t fused_capacity(uint64_t occ) {
 
 struct Ev {
   cudaEvent_t e = nullptr;
-  Ev() { cudaEventCreate(&e); }
-  ~Ev() { if (e) cudaEventDestroy(e); }
+  Ev() : e(pooled_event(true)) {}
+  ~Ev() { pooled_event_put(e, true); }
   Ev(const Ev&) = delete;
   Ev& operator=(const Ev&) = delete;
 };
@@ -2489,8 +2508,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
       // Regions hold 1.5x the mean share of occurrences per span: keep them
       // within a quarter of the device memory, else count with global atomics.
       // The two-level pass also holds the coarse buckets (1.125x) meanwhile.
-      size_t fr = 0, tot = 0;
-      SPK_CUDA(cudaMemGetInfo(&fr, &tot));
+      const uint64_t tot = ctx->total_mem;
       partitioned = (occ0 + (occ0 >> 1) + (1u << 20)) * (uint64_t)nl * 8 <= tot / 4;
       two_level_fits = (occ0 * 3 + (1u << 22)) * (uint64_t)nl * 8 <= tot / 4;
     }
@@ -3009,15 +3027,16 @@ struct SideStream {
   cudaStream_t s = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int open() {
-    SPK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    SPK_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-    SPK_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    s = pooled_stream();
+    fork = pooled_event(false);
+    join = pooled_event(false);
+    if (!s || !fork || !join) return fail(SPK_E_CUDA, "side stream or events");
     return SPK_OK;
   }
   ~SideStream() {
-    if (s) cudaStreamDestroy(s);  // pending work still completes
-    if (fork) cudaEventDestroy(fork);
-    if (join) cudaEventDestroy(join);
+    pooled_stream_put(s);  // work still queued on it runs before its next user's
+    pooled_event_put(fork, false);
+    pooled_event_put(join, false);
   }
 };
 
@@ -3035,18 +3054,25 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   if (nranges > kMaxRanges) return kNotThisPath;
   int rc;
   DevBuf scratch;
-  if ((rc = scratch.alloc(S_WORDS * 8, st))) return rc;
+  constexpr int S_ORDER = S_WORDS;  // reads out of order (chunked upload)
+  if ((rc = scratch.alloc((S_WORDS + 1) * 8, st))) return rc;
   uint64_t* sw = scratch.as<uint64_t>();
-  SPK_CUDA(cudaMemsetAsync(sw, 0, S_WORDS * 8, st));
+  SPK_CUDA(cudaMemsetAsync(sw, 0, (S_WORDS + 1) * 8, st));
   unsigned long long* su = (unsigned long long*)sw;
   // ---- the first readback: occurrences, which size the table ----
   Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1;
   SPK_CUDA(cudaEventRecord(e0.e, st));
   k_occ<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv_in.lengths, rv_in.n_reads, k, su + S_OCC0);
   SPK_CUDA(cudaGetLastError());
+  if (rv_in.chunks) {
+    k_read_order<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv_in.offsets, rv_in.lengths, rv_in.n_reads, su + S_ORDER);
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaMemcpyAsync(host + S_ORDER, sw + S_ORDER, 8, cudaMemcpyDeviceToHost, st));
+  }
   SPK_CUDA(cudaMemcpyAsync(host + S_OCC0, sw + S_OCC0, 8, cudaMemcpyDeviceToHost, st));
   SPK_CUDA(cudaStreamSynchronize(st));
   const uint64_t occ0 = host[S_OCC0];
+  const bool per_chunk = rv_in.chunks && host[S_ORDER] == 0;
   uint64_t cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(occ0);
   const uint32_t log2span = nl == 1 ? kPartLog2Span1 : kPartLog2Span2;
   uint32_t log2cap = 0;
@@ -3054,11 +3080,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   if (log2cap <= log2span) return kNotThisPath;
   const uint32_t log2parts = log2cap - log2span;
   if (!SPK_TWO_LEVEL || log2parts <= kCoarseBits || log2parts - kCoarseBits > kFineMaxBits) return kNotThisPath;
-  {
-    size_t fr = 0, tot = 0;
-    SPK_CUDA(cudaMemGetInfo(&fr, &tot));
-    if ((occ0 * 3 + (1u << 22)) * (uint64_t)nl * 8 > tot / 4) return kNotThisPath;
-  }
+  if ((occ0 * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4) return kNotThisPath;
 
   kr.k = k;
   kr.nl = nl;
@@ -3109,9 +3131,31 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
     k_part_uniform<<<1, 128, 0, st>>>(kCoarse, ccap, cbase.as<uint64_t>());
     SPK_CUDA(cudaMemsetAsync(cfill.p, 0, kCoarse * 4 * kFillStride, st));
     CoarseView cv{cregion.as<uint64_t>(), cbase.as<uint64_t>(), cfill.as<unsigned int>(), ccap, errp};
-    if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rv, k, pv, cv, su + S_OCC);
-    else rc = launch_part_coarse<2>(ctx, st, rv, k, pv, cv, su + S_OCC);
-    if (rc) return rc;
+    if (per_chunk) {
+      // the reads of each uploaded piece as soon as it is on the device
+      uint64_t r0 = 0;
+      for (int c = 0; c < rv.chunks->n; c++) {
+        SPK_CUDA(cudaStreamWaitEvent(st, rv.chunks->ready[c], 0));
+        const uint64_t r1 = std::min<uint64_t>(std::max<uint64_t>(rv.chunks->read_end[c], r0), rv.n_reads);
+        if (r1 > r0) {
+          ReadsView rc_ = rv;
+          rc_.offsets += r0;
+          rc_.lengths += r0;
+          rc_.n_reads = r1 - r0;
+          if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rc_, k, pv, cv, su + S_OCC);
+          else rc = launch_part_coarse<2>(ctx, st, rc_, k, pv, cv, su + S_OCC);
+          if (rc) return rc;
+          launches++;
+        }
+        r0 = r1;
+      }
+      launches--;  // counted below
+    } else {
+      if (rv.chunks) SPK_CUDA(cudaStreamWaitEvent(st, rv.chunks->ready[rv.chunks->n - 1], 0));
+      if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rv, k, pv, cv, su + S_OCC);
+      else rc = launch_part_coarse<2>(ctx, st, rv, k, pv, cv, su + S_OCC);
+      if (rc) return rc;
+    }
     k_coarse_chunks<<<1, 32, 0, st>>>(cv, cfirst.as<uint32_t>());
     if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
     else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
@@ -3328,6 +3372,8 @@ static int count_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsVie
                    const spk_count_opts& o, KResult& kr) {
   const int rc = count_one_k_list(ctx, st, host, rv, k, o, kr);
   if (rc != kNotThisPath && rc != kRedo) return rc;
+  // every uploaded piece of the reads, before the general path reads them
+  if (rv.chunks) SPK_CUDA(cudaStreamWaitEvent(st, rv.chunks->ready[rv.chunks->n - 1], 0));
   SPK_CUDA(cudaStreamSynchronize(st));  // the abandoned job's buffers are freed in stream order
   kr = KResult();
   const int rc2 = count_one_k(ctx, st, host, rv, k, o, kr);
@@ -3349,8 +3395,8 @@ int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t 
   // k values are independent, so each counts concurrently on its own stream
   // and staging block over the same read-only reads, once the reads that st
   // uploads are ready.
-  cudaEvent_t ready;
-  SPK_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  cudaEvent_t ready = pooled_event(false);
+  if (!ready) return fail(SPK_E_CUDA, "event");
   SPK_CUDA(cudaEventRecord(ready, st));
   std::vector<std::unique_ptr<KResult>> krs(n_k);
   std::vector<int> rcs(n_k, SPK_OK);
@@ -3363,15 +3409,15 @@ int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t 
       uint64_t* h = staging_acquire(ctx);
       int rc = SPK_OK;
       if (!h) rc = fail(SPK_E_OOM, "pinned host staging allocation failed");
-      else if (cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) != cudaSuccess)
-        rc = cuda_fail(cudaGetLastError(), "per-k stream");
+      else if (!(s2 = pooled_stream()))
+        rc = fail(SPK_E_CUDA, "per-k stream");
       auto kr = std::make_unique<KResult>();
       if (!rc && cudaStreamWaitEvent(s2, ready, 0) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "wait");
       if (!rc) rc = count_k(ctx, s2, h, rv, ks[i], o, *kr);
       if (s2) {
         cudaStreamSynchronize(s2);
         rehome(*kr, st);
-        cudaStreamDestroy(s2);
+        pooled_stream_put(s2);
       }
       staging_release(ctx, h);
       if (rc) errs[i] = spk_last_error();
@@ -3380,7 +3426,7 @@ int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t 
     });
   }
   for (auto& t : th) t.join();
-  cudaEventDestroy(ready);
+  pooled_event_put(ready, false);
   for (int i = 0; i < n_k; i++)
     if (rcs[i]) return fail(rcs[i], "k=" + std::to_string(ks[i]) + ": " + errs[i]);
   for (int i = 0; i < n_k; i++) res->ks.push_back(std::move(krs[i]));

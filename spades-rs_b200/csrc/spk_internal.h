@@ -58,6 +58,19 @@ struct DevBuf {
 };
 
 // ---- packed reads on the device --------------------------------------------
+// Packed data copied up in chunks on a copy stream (spk_count with host
+// buffers): chunk c holds bytes [0, byte_end[c]) once ready[c] has fired,
+// and, when the reads lie in order (each read at or after the end of the one
+// before it, which the device checks), reads [0, read_end[c]) lie in it.
+// Offsets and lengths are on the device before the count starts.
+constexpr int kMaxReadChunks = 8;
+struct ReadChunks {
+  int n = 0;
+  uint64_t byte_end[kMaxReadChunks] = {};
+  uint64_t read_end[kMaxReadChunks] = {};
+  cudaEvent_t ready[kMaxReadChunks] = {};
+};
+
 struct ReadsView {
   const uint64_t* words;    // packed bytes viewed as 64-bit words (8-byte aligned base)
   const uint64_t* offsets;  // byte offset of each read, relative to byte_base
@@ -66,6 +79,7 @@ struct ReadsView {
   uint64_t byte_base;       // byte offset of data[0] from `words`
   uint64_t data_len;        // bytes of packed data; reads beyond it are rejected
   int* err;                 // device error word: bit 2 set for an out-of-bounds read
+  const ReadChunks* chunks; // host: the data still arriving in chunks, or nullptr
 };
 
 // ---- count table --------------------------------------------------------------
@@ -127,6 +141,15 @@ struct KResult {
 
 struct spk_result_impl;
 
+// Non-blocking streams and events of the current device, reused across jobs
+// (a job then makes no stream or event creation call, which can wait on
+// other clients of the driver).  A stream handed back may still have work
+// queued; its next user's work runs after it.
+cudaStream_t pooled_stream();
+void pooled_stream_put(cudaStream_t s);
+cudaEvent_t pooled_event(bool timing);
+void pooled_event_put(cudaEvent_t e, bool timing);
+
 }  // namespace spk
 
 // ---- opaque handles --------------------------------------------------------------
@@ -137,6 +160,7 @@ struct spk_ctx {
   cudaMemPool_t pool = nullptr;
   int sm_count = 0;
   size_t l2_bytes = 0;
+  size_t total_mem = 0;     // device memory (the partitioned passes size against it)
   spk::DevBuf scratch;      // small device scratch (counters, flags)
   // Pinned host staging blocks (kStagingBytes each) for counters read back
   // during a count.  Every result holds its own block, so jobs that run
@@ -159,6 +183,15 @@ struct spk_result {
   spk_ctx* ctx = nullptr;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // chunked upload of the packed data (copy stream and its events), kept
+  // until the count has used the reads
+  spk::ReadChunks chunks;
+  cudaStream_t copy_stream = nullptr;
+  ~spk_result() {
+    for (int c = 0; c < chunks.n; c++)
+      if (chunks.ready[c]) spk::pooled_event_put(chunks.ready[c], false);
+    if (copy_stream) spk::pooled_stream_put(copy_stream);
+  }
   spk_count_opts opts{};
   std::vector<std::unique_ptr<spk::KResult>> ks;
   spk::DevBuf reads;  // device copy of the packed reads (when copied in by spk_count)

@@ -33,38 +33,71 @@ static uint64_t next_pow2_u64(uint64_t x) {
   return p;
 }
 
-// Device bytes a job is expected to hold at its peak (per k, the k values of
-// a job run one after another and earlier results stay resident):
-//   reads                      packed bytes + 12 B per read
-//   Bloom                      both tiers (+ the reference tier)
-//   table                      2^ceil(log2(0.3 occ)) slots, the count-first capacity
-//   partitioned passes         span regions of 1.5 occ keys, Bloom operations of
-//                              3.75 per table slot
-//   list and sort temporaries  twice (key + count) per admitted k-mer, bounded by
-//                              the table
-// Occurrences are bounded by the bases (4 per packed byte).  A job that
-// outgrows the estimate still runs; it only makes concurrent jobs less likely
-// to fit.
-uint64_t job_estimate(const spk_job& j) {
+// Device bytes a job is expected to hold at its peak, per k (the k values of
+// a job run concurrently, so their peaks add up), following the schedule
+// spk_count picks:
+//   occurrences      4 per packed byte less k - 1 per read (reads of >= k bases)
+//   table capacity   next_pow2(0.3 occ), at least 1024 slots
+//   default job      (12 <= k <= 64, partition within a quarter of the device)
+//     first pass     span regions 1.5 occ keys + coarse buckets 1.125 occ keys
+//     span count     regions + list and singleton keys (one entry per slot
+//                    each) + Bloom operations (3.75 per slot) + the list's
+//                    sort temporaries + both tiers
+//   other schedules  the table (slots of 16/32/64 bytes), the interleaved
+//                    tiers, and a list of a quarter of the slots with its sort
+// Reads and outputs (list, edges, kept tiers) are added on top.  A job that
+// outgrows the estimate still runs; the batch re-runs a job that ran out of
+// memory alone after the others.
+uint64_t job_estimate(const spk_job& j, uint64_t total_mem) {
   spk_count_opts o = j.opts;
   const uint64_t bloom_bits = o.bloom_bits ? o.bloom_bits : (512ULL << 20);
   const uint64_t words = std::max<uint64_t>((bloom_bits + 63) / 64, 1);
-  const uint64_t occ = (uint64_t)j.data_len * 4;
+  const uint64_t nranges = (words * 64 + (1ULL << 19) - 1) >> 19;
   uint64_t bytes = j.data_len + 64 + j.n_reads * 12;
-  uint64_t resident = 0, peak = 0;
+  const bool plain = !(o.flags & (SPK_F_GATED | SPK_F_CORRECT | SPK_F_REF_SOLID | SPK_F_DIRECT | SPK_F_KEEP_TABLE)) &&
+                     !(o.n_prior > 0 && o.prior_seqs);
   for (int i = 0; i < j.n_k; i++) {
     const uint32_t k = j.ks ? j.ks[i] : 31;
     const uint64_t nl = (k + 31) / 32;
-    const uint64_t slot = nl == 1 ? 16 : (nl <= 3 ? 32 : 64);
+    const uint64_t b4 = (uint64_t)j.data_len * 4, sub = (uint64_t)j.n_reads * (k - 1);
+    const uint64_t occ = b4 > sub ? b4 - sub : 0;
     const uint64_t cap = std::max<uint64_t>(next_pow2_u64(occ * 3 / 10 + 1), 1024);
+    const uint64_t key = nl * 8, entry = nl * 8 + 4;
     const uint64_t tiers = words * 16 + (o.flags & SPK_F_REF_SOLID ? words * 8 : 0);
-    const uint64_t table = cap * slot;
-    const uint64_t passes = nl <= 2 ? (occ + occ / 2) * nl * 8 + cap * 15 : words * 16;
-    const uint64_t lists = std::min<uint64_t>(occ / 4, cap) * (nl * 8 + 4) * 2;
-    peak = std::max(peak, resident + tiers + table + passes + lists);
-    resident += tiers + table + lists / 2;
+    uint64_t peak;
+    if (plain && nl <= 2 && k >= 12 && (occ * 3 + (1u << 22)) * key <= total_mem / 4) {
+      const uint64_t regions = (occ + occ / 2) * key + (1u << 20) * key;
+      const uint64_t first = regions + (occ + occ / 8 + 8192 * 64) * key;
+      const uint64_t ops = (cap * 3 + cap * 3 / 4 + 1024 * nranges) * 4;
+      const uint64_t count = regions + cap * entry + cap * key + ops + cap * entry + tiers;
+      peak = std::max(first, count);
+    } else {
+      const uint64_t slot = nl == 1 ? 16 : (nl <= 3 ? 32 : 64);
+      peak = cap * slot + tiers + (cap / 4) * entry * 2;
+    }
+    // outputs: the list and about one edge per listed k-mer
+    peak += (cap / 4) * (entry + (k + 32) / 32 * 8);
+    bytes += peak;
   }
-  return bytes + peak;
+  return bytes;
+}
+
+// Device memory a scheduler may budget: what the driver reports free plus
+// what the stream-ordered pool holds cached but unused.
+uint64_t usable_device_memory(spk_ctx* ctx) {
+  size_t f = 0, t = 0;
+  if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  uint64_t reserved = 0, used = 0;
+  if (ctx->pool &&
+      cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+      reserved > used)
+    return f + (reserved - used);
+  cudaGetLastError();
+  return f;
 }
 
 int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out) {
@@ -83,6 +116,8 @@ int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, voi
   ReadsView rv;
   int rc = upload_reads(res, st, j.data, j.data_len, j.offsets, j.lengths, j.n_reads, &rv);
   if (!rc) rc = count_pipeline(ctx, st, rv, 0, ks.data(), (int)ks.size(), res->opts, res);
+  if (res->chunks.n)  // the reads' buffer is freed after every piece has landed
+    cudaStreamWaitEvent(st, res->chunks.ready[res->chunks.n - 1], 0);
   res->reads.release();
   res->offs.release();
   res->lens.release();
@@ -113,7 +148,14 @@ extern "C" {
 
 int spk_job_hbm_estimate(const spk_job* job, uint64_t* bytes) {
   if (!job || !bytes) return fail(SPK_E_INVALID_ARG, "null argument");
-  *bytes = job_estimate(*job);
+  if (!job->ks || job->n_k < 1) return fail(SPK_E_INVALID_ARG, "job has no k");
+  int dev = 0;
+  cudaDeviceProp prop;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    cudaGetLastError();
+    prop.totalGlobalMem = 0;
+  }
+  *bytes = job_estimate(*job, prop.totalGlobalMem ? prop.totalGlobalMem : (180ull << 30));
   return SPK_OK;
 }
 
@@ -122,11 +164,7 @@ int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight) {
   SPK_CUDA(cudaSetDevice(ctx->device));
   std::unique_lock<std::mutex> l(ctx->serve_mu);
   if (ctx->server) return fail(SPK_E_INVALID_ARG, "serving loop already running");
-  if (!hbm_budget_bytes) {
-    size_t f = 0, t = 0;
-    SPK_CUDA(cudaMemGetInfo(&f, &t));
-    hbm_budget_bytes = (uint64_t)(f * 0.9);
-  }
+  if (!hbm_budget_bytes) hbm_budget_bytes = (uint64_t)(usable_device_memory(ctx) * 0.9);
   auto* s = new Server();
   s->budget = hbm_budget_bytes;
   s->sched = std::make_shared<Scheduler>(hbm_budget_bytes, max_inflight > 0 ? max_inflight : 4,
@@ -150,7 +188,7 @@ int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket) {
   if (!ctx->server) return fail(SPK_E_INVALID_ARG, "serving loop not started");
   spk_job j = *job;
   std::vector<uint32_t> ks(job->ks, job->ks + job->n_k);
-  const uint64_t need = job_estimate(j);
+  const uint64_t need = job_estimate(j, ctx->total_mem);
   // The job runs on a worker thread: its error message is taken there and
   // handed to the caller of spk_wait with the status.
   *ticket = ctx->server->sched->submit(need, [ctx, j, ks](void** out, std::string* msg) {
