@@ -571,48 +571,53 @@ def run_c3(args, ctx, log_rank0):
             "speedup_vs_plain": t_plain / t_multi}
 
 
-def run_c4(args, ctx, log_rank0):
-    """Batched uneven samples: 64 samples (genome log-uniform 0.5-12 Mb x --scale,
-    GC 30-70%, 20-200x, 0.5% errors), k=33, host buffers in and solid lists
-    out: spk_count_batch against spk_count on one sample after another.  The
-    read sets come from the native seeded generator."""
+def batched_vs_plain(ctx, scale, steps, warmup, bloom_bits, log_rank0):
+    """64 uneven samples (genome log-uniform 0.5-12 Mb x scale, GC 30-70%,
+    20-200x, 0.5% errors, k=33) from the native generator, host buffers in
+    and solid lists out: spk_count_batch against spk_count on one sample
+    after another.  Returns the measurement as a dict."""
     import torch
     import spk
     from spk import synth
     t0 = time.time()
-    ss = synth.c4_native(64, args.scale)
+    ss = synth.c4_native(64, scale)
     packs = [s.packed for s in ss]
     occ = sum(synth.occurrences(p, 33) for p in packs)
     log_rank0(f"c4: {len(packs)} samples, {occ} occurrences, generated in {time.time() - t0:.1f}s")
-    opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
+    opts = dict(bloom_bits=bloom_bits, flags=spk.SPK_F_EDGES)
 
     # job latency: from the start of the step's work on that job (plain) or
     # of the batch (batched) to the job's solid list on the host
     lat_plain, lat_batch = [], []
+    same = []
 
-    def plain(lat=None):
+    def plain(lat=None, keep=None):
         for p in packs:
             a = time.perf_counter()
             r = spk.count(p, [33], ctx=ctx, **opts)
-            r.solid(0)
+            sk = r.solid(0)
             r.close()
             if lat is not None:
                 lat.append((time.perf_counter() - a) * 1e3)
+            if keep is not None:
+                keep.append(sk)
 
-    def batched(lat=None):
+    def batched(lat=None, keep=None):
         a = time.perf_counter()
         rs = spk.count_batch([spk.Job(p, [33], dict(opts)) for p in packs], ctx=ctx)
         for r in rs:
-            r.solid(0)
+            sk = r.solid(0)
             r.close()
             if lat is not None:
                 lat.append((time.perf_counter() - a) * 1e3)
+            if keep is not None:
+                keep.append(sk)
 
     def timed(fn, lat):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         out = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             torch.cuda.synchronize()
             a = time.perf_counter()
             fn(lat)
@@ -622,22 +627,36 @@ def run_c4(args, ctx, log_rank0):
 
     t_plain = timed(plain, lat_plain)
     t_batch = timed(batched, lat_batch)
+    # identical exact output: every sample's solid list, batched and alone
+    kp, kb = [], []
+    plain(keep=kp)
+    batched(keep=kb)
+    import numpy as np
+    identical = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(kp, kb))
 
     def pct(v):
         v = sorted(v)
         return {"p50": v[len(v) // 2], "p99": v[min(len(v) - 1, int(0.99 * len(v)))]} if v else None
-    return {"metric": METRIC, "value": _gk(occ, t_batch), "unit": "Gk-mers/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-            "data": "synthetic (seeded; no public dataset)",
-            "config": {"workload": f"c4: 64 samples at genome scale {args.scale}, k=33, "
-                                   "spk_count_batch (host buffers in, solid lists out)",
-                       "occurrences": occ, "bloom_bits": args.bloom_bits,
-                       "timing": "host clock around synchronised calls"},
+    return {"workload": f"64 samples, genome 0.5-12 Mb x {scale}, 20-200x, k=33, host buffers in, "
+                        "solid lists out", "occurrences": occ,
+            "value": _gk(occ, t_batch), "ms_per_step": t_batch * 1e3,
             "plain": {"what": "spk_count on one sample after another", "value": _gk(occ, t_plain),
                       "ms_per_step": t_plain * 1e3, "job_latency_ms": pct(lat_plain)},
-            "job_latency_ms": pct(lat_batch),
-            "speedup_vs_plain": t_plain / t_batch}
+            "job_latency_ms": pct(lat_batch), "speedup_vs_plain": t_plain / t_batch,
+            "identical_output": identical, "timing": "host clock around synchronised calls"}
+
+
+def run_c4(args, ctx, log_rank0):
+    """Batched uneven samples at --scale (1.0: the workload as specified)."""
+    b = batched_vs_plain(ctx, args.scale, args.steps, args.warmup, args.bloom_bits, log_rank0)
+    return {"metric": METRIC, "value": b["value"], "unit": "Gk-mers/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": b["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": "c4: " + b["workload"] + "; spk_count_batch", "occurrences": b["occurrences"],
+                       "bloom_bits": args.bloom_bits, "timing": b["timing"]},
+            "plain": b["plain"], "job_latency_ms": b["job_latency_ms"],
+            "speedup_vs_plain": b["speedup_vs_plain"], "identical_output": b["identical_output"]}
 
 
 def run_c5(args, ctx, log_rank0):
@@ -703,6 +722,8 @@ def main():
     ap.add_argument("--bloom-bits", type=int, default=512 << 20)
     ap.add_argument("--cpu-occ", type=int, default=0,
                     help="k-mer occurrences in the CPU baseline sample (0: the whole workload)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-vs-plain measurement of the default run")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the full-size check of one job's result against the oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -863,6 +884,7 @@ def main():
         # algorithmic bytes.
         scatter_ms = sum(i["ms_scatter_kernel"] for i in infos) / len(infos)
         ops = 3 * info["n_distinct"]
+        n_ge2 = info["n_table"] - info["n_singletons"]  # k-mers counted at least twice
         # the read pass that leaves every key in its span's region: one kernel,
         # or two (coarse buckets, then spans) timed together
         sname = "k_part_coarse+k_part_fine" if info.get("part_passes") == 2 else "k_part_scatter"
@@ -870,8 +892,11 @@ def main():
             # read stream and one streamed key write per occurrence (the
             # algorithm's need; the two-level form moves the keys twice more)
             (sname, scatter_ms, occ * (sb + 16)),
-            # keys read back, every table slot written, 4-byte Bloom ops written
-            ("k_part_count", count_ms, occ * 16 + info["table_capacity"] * 32 + ops * 4),
+            # keys read back; out: the k-mers counted twice or more as list
+            # entries (key + count), the singleton keys, and three 4-byte Bloom
+            # operations per distinct k-mer (the table itself is not written)
+            ("k_part_count", count_ms,
+             occ * 16 + n_ge2 * 20 + (info["n_distinct"] - n_ge2) * 16 + ops * 4),
             # Bloom ops read, both tiers written
             ("k_bloom_apply", bloom_ms, ops * 4 + 2 * info["bloom_size_bits"] / 8),
         ]
@@ -935,6 +960,12 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_baseline(p, 1, 0, args.cpu_occ, args.bloom_bits)
 
+    # the metric's batched-vs-plain part: a 64-sample batch at a tenth of the
+    # specified genome sizes (the full batch: --workload c4)
+    batched = None
+    if rank == 0 and not args.no_batched:
+        batched = batched_vs_plain(ctx, 0.1, 1, 1, args.bloom_bits, log)
+
     # full-size parity of one more job against the oracle (rank 0 alone; every
     # rank counts the same reads)
     parity, parity_detail = None, None
@@ -954,6 +985,9 @@ def main():
             "data": "synthetic (seeded; no public dataset)",
             "config": c2_config(p, occ, args, world),
             "parity": parity, "parity_detail": parity_detail,
+            "batched": batched,
+            "speedup_vs_plain": batched["speedup_vs_plain"] if batched else None,
+            "job_latency_ms": batched["job_latency_ms"] if batched else None,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks,
             "result": {"n_solid": info["n_solid"], "n_list": info["n_list"],

@@ -208,8 +208,9 @@ int spk_packed_free(spk_packed* p);
                                   corrected copy.  Implies SPK_F_GATED. */
 #define SPK_F_KEEP_TABLE 0x40u /* keep the count table for spk_result_table_view.  Without it
                                   the partitioned schedule writes the k-mer list directly
-                                  from its spans and never materialises the table; the other
-                                  schedules (and prior contigs) build the table anyway */
+                                  from its spans and never materialises the table, and the
+                                  other schedules (and prior contigs), which need it while
+                                  counting, free it when the job ends */
 
 /* spk_result_info.schedule */
 #define SPK_SCHEDULE_GATED       0u  /* SPK_F_GATED: Bloom pass, then the gated count pass */
@@ -337,8 +338,8 @@ typedef struct spk_table_view {
    * significant), little-endian limbs.  For k <= 64 that equals the Kmer256
    * limbs; for k > 64 the Kmer256 form is (value >> 2(k-64), value & mask). */
 } spk_table_view;
-/* Fails with SPK_E_INVALID_ARG when the job did not build the table (the
- * partitioned schedule without SPK_F_KEEP_TABLE or prior contigs). */
+/* Fails with SPK_E_INVALID_ARG when the job did not keep the table (counted
+ * without SPK_F_KEEP_TABLE). */
 int spk_result_table_view(spk_result* res, int k_index, spk_table_view* view);
 
 /* Unitigs of the solid k-mers: the maximal non-branching paths of their de

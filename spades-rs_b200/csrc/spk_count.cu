@@ -655,7 +655,7 @@ constexpr int kPartCtasPerSm = SPK_PART_CTAS_PER_SM;
 constexpr int kScatterBatch = SPK_SCATTER_BATCH;  // positions per lane in flight in k_part_scatter
 constexpr int kSpanBatch = 2;      // slots per thread in flight in k_part_count's write-out
 #ifndef SPK_COUNT_PREFETCH
-#define SPK_COUNT_PREFETCH 0
+#define SPK_COUNT_PREFETCH 1
 #endif
 constexpr uint32_t kErrRegion = 8;
 
@@ -2413,6 +2413,34 @@ enum {
   S_WORDS = 16 + kHistBins
 };
 
+// What a finished job keeps: the list and edge buffers cut to what they hold
+// (they were sized by bounds: table slots, eight edges per solid k-mer), and
+// the count table only when SPK_F_KEEP_TABLE asks for it.  Results stay
+// resident (serving, batches), so their size decides how many fit.
+static int shrink_to(DevBuf& b, uint64_t used, cudaStream_t st) {
+  used = std::max<uint64_t>(used, 16);
+  if (!b.p || b.bytes <= used + used / 4 + (1u << 20)) return SPK_OK;
+  DevBuf n;
+  int rc;
+  if ((rc = n.alloc(used, st))) return rc;
+  SPK_CUDA(cudaMemcpyAsync(n.p, b.p, used, cudaMemcpyDeviceToDevice, st));
+  b = std::move(n);  // the old buffer is freed after the copy, in stream order
+  return SPK_OK;
+}
+static int keep_results(KResult& kr, cudaStream_t st, uint32_t flags) {
+  int rc;
+  for (int j = 0; j < kr.nl; j++)
+    if ((rc = shrink_to(kr.list[j], kr.list_len * 8, st))) return rc;
+  if ((rc = shrink_to(kr.list[4], kr.list_len * 4, st))) return rc;
+  for (int j = 0; j < kr.nle; j++)
+    if ((rc = shrink_to(kr.edges[j], kr.info.n_edges * 8, st))) return rc;
+  if (!(flags & SPK_F_KEEP_TABLE)) {
+    kr.tslots.release();
+    kr.table.slots = nullptr;
+  }
+  return SPK_OK;
+}
+
 int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv_in, unsigned k,
                 const spk_count_opts& o, KResult& kr) {
   kr.k = k;
@@ -2987,6 +3015,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     kr.seen.release();
     kr.twice.release();
   }
+  if ((rc = keep_results(kr, st, o.flags))) return rc;
   SPK_CUDA(cudaEventRecord(e6.e, st));
   SPK_CUDA(cudaStreamSynchronize(st));
   info.ms_bloom = ms_between(e0, e1);
@@ -3340,6 +3369,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   const unsigned nbig_l = hb[0], nbig_e = hb[1];
   if ((rc = sort_dev_finish(st, lsort, kr.list, &kr.list[4], kr.list_len, nbig_l, host, &launches))) return rc;
   if ((rc = sort_dev_finish(st, esort, kr.edges, nullptr, info.n_edges, nbig_e, host, &launches))) return rc;
+  if ((rc = keep_results(kr, st, o.flags))) return rc;
   SPK_CUDA(cudaEventRecord(e6.e, st));
   SPK_CUDA(cudaStreamSynchronize(st));
   info.ms_bloom = ms_between(e0, e1);
