@@ -688,12 +688,17 @@ def run_c5(args, ctx, log_rank0):
             while time.perf_counter() < due:
                 time.sleep(min(0.002, max(0.0, due - time.perf_counter())))
             tickets.append(srv.submit(spk.Job(p, [55], dict(opts))))
-        lat = []
-        for t in tickets:
+        lat, per_job = [], []
+        for i, t in enumerate(tickets):
             r, ms = srv.wait(t)
             r.solid(0)
+            inf = r.info(0)
             r.close()
             lat.append(ms)
+            per_job.append({"kind": synth.c5_plan(i, args.scale)["kind"],
+                            "occurrences": int(inf["occurrences"]), "latency_ms": round(ms, 1),
+                            "job_ms": round(inf["ms_total"], 1), "schedule": int(inf["schedule"]),
+                            "relayouts": int(inf["part_rescatters"])})
         wall = time.perf_counter() - start
     finally:
         srv.stop()
@@ -707,7 +712,10 @@ def run_c5(args, ctx, log_rank0):
                        "occurrences": occ, "bloom_bits": args.bloom_bits,
                        "timing": "host clock; throughput over the arrival span"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                           "max": float(lat.max())}}
+                           "max": float(lat.max())},
+            # each job: its kind, size, latency (submit to result), device time of the
+            # count, schedule and layout repeats
+            "jobs": per_job}
 
 
 # ---------------------------------------------------------------------------
