@@ -609,7 +609,7 @@ int spk_result_free(spk_result* res) {
   res->lens.release();
   cudaStreamSynchronize(st);
   staging_release(res->ctx, res->h_staging);
-  if (res->own_stream) cudaStreamDestroy(st);
+  if (res->own_stream) pooled_stream_put(st);  // synchronised above: idle
   delete res;
   return SPK_OK;
 }

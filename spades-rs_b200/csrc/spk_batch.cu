@@ -20,7 +20,7 @@ namespace spk {
 int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out);
 uint64_t job_estimate(const spk_job& j, uint64_t total_mem);
 uint64_t usable_device_memory(spk_ctx* ctx);
-constexpr int kBatchInflight = 4;
+constexpr int kBatchInflight = 8;
 }  // namespace spk
 
 extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, spk_result** results) {

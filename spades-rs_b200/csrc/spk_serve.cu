@@ -102,12 +102,11 @@ uint64_t usable_device_memory(spk_ctx* ctx) {
 
 int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, void** out) {
   cudaSetDevice(ctx->device);
-  cudaStream_t st;
-  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return cuda_fail(e, "job stream");
+  cudaStream_t st = pooled_stream();
+  if (!st) return fail(SPK_E_CUDA, "job stream");
   auto* res = result_new(ctx, st, true);
   if (!res) {
-    cudaStreamDestroy(st);
+    pooled_stream_put(st);
     return SPK_E_OOM;
   }
   res->opts = j.opts;
