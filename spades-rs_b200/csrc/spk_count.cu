@@ -751,8 +751,25 @@ __device__ __forceinline__ uint64_t region_base(const PartView& pv, uint32_t p) 
   return pv.uniform ? (uint64_t)p * pv.uniform : pv.base[p];
 }
 
+// Ranking inside a tile.  SPK_COARSE_MATCH 1: every warp ranks its keys of
+// a window among themselves (__match_any_sync on the bucket) and records per
+// (window, warp) bucket counts; a scan over those gives each key its place in
+// the bucket-sorted tile, so keys stay in registers and go to shared memory
+// once.  0: one shared-memory atomic per key on the tile's bucket counters.
+#ifndef SPK_COARSE_MATCH
+#define SPK_COARSE_MATCH 1
+#endif
+constexpr int kCoarseWarps = kCoarseBlock / 32;
+// The fine pass prefetches its next chunk's keys into L2.
+#ifndef SPK_FINE_PREFETCH
+#define SPK_FINE_PREFETCH 1
+#endif
+
 template <int NL>
 size_t coarse_smem() {
+  if (SPK_COARSE_MATCH)
+    return (size_t)kCoarseSlots * NL * 8 + kCoarseSlots + (size_t)kCoarseW * kCoarseWarps * kCoarse * 4 +
+           kCoarse * (4 + 4 + 8);
   return (size_t)kCoarseSlots * NL * 8 * 2 + kCoarseSlots * (1 + 1 + 2) + kCoarse * (4 + 4 + 8);
 }
 
@@ -761,6 +778,155 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
                                                                  CoarseView cv,
                                                                  unsigned long long* __restrict__ occ_out) {
   extern __shared__ __align__(16) unsigned char cs_smem[];
+#if SPK_COARSE_MATCH
+  {
+    uint64_t* ss = (uint64_t*)cs_smem;                            // keys sorted by bucket
+    uint32_t* ucnt = (uint32_t*)(ss + kCoarseSlots * NL);         // [window][warp][bucket]
+    unsigned long long* gbase = (unsigned long long*)(ucnt + kCoarseW * kCoarseWarps * kCoarse);
+    uint32_t* hist = (uint32_t*)(gbase + kCoarse);
+    uint32_t* start = hist + kCoarse;
+    uint8_t* sb = (uint8_t*)(start + kCoarse);                    // bucket of a sorted position
+    constexpr uint32_t kUnits = kCoarseW * kCoarseWarps;
+    const unsigned topsh = 2 * k - 2 - 64 * (NL - 1);
+    const uint64_t topmask =
+        (2 * k - 64 * (NL - 1)) >= 64 ? ~0ULL : ((1ULL << (2 * k - 64 * (NL - 1))) - 1);
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t fshift = pv.log2parts - kCoarseBits;  // span index -> bucket
+    uint64_t occ = 0;
+    const uint64_t ntiles = (R.n_reads + blockDim.x - 1) / blockDim.x;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      const uint64_t r = tile * blockDim.x + threadIdx.x;
+      uint32_t np = 0;
+      uint64_t bit0 = 0;
+      if (r < R.n_reads) {
+        const uint32_t len = __ldg(R.lengths + r);
+        const uint64_t off = __ldg(R.offsets + r);
+        if (off + ((uint64_t)len + 3) / 4 > R.data_len) {  // src/packed_reads.rs:600-602
+          atomicOr(R.err, 4);
+        } else if (len >= k) {
+          np = len - k + 1;
+          bit0 = 8ull * (R.byte_base + off);
+        }
+      }
+      Seq<NL> V, Rc;
+      if (np) {
+        V = extract<NL>(R.words, bit0, k);
+        Rc = revcomp<NL>(V, k);
+      }
+      uint64_t buf = 0, nextbit = bit0 + 2ull * k;
+      unsigned bleft = 0;
+      uint32_t i = 0;
+      while (__syncthreads_or(i < np)) {
+        // ---- roll up to kCoarseW windows, rank each among its warp ----
+        for (uint32_t u = threadIdx.x; u < kUnits * kCoarse; u += blockDim.x) ucnt[u] = 0;
+        __syncthreads();
+        Seq<NL> C[kCoarseW];
+        uint32_t br[kCoarseW];  // bucket << 8 | rank among the warp's keys of that bucket
+#pragma unroll
+        for (int w = 0; w < kCoarseW; w++) {
+          uint32_t b = 0xFFu;
+          if (i < np) {
+            if (i > 0) {
+              if (bleft == 0) {
+                buf = extract<1>(R.words, nextbit, 32).v[0];
+                bleft = 32;
+              }
+              const uint64_t bb = buf >> 62;
+              buf <<= 2;
+              bleft--;
+              nextbit += 2;
+              if (NL == 1) {
+                V.v[0] = ((V.v[0] << 2) | bb) & topmask;
+                Rc.v[0] = (Rc.v[0] >> 2) | ((3 - bb) << topsh);
+              } else {
+                V.v[NL - 1] = ((V.v[NL - 1] << 2) | (V.v[0] >> 62)) & topmask;
+                V.v[0] = (V.v[0] << 2) | bb;
+                Rc.v[0] = (Rc.v[0] >> 2) | (Rc.v[NL - 1] << 62);
+                Rc.v[NL - 1] = (Rc.v[NL - 1] >> 2) | ((3 - bb) << topsh);
+              }
+            }
+            C[w] = seq_le<NL>(V, Rc) ? V : Rc;  // canonical, src/dna.rs:185-192
+            i++;
+            occ++;
+            uint64_t w4[4];
+            kmer256_limbs<NL>(C[w], k, w4);
+            const uint64_t raw0 = hash_seed(hash_pre(w4), kSeed1);
+            const uint32_t p = (uint32_t)(raw0 >> (64 - pv.log2parts));  // log2parts > kCoarseBits
+            if (pv.packed_home)
+              C[w].v[NL - 1] |= (raw0 << pv.log2parts) >> (64 - kHomeBits) << (64 - kHomeBits);
+            b = p >> fshift;
+          }
+          br[w] = b << 8;
+          const unsigned act = __ballot_sync(FULL, b != 0xFFu);
+          if (b != 0xFFu) {
+            const unsigned peers = __match_any_sync(act, b);
+            br[w] |= __popc(peers & lanemask_lt());
+            if (lane == (unsigned)(__ffs(peers) - 1)) ucnt[(w * kCoarseWarps + warp) * kCoarse + b] = __popc(peers);
+          }
+        }
+        __syncthreads();
+        // ---- per bucket: exclusive scan over the (window, warp) units ----
+        if (threadIdx.x < kCoarse) {
+          const uint32_t b = threadIdx.x;
+          uint32_t run = 0;
+          for (uint32_t u = 0; u < kUnits; u++) {
+            const uint32_t c = ucnt[u * kCoarse + b];
+            ucnt[u * kCoarse + b] = run;
+            run += c;
+          }
+          hist[b] = run;
+        }
+        __syncthreads();
+        // ---- bucket starts in the tile, and one reservation per bucket ----
+        if (threadIdx.x < 32) {
+          const uint32_t h0 = hist[2 * lane], h1 = hist[2 * lane + 1];
+          uint32_t x = h0 + h1;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if ((int)lane >= d) x += y;
+          }
+          const uint32_t ex = x - h0 - h1;
+          start[2 * lane] = ex;
+          start[2 * lane + 1] = ex + h0;
+          gbase[2 * lane] =
+              h0 ? coarse_base(cv, 2 * lane) + atomicAdd(cv.fill + (uint64_t)(2 * lane) * kFillStride, h0) : 0;
+          gbase[2 * lane + 1] =
+              h1 ? coarse_base(cv, 2 * lane + 1) + atomicAdd(cv.fill + (uint64_t)(2 * lane + 1) * kFillStride, h1)
+                 : 0;
+        }
+        __syncthreads();
+        // ---- keys straight from registers to their sorted places ----
+#pragma unroll
+        for (int w = 0; w < kCoarseW; w++) {
+          const uint32_t b = br[w] >> 8;
+          if (b == 0xFFu) continue;
+          const uint32_t pos = start[b] + ucnt[(w * kCoarseWarps + warp) * kCoarse + b] + (br[w] & 0xFFu);
+          if (NL == 1) ss[pos] = C[w].v[0];
+          else ((ulonglong2*)ss)[pos] = make_ulonglong2(C[w].v[0], C[w].v[NL - 1]);
+          sb[pos] = (uint8_t)b;
+        }
+        __syncthreads();
+        // ---- contiguous runs out ----
+        const uint32_t total = start[kCoarse - 1] + hist[kCoarse - 1];
+        for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
+          const uint32_t b = sb[j];
+          const uint64_t gi = gbase[b] + (j - start[b]);
+          const uint64_t end = cv.uniform ? (uint64_t)(b + 1) * cv.uniform : cv.base[b + 1];
+          if (gi < end) {
+            if (NL == 1) cv.keys[gi] = ss[j];
+            else *(ulonglong2*)(cv.keys + 2 * gi) = ((const ulonglong2*)ss)[j];
+          } else {
+            atomicOr(cv.err, (int)kErrRegion);
+          }
+        }
+        __syncthreads();
+      }
+    }
+    warp_add_u64(occ_out, occ);
+    return;
+  }
+#endif
   uint64_t* ks = (uint64_t*)cs_smem;                       // keys by slot
   uint64_t* ss = ks + kCoarseSlots * NL;                   // keys sorted by bucket
   unsigned long long* gbase = (unsigned long long*)(ss + kCoarseSlots * NL);
@@ -958,6 +1124,24 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
           C[q].v[NL - 1] = v.y;
         }
       }
+#if SPK_FINE_PREFETCH
+      {
+        // this CTA's next chunk, on its way to L2 while this one is sorted
+        const uint32_t cn = c + gridDim.x;
+        if (cn < nchunks) {
+          uint32_t bn = 0;
+          for (uint32_t step = kCoarse >> 1; step; step >>= 1)
+            if (cfirst[bn + step] <= cn) bn += step;
+          const uint64_t s0n = coarse_base(cv, bn) + (uint64_t)(cn - cfirst[bn]) * kFineChunk;
+          const uint64_t endn = coarse_base(cv, bn) + coarse_len(cv, bn);
+#pragma unroll
+          for (int q = 0; q < PER; q++) {
+            const uint64_t jn = s0n + threadIdx.x + q * kFineBlock;
+            if (jn < endn) asm volatile("prefetch.global.L2 [%0];" ::"l"(cv.keys + (uint64_t)NL * jn));
+          }
+        }
+      }
+#endif
 #pragma unroll
       for (int q = 0; q < PER; q++) {
         const uint32_t j = threadIdx.x + q * kFineBlock;
