@@ -887,19 +887,29 @@ def main():
     # roofline of the dominant kernel (largest share of the step)
     f_adm = info["admitted_occurrences"] / max(info["occurrences"], 1)
     sb = stream_bytes_per_occ()
+    kernel_rates = None
     if info["schedule"] == 3:
-        # Partitioned: the dominant of its three kernels, each with its own
-        # algorithmic bytes.
+        # Partitioned: the dominant of its kernels, each with its own
+        # algorithmic bytes (what the kernel must read and write).
         scatter_ms = sum(i["ms_scatter_kernel"] for i in infos) / len(infos)
         ops = 3 * info["n_distinct"]
         n_ge2 = info["n_table"] - info["n_singletons"]  # k-mers counted at least twice
         # the read pass that leaves every key in its span's region: one kernel,
         # or two (coarse buckets, then spans) timed together
         sname = "k_part_coarse+k_part_fine" if info.get("part_passes") == 2 else "k_part_scatter"
-        cands = [
+        coarse_ms = sum(i.get("ms_coarse_kernel", 0.0) for i in infos) / len(infos)
+        cands = []
+        if coarse_ms > 0 and info.get("part_passes") == 2:
+            # the two partition passes on their own: the coarse pass reads the
+            # read stream and writes one key per occurrence; the fine pass
+            # reads every key back and writes it to its span
+            cands += [("k_part_coarse", coarse_ms, occ * (sb + 16)),
+                      ("k_part_fine", scatter_ms - coarse_ms, occ * 32)]
+        else:
             # read stream and one streamed key write per occurrence (the
             # algorithm's need; the two-level form moves the keys twice more)
-            (sname, scatter_ms, occ * (sb + 16)),
+            cands += [(sname, scatter_ms, occ * (sb + 16))]
+        cands += [
             # keys read back; out: the k-mers counted twice or more as list
             # entries (key + count), the singleton keys, and three 4-byte Bloom
             # operations per distinct k-mer (the table itself is not written)
@@ -909,6 +919,10 @@ def main():
             ("k_bloom_apply", bloom_ms, ops * 4 + 2 * info["bloom_size_bits"] / 8),
         ]
         kname, kms, kbytes = max(cands, key=lambda c: c[1])
+        # every partitioned kernel's algorithmic rate, beside the dominant one
+        kernel_rates = {n: {"ms": round(t, 3), "algorithmic_bytes": int(b),
+                            "achieved_gbs": round(b / (t / 1e3) / 1e9, 1) if t > 0 else None}
+                        for n, t, b in cands}
     elif info["schedule"] == 2 and count_ms >= bloom_ms:
         # Count-first: the read stream and a read-modify-write of the table
         # slot's sector (read + write back) per occurrence.
@@ -955,7 +969,7 @@ def main():
                 "traffic_achieved": (traffic / (kms / 1e3) / 1e9) if traffic else None,
                 "traffic_frac": (traffic / (kms / 1e3) / 1e9 / peak) if traffic else None,
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": kbytes,
-                "kernel_ms": kms, "kernel_share": kms / ms,
+                "kernel_ms": kms, "kernel_share": kms / ms, "kernels": kernel_rates,
                 "job": {"bytes_per_occurrence": job_bytes_per_occ,
                         "achieved": value * job_bytes_per_occ / world,
                         "frac": value * job_bytes_per_occ / world / peak},

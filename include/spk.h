@@ -242,6 +242,10 @@ typedef struct spk_count_opts {
   const uint64_t* prior_offsets;
   const uint32_t* prior_lengths;
   uint64_t n_prior;
+  uint32_t span_groups_log2;  /* default job: count in at least 2^span_groups_log2 groups of spans
+                                 (one pass over the reads each); 0 = as many as the device
+                                 memory needs (usually one) */
+  uint32_t reserved;
 } spk_count_opts;
 
 void spk_count_opts_default(spk_count_opts* opts);
@@ -296,6 +300,10 @@ typedef struct spk_result_info {
   uint32_t part_passes;          /* partitioned: 1 = the keys went to their spans in one pass,
                                     2 = through coarse buckets first (ms_scatter_kernel covers
                                     both passes) */
+  uint32_t span_groups;          /* partitioned: passes over the reads, each partitioning and
+                                    counting one group of spans (read sets too large for one) */
+  float ms_coarse_kernel;        /* two-level partition in one group: the coarse pass alone
+                                    (ms_scatter_kernel - ms_coarse_kernel is the fine pass) */
 } spk_result_info;
 
 int spk_result_count(const spk_result* res, int* n_k);

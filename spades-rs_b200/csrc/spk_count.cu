@@ -630,6 +630,10 @@ struct PartView {
   uint32_t packed_home;      // 1: entries carry their home slot in the span in the top
                              // kHomeBits bits of their top limb (keys leave them zero)
   int* err;                  // bit 3: some region overflowed
+  uint32_t log2groups;       // > 0: the spans come in 2^log2groups groups counted one after
+                             // another; a pass keeps the keys of group `group` only, and its
+                             // regions, buckets and span indices are the group's
+  uint32_t group;
 };
 constexpr uint32_t kHomeBits = 13;  // >= log2 of the largest span
 // Whether keys of k (NL limbs) leave the top kHomeBits bits of their top limb free.
@@ -751,25 +755,8 @@ __device__ __forceinline__ uint64_t region_base(const PartView& pv, uint32_t p) 
   return pv.uniform ? (uint64_t)p * pv.uniform : pv.base[p];
 }
 
-// Ranking inside a tile.  SPK_COARSE_MATCH 1: every warp ranks its keys of
-// a window among themselves (__match_any_sync on the bucket) and records per
-// (window, warp) bucket counts; a scan over those gives each key its place in
-// the bucket-sorted tile, so keys stay in registers and go to shared memory
-// once.  0: one shared-memory atomic per key on the tile's bucket counters.
-#ifndef SPK_COARSE_MATCH
-#define SPK_COARSE_MATCH 1
-#endif
-constexpr int kCoarseWarps = kCoarseBlock / 32;
-// The fine pass prefetches its next chunk's keys into L2.
-#ifndef SPK_FINE_PREFETCH
-#define SPK_FINE_PREFETCH 1
-#endif
-
 template <int NL>
 size_t coarse_smem() {
-  if (SPK_COARSE_MATCH)
-    return (size_t)kCoarseSlots * NL * 8 + kCoarseSlots + (size_t)kCoarseW * kCoarseWarps * kCoarse * 4 +
-           kCoarse * (4 + 4 + 8);
   return (size_t)kCoarseSlots * NL * 8 * 2 + kCoarseSlots * (1 + 1 + 2) + kCoarse * (4 + 4 + 8);
 }
 
@@ -778,155 +765,6 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
                                                                  CoarseView cv,
                                                                  unsigned long long* __restrict__ occ_out) {
   extern __shared__ __align__(16) unsigned char cs_smem[];
-#if SPK_COARSE_MATCH
-  {
-    uint64_t* ss = (uint64_t*)cs_smem;                            // keys sorted by bucket
-    uint32_t* ucnt = (uint32_t*)(ss + kCoarseSlots * NL);         // [window][warp][bucket]
-    unsigned long long* gbase = (unsigned long long*)(ucnt + kCoarseW * kCoarseWarps * kCoarse);
-    uint32_t* hist = (uint32_t*)(gbase + kCoarse);
-    uint32_t* start = hist + kCoarse;
-    uint8_t* sb = (uint8_t*)(start + kCoarse);                    // bucket of a sorted position
-    constexpr uint32_t kUnits = kCoarseW * kCoarseWarps;
-    const unsigned topsh = 2 * k - 2 - 64 * (NL - 1);
-    const uint64_t topmask =
-        (2 * k - 64 * (NL - 1)) >= 64 ? ~0ULL : ((1ULL << (2 * k - 64 * (NL - 1))) - 1);
-    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t fshift = pv.log2parts - kCoarseBits;  // span index -> bucket
-    uint64_t occ = 0;
-    const uint64_t ntiles = (R.n_reads + blockDim.x - 1) / blockDim.x;
-    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-      const uint64_t r = tile * blockDim.x + threadIdx.x;
-      uint32_t np = 0;
-      uint64_t bit0 = 0;
-      if (r < R.n_reads) {
-        const uint32_t len = __ldg(R.lengths + r);
-        const uint64_t off = __ldg(R.offsets + r);
-        if (off + ((uint64_t)len + 3) / 4 > R.data_len) {  // src/packed_reads.rs:600-602
-          atomicOr(R.err, 4);
-        } else if (len >= k) {
-          np = len - k + 1;
-          bit0 = 8ull * (R.byte_base + off);
-        }
-      }
-      Seq<NL> V, Rc;
-      if (np) {
-        V = extract<NL>(R.words, bit0, k);
-        Rc = revcomp<NL>(V, k);
-      }
-      uint64_t buf = 0, nextbit = bit0 + 2ull * k;
-      unsigned bleft = 0;
-      uint32_t i = 0;
-      while (__syncthreads_or(i < np)) {
-        // ---- roll up to kCoarseW windows, rank each among its warp ----
-        for (uint32_t u = threadIdx.x; u < kUnits * kCoarse; u += blockDim.x) ucnt[u] = 0;
-        __syncthreads();
-        Seq<NL> C[kCoarseW];
-        uint32_t br[kCoarseW];  // bucket << 8 | rank among the warp's keys of that bucket
-#pragma unroll
-        for (int w = 0; w < kCoarseW; w++) {
-          uint32_t b = 0xFFu;
-          if (i < np) {
-            if (i > 0) {
-              if (bleft == 0) {
-                buf = extract<1>(R.words, nextbit, 32).v[0];
-                bleft = 32;
-              }
-              const uint64_t bb = buf >> 62;
-              buf <<= 2;
-              bleft--;
-              nextbit += 2;
-              if (NL == 1) {
-                V.v[0] = ((V.v[0] << 2) | bb) & topmask;
-                Rc.v[0] = (Rc.v[0] >> 2) | ((3 - bb) << topsh);
-              } else {
-                V.v[NL - 1] = ((V.v[NL - 1] << 2) | (V.v[0] >> 62)) & topmask;
-                V.v[0] = (V.v[0] << 2) | bb;
-                Rc.v[0] = (Rc.v[0] >> 2) | (Rc.v[NL - 1] << 62);
-                Rc.v[NL - 1] = (Rc.v[NL - 1] >> 2) | ((3 - bb) << topsh);
-              }
-            }
-            C[w] = seq_le<NL>(V, Rc) ? V : Rc;  // canonical, src/dna.rs:185-192
-            i++;
-            occ++;
-            uint64_t w4[4];
-            kmer256_limbs<NL>(C[w], k, w4);
-            const uint64_t raw0 = hash_seed(hash_pre(w4), kSeed1);
-            const uint32_t p = (uint32_t)(raw0 >> (64 - pv.log2parts));  // log2parts > kCoarseBits
-            if (pv.packed_home)
-              C[w].v[NL - 1] |= (raw0 << pv.log2parts) >> (64 - kHomeBits) << (64 - kHomeBits);
-            b = p >> fshift;
-          }
-          br[w] = b << 8;
-          const unsigned act = __ballot_sync(FULL, b != 0xFFu);
-          if (b != 0xFFu) {
-            const unsigned peers = __match_any_sync(act, b);
-            br[w] |= __popc(peers & lanemask_lt());
-            if (lane == (unsigned)(__ffs(peers) - 1)) ucnt[(w * kCoarseWarps + warp) * kCoarse + b] = __popc(peers);
-          }
-        }
-        __syncthreads();
-        // ---- per bucket: exclusive scan over the (window, warp) units ----
-        if (threadIdx.x < kCoarse) {
-          const uint32_t b = threadIdx.x;
-          uint32_t run = 0;
-          for (uint32_t u = 0; u < kUnits; u++) {
-            const uint32_t c = ucnt[u * kCoarse + b];
-            ucnt[u * kCoarse + b] = run;
-            run += c;
-          }
-          hist[b] = run;
-        }
-        __syncthreads();
-        // ---- bucket starts in the tile, and one reservation per bucket ----
-        if (threadIdx.x < 32) {
-          const uint32_t h0 = hist[2 * lane], h1 = hist[2 * lane + 1];
-          uint32_t x = h0 + h1;
-#pragma unroll
-          for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-            if ((int)lane >= d) x += y;
-          }
-          const uint32_t ex = x - h0 - h1;
-          start[2 * lane] = ex;
-          start[2 * lane + 1] = ex + h0;
-          gbase[2 * lane] =
-              h0 ? coarse_base(cv, 2 * lane) + atomicAdd(cv.fill + (uint64_t)(2 * lane) * kFillStride, h0) : 0;
-          gbase[2 * lane + 1] =
-              h1 ? coarse_base(cv, 2 * lane + 1) + atomicAdd(cv.fill + (uint64_t)(2 * lane + 1) * kFillStride, h1)
-                 : 0;
-        }
-        __syncthreads();
-        // ---- keys straight from registers to their sorted places ----
-#pragma unroll
-        for (int w = 0; w < kCoarseW; w++) {
-          const uint32_t b = br[w] >> 8;
-          if (b == 0xFFu) continue;
-          const uint32_t pos = start[b] + ucnt[(w * kCoarseWarps + warp) * kCoarse + b] + (br[w] & 0xFFu);
-          if (NL == 1) ss[pos] = C[w].v[0];
-          else ((ulonglong2*)ss)[pos] = make_ulonglong2(C[w].v[0], C[w].v[NL - 1]);
-          sb[pos] = (uint8_t)b;
-        }
-        __syncthreads();
-        // ---- contiguous runs out ----
-        const uint32_t total = start[kCoarse - 1] + hist[kCoarse - 1];
-        for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
-          const uint32_t b = sb[j];
-          const uint64_t gi = gbase[b] + (j - start[b]);
-          const uint64_t end = cv.uniform ? (uint64_t)(b + 1) * cv.uniform : cv.base[b + 1];
-          if (gi < end) {
-            if (NL == 1) cv.keys[gi] = ss[j];
-            else *(ulonglong2*)(cv.keys + 2 * gi) = ((const ulonglong2*)ss)[j];
-          } else {
-            atomicOr(cv.err, (int)kErrRegion);
-          }
-        }
-        __syncthreads();
-      }
-    }
-    warp_add_u64(occ_out, occ);
-    return;
-  }
-#endif
   uint64_t* ks = (uint64_t*)cs_smem;                       // keys by slot
   uint64_t* ss = ks + kCoarseSlots * NL;                   // keys sorted by bucket
   unsigned long long* gbase = (unsigned long long*)(ss + kCoarseSlots * NL);
@@ -938,7 +776,8 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
   const unsigned topsh = 2 * k - 2 - 64 * (NL - 1);
   const uint64_t topmask = (2 * k - 64 * (NL - 1)) >= 64 ? ~0ULL : ((1ULL << (2 * k - 64 * (NL - 1))) - 1);
   const unsigned lane = threadIdx.x & 31;
-  const uint32_t fshift = pv.log2parts - kCoarseBits;      // span index -> bucket
+  const uint32_t lp = pv.log2parts - pv.log2groups;        // span index bits within a group
+  const uint32_t fshift = lp - kCoarseBits;                // group's span index -> bucket
   if (threadIdx.x < kCoarse) hist[threadIdx.x] = 0;
   uint64_t occ = 0;
   const uint64_t ntiles = (R.n_reads + blockDim.x - 1) / blockDim.x;
@@ -992,17 +831,19 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
           }
           Seq<NL> C = seq_le<NL>(V, Rc) ? V : Rc;  // canonical, src/dna.rs:185-192
           i++;
-          occ++;
+          occ += pv.group == 0;  // every occurrence once over the groups' passes
           uint64_t w4[4];
           kmer256_limbs<NL>(C, k, w4);
           const uint64_t raw0 = hash_seed(hash_pre(w4), kSeed1);
           const uint32_t p = (uint32_t)(raw0 >> (64 - pv.log2parts));  // log2parts > kCoarseBits
           if (pv.packed_home)
             C.v[NL - 1] |= (raw0 << pv.log2parts) >> (64 - kHomeBits) << (64 - kHomeBits);
-          b = (uint8_t)(p >> fshift);
-          if (NL == 1) ks[slot] = C.v[0];
-          else ((ulonglong2*)ks)[slot] = make_ulonglong2(C.v[0], C.v[NL - 1]);
-          rk[slot] = (uint16_t)atomicAdd(&hist[b], 1u);
+          if ((p >> lp) == pv.group) {  // else another pass's
+            b = (uint8_t)((p & ((1u << lp) - 1)) >> fshift);
+            if (NL == 1) ks[slot] = C.v[0];
+            else ((ulonglong2*)ks)[slot] = make_ulonglong2(C.v[0], C.v[NL - 1]);
+            rk[slot] = (uint16_t)atomicAdd(&hist[b], 1u);
+          }
         }
         bk[slot] = b;
       }
@@ -1086,7 +927,7 @@ template <int NL>
 __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, const uint32_t* __restrict__ cfirst,
                                                              PartView pv, unsigned k) {
   extern __shared__ __align__(16) unsigned char fs_smem[];
-  const uint32_t fbits = pv.log2parts - kCoarseBits, nfine = 1u << fbits;
+  const uint32_t fbits = pv.log2parts - pv.log2groups - kCoarseBits, nfine = 1u << fbits;
   uint64_t* ks = (uint64_t*)fs_smem;
   uint64_t* ss = ks + kFineChunk * NL;
   unsigned long long* gbase = (unsigned long long*)(ss + kFineChunk * NL);
@@ -1124,24 +965,6 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
           C[q].v[NL - 1] = v.y;
         }
       }
-#if SPK_FINE_PREFETCH
-      {
-        // this CTA's next chunk, on its way to L2 while this one is sorted
-        const uint32_t cn = c + gridDim.x;
-        if (cn < nchunks) {
-          uint32_t bn = 0;
-          for (uint32_t step = kCoarse >> 1; step; step >>= 1)
-            if (cfirst[bn + step] <= cn) bn += step;
-          const uint64_t s0n = coarse_base(cv, bn) + (uint64_t)(cn - cfirst[bn]) * kFineChunk;
-          const uint64_t endn = coarse_base(cv, bn) + coarse_len(cv, bn);
-#pragma unroll
-          for (int q = 0; q < PER; q++) {
-            const uint64_t jn = s0n + threadIdx.x + q * kFineBlock;
-            if (jn < endn) asm volatile("prefetch.global.L2 [%0];" ::"l"(cv.keys + (uint64_t)NL * jn));
-          }
-        }
-      }
-#endif
 #pragma unroll
       for (int q = 0; q < PER; q++) {
         const uint32_t j = threadIdx.x + q * kFineBlock;
@@ -1406,7 +1229,8 @@ struct ListOut {
   uint32_t* cnt;                // list: counts (nullptr: the table is written instead)
   uint64_t* s0;                 // singletons: limb 0
   uint64_t* s1;                 // singletons: limb 1
-  uint64_t cap;
+  uint64_t cap;                 // list entries
+  uint64_t scap;                // singleton keys
   uint32_t lmin;                // smallest count listed (>= 2 here; singletons are listed
                                 // by admission when lmin is 1)
   unsigned long long* fill;     // [0] list entries, [1] singletons
@@ -1442,7 +1266,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
   uint32_t* rcur = rhist + ((rv.nranges + 1) & ~1u);
   unsigned long long* rbase =
       (unsigned long long*)(rcur + ((NL == 2 && kSortedOps) ? ((rv.nranges + 1) & ~1u) : 0u));
-  const uint32_t nparts = 1u << pv.log2parts;
+  const uint32_t nparts = 1u << (pv.log2parts - pv.log2groups);  // this group's spans
   for (uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
     for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
       if (NL == 1) ((unsigned long long*)keys)[s] = kEmpty;
@@ -1503,7 +1327,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
     }
     if (full) atomicOr(t.err, 1);  // span full: the host regrows the table
     __syncthreads();
-    const uint64_t g0 = (uint64_t)p << t.log2span;
+    const uint64_t g0 = ((uint64_t)pv.group << (pv.log2parts - pv.log2groups) | p) << t.log2span;
     if (OPS && to_list) {
       // Entries of each (round, warp) of the write-out loop below: a ballot
       // per round, then one reservation per span for the list and one for
@@ -1582,7 +1406,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
             }
           } else if (c == 1) {
             const uint64_t q = lbase[1] + lw[1][r * kWarps + warp] + __popc(bs & lanemask_lt());
-            if (q < lo.cap) {
+            if (q < lo.scap) {
               lo.s0[q] = C.v[0];
               if (NL == 2) lo.s1[q] = C.v[NL - 1];
             }
@@ -1982,7 +1806,7 @@ __global__ void __launch_bounds__(kBlock) k_admit_singletons(ListOut lo, unsigne
                                                               const uint64_t* __restrict__ twice,
                                                               unsigned long long* __restrict__ sums) {
   const unsigned lane = threadIdx.x & 31;
-  const uint64_t n = min((uint64_t)lo.fill[1], lo.cap);
+  const uint64_t n = min((uint64_t)lo.fill[1], lo.scap);
   uint64_t adm = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += stride) {
@@ -2411,7 +2235,7 @@ static int launch_part_coarse(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv
 template <int NL>
 static int launch_part_fine(spk_ctx* ctx, cudaStream_t st, const CoarseView& cv, const uint32_t* cfirst,
                             const PartView& pv, unsigned k) {
-  const size_t smem = fine_smem<NL>(1u << (pv.log2parts - kCoarseBits));
+  const size_t smem = fine_smem<NL>(1u << (pv.log2parts - pv.log2groups - kCoarseBits));
   int rc;
   if ((rc = raise_smem_limit((const void*)k_part_fine<NL>, smem))) return rc;
   k_part_fine<NL><<<grid_for(ctx, 2), kFineBlock, smem, st>>>(cv, cfirst, pv, k);
@@ -2424,7 +2248,7 @@ static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, 
                              unsigned k, const FastMod& fm, U128* tiers, const RangeView& rv,
                              const ListOut& lo) {
   size_t smem = ((size_t)1 << t.log2span) * (sizeof(typename SpanKey<NL>::T) + 4);
-  const uint64_t nparts = 1ULL << pv.log2parts;
+  const uint64_t nparts = 1ULL << (pv.log2parts - pv.log2groups);
   const int grid = (int)std::min<uint64_t>(nparts, (uint64_t)ctx->sm_count * kPartCtasPerSm);
   if (rv.ops) {
     smem += ((rv.nranges + 1) & ~1u) * 4 + (size_t)rv.nranges * 8;
@@ -2741,7 +2565,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
         SPK_CUDA(cudaMemsetAsync(sw + S_HIST, 0, kHistBins * 8, st));
         lo = ListOut{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
                      kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(),
-                     nl == 2 ? sgl[1].as<uint64_t>() : nullptr, cap, lmin_pre, su + S_LFILL,
+                     nl == 2 ? sgl[1].as<uint64_t>() : nullptr, cap, cap, lmin_pre, su + S_LFILL,
                      su + S_HIST, su + S_OCC2};
       }
       TableView& t = kr.table;
@@ -3234,6 +3058,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
 // handles them), kRedo after an overflow, else the status.
 // ---------------------------------------------------------------------------
 constexpr int kNotThisPath = -100, kRedo = -101;
+constexpr uint32_t kMaxLog2Groups = 4;  // at most 16 passes over the reads
 
 // A second stream of one job, joined back to the job's stream by events.
 struct SideStream {
@@ -3273,7 +3098,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   SPK_CUDA(cudaMemsetAsync(sw, 0, (S_WORDS + 1) * 8, st));
   unsigned long long* su = (unsigned long long*)sw;
   // ---- the first readback: occurrences, which size the table ----
-  Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1;
+  Ev e0, e1, e2, e3, e4, e5, e6, kb0, kb1, kc0, kc1, ks0, ks1, ksm;
   SPK_CUDA(cudaEventRecord(e0.e, st));
   k_occ<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv_in.lengths, rv_in.n_reads, k, su + S_OCC0);
   SPK_CUDA(cudaGetLastError());
@@ -3292,8 +3117,21 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   while ((1ULL << log2cap) < cap) log2cap++;
   if (log2cap <= log2span) return kNotThisPath;
   const uint32_t log2parts = log2cap - log2span;
-  if (!SPK_TWO_LEVEL || log2parts <= kCoarseBits || log2parts - kCoarseBits > kFineMaxBits) return kNotThisPath;
-  if ((occ0 * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4) return kNotThisPath;
+  // Span groups: a read set whose partition buffers (span regions and coarse
+  // buckets, 2.6 keys per occurrence) would pass a quarter of the device is
+  // partitioned and counted in 2^lg passes, each keeping the keys of one group
+  // of spans (the reads are streamed once per pass).
+  uint32_t lg = std::min<uint32_t>(o.span_groups_log2, kMaxLog2Groups);
+  while (lg < kMaxLog2Groups && ((occ0 >> lg) * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4) lg++;
+  if (((occ0 >> lg) * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4) return kNotThisPath;
+  while (lg > 0 && log2parts - lg <= kCoarseBits) lg--;
+  if (!SPK_TWO_LEVEL || log2parts - lg <= kCoarseBits || log2parts - lg - kCoarseBits > kFineMaxBits ||
+      ((occ0 >> lg) * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4)
+    return kNotThisPath;
+  // One pass: the list and the singleton keys hold up to one entry per table
+  // slot each, so they cannot overflow.  Several: an eighth and a half of the
+  // slots (the mid-job readback sends the job back if either overflowed).
+  const uint64_t lcap_ = lg ? cap >> 3 : cap, scap_ = lg ? cap >> 1 : cap;
 
   kr.k = k;
   kr.nl = nl;
@@ -3320,31 +3158,56 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   TableView& t = kr.table;
   t.err = errp;
   const uint64_t nparts = 1ULL << log2parts;
+  const uint64_t nparts_g = nparts >> lg;  // spans of one group
 
-  // ---- two-level read partition (k_part_coarse, k_part_fine) ----
+  // Buffers of the span count, filled over every group's pass.
+  const bool early_sort = lmin_pre >= 2;
+  SideStream side;
+  if (early_sort && (rc = side.open())) return rc;
+  DevSort lsort, esort;  // after `side`: its buffers are freed on that stream first
+  DevBuf rbase, rfill, ops, sgl[2];
+  const uint64_t share = 3 * (lcap_ + scap_) / 2 / nranges + 1;
+  const uint64_t rcap = share + (share >> 2) + 1024;
+  if ((rc = rbase.alloc((nranges + 1) * 8, st)) || (rc = rfill.alloc(nranges * 4 * kFillStride, st)) ||
+      (rc = ops.alloc(nranges * rcap * 4, st)))
+    return rc;
+  SPK_CUDA(cudaMemsetAsync(rfill.p, 0, nranges * 4 * kFillStride, st));
+  RangeView bv{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), rcap, (uint32_t)nranges,
+               errp};
+  for (int j = 0; j < nl; j++)
+    if ((rc = kr.list[j].alloc(lcap_ * 8, st)) || (rc = sgl[j].alloc(scap_ * 8, st))) return rc;
+  if ((rc = kr.list[4].alloc(lcap_ * 4, st))) return rc;
+  ListOut lo{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
+             kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(), nl == 2 ? sgl[1].as<uint64_t>() : nullptr,
+             lcap_, scap_, lmin_pre, su + S_LFILL, su + S_HIST, su + S_OCC2};
+
+  // ---- two-level read partition (k_part_coarse, k_part_fine) and span
+  // count, once per group of spans ----
   DevBuf base, fill, region;
   const uint64_t per = occ0 / nparts;
   const uint64_t capu = per + (per >> 1) + 256;
-  if ((rc = base.alloc((nparts + 1) * 8, st)) || (rc = fill.alloc(nparts * 4 * kFillStride, st)) ||
-      (rc = region.alloc(nparts * capu * nl * 8, st)))
+  if ((rc = base.alloc((nparts_g + 1) * 8, st)) || (rc = fill.alloc(nparts_g * 4 * kFillStride, st)) ||
+      (rc = region.alloc(nparts_g * capu * nl * 8, st)))
     return rc;
-  k_part_uniform<<<64, kBlock, 0, st>>>((uint32_t)nparts, capu, base.as<uint64_t>());
-  SPK_CUDA(cudaMemsetAsync(fill.p, 0, nparts * 4 * kFillStride, st));
-  PartView pv{region.as<uint64_t>(), base.as<uint64_t>(), fill.as<unsigned int>(), capu, log2parts,
-              home_fits(k, nl) ? 1u : 0u, errp};
+  k_part_uniform<<<64, kBlock, 0, st>>>((uint32_t)nparts_g, capu, base.as<uint64_t>());
+  DevBuf cbase, cfill, cregion, cfirst;
+  const uint64_t cper = (occ0 >> lg) / kCoarse;
+  const uint64_t ccap = cper + (cper >> 3) + 8192;
+  if ((rc = cbase.alloc((kCoarse + 1) * 8, st)) || (rc = cfill.alloc(kCoarse * 4 * kFillStride, st)) ||
+      (rc = cregion.alloc(kCoarse * ccap * nl * 8, st)) || (rc = cfirst.alloc((kCoarse + 1) * 4, st)))
+    return rc;
+  k_part_uniform<<<1, 128, 0, st>>>(kCoarse, ccap, cbase.as<uint64_t>());
   info.part_passes = 2;
+  info.span_groups = 1u << lg;
   SPK_CUDA(cudaEventRecord(ks0.e, st));
+  for (uint32_t g = 0; g < (1u << lg); g++) {
+  SPK_CUDA(cudaMemsetAsync(fill.p, 0, nparts_g * 4 * kFillStride, st));
+  PartView pv{region.as<uint64_t>(), base.as<uint64_t>(), fill.as<unsigned int>(), capu, log2parts,
+              home_fits(k, nl) ? 1u : 0u, errp, lg, g};
   {
-    DevBuf cbase, cfill, cregion, cfirst;
-    const uint64_t cper = occ0 / kCoarse;
-    const uint64_t ccap = cper + (cper >> 3) + 8192;
-    if ((rc = cbase.alloc((kCoarse + 1) * 8, st)) || (rc = cfill.alloc(kCoarse * 4 * kFillStride, st)) ||
-        (rc = cregion.alloc(kCoarse * ccap * nl * 8, st)) || (rc = cfirst.alloc((kCoarse + 1) * 4, st)))
-      return rc;
-    k_part_uniform<<<1, 128, 0, st>>>(kCoarse, ccap, cbase.as<uint64_t>());
     SPK_CUDA(cudaMemsetAsync(cfill.p, 0, kCoarse * 4 * kFillStride, st));
     CoarseView cv{cregion.as<uint64_t>(), cbase.as<uint64_t>(), cfill.as<unsigned int>(), ccap, errp};
-    if (per_chunk) {
+    if (per_chunk && g == 0) {
       // the reads of each uploaded piece as soon as it is on the device
       uint64_t r0 = 0;
       for (int c = 0; c < rv.chunks->n; c++) {
@@ -3369,41 +3232,30 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
       else rc = launch_part_coarse<2>(ctx, st, rv, k, pv, cv, su + S_OCC);
       if (rc) return rc;
     }
+    if (lg == 0) SPK_CUDA(cudaEventRecord(ksm.e, st));
     k_coarse_chunks<<<1, 32, 0, st>>>(cv, cfirst.as<uint32_t>());
     if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
     else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
     if (rc) return rc;
     SPK_CUDA(cudaGetLastError());
-    launches += 5;  // 2 x k_part_uniform, k_part_coarse, k_coarse_chunks, k_part_fine
+    launches += 3;  // k_part_coarse, k_coarse_chunks, k_part_fine
   }
-  SPK_CUDA(cudaEventRecord(ks1.e, st));
+  if (g + 1 == (1u << lg)) SPK_CUDA(cudaEventRecord(ks1.e, st));
 
-  // ---- span count: the list, the singleton keys and the binned Bloom ops ----
-  const bool early_sort = lmin_pre >= 2;
-  SideStream side;
-  if (early_sort && (rc = side.open())) return rc;
-  DevSort lsort, esort;  // after `side`: its buffers are freed on that stream first
-  DevBuf rbase, rfill, ops, sgl[2];
+  // ---- span count of this group: the list, the singleton keys and the binned Bloom ops ----
+  if (g == 0) SPK_CUDA(cudaEventRecord(kc0.e, st));
+  if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
+  else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
+  if (rc) return rc;
+  SPK_CUDA(cudaGetLastError());
+  launches++;
+  }  // span groups
+  launches += 2;  // k_part_uniform x 2
+  cregion.release();
+  cbase.release();
+  cfill.release();
+  cfirst.release();
   {
-    const uint64_t share = 3 * cap / nranges + 1;
-    const uint64_t rcap = share + (share >> 2) + 1024;
-    if ((rc = rbase.alloc((nranges + 1) * 8, st)) || (rc = rfill.alloc(nranges * 4 * kFillStride, st)) ||
-        (rc = ops.alloc(nranges * rcap * 4, st)))
-      return rc;
-    SPK_CUDA(cudaMemsetAsync(rfill.p, 0, nranges * 4 * kFillStride, st));
-    RangeView bv{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), rcap, (uint32_t)nranges,
-                 errp};
-    for (int j = 0; j < nl; j++)
-      if ((rc = kr.list[j].alloc(cap * 8, st)) || (rc = sgl[j].alloc(cap * 8, st))) return rc;
-    if ((rc = kr.list[4].alloc(cap * 4, st))) return rc;
-    ListOut lo{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
-               kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(), nl == 2 ? sgl[1].as<uint64_t>() : nullptr,
-               cap, lmin_pre, su + S_LFILL, su + S_HIST, su + S_OCC2};
-    SPK_CUDA(cudaEventRecord(kc0.e, st));
-    if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
-    else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
-    if (rc) return rc;
-    SPK_CUDA(cudaGetLastError());
     SPK_CUDA(cudaEventRecord(kc1.e, st));
     if (early_sort) {
       // The list is final once the spans are counted (singletons are not
@@ -3411,7 +3263,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
       // the Bloom tiers, admits the singletons and finds the cutoff.
       SPK_CUDA(cudaEventRecord(side.fork, st));
       SPK_CUDA(cudaStreamWaitEvent(side.s, side.fork, 0));
-      if ((rc = sort_dev_enqueue(side.s, nl, cap, su + S_LFILL, 2 * k, kr.list, &kr.list[4], nullptr, lsort,
+      if ((rc = sort_dev_enqueue(side.s, nl, lcap_, su + S_LFILL, 2 * k, kr.list, &kr.list[4], nullptr, lsort,
                                  &launches)))
         return rc;
       SPK_CUDA(cudaEventRecord(side.join, side.s));
@@ -3430,7 +3282,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
     ops.release();
     rbase.release();
     rfill.release();
-    launches += 2;
+    launches += 1;
     SPK_CUDA(cudaEventRecord(e1.e, st));
     SPK_CUDA(cudaEventRecord(e2.e, st));
     // ---- singleton admission, histogram, cutoff ----
@@ -3469,8 +3321,10 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   info.n_distinct = n2 + host[S_LFILL + 1];
   info.admitted_occurrences = host[S_OCC2] + adm1;
   kr.list_len = host[S_LFILL];
-  if (kr.list_len > cap || host[S_LFILL + 1] > cap)
+  if (kr.list_len > lcap_ || host[S_LFILL + 1] > scap_) {
+    if (lg) return kRedo;  // a share of the slots was too small
     return fail(SPK_E_CUDA, "k-mer list larger than the table it came from");
+  }
   auto hist_from = [&](uint32_t c0) {
     uint64_t ns = 0;
     for (int c = (int)c0; c < kHistBins; c++) ns += host[S_HIST + c];
@@ -3565,6 +3419,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   info.ms_bloom_kernel = ms_between(kb0, kb1);
   info.ms_count_kernel = ms_between(kc0, kc1);
   info.ms_scatter_kernel = ms_between(ks0, ks1);
+  info.ms_coarse_kernel = lg == 0 ? ms_between(ks0, ksm) : 0.f;
   info.kernel_launches = launches;
   info.schedule = SPK_SCHEDULE_PARTITIONED;
   return SPK_OK;

@@ -243,7 +243,8 @@ class PackedReads:
 # ---------------------------------------------------------------------------
 def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: int = 2,
               min_coverage: float = 5.0, flags: Optional[int] = None,
-              table_log2: int = 0, priors: Optional[Sequence[bytes]] = None) -> CountOpts:
+              table_log2: int = 0, priors: Optional[Sequence[bytes]] = None,
+              span_groups_log2: int = 0) -> CountOpts:
     """spk_count_opts.  priors: prior/trusted contigs as ASCII byte strings
     (src/assemble.rs:244-284); the returned options keep them alive."""
     o = CountOpts()
@@ -253,6 +254,7 @@ def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: i
     o.list_min_count = list_min_count
     o.min_coverage = min_coverage
     o.table_log2 = table_log2
+    o.span_groups_log2 = span_groups_log2
     if flags is not None:
         o.flags = flags
     if priors:

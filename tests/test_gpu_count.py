@@ -507,3 +507,39 @@ def test_table_view_needs_keep_table(spk):
     for x, y in zip(a.kmers(0), b.kmers(0)):
         np.testing.assert_array_equal(x, y)
     np.testing.assert_array_equal(a.edges(0), b.edges(0))
+
+
+@pytest.mark.parametrize("k", [21, 55])
+def test_span_groups_equal_one_pass(spk, ora, k):
+    """Read sets too large for one partition pass are counted in groups of
+    spans, one pass over the reads each (forced here with span_groups_log2):
+    the whole admitted table, both tiers, cutoff and edges equal the oracle's
+    and the one-pass result."""
+    import os
+    from spk import synth
+    p = synth.c2(0.05).packed
+    bits = 1 << 26
+    tw = ora.count(p.data, p.offsets, p.lengths, k, bits, mode=ora.MODE_TWICE, threads=os.cpu_count() or 1)
+    tk, tc = tw.table(1)
+    oseen, otwice = tw.bloom()
+    one = spk.count(p, [k], bloom_bits=bits, list_min_count=1, table_log2=24)
+    for lg in (1, 2):
+        r = spk.count(p, [k], bloom_bits=bits, list_min_count=1, table_log2=24, span_groups_log2=lg)
+        info = r.info(0)
+        assert info["span_groups"] == 1 << lg and info["schedule"] == 3
+        gk, gc = r.kmers(0, 1)
+        np.testing.assert_array_equal(gk, tk)
+        np.testing.assert_array_equal(gc, tc)
+        seen, twice = r.bloom(0)
+        np.testing.assert_array_equal(seen, oseen)
+        np.testing.assert_array_equal(twice, otwice)
+        assert info["occurrences"] == one.info(0)["occurrences"]
+        assert info["cutoff"] == ora.cutoff(tc, 5.0) == one.info(0)["cutoff"]
+        np.testing.assert_array_equal(r.edges(0), one.edges(0))
+        # the default listing (count >= 2) through the same groups
+        d = spk.count(p, [k], bloom_bits=bits, table_log2=24, span_groups_log2=lg)
+        dk, dc = d.kmers(0)
+        np.testing.assert_array_equal(dk, tk[tc >= 2])
+        np.testing.assert_array_equal(dc, tc[tc >= 2])
+        r.close()
+        d.close()
