@@ -986,7 +986,7 @@ def main():
     # specified genome sizes (the full batch: --workload c4)
     batched = None
     if rank == 0 and not args.no_batched:
-        batched = batched_vs_plain(ctx, 0.1, 1, 1, args.bloom_bits, log)
+        batched = batched_vs_plain(ctx, 0.1, 2, 3, args.bloom_bits, log)
 
     # full-size parity of one more job against the oracle (rank 0 alone; every
     # rank counts the same reads)

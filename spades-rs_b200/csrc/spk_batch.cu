@@ -59,7 +59,7 @@ extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, sp
         const int rc = run_job(ctx, j, ks, out);
         if (rc) *err = spk_last_error();
         return rc;
-      });
+      }, need[i] > budget / 4);  // a large job runs alone
     }
     for (int i = 0; i < n_jobs; i++) {
       int st = 0;

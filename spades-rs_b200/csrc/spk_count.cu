@@ -3160,26 +3160,34 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   const uint64_t nparts = 1ULL << log2parts;
   const uint64_t nparts_g = nparts >> lg;  // spans of one group
 
-  // Buffers of the span count, filled over every group's pass.
+  // Buffers of the span count, filled over every group's pass (allocated
+  // after the first group's partition, when a single group has freed its
+  // coarse buckets, so that they never coexist).
   const bool early_sort = lmin_pre >= 2;
   SideStream side;
   if (early_sort && (rc = side.open())) return rc;
   DevSort lsort, esort;  // after `side`: its buffers are freed on that stream first
   DevBuf rbase, rfill, ops, sgl[2];
-  const uint64_t share = 3 * (lcap_ + scap_) / 2 / nranges + 1;
-  const uint64_t rcap = share + (share >> 2) + 1024;
-  if ((rc = rbase.alloc((nranges + 1) * 8, st)) || (rc = rfill.alloc(nranges * 4 * kFillStride, st)) ||
-      (rc = ops.alloc(nranges * rcap * 4, st)))
-    return rc;
-  SPK_CUDA(cudaMemsetAsync(rfill.p, 0, nranges * 4 * kFillStride, st));
-  RangeView bv{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), rcap, (uint32_t)nranges,
-               errp};
-  for (int j = 0; j < nl; j++)
-    if ((rc = kr.list[j].alloc(lcap_ * 8, st)) || (rc = sgl[j].alloc(scap_ * 8, st))) return rc;
-  if ((rc = kr.list[4].alloc(lcap_ * 4, st))) return rc;
-  ListOut lo{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
-             kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(), nl == 2 ? sgl[1].as<uint64_t>() : nullptr,
-             lcap_, scap_, lmin_pre, su + S_LFILL, su + S_HIST, su + S_OCC2};
+  RangeView bv{};
+  ListOut lo{};
+  auto alloc_count_buffers = [&]() -> int {
+    int r2;
+    const uint64_t share = 3 * (lcap_ + scap_) / 2 / nranges + 1;
+    const uint64_t rcap = share + (share >> 2) + 1024;
+    if ((r2 = rbase.alloc((nranges + 1) * 8, st)) || (r2 = rfill.alloc(nranges * 4 * kFillStride, st)) ||
+        (r2 = ops.alloc(nranges * rcap * 4, st)))
+      return r2;
+    SPK_CUDA(cudaMemsetAsync(rfill.p, 0, nranges * 4 * kFillStride, st));
+    bv = RangeView{ops.as<uint32_t>(), rbase.as<uint64_t>(), rfill.as<unsigned int>(), rcap, (uint32_t)nranges,
+                   errp};
+    for (int j = 0; j < nl; j++)
+      if ((r2 = kr.list[j].alloc(lcap_ * 8, st)) || (r2 = sgl[j].alloc(scap_ * 8, st))) return r2;
+    if ((r2 = kr.list[4].alloc(lcap_ * 4, st))) return r2;
+    lo = ListOut{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
+                 kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(), nl == 2 ? sgl[1].as<uint64_t>() : nullptr,
+                 lcap_, scap_, lmin_pre, su + S_LFILL, su + S_HIST, su + S_OCC2};
+    return SPK_OK;
+  };
 
   // ---- two-level read partition (k_part_coarse, k_part_fine) and span
   // count, once per group of spans ----
@@ -3241,6 +3249,13 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
     launches += 3;  // k_part_coarse, k_coarse_chunks, k_part_fine
   }
   if (g + 1 == (1u << lg)) SPK_CUDA(cudaEventRecord(ks1.e, st));
+  if (lg == 0) {  // one group: its coarse buckets are done with
+    cregion.release();
+    cbase.release();
+    cfill.release();
+    cfirst.release();
+  }
+  if (g == 0 && (rc = alloc_count_buffers())) return rc;
 
   // ---- span count of this group: the list, the singleton keys and the binned Bloom ops ----
   if (g == 0) SPK_CUDA(cudaEventRecord(kc0.e, st));

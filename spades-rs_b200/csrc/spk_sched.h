@@ -40,6 +40,7 @@ struct SchedJob {
   void* result = nullptr;
   std::string msg;                   // error message of a failed job
   int waiters = 0;                   // callers inside wait() for this job
+  bool exclusive = false;            // runs with no other job in flight
 };
 
 class Scheduler {
@@ -93,11 +94,15 @@ class Scheduler {
     }
   }
 
-  uint64_t submit(uint64_t need, std::function<int(void**, std::string*)> run) {
+  // exclusive: the job is admitted only when no other job runs, and no other
+  // job is admitted while it runs (jobs of a large share of the budget, whose
+  // neighbours would fragment the memory they need).
+  uint64_t submit(uint64_t need, std::function<int(void**, std::string*)> run, bool exclusive = false) {
     std::unique_lock<std::mutex> l(mu_);
     auto j = std::make_shared<SchedJob>();
     j->ticket = ++next_ticket_;
     j->need = need;
+    j->exclusive = exclusive;
     j->run = std::move(run);
     j->t_submit = std::chrono::steady_clock::now();
     jobs_[j->ticket] = j;
@@ -164,14 +169,17 @@ class Scheduler {
     std::unique_lock<std::mutex> l(mu_);
     for (;;) {
       cv_.wait(l, [&] {
-        return stopping_ || (!queue_.empty() && inflight_ < max_inflight_ &&
-                             in_use_ + queue_.front()->need <= budget_);
+        if (stopping_) return true;
+        if (queue_.empty() || inflight_ >= max_inflight_ || exclusive_running_) return false;
+        const auto& f = queue_.front();
+        return f->exclusive ? inflight_ == 0 : in_use_ + f->need <= budget_;
       });
       if (stopping_) break;
       auto j = queue_.front();
       queue_.pop_front();
       in_use_ += j->need;
       inflight_++;
+      if (j->exclusive) exclusive_running_ = true;
       if (inflight_ > peak_inflight_) peak_inflight_ = inflight_;
       j->t_start = std::chrono::steady_clock::now();
       std::thread([this, j] {
@@ -186,6 +194,7 @@ class Scheduler {
         j->done = true;
         in_use_ -= j->need;
         inflight_--;
+        if (j->exclusive) exclusive_running_ = false;
         cv_.notify_all();
         done_cv_.notify_all();
       }).detach();
@@ -204,6 +213,7 @@ class Scheduler {
   int inflight_ = 0;
   int peak_inflight_ = 0;
   bool stopping_ = false;
+  bool exclusive_running_ = false;
   std::function<void(void*)> free_result_;
 };
 

@@ -65,12 +65,17 @@ uint64_t job_estimate(const spk_job& j, uint64_t total_mem) {
     const uint64_t key = nl * 8, entry = nl * 8 + 4;
     const uint64_t tiers = words * 16 + (o.flags & SPK_F_REF_SOLID ? words * 8 : 0);
     uint64_t peak;
-    if (plain && nl <= 2 && k >= 12 && (occ * 3 + (1u << 22)) * key <= total_mem / 4) {
-      const uint64_t regions = (occ + occ / 2) * key + (1u << 20) * key;
-      const uint64_t first = regions + (occ + occ / 8 + 8192 * 64) * key;
-      const uint64_t ops = (cap * 3 + cap * 3 / 4 + 1024 * nranges) * 4;
-      const uint64_t count = regions + cap * entry + cap * key + ops + cap * entry + tiers;
-      peak = std::max(first, count);
+    // span groups: as many passes as keep the partition within a quarter of the device
+    uint32_t lg = 0;
+    while (lg < 4 && ((occ >> lg) * 3 + (1u << 22)) * key > total_mem / 4) lg++;
+    if (plain && nl <= 2 && k >= 12 && ((occ >> lg) * 3 + (1u << 22)) * key <= total_mem / 4) {
+      const uint64_t og = occ >> lg;
+      const uint64_t lcap = lg ? cap / 8 : cap, scap = lg ? cap / 2 : cap;
+      const uint64_t regions = (og + og / 2) * key + (1u << 20) * key;
+      const uint64_t first = regions + (og + og / 8 + 8192 * 64) * key;
+      const uint64_t ops = (3 * (lcap + scap) / 2 * 5 / 4 + 1024 * nranges) * 4;
+      const uint64_t count = regions + lcap * entry + scap * key + ops + lcap * entry + tiers;
+      peak = std::max(first, count) + (lg ? count - regions : 0);
     } else {
       const uint64_t slot = nl == 1 ? 16 : (nl <= 3 ? 32 : 64);
       peak = cap * slot + tiers + (cap / 4) * entry * 2;
@@ -194,7 +199,7 @@ int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket) {
     const int rc = run_job(ctx, j, ks, out);
     if (rc) *msg = spk_last_error();
     return rc;
-  });
+  }, need > ctx->server->budget / 4);  // a large job runs alone
   return SPK_OK;
 }
 

@@ -145,8 +145,41 @@ static void uncollected_results_freed() {
   CHECK(st == Scheduler::kAdmissionError);
 }
 
+// An exclusive job waits for the running jobs to finish and runs alone;
+// nothing is admitted next to it.
+static void exclusive_runs_alone() {
+  std::atomic<int> running{0}, overlap_with_big{0};
+  std::atomic<bool> big_running{false};
+  Scheduler s(100, 8);
+  std::vector<uint64_t> t;
+  auto small = [&](void** out, std::string*) {
+    running++;
+    if (big_running) overlap_with_big++;
+    std::this_thread::sleep_for(15ms);
+    running--;
+    *out = nullptr;
+    return 0;
+  };
+  for (int i = 0; i < 3; i++) t.push_back(s.submit(1, small));
+  t.push_back(s.submit(50, [&](void**, std::string*) {
+    if (running.load() != 0) overlap_with_big++;
+    big_running = true;
+    std::this_thread::sleep_for(30ms);
+    big_running = false;
+    return 0;
+  }, true));
+  for (int i = 0; i < 3; i++) t.push_back(s.submit(1, small));
+  for (auto x : t) {
+    int st = -1;
+    CHECK(s.wait(x, -1, &st, nullptr, nullptr) == 1 && st == 0);
+  }
+  CHECK(overlap_with_big.load() == 0);
+  CHECK(s.peak_inflight() >= 2);  // the small ones did share the device
+}
+
 int main() {
   admission();
+  exclusive_runs_alone();
   error_message();
   waiter_survives_stop();
   uncollected_results_freed();
