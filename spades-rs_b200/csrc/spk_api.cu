@@ -140,26 +140,17 @@ FastMod make_fastmod(uint64_t d) {
 int DevBuf::alloc(size_t n, cudaStream_t s) {
   release();
   if (n == 0) n = 16;
+  // No trimming of the pool here: other jobs may be running on the same
+  // pool, and giving its cached memory back would make all of them map it
+  // again (tens of ms per GB).  A job that runs out reports SPK_E_OOM; the
+  // batch runs it again alone after trimming (spk_count_batch).
   cudaError_t e = cudaMallocAsync(&p, n, s);
   if (e != cudaSuccess) {
     cudaGetLastError();
     p = nullptr;
-    // Give cached pool memory back to the driver once and retry.
-    cudaMemPool_t pool;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      cudaStreamSynchronize(s);
-      cudaMemPoolTrimTo(pool, 0);
-      e = cudaMallocAsync(&p, n, s);
-    }
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      p = nullptr;
-      char msg[128];
-      snprintf(msg, sizeof msg, "device allocation of %zu bytes failed", n);
-      return fail(SPK_E_OOM, msg);
-    }
+    char msg[128];
+    snprintf(msg, sizeof msg, "device allocation of %zu bytes failed", n);
+    return fail(SPK_E_OOM, msg);
   }
   bytes = n;
   st = s;

@@ -69,9 +69,13 @@ extern "C" int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, sp
       sts[i] = st;
     }
   }
-  // A job that ran out of device memory next to the others runs again alone.
+  // A job that ran out of device memory next to the others runs again alone,
+  // with the pool's cached memory given back first (fragments of the other
+  // jobs' buffers may be what it could not fit).
   for (int i = 0; i < n_jobs; i++) {
     if (sts[i] == SPK_E_OOM) {
+      cudaDeviceSynchronize();
+      if (ctx->pool) cudaMemPoolTrimTo(ctx->pool, 0);
       const spk_job& j = jobs[i];
       std::vector<uint32_t> ks(j.ks, j.ks + j.n_k);
       void* r = nullptr;
