@@ -200,7 +200,7 @@ int spk_packed_free(spk_packed* p);
                                   and admit singletons afterwards) with a table that holds
                                   only admitted k-mers, for read sets too large for that */
 #define SPK_F_DIRECT     0x10u /* count-first with one global-table atomic per occurrence
-                                  instead of the partitioned passes (k <= 64) */
+                                  instead of the partitioned passes */
 #define SPK_F_CORRECT    0x20u /* Stage 3 with error correction (config.error_correct,
                                   src/assemble.rs:183-191): after the Bloom pass every read
                                   is corrected against the twice tier (src/hammer.rs:34-121)
@@ -217,11 +217,12 @@ int spk_packed_free(spk_packed* p);
 #define SPK_SCHEDULE_FUSED       1u  /* SPK_F_REF_SOLID: one read pass with the per-occurrence
                                         Bloom inserts the reference solid tier needs */
 #define SPK_SCHEDULE_COUNT_FIRST 2u  /* one read pass counting every k-mer into the table with
-                                        global atomics (k > 64, or SPK_F_DIRECT); the Bloom
-                                        tiers are derived from the table afterwards */
-#define SPK_SCHEDULE_PARTITIONED 3u  /* default for k <= 64: the read pass scatters keys by table
-                                        span, each span is counted in shared memory and written
-                                        once, with the Bloom tiers derived from its counts */
+                                        global atomics (SPK_F_DIRECT; k = 96; k > 64 on read sets
+                                        too small for two partition levels); the Bloom tiers are
+                                        derived from the table afterwards */
+#define SPK_SCHEDULE_PARTITIONED 3u  /* the default: the read pass scatters keys by table span,
+                                        each span is counted in shared memory and written once,
+                                        with the Bloom tiers derived from its counts */
 
 typedef struct spk_count_opts {
   uint64_t bloom_bits;    /* bits per tier; 0 = 512 Mi (src/assemble.rs:84) */

@@ -233,8 +233,8 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
   const size_t tail = data_len & ~(size_t)7;
   SPK_CUDA(cudaMemsetAsync(res->reads.as<uint8_t>() + tail, 0, padded - tail, st));
   if (n_reads) {
-    SPK_CUDA(cudaMemcpyAsync(res->offs.p, offsets, n_reads * 8, cudaMemcpyHostToDevice, st));
-    SPK_CUDA(cudaMemcpyAsync(res->lens.p, lengths, n_reads * 4, cudaMemcpyHostToDevice, st));
+    if ((rc = xfer_h2d(res->ctx, res->offs.p, offsets, n_reads * 8, st))) return rc;
+    if ((rc = xfer_h2d(res->ctx, res->lens.p, lengths, n_reads * 4, st))) return rc;
   }
   rv->words = res->reads.as<uint64_t>();
   rv->offsets = res->offs.as<uint64_t>();
@@ -244,10 +244,7 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
   rv->data_len = data_len;
   rv->err = nullptr;
   rv->chunks = nullptr;
-  if (data_len < kChunkedUploadMin || n_reads < 2) {
-    if (data_len) SPK_CUDA(cudaMemcpyAsync(res->reads.p, data, data_len, cudaMemcpyHostToDevice, st));
-    return SPK_OK;
-  }
+  if (data_len < kChunkedUploadMin || n_reads < 2) return xfer_h2d(res->ctx, res->reads.p, data, data_len, st);
   // Large read sets: the data go up in kUploadChunks pieces on a copy stream,
   // so that the count's first pass works on the reads of a piece while the
   // next one is copied.  Reads [0, read_end[c]) end at least 64 bytes before
@@ -278,9 +275,8 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
     }
     ch.ready[c] = pooled_event(false);
     if (!ch.ready[c]) return fail(SPK_E_CUDA, "upload event");
-    if (b1 > b0)
-      SPK_CUDA(cudaMemcpyAsync(res->reads.as<uint8_t>() + b0, data + b0, b1 - b0, cudaMemcpyHostToDevice,
-                               res->copy_stream));
+    if (b1 > b0 && (rc = xfer_h2d(res->ctx, res->reads.as<uint8_t>() + b0, data + b0, b1 - b0, res->copy_stream)))
+      return rc;
     SPK_CUDA(cudaEventRecord(ch.ready[c], res->copy_stream));
     b0 = b1;
   }
@@ -362,6 +358,7 @@ int spk_ctx_destroy(spk_ctx* ctx) {
   if (!ctx) return SPK_OK;
   cudaSetDevice(ctx->device);
   serve_shutdown(ctx);
+  xfer_shutdown(ctx);
   ctx->scratch.release();
   cudaStreamSynchronize(ctx->stream);
   for (uint64_t* b : ctx->staging_all) cudaFreeHost(b);

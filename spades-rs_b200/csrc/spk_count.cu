@@ -411,6 +411,9 @@ template <int NL>
 __device__ __forceinline__ void table_add(const TableView& t, const Seq<NL>& C, uint64_t home,
                                           uint32_t n, const SlotPeek* peek = nullptr) {
   for (uint32_t i = 0; i < t.max_probe; i++) {
+    // A table too full for its k-mers is regrown and the pass repeated: once
+    // another thread has found that out, long probe sequences stop.
+    if ((i & 63) == 63 && (*(volatile int*)t.err & 1)) return;
     const uint64_t s = probe_slot(t, home, i);
     uint64_t* kp = slot_key<NL>(t, s);
     if (NL == 1) {
@@ -663,6 +666,70 @@ constexpr int kSpanBatch = 2;      // slots per thread in flight in k_part_count
 #endif
 constexpr uint32_t kErrRegion = 8;
 
+// Region, bucket and tile entries: the key's NL limbs side by side (one
+// 16-byte access for k <= 64, two for k > 96, three 8-byte ones for 65-96).
+template <int NL>
+__device__ __forceinline__ void key_put(uint64_t* p, uint64_t i, const Seq<NL>& C) {
+  if constexpr (NL == 1) {
+    p[i] = C.v[0];
+  } else if constexpr (NL == 2) {
+    *(ulonglong2*)(p + 2 * i) = make_ulonglong2(C.v[0], C.v[1]);
+  } else if constexpr (NL == 4) {
+    ((ulonglong2*)(p + 4 * i))[0] = make_ulonglong2(C.v[0], C.v[1]);
+    ((ulonglong2*)(p + 4 * i))[1] = make_ulonglong2(C.v[2], C.v[3]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < NL; j++) p[(uint64_t)NL * i + j] = C.v[j];
+  }
+}
+template <int NL>
+__device__ __forceinline__ Seq<NL> key_get(const uint64_t* p, uint64_t i) {
+  Seq<NL> C;
+  if constexpr (NL == 1) {
+    C.v[0] = p[i];
+  } else if constexpr (NL == 2) {
+    const ulonglong2 v = *(const ulonglong2*)(p + 2 * i);
+    C.v[0] = v.x;
+    C.v[1] = v.y;
+  } else if constexpr (NL == 4) {
+    const ulonglong2 a = ((const ulonglong2*)(p + 4 * i))[0], b = ((const ulonglong2*)(p + 4 * i))[1];
+    C.v[0] = a.x;
+    C.v[1] = a.y;
+    C.v[2] = b.x;
+    C.v[3] = b.y;
+  } else {
+#pragma unroll
+    for (int j = 0; j < NL; j++) C.v[j] = p[(uint64_t)NL * i + j];
+  }
+  return C;
+}
+// The same load from global memory, streaming (each entry is read once).
+template <int NL>
+__device__ __forceinline__ Seq<NL> key_get_cs(const uint64_t* p, uint64_t i) {
+  Seq<NL> C;
+  if constexpr (NL == 1) {
+    C.v[0] = __ldcs(p + i);
+  } else if constexpr (NL == 2) {
+    const ulonglong2 v = __ldcs((const ulonglong2*)(p + 2 * i));
+    C.v[0] = v.x;
+    C.v[1] = v.y;
+  } else if constexpr (NL == 4) {
+    const ulonglong2 a = __ldcs((const ulonglong2*)(p + 4 * i)), b = __ldcs((const ulonglong2*)(p + 4 * i) + 1);
+    C.v[0] = a.x;
+    C.v[1] = a.y;
+    C.v[2] = b.x;
+    C.v[3] = b.y;
+  } else {
+#pragma unroll
+    for (int j = 0; j < NL; j++) C.v[j] = __ldcs(p + (uint64_t)NL * i + j);
+  }
+  return C;
+}
+template <int NL>
+__device__ __forceinline__ void key_copy(uint64_t* d, uint64_t di, const uint64_t* s, uint64_t si) {
+  key_put<NL>(d, di, key_get<NL>(s, si));
+}
+
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_part_scatter(ReadsView R, unsigned k, PartView pv,
                                                           unsigned long long* __restrict__ occ_out) {
@@ -722,7 +789,7 @@ __global__ void __launch_bounds__(kBlock) k_part_scatter(ReadsView R, unsigned k
 // twice, each time through shared memory, so every global store is part of a
 // contiguous run:
 //   k_part_coarse  one read per thread; per round each thread rolls
-//                  kCoarseW windows into a shared-memory tile, the tile is
+//                  coarse_w windows into a shared-memory tile, the tile is
 //                  counting-sorted by coarse bucket (the top kCoarseBits bits
 //                  of the span index), each bucket's run is reserved with one
 //                  atomic and written out contiguously.
@@ -734,12 +801,19 @@ __global__ void __launch_bounds__(kBlock) k_part_scatter(ReadsView R, unsigned k
 constexpr uint32_t kCoarseBits = 6;
 constexpr uint32_t kCoarse = 1u << kCoarseBits;
 constexpr int kCoarseBlock = 512;
-constexpr int kCoarseW = 4;                              // windows per thread per round
-constexpr uint32_t kCoarseSlots = kCoarseBlock * kCoarseW;
+// windows per thread per round: the tile (keys twice over) stays within half
+// an SM's shared memory, so two CTAs share an SM
+template <int NL>
+constexpr int coarse_w() { return NL <= 3 ? 4 : 2; }
+template <int NL>
+constexpr uint32_t coarse_slots() { return kCoarseBlock * coarse_w<NL>(); }
 constexpr int kFineBlock = 512;
-constexpr uint32_t kFineChunk = 2048;                    // keys per chunk
+// keys per chunk of k_part_fine
+template <int NL>
+constexpr uint32_t fine_chunk() { return NL <= 2 ? 2048 : 1024; }
 constexpr uint32_t kFineMaxBits = 12;                    // spans per coarse bucket <= 2^12
-static_assert(kFineChunk % kFineBlock == 0, "k_part_fine loads whole rounds of keys");
+static_assert(fine_chunk<1>() % kFineBlock == 0 && fine_chunk<4>() % kFineBlock == 0,
+              "k_part_fine loads whole rounds of keys");
 
 struct CoarseView {
   uint64_t* keys;        // NL u64 per entry
@@ -757,7 +831,8 @@ __device__ __forceinline__ uint64_t region_base(const PartView& pv, uint32_t p) 
 
 template <int NL>
 size_t coarse_smem() {
-  return (size_t)kCoarseSlots * NL * 8 * 2 + kCoarseSlots * (1 + 1 + 2) + kCoarse * (4 + 4 + 8);
+  constexpr uint32_t kSlots = coarse_slots<NL>();
+  return (size_t)kSlots * NL * 8 * 2 + kSlots * (1 + 1 + 2) + kCoarse * (4 + 4 + 8);
 }
 
 template <int NL>
@@ -765,6 +840,8 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
                                                                  CoarseView cv,
                                                                  unsigned long long* __restrict__ occ_out) {
   extern __shared__ __align__(16) unsigned char cs_smem[];
+  constexpr uint32_t kCoarseSlots = coarse_slots<NL>();
+  constexpr int kCoarseW = coarse_w<NL>();
   uint64_t* ks = (uint64_t*)cs_smem;                       // keys by slot
   uint64_t* ss = ks + kCoarseSlots * NL;                   // keys sorted by bucket
   unsigned long long* gbase = (unsigned long long*)(ss + kCoarseSlots * NL);
@@ -823,9 +900,13 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
               V.v[0] = ((V.v[0] << 2) | bb) & topmask;
               Rc.v[0] = (Rc.v[0] >> 2) | ((3 - bb) << topsh);
             } else {
-              V.v[NL - 1] = ((V.v[NL - 1] << 2) | (V.v[0] >> 62)) & topmask;
+              // the window moves one base: V left by 2 bits, Rc right by 2
+#pragma unroll
+              for (int j = NL - 1; j >= 1; j--) V.v[j] = (V.v[j] << 2) | (V.v[j - 1] >> 62);
               V.v[0] = (V.v[0] << 2) | bb;
-              Rc.v[0] = (Rc.v[0] >> 2) | (Rc.v[NL - 1] << 62);
+              V.v[NL - 1] &= topmask;
+#pragma unroll
+              for (int j = 0; j < NL - 1; j++) Rc.v[j] = (Rc.v[j] >> 2) | (Rc.v[j + 1] << 62);
               Rc.v[NL - 1] = (Rc.v[NL - 1] >> 2) | ((3 - bb) << topsh);
             }
           }
@@ -840,8 +921,7 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
             C.v[NL - 1] |= (raw0 << pv.log2parts) >> (64 - kHomeBits) << (64 - kHomeBits);
           if ((p >> lp) == pv.group) {  // else another pass's
             b = (uint8_t)((p & ((1u << lp) - 1)) >> fshift);
-            if (NL == 1) ks[slot] = C.v[0];
-            else ((ulonglong2*)ks)[slot] = make_ulonglong2(C.v[0], C.v[NL - 1]);
+            key_put<NL>(ks, slot, C);
             rk[slot] = (uint16_t)atomicAdd(&hist[b], 1u);
           }
         }
@@ -869,8 +949,7 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
         const uint8_t b = bk[slot];
         if (b == 0xFF) continue;
         const uint32_t pos = start[b] + rk[slot];
-        if (NL == 1) ss[pos] = ks[slot];
-        else ((ulonglong2*)ss)[pos] = ((const ulonglong2*)ks)[slot];
+        key_copy<NL>(ss, pos, ks, slot);
         sb[pos] = b;
       }
       __syncthreads();
@@ -881,8 +960,7 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
         const uint64_t gi = gbase[b] + (j - start[b]);
         const uint64_t end = cv.uniform ? (uint64_t)(b + 1) * cv.uniform : cv.base[b + 1];
         if (gi < end) {
-          if (NL == 1) cv.keys[gi] = ss[j];
-          else *(ulonglong2*)(cv.keys + 2 * gi) = ((const ulonglong2*)ss)[j];
+          key_copy<NL>(cv.keys, gi, ss, j);
         } else {
           atomicOr(cv.err, (int)kErrRegion);
         }
@@ -901,12 +979,12 @@ __device__ __forceinline__ uint64_t coarse_len(const CoarseView& cv, uint32_t b)
   return min((uint64_t)cv.fill[(uint64_t)b * kFillStride], capb);
 }
 
-// cfirst[b] = the first chunk of bucket b (kFineChunk keys per chunk);
+// cfirst[b] = the first chunk of bucket b (`chunk` keys per chunk);
 // cfirst[kCoarse] = the number of chunks.  One warp.
-__global__ void k_coarse_chunks(CoarseView cv, uint32_t* __restrict__ cfirst) {
+__global__ void k_coarse_chunks(CoarseView cv, uint32_t chunk, uint32_t* __restrict__ cfirst) {
   const unsigned lane = threadIdx.x & 31;
-  const uint32_t c0 = (uint32_t)((coarse_len(cv, 2 * lane) + kFineChunk - 1) / kFineChunk);
-  const uint32_t c1 = (uint32_t)((coarse_len(cv, 2 * lane + 1) + kFineChunk - 1) / kFineChunk);
+  const uint32_t c0 = (uint32_t)((coarse_len(cv, 2 * lane) + chunk - 1) / chunk);
+  const uint32_t c1 = (uint32_t)((coarse_len(cv, 2 * lane + 1) + chunk - 1) / chunk);
   uint32_t x = c0 + c1;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
@@ -920,13 +998,15 @@ __global__ void k_coarse_chunks(CoarseView cv, uint32_t* __restrict__ cfirst) {
 
 template <int NL>
 size_t fine_smem(uint32_t nfine) {
-  return (size_t)kFineChunk * NL * 8 * 2 + (size_t)kFineChunk * (2 + 2 + 2) + (size_t)nfine * (8 + 4 + 4) + 64;
+  constexpr uint32_t kChunk = fine_chunk<NL>();
+  return (size_t)kChunk * NL * 8 * 2 + (size_t)kChunk * (2 + 2 + 2) + (size_t)nfine * (8 + 4 + 4) + 64;
 }
 
 template <int NL>
 __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, const uint32_t* __restrict__ cfirst,
                                                              PartView pv, unsigned k) {
   extern __shared__ __align__(16) unsigned char fs_smem[];
+  constexpr uint32_t kFineChunk = fine_chunk<NL>();
   const uint32_t fbits = pv.log2parts - pv.log2groups - kCoarseBits, nfine = 1u << fbits;
   uint64_t* ks = (uint64_t*)fs_smem;
   uint64_t* ss = ks + kFineChunk * NL;
@@ -957,20 +1037,13 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
       for (int q = 0; q < PER; q++) {
         const uint32_t j = threadIdx.x + q * kFineBlock;
         if (j >= n) continue;
-        if (NL == 1) {
-          C[q].v[0] = __ldcs(cv.keys + s0 + j);
-        } else {
-          const ulonglong2 v = __ldcs((const ulonglong2*)(cv.keys + 2 * (s0 + j)));
-          C[q].v[0] = v.x;
-          C[q].v[NL - 1] = v.y;
-        }
+        C[q] = key_get_cs<NL>(cv.keys, s0 + j);
       }
 #pragma unroll
       for (int q = 0; q < PER; q++) {
         const uint32_t j = threadIdx.x + q * kFineBlock;
         if (j >= n) continue;
-        if (NL == 1) ks[j] = C[q].v[0];
-        else ((ulonglong2*)ks)[j] = make_ulonglong2(C[q].v[0], C[q].v[NL - 1]);
+        key_put<NL>(ks, j, C[q]);
         if (pv.packed_home) C[q].v[NL - 1] &= ~0ULL >> kHomeBits;
         uint64_t w4[4];
         kmer256_limbs<NL>(C[q], k, w4);
@@ -1007,8 +1080,7 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
       const uint32_t f = fb[j];
       const uint32_t pos = start[f] + rk[j];
-      if (NL == 1) ss[pos] = ks[j];
-      else ((ulonglong2*)ss)[pos] = ((const ulonglong2*)ks)[j];
+      key_copy<NL>(ss, pos, ks, j);
       sf[pos] = (uint16_t)f;
     }
     __syncthreads();
@@ -1018,8 +1090,7 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
       const uint64_t gi = gbase[f] + (j - start[f]);
       const uint64_t end = pv.uniform ? (uint64_t)(pg + 1) * pv.uniform : pv.base[pg + 1];
       if (gi < end) {
-        if (NL == 1) pv.keys[gi] = ss[j];
-        else *(ulonglong2*)(pv.keys + 2 * gi) = ((const ulonglong2*)ss)[j];
+        key_copy<NL>(pv.keys, gi, ss, j);
       } else {
         atomicOr(pv.err, (int)kErrRegion);
       }
@@ -1039,22 +1110,40 @@ template <>
 struct SpanKey<2> {
   typedef U128 T;
 };
-
-// One probe step at slot s of the shared-memory span: true when the
-// occurrence of C is counted there (C found, or s empty and claimed for C).
 template <int NL>
-__device__ __forceinline__ bool span_step(typename SpanKey<NL>::T* keys, uint32_t* cnt, uint32_t s,
-                                          const Seq<NL>& C) {
-  if (NL == 1) {
+struct WideKey {
+  unsigned long long v[NL];
+};
+template <>
+struct SpanKey<3> {
+  typedef WideKey<3> T;
+};
+template <>
+struct SpanKey<4> {
+  typedef WideKey<4> T;
+};
+// k > 64: a slot's count word is also its state.  0: empty; kSpanClaimed:
+// its claimer is writing the key (it publishes the key and sets the count to
+// 1 in the same step, so the state never outlasts that step); else settled,
+// and the count.
+constexpr uint32_t kSpanClaimed = 0xFFFFFFFFu;
+
+// One probe step at slot s of the shared-memory span: 1 when the
+// occurrence of C is counted there (C found, or s empty and claimed for C),
+// 0 when s holds another key, 2 when s is being claimed (k > 64: look again).
+template <int NL>
+__device__ __forceinline__ int span_step(typename SpanKey<NL>::T* keys, uint32_t* cnt, uint32_t s,
+                                         const Seq<NL>& C) {
+  if constexpr (NL == 1) {
     unsigned long long* kp = (unsigned long long*)&keys[s];
     const unsigned long long cur = *(volatile unsigned long long*)kp;
-    if (cur == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
+    if (cur == C.v[0]) { atomicAdd(cnt + s, 1u); return 1; }
     if (cur == kEmpty) {
       const unsigned long long old = atomicCAS(kp, kEmpty, (unsigned long long)C.v[0]);
-      if (old == kEmpty || old == C.v[0]) { atomicAdd(cnt + s, 1u); return true; }
+      if (old == kEmpty || old == C.v[0]) { atomicAdd(cnt + s, 1u); return 1; }
     }
-    return false;
-  } else {
+    return 0;
+  } else if constexpr (NL == 2) {
     U128* kp = (U128*)&keys[s];
     U128 cur;
     cur.x = ((volatile unsigned long long*)kp)[0];
@@ -1062,16 +1151,38 @@ __device__ __forceinline__ bool span_step(typename SpanKey<NL>::T* keys, uint32_
     if (cur.x != kEmpty && cur.y != kEmpty) {
       // settled (a slot changes once, from empty to its key; a read that
       // overlaps that change has an empty half and takes the CAS below)
-      if (cur.x == C.v[0] && cur.y == C.v[NL - 1]) { atomicAdd(cnt + s, 1u); return true; }
-      return false;
+      if (cur.x == C.v[0] && cur.y == C.v[NL - 1]) { atomicAdd(cnt + s, 1u); return 1; }
+      return 0;
     }
     const U128 e{kEmpty, kEmpty}, mine{C.v[0], C.v[NL - 1]};
     const U128 old = atomicCAS(kp, e, mine);
     if ((old.x == kEmpty && old.y == kEmpty) || (old.x == mine.x && old.y == mine.y)) {
       atomicAdd(cnt + s, 1u);
-      return true;
+      return 1;
     }
-    return false;
+    return 0;
+  } else {
+    uint32_t c = *(volatile uint32_t*)(cnt + s);
+    if (c == 0) {
+      c = atomicCAS(cnt + s, 0u, kSpanClaimed);
+      if (c == 0) {
+        volatile unsigned long long* kp = keys[s].v;
+#pragma unroll
+        for (int j = 0; j < NL; j++) kp[j] = C.v[j];
+        __threadfence_block();
+        atomicExch(cnt + s, 1u);
+        return 1;
+      }
+    }
+    if (c == kSpanClaimed) return 2;
+    __threadfence_block();  // the settled key was written before its count
+    const volatile unsigned long long* kp = keys[s].v;
+    bool eq = true;
+#pragma unroll
+    for (int j = 0; j < NL; j++) eq &= kp[j] == C.v[j];
+    if (!eq) return 0;
+    atomicAdd(cnt + s, 1u);
+    return 1;
   }
 }
 
@@ -1224,11 +1335,9 @@ __device__ __forceinline__ void span_emit_sorted(const typename SpanKey<NL>::T* 
 // k-mer at most once, so cap (the table's slot count) bounds each.
 constexpr int kHistBins = 256;  // counts >= 255 share the last bin
 struct ListOut {
-  uint64_t* l0;                 // list: limb 0 (SoA)
-  uint64_t* l1;                 // list: limb 1 (k > 32)
+  uint64_t* l[4];               // list: limbs 0..NL-1 (SoA)
   uint32_t* cnt;                // list: counts (nullptr: the table is written instead)
-  uint64_t* s0;                 // singletons: limb 0
-  uint64_t* s1;                 // singletons: limb 1
+  uint64_t* s[4];               // singletons: limbs 0..NL-1
   uint64_t cap;                 // list entries
   uint64_t scap;                // singleton keys
   uint32_t lmin;                // smallest count listed (>= 2 here; singletons are listed
@@ -1251,6 +1360,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
   __shared__ uint32_t lw[2][kRounds * kWarps];
   __shared__ unsigned long long lbase[2];
   __shared__ unsigned s_hist[kHistBins];
+  __shared__ int s_full;  // this span, or an earlier one of the launch, ran out of slots
   const bool to_list = lo.cnt != nullptr;
   const uint32_t lmin = lo.lmin < 2 ? 2u : lo.lmin;
   uint64_t occ2 = 0;
@@ -1265,18 +1375,31 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
   // k <= 64 with sorted emission: a cursor per range (the ops placed so far)
   uint32_t* rcur = rhist + ((rv.nranges + 1) & ~1u);
   unsigned long long* rbase =
-      (unsigned long long*)(rcur + ((NL == 2 && kSortedOps) ? ((rv.nranges + 1) & ~1u) : 0u));
+      (unsigned long long*)(rcur + ((NL >= 2 && kSortedOps) ? ((rv.nranges + 1) & ~1u) : 0u));
   const uint32_t nparts = 1u << (pv.log2parts - pv.log2groups);  // this group's spans
   for (uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
+    // A span that ran out of slots sends the job back with more slots: the
+    // spans after it are skipped (their counts would be dropped).
+    if (threadIdx.x == 0) s_full = *(volatile int*)t.err & 1;
+    __syncthreads();
+    if (s_full) break;
     for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
-      if (NL == 1) ((unsigned long long*)keys)[s] = kEmpty;
-      else ((U128*)keys)[s] = U128{kEmpty, kEmpty};
+      if constexpr (NL == 1) {
+        ((unsigned long long*)keys)[s] = kEmpty;
+      } else if constexpr (NL == 2) {
+        ((U128*)keys)[s] = U128{kEmpty, kEmpty};
+      } else {
+        // (k > 64: the count marks empty slots; all-ones keys mark them for
+        // the sorted emission of the Bloom operations)
+#pragma unroll
+        for (int j = 0; j < NL; j++) keys[s].v[j] = kEmpty;
+      }
       cnt[s] = 0;
     }
     if (OPS)
       for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) {
         rhist[r] = 0;
-        if (NL == 2 && kSortedOps) rcur[r] = 0;
+        if (NL >= 2 && kSortedOps) rcur[r] = 0;
       }
     __syncthreads();
     const uint64_t b = pv.base[p];
@@ -1289,17 +1412,11 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
       uint64_t i = b + threadIdx.x;
       bool have = false;
       Seq<NL> C;
-      uint32_t home = 0, step = 0;
+      uint32_t home = 0, step = 0, waits = 0;
       for (;;) {
         if (!have) {
-          if (i >= e) break;
-          if (NL == 1) {
-            C.v[0] = __ldcs(pv.keys + i);
-          } else {
-            const ulonglong2 v = __ldcs((const ulonglong2*)(pv.keys + 2 * i));
-            C.v[0] = v.x;
-            C.v[NL - 1] = v.y;
-          }
+          if (i >= e || *(volatile int*)&s_full) break;
+          C = key_get_cs<NL>(pv.keys, i);
           i += blockDim.x;
 #if SPK_COUNT_PREFETCH
           // the key this lane takes next, on its way to L1 while this one is placed
@@ -1316,17 +1433,26 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
           }
           have = true;
           step = 0;
+          waits = 0;
         }
-        if (span_step<NL>(keys, cnt, (home + step) & (S - 1), C)) {
+        const int got = span_step<NL>(keys, cnt, (home + step) & (S - 1), C);
+        if (got == 1) {
           have = false;
-        } else if (++step == S) {
-          full = true;  // every slot probed
+        } else if (got == 0) {
+          if (++step == S) {
+            full = true;  // every slot probed
+            have = false;
+            s_full = 1;
+          }
+        } else if (++waits > kSpinLimit) {
+          atomicOr(t.err, 2);  // a claim that never settled: the job fails
           have = false;
         }
       }
     }
     if (full) atomicOr(t.err, 1);  // span full: the host regrows the table
     __syncthreads();
+    if (s_full) break;
     const uint64_t g0 = ((uint64_t)pv.group << (pv.log2parts - pv.log2groups) | p) << t.log2span;
     if (OPS && to_list) {
       // Entries of each (round, warp) of the write-out loop below: a ballot
@@ -1378,13 +1504,13 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
         if (!to_list && s >= S) continue;
         const uint32_t c = s < S ? cnt[s] : 0u;
         Seq<NL> C;
-        if (NL == 1) {
+        if constexpr (NL == 1) {
           C.v[0] = c ? ((unsigned long long*)keys)[s] : kEmpty;
           if (!to_list) {
             ulonglong2* gp = (ulonglong2*)slot_key<NL>(t, g0 + s);
             *gp = make_ulonglong2(C.v[0], (unsigned long long)c);
           }
-        } else {
+        } else if constexpr (NL == 2) {
           const U128 kv = c ? ((U128*)keys)[s] : U128{kEmpty, kEmpty};
           C.v[0] = kv.x;
           C.v[NL - 1] = kv.y;
@@ -1393,6 +1519,10 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
             gp[0] = make_ulonglong2(kv.x, kv.y);
             gp[1] = make_ulonglong2((unsigned long long)c, 0ULL);
           }
+        } else {
+          // k > 64 runs in list mode only
+#pragma unroll
+          for (int j = 0; j < NL; j++) C.v[j] = c ? keys[s].v[j] : kEmpty;
         }
         if (to_list) {
           // (lanes past the span's end have c == 0 and take part in the ballots only)
@@ -1400,15 +1530,15 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
           if (c >= lmin) {
             const uint64_t q = lbase[0] + lw[0][r * kWarps + warp] + __popc(bl & lanemask_lt());
             if (q < lo.cap) {
-              lo.l0[q] = C.v[0];
-              if (NL == 2) lo.l1[q] = C.v[NL - 1];
+#pragma unroll
+              for (int j = 0; j < NL; j++) lo.l[j][q] = C.v[j];
               lo.cnt[q] = c;
             }
           } else if (c == 1) {
             const uint64_t q = lbase[1] + lw[1][r * kWarps + warp] + __popc(bs & lanemask_lt());
             if (q < lo.scap) {
-              lo.s0[q] = C.v[0];
-              if (NL == 2) lo.s1[q] = C.v[NL - 1];
+#pragma unroll
+              for (int j = 0; j < NL; j++) lo.s[j][q] = C.v[j];
             }
           }
         }
@@ -1418,15 +1548,15 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
 #pragma unroll
         for (int j = 0; j < 3; j++) {
           atomicAdd(rhist + (uint32_t)(pos[j] >> kLog2Range), 1u);
-          // k <= 64: the written-out key's slot keeps the three positions as
+          // k > 32: the written-out key's slot keeps the three positions as
           // (range << kLog2Range | offset), at most 31 bits each
-          if (NL == 2) ((uint32_t*)&keys[s])[j] = (uint32_t)pos[j];
+          if (NL >= 2) ((uint32_t*)&keys[s])[j] = (uint32_t)pos[j];
         }
         // with the sorted emission the count array is reused: the slot's
         // stash keeps "count >= 2" in bit 31 of its first position (positions
         // are below 2^31 since there are at most 2^12 ranges); an empty
         // slot's stash stays all ones
-        if (NL == 2 && kSortedOps && c >= 2) ((uint32_t*)&keys[s])[0] |= 0x80000000u;
+        if (NL >= 2 && kSortedOps && c >= 2) ((uint32_t*)&keys[s])[0] |= 0x80000000u;
       }
       __syncthreads();
       // One reservation per non-empty range; rhist then counts the span's
@@ -1434,10 +1564,10 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
       for (uint32_t r = threadIdx.x; r < rv.nranges; r += blockDim.x) {
         const uint32_t n = rhist[r];
         rbase[r] = n ? range_base(rv, r) + atomicAdd(rv.fill + (uint64_t)r * kFillStride, n) : 0ULL;
-        if (!(NL == 2 && kSortedOps)) rhist[r] = 0;
+        if (!(NL >= 2 && kSortedOps)) rhist[r] = 0;
       }
       __syncthreads();
-      if (NL == 2 && kSortedOps) {
+      if (NL >= 2 && kSortedOps) {
         span_emit_sorted<NL>(keys, cnt, S, rhist, rcur, rbase, rv);
       } else {
       // Emit the operations.
@@ -1445,7 +1575,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
         const uint32_t c = cnt[s];
         if (!c) continue;
         uint32_t pk[3];
-        if (NL == 2) {
+        if (NL >= 2) {
 #pragma unroll
           for (int j = 0; j < 3; j++) pk[j] = ((const uint32_t*)&keys[s])[j];
         } else {
@@ -1471,6 +1601,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
       }
       continue;
     }
+    if constexpr (NL <= 2) {
     constexpr int U = kSpanBatch;
     for (uint32_t s0 = threadIdx.x; s0 < S; s0 += U * blockDim.x) {
       uint32_t c[U];
@@ -1502,6 +1633,7 @@ __global__ void __launch_bounds__(kPartBlock, kPartCtasPerSm) k_part_count(PartV
       }
       // The Bloom operations of these k-mers (see k_bloom_from_table).
       bloom_ops_distinct<U>(tiers, pos, c);
+    }
     }
     __syncthreads();
   }
@@ -1814,8 +1946,8 @@ __global__ void __launch_bounds__(kBlock) k_admit_singletons(ListOut lo, unsigne
     bool admit = false;
     Seq<NL> C;
     if (i < n) {
-      C.v[0] = __ldcs(lo.s0 + i);
-      if (NL == 2) C.v[NL - 1] = __ldcs(lo.s1 + i);
+#pragma unroll
+      for (int j = 0; j < NL; j++) C.v[j] = __ldcs(lo.s[j] + i);
       uint64_t raw[3], pos[3];
       bloom_positions<NL>(C, k, fm, raw, pos);
       const uint64_t a = __ldg(twice + (pos[0] >> 6)), b = __ldg(twice + (pos[1] >> 6)),
@@ -1830,8 +1962,8 @@ __global__ void __launch_bounds__(kBlock) k_admit_singletons(ListOut lo, unsigne
         if (lane == 0) wb = atomicAdd(lo.fill, (unsigned long long)__popc(m));
         const uint64_t q = __shfl_sync(FULL, wb, 0) + __popc(m & lanemask_lt());
         if (admit && q < lo.cap) {
-          lo.l0[q] = C.v[0];
-          if (NL == 2) lo.l1[q] = C.v[NL - 1];
+#pragma unroll
+          for (int j = 0; j < NL; j++) lo.l[j][q] = C.v[j];
           lo.cnt[q] = 1;
         }
       }
@@ -1941,9 +2073,15 @@ __device__ __forceinline__ uint64_t filter_bit(const SetView& sv, uint64_t raw0)
   return raw0 & ((1ULL << sv.log2filter) - 1);
 }
 
+// Wide keys (k > 64) take a slot with a CAS on their top limb and then write
+// the others: the keys inserted are distinct, and lookups run in a later
+// kernel.  The top limb of a key with 2k < 64 NL has unused high bits, so it
+// is never all-ones (k = 96 fills it and does not use the set).
+struct ListCols {
+  const uint64_t* p[4];
+};
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_solid_set(const uint64_t* l0, const uint64_t* l1,
-                                                       const uint32_t* __restrict__ cnt, uint64_t n,
+__global__ void __launch_bounds__(kBlock) k_solid_set(ListCols L, const uint32_t* __restrict__ cnt, uint64_t n,
                                                        const uint32_t* __restrict__ thr, unsigned k,
                                                        SetView sv) {
   const uint32_t cutoff = thr[0];
@@ -1952,8 +2090,8 @@ __global__ void __launch_bounds__(kBlock) k_solid_set(const uint64_t* l0, const 
        i += (uint64_t)gridDim.x * blockDim.x) {
     if (cnt[i] < cutoff) continue;
     Seq<NL> C;
-    C.v[0] = l0[i];
-    if (NL == 2) C.v[NL - 1] = l1[i];
+#pragma unroll
+    for (int j = 0; j < NL; j++) C.v[j] = L.p[j][i];
     uint64_t w4[4];
     kmer256_limbs<NL>(C, k, w4);
     const uint64_t raw0 = hash_seed(hash_pre(w4), kSeed1);
@@ -1962,12 +2100,19 @@ __global__ void __launch_bounds__(kBlock) k_solid_set(const uint64_t* l0, const 
     uint64_t h = raw0 >> (64 - sv.log2cap);
     // keys are distinct and the set is at most 2/3 full, so a free slot is found
     for (uint64_t probe = 0; probe <= mask; probe++, h = (h + 1) & mask) {
-      if (NL == 1) {
+      if constexpr (NL == 1) {
         if (atomicCAS((unsigned long long*)sv.keys + h, kEmpty, (unsigned long long)C.v[0]) == kEmpty)
           break;
-      } else {
+      } else if constexpr (NL == 2) {
         const U128 old = atomicCAS((U128*)sv.keys + h, U128{kEmpty, kEmpty}, U128{C.v[0], C.v[NL - 1]});
         if (old.x == kEmpty && old.y == kEmpty) break;
+      } else {
+        uint64_t* kp = sv.keys + (uint64_t)NL * h;
+        if (atomicCAS((unsigned long long*)(kp + NL - 1), kEmpty, (unsigned long long)C.v[NL - 1]) == kEmpty) {
+#pragma unroll
+          for (int j = 0; j < NL - 1; j++) kp[j] = C.v[j];
+          break;
+        }
       }
     }
   }
@@ -1980,14 +2125,22 @@ __device__ __forceinline__ bool set_has(const SetView& sv, const Seq<NL>& C, uin
   const uint64_t mask = (1ULL << sv.log2cap) - 1;
   uint64_t h = raw0 >> (64 - sv.log2cap);
   for (uint64_t probe = 0; probe <= mask; probe++, h = (h + 1) & mask) {
-    if (NL == 1) {
+    if constexpr (NL == 1) {
       const uint64_t v = __ldg(sv.keys + h);
       if (v == C.v[0]) return true;
       if (v == kEmpty) return false;
-    } else {
+    } else if constexpr (NL == 2) {
       const ulonglong2 v = __ldg((const ulonglong2*)sv.keys + h);
       if (v.x == C.v[0] && v.y == C.v[NL - 1]) return true;
       if (v.x == kEmpty && v.y == kEmpty) return false;
+    } else {
+      const uint64_t* kp = sv.keys + (uint64_t)NL * h;
+      const uint64_t top = __ldg(kp + NL - 1);
+      if (top == kEmpty) return false;
+      bool eq = top == C.v[NL - 1];
+#pragma unroll
+      for (int j = 0; j < NL - 1; j++) eq &= __ldg(kp + j) == C.v[j];
+      if (eq) return true;
     }
   }
   return false;
@@ -2189,6 +2342,11 @@ __global__ void __launch_bounds__(kBlock) k_read_order(const uint64_t* __restric
 // ---------------------------------------------------------------------------
 static int grid_for(spk_ctx* ctx, int blocks_per_sm) { return ctx->sm_count * blocks_per_sm; }
 
+// F<NL>(args...) for the key width nl at run time (F returns a status).
+#define SPK_NL_CALL(nl, F, ...)                                                              \
+  ((nl) == 1 ? F<1>(__VA_ARGS__) : (nl) == 2 ? F<2>(__VA_ARGS__) : (nl) == 3 ? F<3>(__VA_ARGS__) \
+                                                                             : F<4>(__VA_ARGS__))
+
 #define SPK_DISPATCH_NL(nl, F, ...)                 \
   switch (nl) {                                     \
     case 1: F<1>(__VA_ARGS__); break;               \
@@ -2197,6 +2355,11 @@ static int grid_for(spk_ctx* ctx, int blocks_per_sm) { return ctx->sm_count * bl
     default: F<4>(__VA_ARGS__); break;              \
   }
 
+template <int NL>
+static void launch_admit_singletons(spk_ctx* ctx, cudaStream_t st, const ListOut& lo, unsigned k,
+                                    const FastMod& fm, const uint64_t* twice, unsigned long long* sums) {
+  k_admit_singletons<NL><<<grid_for(ctx, 8), kBlock, 0, st>>>(lo, k, fm, twice, sums);
+}
 template <int NL>
 static void launch_fused(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
                          const FastMod& fm, U128* tiers, unsigned long long* ref,
@@ -2252,15 +2415,17 @@ static int launch_part_count(spk_ctx* ctx, cudaStream_t st, const PartView& pv, 
   const int grid = (int)std::min<uint64_t>(nparts, (uint64_t)ctx->sm_count * kPartCtasPerSm);
   if (rv.ops) {
     smem += ((rv.nranges + 1) & ~1u) * 4 + (size_t)rv.nranges * 8;
-    if (NL == 2 && kSortedOps) smem += ((rv.nranges + 1) & ~1u) * 4;  // range cursors
+    if (NL >= 2 && kSortedOps) smem += ((rv.nranges + 1) & ~1u) * 4;  // range cursors
     int rc;
     if ((rc = raise_smem_limit((const void*)k_part_count<NL, true>, smem))) return rc;
     k_part_count<NL, true><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv, lo);
-  } else {
+  } else if constexpr (NL <= 2) {
     int rc;
     if ((rc = raise_smem_limit((const void*)k_part_count<NL, false>, smem))) return rc;
     ListOut none{};  // the in-place Bloom form writes the table
     k_part_count<NL, false><<<grid, kPartBlock, smem, st>>>(pv, t, k, fm, tiers, rv, none);
+  } else {
+    return fail(SPK_E_INVALID_ARG, "k > 64 counts spans in list mode only");
   }
   return SPK_OK;
 }
@@ -2273,8 +2438,9 @@ static int launch_bloom_apply(spk_ctx* ctx, cudaStream_t st, const RangeView& rv
   k_bloom_apply<<<grid, kApplyBlock, smem, st>>>(rv, num_words, seen, twice, pops);
   return SPK_OK;
 }
-// Spans of the partitioned schedule: 8192 slots of 12 bytes (k <= 32) or
-// 4096 of 20 bytes (k <= 64) in shared memory, two CTAs per SM.
+// Spans of the partitioned schedule: 8192 slots of 12 bytes (k <= 32), 4096
+// of 20 bytes (k <= 64) or 2048 of 28 / 36 bytes (k <= 96 / 127) in shared
+// memory, two CTAs per SM.
 #ifndef SPK_PART_LOG2SPAN1
 #define SPK_PART_LOG2SPAN1 13
 #endif
@@ -2282,6 +2448,10 @@ static int launch_bloom_apply(spk_ctx* ctx, cudaStream_t st, const RangeView& rv
 #define SPK_PART_LOG2SPAN2 12
 #endif
 constexpr uint32_t kPartLog2Span1 = SPK_PART_LOG2SPAN1, kPartLog2Span2 = SPK_PART_LOG2SPAN2;
+constexpr uint32_t kPartLog2SpanWide = 11;
+static uint32_t part_log2span(int nl) {
+  return nl == 1 ? kPartLog2Span1 : nl == 2 ? kPartLog2Span2 : kPartLog2SpanWide;
+}
 
 template <int NL>
 static void launch_bloom(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, unsigned k,
@@ -2314,7 +2484,7 @@ static void launch_edges_t(spk_ctx* ctx, cudaStream_t st, uint64_t* l[4], const 
                            uint64_t n, const uint32_t* thr, const TableView& t, const SetView* sv,
                            unsigned k, uint64_t* e[4], uint64_t out_cap,
                            unsigned long long* counter) {
-  if (sv && NL <= 2)
+  if (sv)
     k_edges<NL, NLE, true><<<grid_for(ctx, 8), kBlock, 0, st>>>(
         l[0], l[1], l[2], l[3], cnt, n, thr, t, *sv, k, e[0], e[1], e[2], e[3], out_cap, counter);
   else
@@ -2322,7 +2492,7 @@ static void launch_edges_t(spk_ctx* ctx, cudaStream_t st, uint64_t* l[4], const 
         l[0], l[1], l[2], l[3], cnt, n, thr, t, SetView{nullptr, 0, 0, nullptr}, k, e[0], e[1], e[2], e[3],
         out_cap, counter);
 }
-// sv: the solid set (k <= 64), or nullptr to probe the count table.
+// sv: the solid set, or nullptr to probe the count table.
 static void launch_edges(spk_ctx* ctx, cudaStream_t st, int nl, int nle, uint64_t* l[4],
                          const uint32_t* cnt, uint64_t n, const uint32_t* thr, const TableView& t,
                          const SetView* sv, unsigned k, uint64_t* e[4], uint64_t out_cap,
@@ -2331,9 +2501,20 @@ static void launch_edges(spk_ctx* ctx, cudaStream_t st, int nl, int nle, uint64_
   else if (nl == 1) launch_edges_t<1, 2>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
   else if (nl == 2 && nle == 2) launch_edges_t<2, 2>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
   else if (nl == 2) launch_edges_t<2, 3>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
-  else if (nl == 3 && nle == 3) launch_edges_t<3, 3>(ctx, st, l, cnt, n, thr, t, nullptr, k, e, out_cap, counter);
-  else if (nl == 3) launch_edges_t<3, 4>(ctx, st, l, cnt, n, thr, t, nullptr, k, e, out_cap, counter);
-  else launch_edges_t<4, 4>(ctx, st, l, cnt, n, thr, t, nullptr, k, e, out_cap, counter);
+  else if (nl == 3 && nle == 3) launch_edges_t<3, 3>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
+  else if (nl == 3) launch_edges_t<3, 4>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
+  else launch_edges_t<4, 4>(ctx, st, l, cnt, n, thr, t, sv, k, e, out_cap, counter);
+}
+static void launch_solid_set(spk_ctx* ctx, cudaStream_t st, int nl, uint64_t* const l[4], const uint32_t* cnt,
+                             uint64_t n, const uint32_t* thr, unsigned k, const SetView& sv) {
+  const ListCols L{{l[0], l[1], l[2], l[3]}};
+  const int g = grid_for(ctx, 8);
+  switch (nl) {
+    case 1: k_solid_set<1><<<g, kBlock, 0, st>>>(L, cnt, n, thr, k, sv); break;
+    case 2: k_solid_set<2><<<g, kBlock, 0, st>>>(L, cnt, n, thr, k, sv); break;
+    case 3: k_solid_set<3><<<g, kBlock, 0, st>>>(L, cnt, n, thr, k, sv); break;
+    default: k_solid_set<4><<<g, kBlock, 0, st>>>(L, cnt, n, thr, k, sv); break;
+  }
 }
 
 static uint64_t next_pow2(uint64_t x) {
@@ -2363,6 +2544,13 @@ static uint64_t gated_capacity(uint64_t m, uint64_t pop_seen, uint64_t pop_twice
 // up) and doubles, with a recount, if a probe sequence overflows.
 static uint64_t fused_capacity(uint64_t occ) {
   return std::max<uint64_t>(next_pow2(occ * 3 / 10 + 1), 1024);
+}
+// Slots of the span count: the distinct share of the occurrences grows with
+// k (a read has fewer windows, a sequencing error makes more new k-mers),
+// from 0.11 at k = 21 to 0.27 at k = 55, 0.36 at k = 77, 0.44 at k = 99 and
+// 0.56 at k = 127 on 150 bp reads at 100x with 1% errors.
+static uint64_t list_capacity(uint64_t occ, int nl) {
+  return nl <= 2 ? fused_capacity(occ) : std::max<uint64_t>(next_pow2(occ * 9 / 20 + 1), 1024);
 }
 
 struct Ev {
@@ -2420,6 +2608,25 @@ enum {
   S_HIST = 16,           /* 256 words */
   S_WORDS = 16 + kHistBins
 };
+
+// The span count's list output over kr's list buffers and the singleton key
+// buffers sgl (kr.nl limbs each), with the fills and histogram in scratch.
+static ListOut list_out(KResult& kr, DevBuf* sgl, uint64_t lcap, uint64_t scap, uint32_t lmin,
+                        unsigned long long* su) {
+  ListOut lo{};
+  for (int j = 0; j < kr.nl; j++) {
+    lo.l[j] = kr.list[j].as<uint64_t>();
+    lo.s[j] = sgl[j].as<uint64_t>();
+  }
+  lo.cnt = kr.list[4].as<uint32_t>();
+  lo.cap = lcap;
+  lo.scap = scap;
+  lo.lmin = lmin;
+  lo.fill = su + S_LFILL;
+  lo.hist = su + S_HIST;
+  lo.occ2 = su + S_OCC2;
+  return lo;
+}
 
 // What a finished job keeps: the list and edge buffers cut to what they hold
 // (they were sized by bounds: table slots, eight edges per solid k-mer), and
@@ -2530,7 +2737,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
   RangeView bv{nullptr, nullptr, nullptr, 0, (uint32_t)nranges, errp};
   bool list_mode = false;  // the span count wrote the list (no table)
   ListOut lo{};
-  DevBuf sgl[2];           // list mode: keys of the k-mers counted once
+  DevBuf sgl[4];           // list mode: keys of the k-mers counted once
   if (!gated) {
     // ---- fused: Bloom and the count of every k-mer in one pass ----
     k_occ<<<grid_for(ctx, 2), kBlock, 0, st>>>(rv.lengths, rv.n_reads, k, su + S_OCC0);
@@ -2538,7 +2745,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     launches++;
     if ((rc = fetch(S_OCC0 + 1))) return rc;
     const uint64_t occ0 = host[S_OCC0];
-    cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(occ0);
+    cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : list_capacity(occ0, nl);
     bool two_level_fits = false;
     if (partitioned) {
       // Regions hold 1.5x the mean share of occurrences per span: keep them
@@ -2563,10 +2770,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
         if ((rc = kr.list[4].alloc(cap * 4, st))) return rc;
         SPK_CUDA(cudaMemsetAsync(sw + S_LFILL, 0, 3 * 8, st));  // fills and S_OCC2
         SPK_CUDA(cudaMemsetAsync(sw + S_HIST, 0, kHistBins * 8, st));
-        lo = ListOut{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
-                     kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(),
-                     nl == 2 ? sgl[1].as<uint64_t>() : nullptr, cap, cap, lmin_pre, su + S_LFILL,
-                     su + S_HIST, su + S_OCC2};
+        lo = list_out(kr, sgl, cap, cap, lmin_pre, su);
       }
       TableView& t = kr.table;
       t.err = errp;
@@ -2623,7 +2827,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
           if ((rc = fetch(S_ERR + 1))) return rc;
           if ((int)host[S_ERR] & kErrRegion) return fail(SPK_E_CUDA, "coarse bucket overflow after resizing");
         }
-        k_coarse_chunks<<<1, 32, 0, st>>>(cv, cfirst.as<uint32_t>());
+        k_coarse_chunks<<<1, 32, 0, st>>>(cv, fine_chunk<2>(), cfirst.as<uint32_t>());
         if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
         else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
         if (rc) return rc;
@@ -2999,12 +3203,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
       SPK_CUDA(cudaMemsetAsync(set.p, 0xFF, (1ULL << lg) * nl * 8, st));
       SPK_CUDA(cudaMemsetAsync(filt.p, 0, (1ULL << lf) / 8, st));
       sv = SetView{set.as<uint64_t>(), lg, lf, filt.as<uint32_t>()};
-      if (nl == 1)
-        k_solid_set<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[0], kr.list[4].as<uint32_t>(),
-                                                           kr.list_len, thr, k, sv);
-      else
-        k_solid_set<2><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[1], kr.list[4].as<uint32_t>(),
-                                                           kr.list_len, thr, k, sv);
+      launch_solid_set(ctx, st, nl, lp, kr.list[4].as<uint32_t>(), kr.list_len, thr, k, sv);
       SPK_CUDA(cudaGetLastError());
       launches++;
     }
@@ -3057,7 +3256,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
 // Returns kNotThisPath when the inputs need another layout (count_one_k
 // handles them), kRedo after an overflow, else the status.
 // ---------------------------------------------------------------------------
-constexpr int kNotThisPath = -100, kRedo = -101;
+constexpr int kNotThisPath = -100, kRedo = -101, kGrow = -102;
 constexpr uint32_t kMaxLog2Groups = 4;  // at most 16 passes over the reads
 
 // A second stream of one job, joined back to the job's stream by events.
@@ -3081,7 +3280,8 @@ struct SideStream {
 int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv_in, unsigned k,
                      const spk_count_opts& o, KResult& kr) {
   const int nl = (int)((k + 31) / 32);
-  if (k < 12 || nl > 2) return kNotThisPath;
+  // (k = 96 fills its top limb, which the solid set's empty mark needs free)
+  if (k < 12 || (nl >= 3 && 2 * k == 64u * nl)) return kNotThisPath;
   if (o.flags & (SPK_F_GATED | SPK_F_CORRECT | SPK_F_REF_SOLID | SPK_F_DIRECT | SPK_F_KEEP_TABLE))
     return kNotThisPath;
   if (o.n_prior > 0 && o.prior_seqs && o.prior_offsets && o.prior_lengths) return kNotThisPath;
@@ -3111,8 +3311,8 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   SPK_CUDA(cudaStreamSynchronize(st));
   const uint64_t occ0 = host[S_OCC0];
   const bool per_chunk = rv_in.chunks && host[S_ORDER] == 0;
-  uint64_t cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : fused_capacity(occ0);
-  const uint32_t log2span = nl == 1 ? kPartLog2Span1 : kPartLog2Span2;
+  uint64_t cap = o.table_log2 ? (1ULL << std::min<uint32_t>(o.table_log2, 40)) : list_capacity(occ0, nl);
+  const uint32_t log2span = part_log2span(nl);
   uint32_t log2cap = 0;
   while ((1ULL << log2cap) < cap) log2cap++;
   if (log2cap <= log2span) return kNotThisPath;
@@ -3121,17 +3321,25 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   // buckets, 2.6 keys per occurrence) would pass a quarter of the device is
   // partitioned and counted in 2^lg passes, each keeping the keys of one group
   // of spans (the reads are streamed once per pass).
+  // Span regions hold 1.5x their mean share of occurrences, 2x for the
+  // smaller spans of keys wider than 64 bits (fewer k-mers per span, so its
+  // share varies more); the coarse buckets 1.125x.
+  const uint64_t part_keys4 = nl >= 3 ? 13 : 11;  // regions + buckets, in quarter keys per occurrence
+  auto part_bytes = [&](uint32_t g) { return ((occ0 >> g) * part_keys4 / 4 + (1u << 22)) * (uint64_t)nl * 8; };
   uint32_t lg = std::min<uint32_t>(o.span_groups_log2, kMaxLog2Groups);
-  while (lg < kMaxLog2Groups && ((occ0 >> lg) * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4) lg++;
-  if (((occ0 >> lg) * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4) return kNotThisPath;
+  while (lg < kMaxLog2Groups && part_bytes(lg) > ctx->total_mem / 4) lg++;
+  if (part_bytes(lg) > ctx->total_mem / 4) return kNotThisPath;
   while (lg > 0 && log2parts - lg <= kCoarseBits) lg--;
   if (!SPK_TWO_LEVEL || log2parts - lg <= kCoarseBits || log2parts - lg - kCoarseBits > kFineMaxBits ||
-      ((occ0 >> lg) * 3 + (1u << 22)) * (uint64_t)nl * 8 > ctx->total_mem / 4)
+      part_bytes(lg) > ctx->total_mem / 4)
     return kNotThisPath;
-  // One pass: the list and the singleton keys hold up to one entry per table
-  // slot each, so they cannot overflow.  Several: an eighth and a half of the
-  // slots (the mid-job readback sends the job back if either overflowed).
-  const uint64_t lcap_ = lg ? cap >> 3 : cap, scap_ = lg ? cap >> 1 : cap;
+  // The span count holds at most one distinct k-mer per slot (a full span
+  // sends the job back), so the singleton keys and the list, up to one entry
+  // per slot each, cannot overflow.  With several groups (large read sets)
+  // the list gets half the slots: k-mers counted twice or more are a small
+  // share of the distinct ones (the mid-job readback sends the job back if
+  // it overflowed).
+  const uint64_t lcap_ = lg ? cap >> 1 : cap, scap_ = cap;
 
   kr.k = k;
   kr.nl = nl;
@@ -3167,12 +3375,12 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   SideStream side;
   if (early_sort && (rc = side.open())) return rc;
   DevSort lsort, esort;  // after `side`: its buffers are freed on that stream first
-  DevBuf rbase, rfill, ops, sgl[2];
+  DevBuf rbase, rfill, ops, sgl[4];
   RangeView bv{};
   ListOut lo{};
   auto alloc_count_buffers = [&]() -> int {
     int r2;
-    const uint64_t share = 3 * (lcap_ + scap_) / 2 / nranges + 1;
+    const uint64_t share = 3 * cap / nranges + 1;  // three per distinct k-mer
     const uint64_t rcap = share + (share >> 2) + 1024;
     if ((r2 = rbase.alloc((nranges + 1) * 8, st)) || (r2 = rfill.alloc(nranges * 4 * kFillStride, st)) ||
         (r2 = ops.alloc(nranges * rcap * 4, st)))
@@ -3183,9 +3391,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
     for (int j = 0; j < nl; j++)
       if ((r2 = kr.list[j].alloc(lcap_ * 8, st)) || (r2 = sgl[j].alloc(scap_ * 8, st))) return r2;
     if ((r2 = kr.list[4].alloc(lcap_ * 4, st))) return r2;
-    lo = ListOut{kr.list[0].as<uint64_t>(), nl == 2 ? kr.list[1].as<uint64_t>() : nullptr,
-                 kr.list[4].as<uint32_t>(), sgl[0].as<uint64_t>(), nl == 2 ? sgl[1].as<uint64_t>() : nullptr,
-                 lcap_, scap_, lmin_pre, su + S_LFILL, su + S_HIST, su + S_OCC2};
+    lo = list_out(kr, sgl, lcap_, scap_, lmin_pre, su);
     return SPK_OK;
   };
 
@@ -3193,7 +3399,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   // count, once per group of spans ----
   DevBuf base, fill, region;
   const uint64_t per = occ0 / nparts;
-  const uint64_t capu = per + (per >> 1) + 256;
+  const uint64_t capu = nl >= 3 ? 2 * per + 512 : per + (per >> 1) + 256;
   if ((rc = base.alloc((nparts_g + 1) * 8, st)) || (rc = fill.alloc(nparts_g * 4 * kFillStride, st)) ||
       (rc = region.alloc(nparts_g * capu * nl * 8, st)))
     return rc;
@@ -3226,8 +3432,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
           rc_.offsets += r0;
           rc_.lengths += r0;
           rc_.n_reads = r1 - r0;
-          if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rc_, k, pv, cv, su + S_OCC);
-          else rc = launch_part_coarse<2>(ctx, st, rc_, k, pv, cv, su + S_OCC);
+          rc = SPK_NL_CALL(nl, launch_part_coarse, ctx, st, rc_, k, pv, cv, su + S_OCC);
           if (rc) return rc;
           launches++;
         }
@@ -3236,14 +3441,12 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
       launches--;  // counted below
     } else {
       if (rv.chunks) SPK_CUDA(cudaStreamWaitEvent(st, rv.chunks->ready[rv.chunks->n - 1], 0));
-      if (nl == 1) rc = launch_part_coarse<1>(ctx, st, rv, k, pv, cv, su + S_OCC);
-      else rc = launch_part_coarse<2>(ctx, st, rv, k, pv, cv, su + S_OCC);
+      rc = SPK_NL_CALL(nl, launch_part_coarse, ctx, st, rv, k, pv, cv, su + S_OCC);
       if (rc) return rc;
     }
     if (lg == 0) SPK_CUDA(cudaEventRecord(ksm.e, st));
-    k_coarse_chunks<<<1, 32, 0, st>>>(cv, cfirst.as<uint32_t>());
-    if (nl == 1) rc = launch_part_fine<1>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
-    else rc = launch_part_fine<2>(ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
+    k_coarse_chunks<<<1, 32, 0, st>>>(cv, nl <= 2 ? fine_chunk<2>() : fine_chunk<4>(), cfirst.as<uint32_t>());
+    rc = SPK_NL_CALL(nl, launch_part_fine, ctx, st, cv, cfirst.as<uint32_t>(), pv, k);
     if (rc) return rc;
     SPK_CUDA(cudaGetLastError());
     launches += 3;  // k_part_coarse, k_coarse_chunks, k_part_fine
@@ -3259,8 +3462,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
 
   // ---- span count of this group: the list, the singleton keys and the binned Bloom ops ----
   if (g == 0) SPK_CUDA(cudaEventRecord(kc0.e, st));
-  if (nl == 1) rc = launch_part_count<1>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
-  else rc = launch_part_count<2>(ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
+  rc = SPK_NL_CALL(nl, launch_part_count, ctx, st, pv, t, k, kr.fm, nullptr, bv, lo);
   if (rc) return rc;
   SPK_CUDA(cudaGetLastError());
   launches++;
@@ -3301,12 +3503,8 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
     SPK_CUDA(cudaEventRecord(e1.e, st));
     SPK_CUDA(cudaEventRecord(e2.e, st));
     // ---- singleton admission, histogram, cutoff ----
-    if (nl == 1)
-      k_admit_singletons<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lo, k, kr.fm, kr.twice.as<uint64_t>(),
-                                                                 su + S_SUMS + 1);
-    else
-      k_admit_singletons<2><<<grid_for(ctx, 8), kBlock, 0, st>>>(lo, k, kr.fm, kr.twice.as<uint64_t>(),
-                                                                 su + S_SUMS + 1);
+    SPK_DISPATCH_NL(nl, launch_admit_singletons, ctx, st, lo, k, kr.fm, kr.twice.as<uint64_t>(),
+                    su + S_SUMS + 1);
     SPK_CUDA(cudaGetLastError());
     launches++;
   }
@@ -3320,7 +3518,8 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   SPK_CUDA(cudaStreamSynchronize(st));
   const int err = (int)host[S_ERR];
   if (err & 4) return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
-  if (err & (1 | kErrRegion | kErrRange)) return kRedo;  // a full span or an overflowed region
+  if (err & (kErrRegion | kErrRange)) return kRedo;  // an overflowed region
+  if (err & 1) return kGrow;                           // a span with more distinct k-mers than slots
   info.occurrences = host[S_OCC];
   info.seen_popcount = host[S_POPS];
   info.twice_popcount = host[S_POPS + 1];
@@ -3388,12 +3587,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
     SPK_CUDA(cudaMemsetAsync(set.p, 0xFF, (1ULL << lg) * nl * 8, st));
     SPK_CUDA(cudaMemsetAsync(filt.p, 0, (1ULL << lf) / 8, st));
     SetView sv{set.as<uint64_t>(), lg, lf, filt.as<uint32_t>()};
-    if (nl == 1)
-      k_solid_set<1><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[0], kr.list[4].as<uint32_t>(),
-                                                         kr.list_len, thr, k, sv);
-    else
-      k_solid_set<2><<<grid_for(ctx, 8), kBlock, 0, st>>>(lp[0], lp[1], kr.list[4].as<uint32_t>(),
-                                                         kr.list_len, thr, k, sv);
+    launch_solid_set(ctx, st, nl, lp, kr.list[4].as<uint32_t>(), kr.list_len, thr, k, sv);
     SPK_CUDA(cudaGetLastError());
     launch_edges(ctx, st, nl, kr.nle, lp, kr.list[4].as<uint32_t>(), kr.list_len, thr, kr.table, &sv, k, ep,
                  ecap, su + S_EDGES);
@@ -3454,7 +3648,21 @@ static void rehome(KResult& kr, cudaStream_t s) {
 // overflow there) the general one.
 static int count_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv, unsigned k,
                    const spk_count_opts& o, KResult& kr) {
-  const int rc = count_one_k_list(ctx, st, host, rv, k, o, kr);
+  int rc = count_one_k_list(ctx, st, host, rv, k, o, kr);
+  // A span with more distinct k-mers than slots: twice the slots, twice at most.
+  for (uint32_t grow = 1; rc == kGrow && grow <= 2; grow++) {
+    SPK_CUDA(cudaStreamSynchronize(st));  // the abandoned job's buffers are freed in stream order
+    spk_count_opts og = o;
+    og.table_log2 = kr.table.log2cap + 1;
+    kr = KResult();
+    rc = count_one_k_list(ctx, st, host, rv, k, og, kr);
+    if (rc == SPK_OK) {
+      kr.info.table_regrows = grow;
+      return SPK_OK;
+    }
+    if (rc == SPK_E_OOM) rc = kRedo;  // the general path instead
+  }
+  if (rc == kGrow) rc = kRedo;
   if (rc != kNotThisPath && rc != kRedo) return rc;
   // every uploaded piece of the reads, before the general path reads them
   if (rv.chunks) SPK_CUDA(cudaStreamWaitEvent(st, rv.chunks->ready[rv.chunks->n - 1], 0));
@@ -3545,10 +3753,9 @@ static int copy_out(spk_result* res, KResult& kr, int kind, int nl, DevBuf* limb
     *n_inout = m;
     return fail(SPK_E_INVALID_ARG, "output buffer too small");
   }
-  if (m) {
-    if (keys) SPK_CUDA(cudaMemcpyAsync(keys, cv.keys.p, m * nl * 8, cudaMemcpyDeviceToHost, st));
-    if (counts && cin) SPK_CUDA(cudaMemcpyAsync(counts, cv.cnt.p, m * 4, cudaMemcpyDeviceToHost, st));
-  }
+  int rc;
+  if (m && keys && (rc = xfer_d2h(res->ctx, keys, cv.keys.p, m * nl * 8, st))) return rc;
+  if (m && counts && cin && (rc = xfer_d2h(res->ctx, counts, cv.cnt.p, m * 4, st))) return rc;
   SPK_CUDA(cudaStreamSynchronize(st));
   *n_inout = m;
   return SPK_OK;

@@ -150,6 +150,16 @@ void pooled_stream_put(cudaStream_t s);
 cudaEvent_t pooled_event(bool timing);
 void pooled_event_put(cudaEvent_t e, bool timing);
 
+// Copies between host memory and the device on stream st (spk_xfer.cu).
+// Pageable host memory goes through pinned chunks with several host threads;
+// pinned memory is copied directly.  xfer_h2d returns once every piece is
+// enqueued (the host source may be reused); xfer_d2h once the data is on the
+// host.
+struct XferPool;
+int xfer_h2d(spk_ctx* ctx, void* dst, const void* src, size_t n, cudaStream_t st);
+int xfer_d2h(spk_ctx* ctx, void* dst, const void* src, size_t n, cudaStream_t st);
+void xfer_shutdown(spk_ctx* ctx);
+
 }  // namespace spk
 
 // ---- opaque handles --------------------------------------------------------------
@@ -170,6 +180,10 @@ struct spk_ctx {
   // serving
   struct Server* server = nullptr;
   std::mutex serve_mu;
+  // host threads and pinned chunks for copies from and to pageable memory
+  // (created on first use)
+  spk::XferPool* xfer = nullptr;
+  std::mutex xfer_mu;
 };
 
 struct spk_bloom {

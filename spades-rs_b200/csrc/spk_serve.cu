@@ -61,19 +61,22 @@ uint64_t job_estimate(const spk_job& j, uint64_t total_mem) {
     const uint64_t nl = (k + 31) / 32;
     const uint64_t b4 = (uint64_t)j.data_len * 4, sub = (uint64_t)j.n_reads * (k - 1);
     const uint64_t occ = b4 > sub ? b4 - sub : 0;
-    const uint64_t cap = std::max<uint64_t>(next_pow2_u64(occ * 3 / 10 + 1), 1024);
+    // slots: 0.3 of the occurrences for k <= 64, 0.45 above (more distinct k-mers per read)
+    const uint64_t cap = std::max<uint64_t>(next_pow2_u64(nl <= 2 ? occ * 3 / 10 + 1 : occ * 9 / 20 + 1), 1024);
     const uint64_t key = nl * 8, entry = nl * 8 + 4;
     const uint64_t tiers = words * 16 + (o.flags & SPK_F_REF_SOLID ? words * 8 : 0);
     uint64_t peak;
     // span groups: as many passes as keep the partition within a quarter of the device
+    const uint64_t q4 = nl >= 3 ? 13 : 11;  // partition keys per occurrence, in quarters
     uint32_t lg = 0;
-    while (lg < 4 && ((occ >> lg) * 3 + (1u << 22)) * key > total_mem / 4) lg++;
-    if (plain && nl <= 2 && k >= 12 && ((occ >> lg) * 3 + (1u << 22)) * key <= total_mem / 4) {
+    while (lg < 4 && ((occ >> lg) * q4 / 4 + (1u << 22)) * key > total_mem / 4) lg++;
+    if (plain && k >= 12 && !(nl >= 3 && 2 * k == 64 * nl) &&
+        ((occ >> lg) * q4 / 4 + (1u << 22)) * key <= total_mem / 4) {
       const uint64_t og = occ >> lg;
-      const uint64_t lcap = lg ? cap / 8 : cap, scap = lg ? cap / 2 : cap;
-      const uint64_t regions = (og + og / 2) * key + (1u << 20) * key;
+      const uint64_t lcap = lg ? cap / 2 : cap, scap = cap;
+      const uint64_t regions = (nl >= 3 ? 2 * og : og + og / 2) * key + (1u << 20) * key;
       const uint64_t first = regions + (og + og / 8 + 8192 * 64) * key;
-      const uint64_t ops = (3 * (lcap + scap) / 2 * 5 / 4 + 1024 * nranges) * 4;
+      const uint64_t ops = (3 * cap * 5 / 4 + 1024 * nranges) * 4;
       const uint64_t count = regions + lcap * entry + scap * key + ops + lcap * entry + tiers;
       peak = std::max(first, count) + (lg ? count - regions : 0);
     } else {

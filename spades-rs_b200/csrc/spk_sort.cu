@@ -493,6 +493,32 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_local(Limbs T, const uint32_t* 
   }
 }
 
+// The buckets k_bs_local left unsorted, side by side: seg[3i..3i+2] = (offset
+// in the concatenation C, offset in the list L, size).  Gathers L's segments
+// into C (back = false) or writes C's back into L; one CTA per segment.
+template <int NL, bool HASV>
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_segments(Limbs L, uint32_t* lv, Limbs C, uint32_t* cv,
+                                                           const uint32_t* __restrict__ seg, bool back) {
+  const uint32_t co = seg[3 * blockIdx.x], lo = seg[3 * blockIdx.x + 1], m = seg[3 * blockIdx.x + 2];
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+#pragma unroll
+    for (int j = 0; j < NL; j++) {
+      if (back) L.p[j][lo + i] = C.p[j][co + i];
+      else C.p[j][co + i] = L.p[j][lo + i];
+    }
+    if (HASV) {
+      if (back) lv[lo + i] = cv[co + i];
+      else cv[co + i] = lv[lo + i];
+    }
+  }
+}
+template <int NL>
+static void launch_segments(cudaStream_t st, bool hasv, Limbs L, uint32_t* lv, Limbs C, uint32_t* cv,
+                            const uint32_t* seg, uint32_t nseg, bool back) {
+  if (hasv) k_bs_segments<NL, true><<<nseg, BS_BLOCK, 0, st>>>(L, lv, C, cv, seg, back);
+  else k_bs_segments<NL, false><<<nseg, BS_BLOCK, 0, st>>>(L, lv, C, cv, seg, back);
+}
+
 template <int NL, bool HASV>
 static int bs_launch(cudaStream_t st, Limbs K, uint32_t* v, Limbs T, uint32_t* tv, uint64_t n,
                      const unsigned long long* n_dev, unsigned limb, unsigned sh, uint32_t nb,
@@ -674,28 +700,51 @@ int sort_dev_finish(cudaStream_t st, DevSort& ds, DevBuf* keys, DevBuf* vals, ui
     if (vals) SPK_CUDA(cudaMemcpyAsync(v, tvp, n_host * 4, cudaMemcpyDeviceToDevice, st));
     rc = radix_sort_bufs(st, nl, n_host, ds.nbits, keys, vals, launches);
   } else if (nbig_host > 0) {
-    uint64_t* hs = h_staging + BS_STAGE_WORDS;
+    // The large buckets side by side, in list order, sorted as one array on
+    // their whole keys (their top bits keep the buckets apart), then put
+    // back: one sort however many buckets there are.
+    uint32_t* hs = (uint32_t*)(h_staging + BS_STAGE_WORDS);
     SPK_CUDA(cudaMemcpyAsync(hs, ds.big.p, (size_t)nbig_host * 12, cudaMemcpyDeviceToHost, st));
     SPK_CUDA(cudaStreamSynchronize(st));
-    std::vector<uint32_t> bl((const uint32_t*)hs, (const uint32_t*)hs + 3 * nbig_host);
-    const unsigned hi_bit = ds.nbits - ds.bbits;
-    rc = SPK_OK;
-    for (unsigned q = 0; q < nbig_host && !rc; q++) {
-      const uint64_t o = bl[3 * q + 1], m = bl[3 * q + 2];
-      DevBuf bk[4], bvv;
-      for (int j = 0; j < nl; j++) {
-        if ((rc = bk[j].alloc(m * 8, st))) return rc;
-        SPK_CUDA(cudaMemcpyAsync(bk[j].p, ds.tk[j].as<uint64_t>() + o, m * 8, cudaMemcpyDeviceToDevice, st));
-      }
-      if (vals) {
-        if ((rc = bvv.alloc(m * 4, st))) return rc;
-        SPK_CUDA(cudaMemcpyAsync(bvv.p, tvp + o, m * 4, cudaMemcpyDeviceToDevice, st));
-      }
-      if ((rc = radix_sort_bufs(st, nl, m, hi_bit, bk, vals ? &bvv : nullptr, launches))) return rc;
-      for (int j = 0; j < nl; j++)
-        SPK_CUDA(cudaMemcpyAsync(keys[j].as<uint64_t>() + o, bk[j].p, m * 8, cudaMemcpyDeviceToDevice, st));
-      if (vals) SPK_CUDA(cudaMemcpyAsync(v + o, bvv.p, m * 4, cudaMemcpyDeviceToDevice, st));
+    std::vector<std::pair<uint32_t, uint32_t>> segs(nbig_host);  // (offset in the list, size)
+    for (unsigned q = 0; q < nbig_host; q++) segs[q] = {hs[3 * q + 1], hs[3 * q + 2]};
+    std::sort(segs.begin(), segs.end());
+    uint64_t total = 0;
+    for (unsigned q = 0; q < nbig_host; q++) {
+      hs[3 * q] = (uint32_t)total;
+      hs[3 * q + 1] = segs[q].first;
+      hs[3 * q + 2] = segs[q].second;
+      total += segs[q].second;
     }
+    uint32_t* seg = ds.big.as<uint32_t>();
+    SPK_CUDA(cudaMemcpyAsync(seg, hs, (size_t)nbig_host * 12, cudaMemcpyHostToDevice, st));
+    DevBuf ck[4], cvb;
+    Limbs L{}, Cc{};
+    for (int j = 0; j < nl; j++) {
+      if ((rc = ck[j].alloc(total * 8, st))) return rc;
+      L.p[j] = keys[j].as<uint64_t>();
+      Cc.p[j] = ck[j].as<uint64_t>();
+    }
+    if (vals && (rc = cvb.alloc(total * 4, st))) return rc;
+    uint32_t* cvp = vals ? cvb.as<uint32_t>() : nullptr;
+    switch (nl) {
+      case 1: launch_segments<1>(st, vals, L, v, Cc, cvp, seg, nbig_host, false); break;
+      case 2: launch_segments<2>(st, vals, L, v, Cc, cvp, seg, nbig_host, false); break;
+      case 3: launch_segments<3>(st, vals, L, v, Cc, cvp, seg, nbig_host, false); break;
+      default: launch_segments<4>(st, vals, L, v, Cc, cvp, seg, nbig_host, false); break;
+    }
+    SPK_CUDA(cudaGetLastError());
+    if ((rc = radix_sort_bufs(st, nl, total, ds.nbits, ck, vals ? &cvb : nullptr, launches))) return rc;
+    for (int j = 0; j < nl; j++) Cc.p[j] = ck[j].as<uint64_t>();  // the sort may have swapped buffers
+    cvp = vals ? cvb.as<uint32_t>() : nullptr;
+    switch (nl) {
+      case 1: launch_segments<1>(st, vals, L, v, Cc, cvp, seg, nbig_host, true); break;
+      case 2: launch_segments<2>(st, vals, L, v, Cc, cvp, seg, nbig_host, true); break;
+      case 3: launch_segments<3>(st, vals, L, v, Cc, cvp, seg, nbig_host, true); break;
+      default: launch_segments<4>(st, vals, L, v, Cc, cvp, seg, nbig_host, true); break;
+    }
+    SPK_CUDA(cudaGetLastError());
+    if (launches) *launches += 2;
   } else {
     rc = SPK_OK;
   }

@@ -157,7 +157,8 @@ def test_count_matches_golden(spk, name, flags):
         np.testing.assert_array_equal(r2.edges(0), g["edges"])
 
 
-@pytest.mark.parametrize("k", [1, 11, 15, 21, 31, 32, 33, 47, 55, 63, 64, 65, 77, 96, 99, 127])
+@pytest.mark.parametrize("k", [1, 11, 15, 21, 31, 32, 33, 47, 55, 63, 64, 65, 77, 89, 90, 95, 96, 97, 99, 121,
+                               122, 127])
 def test_count_all_key_widths(spk, ora, k):
     data, offs, lens = synth_small_packed()
     check_against_oracle(spk, ora, data, offs, lens, k, 1 << 20)
@@ -278,13 +279,21 @@ def test_solid_cutoff_and_seam(spk, ora):
 
 
 def test_schedules(spk):
-    """Partitioned count-first by default for k <= 64 and count-first with
-    global atomics above; the reference solid tier selects the fused pass and
-    SPK_F_GATED the two-pass schedule."""
+    """Partitioned count-first by default: with a one-level partition for k
+    <= 64 on small read sets, two levels otherwise, and for k > 64 once the
+    read set has enough spans for two levels (else, and for k = 96, whose keys
+    fill three limbs, count-first with global atomics); the reference solid
+    tier selects the fused pass and SPK_F_GATED the two-pass schedule."""
+    from spk import synth
     data, offs, lens = synth_small_packed()
     assert spk.count((data, offs, lens), [55]).info(0)["schedule"] == 3
     assert spk.count((data, offs, lens), [21]).info(0)["schedule"] == 3
     assert spk.count((data, offs, lens), [77]).info(0)["schedule"] == 2
+    p = synth.c2(0.05).packed
+    for k, sched in ((77, 3), (127, 3), (96, 2)):
+        i = spk.count(p, [k], bloom_bits=1 << 26).info(0)
+        assert i["schedule"] == sched, k
+        assert i["part_passes"] == (2 if sched == 3 else 0), k
     assert spk.count((data, offs, lens), [55], flags=DIRECT).info(0)["schedule"] == 2
     assert spk.count((data, offs, lens), [55], flags=ALL).info(0)["schedule"] == 1
     assert spk.count((data, offs, lens), [55], flags=GATED).info(0)["schedule"] == 0
@@ -435,6 +444,73 @@ def test_large_lists_bucket_sort(spk, ora):
     np.testing.assert_array_equal(r.edges(0), ora.edges(sk, k))
 
 
+@pytest.mark.parametrize("k,table_log2", [(55, 21), (77, 22)])
+def test_span_count_grows_full_spans(spk, ora, k, table_log2):
+    """Too few slots for the distinct k-mers (forced with table_log2): spans
+    run out of slots, the job stops early and runs again with twice the
+    slots; the admitted table, tiers, cutoff and edges equal the oracle's."""
+    import os
+    from spk import synth
+    p = synth.c2(0.05).packed
+    bits = 1 << 26
+    tw = ora.count(p.data, p.offsets, p.lengths, k, bits, mode=ora.MODE_TWICE, threads=os.cpu_count() or 1)
+    tk, tc = tw.table(1)
+    oseen, otwice = tw.bloom()
+    r = spk.count(p, [k], bloom_bits=bits, list_min_count=1, table_log2=table_log2, flags=BASE)
+    info = r.info(0)
+    assert info["n_distinct"] > 3 << (table_log2 - 2)  # most spans over their slots at first
+    assert info["schedule"] == 3 and info["table_regrows"] >= 1
+    assert info["table_capacity"] == 1 << (table_log2 + info["table_regrows"])
+    gk, gc = r.kmers(0, 1)
+    np.testing.assert_array_equal(gk, tk)
+    np.testing.assert_array_equal(gc, tc)
+    seen, twice = r.bloom(0)
+    np.testing.assert_array_equal(seen, oseen)
+    np.testing.assert_array_equal(twice, otwice)
+    assert info["cutoff"] == ora.cutoff(tc, 5.0)
+    sk, _ = r.solid(0)
+    np.testing.assert_array_equal(r.edges(0), ora.edges(sk, k))
+
+
+@pytest.mark.parametrize("k", [55, 77])
+def test_many_large_buckets_sort(spk, ora, k):
+    """Lists with many top-bits buckets over their shared-memory size (40
+    eight-base prefixes with 3000 listed k-mers each): those buckets are
+    sorted together as one array, and the list and edges equal the oracle's."""
+    import os
+    from spk import synth
+    p = synth.c2(0.05).packed
+    rng = np.random.default_rng(11)
+    prefixes = rng.integers(0, 4, (40, 8), dtype=np.uint8)
+    prefixes[:, 0] = 0  # a leading A: mostly the canonical strand
+    rows = []
+    for pre in prefixes:
+        for _ in range(3000):
+            r = np.concatenate([pre, rng.integers(0, 4, k - 8, dtype=np.uint8)])
+            rows += [r, r]  # twice, so that the k-mer is listed (count >= 2)
+    d2, o2, l2 = _pack_codes(rows)
+    data = np.concatenate([p.data, d2])
+    offs = np.concatenate([p.offsets, o2 + np.uint64(p.data.size)])
+    lens = np.concatenate([p.lengths, l2])
+    bits = 1 << 26
+    ref = ora.count(data, offs, lens, k, bits, mode=ora.MODE_TWICE, keep_bloom=False,
+                    threads=os.cpu_count() or 1)
+    tk, tc = ref.table(2)
+    # the first eight bases: the top 16 bits of the key (Kmer256 keeps the
+    # first 64 bases of a k > 64 in its low half, limb 1 on top)
+    nl = nlimbs(k)
+    top = tk[:, 1] >> np.uint64(48) if k > 64 else tk[:, nl - 1] >> np.uint64(2 * k - 64 * (nl - 1) - 16)
+    _, sizes = np.unique(top, return_counts=True)
+    assert tk.shape[0] > (1 << 18) and int((sizes > 2048).sum()) >= 20
+    r = spk.count((data, offs, lens), [k], bloom_bits=bits)
+    assert r.info(0)["schedule"] == 3
+    gk, gc = r.kmers(0)
+    np.testing.assert_array_equal(gk, tk)
+    np.testing.assert_array_equal(gc, tc)
+    sk, _ = r.solid(0)
+    np.testing.assert_array_equal(r.edges(0), ora.edges(sk, k))
+
+
 @pytest.mark.parametrize("k", [31, 55, 77])
 def test_prior_contigs(spk, ora, k):
     """Prior and trusted contigs (src/assemble.rs:244-284) add their boost to
@@ -509,7 +585,7 @@ def test_table_view_needs_keep_table(spk):
     np.testing.assert_array_equal(a.edges(0), b.edges(0))
 
 
-@pytest.mark.parametrize("k", [21, 55])
+@pytest.mark.parametrize("k", [21, 55, 77])
 def test_span_groups_equal_one_pass(spk, ora, k):
     """Read sets too large for one partition pass are counted in groups of
     spans, one pass over the reads each (forced here with span_groups_log2):
