@@ -223,7 +223,8 @@ constexpr uint64_t kChunkedUploadMin = 32ull << 20;  // bytes of packed data
 constexpr int kUploadChunks = 4;
 
 int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t data_len,
-                 const uint64_t* offsets, const uint32_t* lengths, size_t n_reads, ReadsView* rv) {
+                 const uint64_t* offsets, const uint32_t* lengths, size_t n_reads, ReadsView* rv,
+                 bool chunked) {
   int rc;
   const size_t padded = ((data_len + 7) / 8) * 8 + 64;
   if ((rc = res->reads.alloc(padded, st))) return rc;
@@ -244,7 +245,8 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
   rv->data_len = data_len;
   rv->err = nullptr;
   rv->chunks = nullptr;
-  if (data_len < kChunkedUploadMin || n_reads < 2) return xfer_h2d(res->ctx, res->reads.p, data, data_len, st);
+  if (!chunked || data_len < kChunkedUploadMin || n_reads < 2)
+    return xfer_h2d(res->ctx, res->reads.p, data, data_len, st);
   // Large read sets: the data go up in kUploadChunks pieces on a copy stream,
   // so that the count's first pass works on the reads of a piece while the
   // next one is copied.  Reads [0, read_end[c]) end at least 64 bytes before
@@ -338,6 +340,12 @@ int spk_ctx_create(int device, spk_ctx** out) {
     uint64_t thr = ~0ULL;  // keep freed blocks cached in the pool
     e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
+#ifdef SPK_AB_POOL_NODEPS
+  if (e == cudaSuccess) {
+    int z = 0;
+    e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolReuseAllowInternalDependencies, &z);
+  }
+#endif
   // The hot kernels make random 8-32 byte accesses (Bloom words, table
   // slots); fetch only the 32-byte sector that was asked for.  This is a
   // limit of this process's context, not a device setting.
@@ -361,6 +369,12 @@ int spk_ctx_destroy(spk_ctx* ctx) {
   xfer_shutdown(ctx);
   ctx->scratch.release();
   cudaStreamSynchronize(ctx->stream);
+  for (cudaStream_t& s : ctx->batch_streams)
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+      s = nullptr;
+    }
   for (uint64_t* b : ctx->staging_all) cudaFreeHost(b);
   cudaStreamDestroy(ctx->own_stream);
   if (ctx->pool) cudaMemPoolTrimTo(ctx->pool, 0);
@@ -473,7 +487,7 @@ int spk_count(spk_ctx* ctx, const uint8_t* data, size_t data_len, const uint64_t
   if (!res) return SPK_E_OOM;
   res->opts = resolve_opts(opts);
   ReadsView rv;
-  rc = upload_reads(res, ctx->stream, data, data_len, offsets, lengths, n_reads, &rv);
+  rc = upload_reads(res, ctx->stream, data, data_len, offsets, lengths, n_reads, &rv, true);
   if (!rc) rc = count_pipeline(ctx, ctx->stream, rv, 0, ks, n_k, res->opts, res);
   if (res->chunks.n)  // the reads' buffer is freed after every piece has landed
     cudaStreamWaitEvent(ctx->stream, res->chunks.ready[res->chunks.n - 1], 0);

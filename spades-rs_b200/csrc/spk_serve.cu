@@ -25,7 +25,8 @@ struct Server {
 namespace spk {
 
 int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t data_len,
-                 const uint64_t* offsets, const uint32_t* lengths, size_t n_reads, ReadsView* rv);
+                 const uint64_t* offsets, const uint32_t* lengths, size_t n_reads, ReadsView* rv,
+                 bool chunked);
 
 static uint64_t next_pow2_u64(uint64_t x) {
   uint64_t p = 1;
@@ -121,7 +122,7 @@ int run_job(spk_ctx* ctx, const spk_job& j, const std::vector<uint32_t>& ks, voi
   if (!res->opts.bloom_bits) res->opts.bloom_bits = 512ULL << 20;
   if (!res->opts.list_min_count) res->opts.list_min_count = 2;
   ReadsView rv;
-  int rc = upload_reads(res, st, j.data, j.data_len, j.offsets, j.lengths, j.n_reads, &rv);
+  int rc = upload_reads(res, st, j.data, j.data_len, j.offsets, j.lengths, j.n_reads, &rv, true);
   if (!rc) rc = count_pipeline(ctx, st, rv, 0, ks.data(), (int)ks.size(), res->opts, res);
   if (res->chunks.n)  // the reads' buffer is freed after every piece has landed
     cudaStreamWaitEvent(st, res->chunks.ready[res->chunks.n - 1], 0);
