@@ -574,7 +574,7 @@ def run_c3(args, ctx, log_rank0):
 def batched_vs_plain(ctx, scale, steps, warmup, bloom_bits, log_rank0):
     """64 uneven samples (genome log-uniform 0.5-12 Mb x scale, GC 30-70%,
     20-200x, 0.5% errors, k=33) from the native generator, host buffers in
-    and solid lists out: spk_count_batch against spk_count on one sample
+    and solid lists out: the batch pipeline (spk_batch_start / spk_batch_next) against spk_count on one sample
     after another.  Returns the measurement as a dict."""
     import torch
     import spk
@@ -603,9 +603,10 @@ def batched_vs_plain(ctx, scale, steps, warmup, bloom_bits, log_rank0):
                 keep.append(sk)
 
     def batched(lat=None, keep=None):
+        # results handed out in job order as they finish (spk_batch_next), each
+        # downloaded while the samples after it still upload and count
         a = time.perf_counter()
-        rs = spk.count_batch([spk.Job(p, [33], dict(opts)) for p in packs], ctx=ctx)
-        for r in rs:
+        for _, r in spk.count_batch_iter([spk.Job(p, [33], dict(opts)) for p in packs], ctx=ctx):
             sk = r.solid(0)
             r.close()
             if lat is not None:
@@ -623,10 +624,12 @@ def batched_vs_plain(ctx, scale, steps, warmup, bloom_bits, log_rank0):
             fn(lat)
             torch.cuda.synchronize()
             out.append(time.perf_counter() - a)
-        return sum(out) / len(out)
+        return out
 
-    t_plain = timed(plain, lat_plain)
-    t_batch = timed(batched, lat_batch)
+    steps_plain = timed(plain, lat_plain)
+    steps_batch = timed(batched, lat_batch)
+    t_plain = sum(steps_plain) / len(steps_plain)
+    t_batch = sum(steps_batch) / len(steps_batch)
     # identical exact output: every sample's solid list, batched and alone
     kp, kb = [], []
     plain(keep=kp)
@@ -640,8 +643,10 @@ def batched_vs_plain(ctx, scale, steps, warmup, bloom_bits, log_rank0):
     return {"workload": f"64 samples, genome 0.5-12 Mb x {scale}, 20-200x, k=33, host buffers in, "
                         "solid lists out", "occurrences": occ,
             "value": _gk(occ, t_batch), "ms_per_step": t_batch * 1e3,
+            "step_ms": [round(x * 1e3, 1) for x in steps_batch],
             "plain": {"what": "spk_count on one sample after another", "value": _gk(occ, t_plain),
-                      "ms_per_step": t_plain * 1e3, "job_latency_ms": pct(lat_plain)},
+                      "ms_per_step": t_plain * 1e3, "step_ms": [round(x * 1e3, 1) for x in steps_plain],
+                      "job_latency_ms": pct(lat_plain)},
             "job_latency_ms": pct(lat_batch), "speedup_vs_plain": t_plain / t_batch,
             "identical_output": identical, "timing": "host clock around synchronised calls"}
 
@@ -653,7 +658,7 @@ def run_c4(args, ctx, log_rank0):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": b["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded; no public dataset)",
-            "config": {"workload": "c4: " + b["workload"] + "; spk_count_batch", "occurrences": b["occurrences"],
+            "config": {"workload": "c4: " + b["workload"] + "; spk_batch_start / spk_batch_next", "occurrences": b["occurrences"],
                        "bloom_bits": args.bloom_bits, "timing": b["timing"]},
             "plain": b["plain"], "job_latency_ms": b["job_latency_ms"],
             "speedup_vs_plain": b["speedup_vs_plain"], "identical_output": b["identical_output"]}
@@ -989,7 +994,7 @@ def main():
     # specified genome sizes (the full batch: --workload c4)
     batched = None
     if rank == 0 and not args.no_batched:
-        batched = batched_vs_plain(ctx, 0.1, 2, 3, args.bloom_bits, log)
+        batched = batched_vs_plain(ctx, 0.1, 5, 4, args.bloom_bits, log)
 
     # full-size parity of one more job against the oracle (rank 0 alone; every
     # rank counts the same reads)

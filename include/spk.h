@@ -387,10 +387,31 @@ typedef struct spk_job {
   spk_count_opts opts;
 } spk_job;
 
-/* Counts several independent read sets in one batched device pass (samples
- * of uneven size, each with its own Bloom and table).  results[i] receives
- * job i's result, identical to spk_count on that job alone. */
+/* Counts several independent read sets as one pipeline (samples of uneven
+ * size, each with its own Bloom and table): one host thread uploads the jobs'
+ * reads ahead on an upload stream while two lanes count them in order, so a
+ * job's copies overlap the counts before it.  results[i] receives job i's
+ * result, identical to spk_count on that job alone; if a job fails, every
+ * result is freed and its status is returned.  Replaces the serial per-sample
+ * (and per-k) loop of run_multik_assembly (src/multik.rs:109-178) for
+ * independent samples. */
 int spk_count_batch(spk_ctx* ctx, const spk_job* jobs, int n_jobs, spk_result** results);
+
+/* The same pipeline with the results handed out as they finish.
+ * spk_batch_start starts it (host buffers and the jobs array's contents must
+ * stay valid until spk_batch_end; the ks arrays are copied).  spk_batch_next
+ * waits for the next job in job order and hands over its result (the caller
+ * frees it with spk_result_free), so the caller's downloads of one result
+ * overlap the counts of the jobs after it; a failed job returns its status
+ * with *index set and no result, and the batch goes on.  After the last job
+ * it returns SPK_E_NOT_FOUND.  spk_batch_end waits for the batch's threads
+ * and frees the results never handed out.  One batch runs at a time on a
+ * context (a second spk_batch_start waits).  A batch result's later work
+ * (downloads, unitigs) runs on the batch's result stream, in call order. */
+typedef struct spk_batch spk_batch;
+int spk_batch_start(spk_ctx* ctx, const spk_job* jobs, int n_jobs, spk_batch** batch);
+int spk_batch_next(spk_batch* batch, int* index, spk_result** result);
+int spk_batch_end(spk_batch* batch);
 
 /* Serving loop.  spk_serve_start starts a scheduler thread that admits
  * submitted jobs while their estimated HBM need fits in hbm_budget_bytes

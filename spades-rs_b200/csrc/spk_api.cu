@@ -340,12 +340,6 @@ int spk_ctx_create(int device, spk_ctx** out) {
     uint64_t thr = ~0ULL;  // keep freed blocks cached in the pool
     e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
-#ifdef SPK_AB_POOL_NODEPS
-  if (e == cudaSuccess) {
-    int z = 0;
-    e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolReuseAllowInternalDependencies, &z);
-  }
-#endif
   // The hot kernels make random 8-32 byte accesses (Bloom words, table
   // slots); fetch only the 32-byte sector that was asked for.  This is a
   // limit of this process's context, not a device setting.

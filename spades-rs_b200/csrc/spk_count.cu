@@ -3643,6 +3643,12 @@ static void rehome(KResult& kr, cudaStream_t s) {
   for (DevBuf& b : kr.list) b.st = s;
   for (DevBuf& b : kr.edges) b.st = s;
 }
+// Every buffer of a finished result (its work on its old stream ordered
+// before `s`): frees go to `s` from now on.
+void rehome_result(spk_result* res, cudaStream_t s) {
+  for (auto& kr : res->ks) rehome(*kr, s);
+  res->reads.st = res->offs.st = res->lens.st = s;
+}
 
 // One k: the job with few round trips where it applies, else (or after an
 // overflow there) the general one.

@@ -192,6 +192,8 @@ struct spk_ctx {
   // a batch that gave every job streams of its own).
   cudaStream_t batch_streams[4] = {};
   std::mutex batch_mu;  // one batch at a time per context
+  std::condition_variable batch_cv;
+  bool batch_active = false;
 };
 
 struct spk_bloom {

@@ -21,7 +21,7 @@ from ._lib import (SPK_F_CORRECT, SPK_F_DIRECT, SPK_F_EDGES, SPK_F_GATED, SPK_F_
                    SPK_SCHEDULE_COUNT_FIRST, SPK_SCHEDULE_FUSED, SPK_SCHEDULE_GATED,
                    SPK_SCHEDULE_PARTITIONED, SpkError, lib, lib_path, validate_k)
 from .api import (Context, CountResult, DevicePackedReads, Job, PackedReads, Server, TwoTierFilter, count,
-                  count_batch, count_device, count_solid_kmers, default_context, ingest, kmer256_from_limbs,
+                  count_batch, count_batch_iter, count_device, count_solid_kmers, default_context, ingest, kmer256_from_limbs,
                   limbs_from_kmer256, nlimbs)
 
 __all__ = [
@@ -30,6 +30,6 @@ __all__ = [
     "SPK_SCHEDULE_COUNT_FIRST", "SPK_SCHEDULE_FUSED", "SPK_SCHEDULE_GATED", "SPK_SCHEDULE_PARTITIONED",
     "SpkError", "lib", "lib_path",
     "validate_k", "Context", "CountResult", "DevicePackedReads", "Job", "PackedReads", "Server",
-    "TwoTierFilter", "count", "count_batch", "count_device", "count_solid_kmers", "default_context", "ingest",
+    "TwoTierFilter", "count", "count_batch", "count_batch_iter", "count_device", "count_solid_kmers", "default_context", "ingest",
     "kmer256_from_limbs", "limbs_from_kmer256", "nlimbs",
 ]

@@ -130,6 +130,9 @@ _SIGS = [
                                      u64p]),
     ("spk_result_free", C.c_int, [vp]),
     ("spk_count_batch", C.c_int, [vp, C.POINTER(JobC), C.c_int, C.POINTER(vp)]),
+    ("spk_batch_start", C.c_int, [vp, C.POINTER(JobC), C.c_int, C.POINTER(vp)]),
+    ("spk_batch_next", C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(vp)]),
+    ("spk_batch_end", C.c_int, [vp]),
     ("spk_serve_start", C.c_int, [vp, C.c_uint64, C.c_int]),
     ("spk_serve_stop", C.c_int, [vp]),
     ("spk_job_hbm_estimate", C.c_int, [C.POINTER(JobC), u64p]),

@@ -528,11 +528,30 @@ class Job:
 
 
 def count_batch(jobs: List[Job], ctx: Optional[Context] = None) -> List[CountResult]:
+    """spk_count_batch: every job's result, each identical to count() on that job alone."""
     ctx = ctx or default_context()
     cj = (JobC * len(jobs))(*[j.to_c() for j in jobs])
     outs = (vp * len(jobs))()
     check(lib().spk_count_batch(ctx.h, cj, len(jobs), outs))
     return [CountResult(outs[i], ctx) for i in range(len(jobs))]
+
+
+def count_batch_iter(jobs: List[Job], ctx: Optional[Context] = None):
+    """spk_batch_start / spk_batch_next / spk_batch_end: yields (index,
+    result) in job order as each job finishes, while the jobs after it are
+    still uploading and counting.  A failed job raises SpkError (the batch is
+    ended, and the results not yet yielded are freed)."""
+    ctx = ctx or default_context()
+    cj = (JobC * len(jobs))(*[j.to_c() for j in jobs])
+    b = vp()
+    check(lib().spk_batch_start(ctx.h, cj, len(jobs), C.byref(b)))
+    try:
+        for _ in range(len(jobs)):
+            i, r = C.c_int(-1), vp()
+            check(lib().spk_batch_next(b, C.byref(i), C.byref(r)))
+            yield i.value, CountResult(r.value, ctx)
+    finally:
+        lib().spk_batch_end(b)
 
 
 class Server:

@@ -69,6 +69,42 @@ def test_batch_reports_the_failing_job(spk, samples):
 
 def test_empty_batch(spk):
     assert spk.count_batch([]) == []
+    assert list(spk.count_batch_iter([])) == []
+
+
+def test_streamed_batch_equals_one_at_a_time(spk, samples):
+    """spk_batch_next hands the results out in job order as they finish; each
+    is downloaded while the jobs after it still count, and equals count()
+    on its sample alone."""
+    ks = [[33], [55], [21, 33], [33], [55], [77]]
+    jobs = [spk.Job(p, k, dict(OPTS)) for p, k in zip(samples, ks)]
+    seen = []
+    for i, r in spk.count_batch_iter(jobs):
+        seen.append(i)
+        same_result(r, spk.count(samples[i], ks[i], **OPTS), len(ks[i]))
+        r.close()
+    assert seen == list(range(len(jobs)))
+
+
+def test_streamed_batch_goes_on_after_a_failed_job(spk, samples):
+    """A job that fails raises at its turn; the results handed out before it
+    stay valid, and the batch ends cleanly."""
+    good = spk.Job(samples[0], [33], dict(OPTS))
+    d, o, l = samples[3].data, samples[3].offsets.copy(), samples[3].lengths
+    o[-1] = d.size + 100
+    bad = spk.Job((d, o, l), [33], dict(OPTS))
+    got = []
+    with pytest.raises(spk.SpkError) as e:
+        for i, r in spk.count_batch_iter([good, bad, good]):
+            got.append((i, r))
+    assert e.value.code == 1 and "job 1" in str(e.value)
+    assert [i for i, _ in got] == [0]
+    same_result(got[0][1], spk.count(samples[0], [33], **OPTS), 1)
+    got[0][1].close()
+    # the context takes a new batch afterwards
+    r = spk.count_batch([good])[0]
+    same_result(r, spk.count(samples[0], [33], **OPTS), 1)
+    r.close()
 
 
 def test_multik_concurrent_equals_single_k(spk, samples):
