@@ -996,65 +996,158 @@ __global__ void k_coarse_chunks(CoarseView cv, uint32_t chunk, uint32_t* __restr
   if (lane == 31) cfirst[kCoarse] = x;
 }
 
+// ---- bulk copies into shared memory (the fine pass's staged chunks) ----
+// One thread issues cp.async.bulk (the TMA's untiled copy: 16-byte aligned
+// addresses, a multiple of 16 bytes) from this GPU's global memory into the
+// CTA's shared memory, completing on an mbarrier; the threads wait on the
+// barrier's phase with a bounded number of polls.  No multicast.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Orders this thread's earlier generic-proxy accesses of shared memory (after
+// a barrier: the CTA's) before later bulk-copy writes into it.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* m) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(m))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Polls of a staged copy's barrier before the kernel gives up (a copy of a
+// chunk takes microseconds; this is tens of milliseconds).
+constexpr uint32_t kStageSpinLimit = 1u << 20;
+constexpr uint32_t kErrStage = 32;  // a staged copy never completed (the job fails)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t parity) {
+  for (uint32_t i = 0; i < kStageSpinLimit; i++)
+    if (mbar_try_wait(m, parity)) return true;
+  return false;
+}
+
 template <int NL>
 size_t fine_smem(uint32_t nfine) {
   constexpr uint32_t kChunk = fine_chunk<NL>();
-  return (size_t)kChunk * NL * 8 * 2 + (size_t)kChunk * (2 + 2 + 2) + (size_t)nfine * (8 + 4 + 4) + 64;
+  // two chunk buffers, then per key: span, rank, sorted slot, span of a sorted position
+  return (size_t)kChunk * NL * 8 * 2 + (size_t)kChunk * (2 + 2 + 2 + 2) + (size_t)nfine * (8 + 4 + 4) + 64;
 }
 
+// Chunk c of the coarse buckets: its bucket, first key and length.
+struct FineChunkAt {
+  uint32_t b;
+  uint64_t s0;
+  uint32_t n;
+};
+__device__ __forceinline__ FineChunkAt fine_chunk_at(const CoarseView& cv, const uint32_t* cfirst, uint32_t c,
+                                                     uint32_t chunk) {
+  uint32_t b = 0;  // cfirst[b] <= c < cfirst[b + 1]
+  for (uint32_t step = kCoarse >> 1; step; step >>= 1)
+    if (cfirst[b + step] <= c) b += step;
+  const uint64_t bb = coarse_base(cv, b);
+  const uint64_t bend = bb + coarse_len(cv, b);
+  const uint64_t s0 = bb + (uint64_t)(c - cfirst[b]) * chunk;
+  return FineChunkAt{b, s0, (uint32_t)min((uint64_t)chunk, bend - s0)};
+}
+
+// k_part_fine: chunks of each coarse bucket (kFineChunk keys) are sorted by
+// span and written to the span regions.  Each CTA walks its chunks with two
+// shared-memory buffers: while it ranks and writes out one chunk, the bulk
+// copy of its next chunk lands in the other buffer (a chunk whose start or
+// size is not a multiple of 16 bytes is loaded by the threads instead).  The
+// keys are ranked within their span, and the write-out reads them in span
+// order through a permutation, so every global store is part of a contiguous
+// run of one span.
 template <int NL>
 __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, const uint32_t* __restrict__ cfirst,
                                                              PartView pv, unsigned k) {
   extern __shared__ __align__(16) unsigned char fs_smem[];
   constexpr uint32_t kFineChunk = fine_chunk<NL>();
   const uint32_t fbits = pv.log2parts - pv.log2groups - kCoarseBits, nfine = 1u << fbits;
-  uint64_t* ks = (uint64_t*)fs_smem;
-  uint64_t* ss = ks + kFineChunk * NL;
-  unsigned long long* gbase = (unsigned long long*)(ss + kFineChunk * NL);
+  uint64_t* const kbuf0 = (uint64_t*)fs_smem;
+  uint64_t* const kbuf1 = kbuf0 + kFineChunk * NL;
+  unsigned long long* gbase = (unsigned long long*)(kbuf1 + kFineChunk * NL);
   uint32_t* hist = (uint32_t*)(gbase + nfine);
   uint32_t* start = hist + nfine;
   uint16_t* fb = (uint16_t*)(start + nfine);  // span (in the bucket) of a loaded key
   uint16_t* rk = fb + kFineChunk;             // its rank in that span
-  uint16_t* sf = rk + kFineChunk;             // span of a sorted position
+  uint16_t* perm = rk + kFineChunk;           // the loaded key at a sorted position
+  uint16_t* sf = perm + kFineChunk;           // span of a sorted position
   __shared__ uint32_t wsum[kFineBlock / 32];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t staged[2];  // the chunk in buffer i comes by bulk copy
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t nchunks = cfirst[kCoarse];
-  for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
-    uint32_t b = 0;  // cfirst[b] <= c < cfirst[b + 1]
-    for (uint32_t step = kCoarse >> 1; step; step >>= 1)
-      if (cfirst[b + step] <= c) b += step;
-    const uint64_t bb = coarse_base(cv, b);
-    const uint64_t bend = bb + coarse_len(cv, b);
-    const uint64_t s0 = bb + (uint64_t)(c - cfirst[b]) * kFineChunk;
-    const uint32_t n = (uint32_t)min((uint64_t)kFineChunk, bend - s0);
+  // (thread 0) the bulk copy of chunk c into buffer i, if its bytes allow one
+  auto issue = [&](uint32_t c, int i) {
+    const FineChunkAt ch = fine_chunk_at(cv, cfirst, c, kFineChunk);
+    const uint64_t* src = cv.keys + ch.s0 * NL;
+    const uint32_t bytes = ch.n * (uint32_t)(NL * 8);
+    const bool ok = ((uintptr_t)src & 15) == 0 && (bytes & 15) == 0 && bytes > 0;
+    staged[i] = ok;
+    if (ok) {
+      fence_proxy_async_smem();  // the buffer's last chunk was read before the barrier
+      bulk_g2s(i ? kbuf1 : kbuf0, src, bytes, &mbar[i]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    fence_mbar_init();
+    staged[0] = staged[1] = 0;
+    if (blockIdx.x < nchunks) issue(blockIdx.x, 0);
+  }
+  __syncthreads();
+  uint32_t ph0 = 0, ph1 = 0;  // phase to wait for on each buffer's barrier
+  int buf = 0;
+  for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x, buf ^= 1) {
+    // the next chunk's copy into the other buffer, whose chunk was finished
+    // before the barrier that ended the last round
+    if (threadIdx.x == 0 && c + gridDim.x < nchunks) issue(c + gridDim.x, buf ^ 1);
+    const FineChunkAt ch = fine_chunk_at(cv, cfirst, c, kFineChunk);
+    const uint32_t b = ch.b, n = ch.n;
+    uint64_t* ks = buf ? kbuf1 : kbuf0;
     for (uint32_t f = threadIdx.x; f < nfine; f += blockDim.x) hist[f] = 0;
-    __syncthreads();
-    {
-      // every key of this thread loaded before any is processed
-      constexpr int PER = kFineChunk / kFineBlock;
-      Seq<NL> C[PER];
-#pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const uint32_t j = threadIdx.x + q * kFineBlock;
-        if (j >= n) continue;
-        C[q] = key_get_cs<NL>(cv.keys, s0 + j);
+    bool ok = true;
+    if (staged[buf]) {
+      ok = mbar_wait_bounded(&mbar[buf], buf ? ph1 : ph0);
+      if (buf) ph1 ^= 1;
+      else ph0 ^= 1;
+    } else {
+      for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) key_put<NL>(ks, j, key_get_cs<NL>(cv.keys, ch.s0 + j));
+    }
+    if (__syncthreads_or(!ok)) {
+      // A copy that never completed: report it, give the other buffer's copy
+      // (if one was issued) a bounded wait, and stop.
+      if (threadIdx.x == 0) {
+        atomicOr(pv.err, (int)kErrStage);
+        if (c + gridDim.x < nchunks && staged[buf ^ 1]) mbar_wait_bounded(&mbar[buf ^ 1], buf ? ph0 : ph1);
       }
-#pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const uint32_t j = threadIdx.x + q * kFineBlock;
-        if (j >= n) continue;
-        key_put<NL>(ks, j, C[q]);
-        if (pv.packed_home) C[q].v[NL - 1] &= ~0ULL >> kHomeBits;
-        uint64_t w4[4];
-        kmer256_limbs<NL>(C[q], k, w4);
-        const uint32_t p = (uint32_t)(hash_seed(hash_pre(w4), kSeed1) >> (64 - pv.log2parts));
-        const uint32_t f = p & (nfine - 1);
-        fb[j] = (uint16_t)f;
-        rk[j] = (uint16_t)atomicAdd(&hist[f], 1u);
-      }
+      return;
+    }
+    // rank every key within its span
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+      Seq<NL> C = key_get<NL>(ks, j);
+      if (pv.packed_home) C.v[NL - 1] &= ~0ULL >> kHomeBits;
+      uint64_t w4[4];
+      kmer256_limbs<NL>(C, k, w4);
+      const uint32_t p = (uint32_t)(hash_seed(hash_pre(w4), kSeed1) >> (64 - pv.log2parts));
+      const uint32_t f = p & (nfine - 1);
+      fb[j] = (uint16_t)f;
+      rk[j] = (uint16_t)atomicAdd(&hist[f], 1u);
     }
     __syncthreads();
-    // exclusive scan of hist (each thread a run of consecutive spans)
+    // exclusive scan of hist (each thread a run of consecutive spans), and
+    // one reservation per span in its region
     const uint32_t per = (nfine + blockDim.x - 1) / blockDim.x;
     const uint32_t f0 = min(nfine, threadIdx.x * per), f1 = min(nfine, f0 + per);
     uint32_t run = 0;
@@ -1080,7 +1173,7 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
       const uint32_t f = fb[j];
       const uint32_t pos = start[f] + rk[j];
-      key_copy<NL>(ss, pos, ks, j);
+      perm[pos] = (uint16_t)j;
       sf[pos] = (uint16_t)f;
     }
     __syncthreads();
@@ -1090,7 +1183,7 @@ __global__ void __launch_bounds__(kFineBlock, 2) k_part_fine(CoarseView cv, cons
       const uint64_t gi = gbase[f] + (j - start[f]);
       const uint64_t end = pv.uniform ? (uint64_t)(pg + 1) * pv.uniform : pv.base[pg + 1];
       if (gi < end) {
-        key_copy<NL>(pv.keys, gi, ss, j);
+        key_put<NL>(pv.keys, gi, key_get<NL>(ks, perm[j]));
       } else {
         atomicOr(pv.err, (int)kErrRegion);
       }
@@ -2725,6 +2818,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
     if ((int)host[S_ERR] & 4)
       return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
     if ((int)host[S_ERR] & 2) return fail(SPK_E_TIMEOUT, "count table: claim wait timed out");
+    if ((int)host[S_ERR] & (int)kErrStage) return fail(SPK_E_TIMEOUT, "partition: a staged copy never completed");
     return SPK_OK;
   };
 
@@ -2795,7 +2889,7 @@ int count_one_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& 
         // ---- coarse buckets, then spans (k_part_coarse, k_part_fine) ----
         DevBuf cbase, cfill, cregion, cfirst;
         const uint64_t cper = occ0 / kCoarse;
-        const uint64_t ccap = cper + (cper >> 3) + 8192;
+        const uint64_t ccap = (cper + (cper >> 3) + 8192 + 1) & ~1ULL;  // even: chunks start 16-byte aligned
         if ((rc = cbase.alloc((kCoarse + 1) * 8, st)) || (rc = cfill.alloc(kCoarse * 4 * kFillStride, st)) ||
             (rc = cregion.alloc(kCoarse * ccap * nl * 8, st)) || (rc = cfirst.alloc((kCoarse + 1) * 4, st)))
           return rc;
@@ -3406,7 +3500,7 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   k_part_uniform<<<64, kBlock, 0, st>>>((uint32_t)nparts_g, capu, base.as<uint64_t>());
   DevBuf cbase, cfill, cregion, cfirst;
   const uint64_t cper = (occ0 >> lg) / kCoarse;
-  const uint64_t ccap = cper + (cper >> 3) + 8192;
+  const uint64_t ccap = (cper + (cper >> 3) + 8192 + 1) & ~1ULL;  // even: chunks start 16-byte aligned
   if ((rc = cbase.alloc((kCoarse + 1) * 8, st)) || (rc = cfill.alloc(kCoarse * 4 * kFillStride, st)) ||
       (rc = cregion.alloc(kCoarse * ccap * nl * 8, st)) || (rc = cfirst.alloc((kCoarse + 1) * 4, st)))
     return rc;
@@ -3518,6 +3612,8 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   SPK_CUDA(cudaStreamSynchronize(st));
   const int err = (int)host[S_ERR];
   if (err & 4) return fail(SPK_E_INVALID_ARG, "a read extends past the end of the packed data");
+  if (err & 2) return fail(SPK_E_TIMEOUT, "count table: claim wait timed out");
+  if (err & (int)kErrStage) return fail(SPK_E_TIMEOUT, "partition: a staged copy never completed");
   if (err & (kErrRegion | kErrRange)) return kRedo;  // an overflowed region
   if (err & 1) return kGrow;                           // a span with more distinct k-mers than slots
   info.occurrences = host[S_OCC];
