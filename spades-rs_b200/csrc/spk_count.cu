@@ -801,10 +801,13 @@ __global__ void __launch_bounds__(kBlock) k_part_scatter(ReadsView R, unsigned k
 constexpr uint32_t kCoarseBits = 6;
 constexpr uint32_t kCoarse = 1u << kCoarseBits;
 constexpr int kCoarseBlock = 512;
-// windows per thread per round: the tile (keys twice over) stays within half
-// an SM's shared memory, so two CTAs share an SM
+// windows per thread per round: the tile (its keys, and a bucket, rank and
+// sorted slot per key) stays within half an SM's shared memory, so two CTAs
+// share an SM
+// (4,096 keys for k <= 64: 2.90 -> 2.57 ms at k = 55 against 2,048, and
+// 3.19 -> 2.75 at k = 21; 24-byte keys keep 2,048, which leaves two CTAs)
 template <int NL>
-constexpr int coarse_w() { return NL <= 3 ? 4 : 2; }
+constexpr int coarse_w() { return NL <= 2 ? 8 : 4; }
 template <int NL>
 constexpr uint32_t coarse_slots() { return kCoarseBlock * coarse_w<NL>(); }
 constexpr int kFineBlock = 512;
@@ -832,7 +835,7 @@ __device__ __forceinline__ uint64_t region_base(const PartView& pv, uint32_t p) 
 template <int NL>
 size_t coarse_smem() {
   constexpr uint32_t kSlots = coarse_slots<NL>();
-  return (size_t)kSlots * NL * 8 * 2 + kSlots * (1 + 1 + 2) + kCoarse * (4 + 4 + 8);
+  return (size_t)kSlots * NL * 8 + kSlots * (1 + 1 + 2 + 2) + kCoarse * (4 + 4 + 8);
 }
 
 template <int NL>
@@ -843,12 +846,12 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
   constexpr uint32_t kCoarseSlots = coarse_slots<NL>();
   constexpr int kCoarseW = coarse_w<NL>();
   uint64_t* ks = (uint64_t*)cs_smem;                       // keys by slot
-  uint64_t* ss = ks + kCoarseSlots * NL;                   // keys sorted by bucket
-  unsigned long long* gbase = (unsigned long long*)(ss + kCoarseSlots * NL);
+  unsigned long long* gbase = (unsigned long long*)(ks + kCoarseSlots * NL);
   uint32_t* hist = (uint32_t*)(gbase + kCoarse);
   uint32_t* start = hist + kCoarse;
   uint16_t* rk = (uint16_t*)(start + kCoarse);             // rank of a slot in its bucket
-  uint8_t* bk = (uint8_t*)(rk + kCoarseSlots);             // bucket of a slot (0xFF: none)
+  uint16_t* perm = rk + kCoarseSlots;                      // slot of a sorted position
+  uint8_t* bk = (uint8_t*)(perm + kCoarseSlots);           // bucket of a slot (0xFF: none)
   uint8_t* sb = bk + kCoarseSlots;                         // bucket of a sorted position
   const unsigned topsh = 2 * k - 2 - 64 * (NL - 1);
   const uint64_t topmask = (2 * k - 64 * (NL - 1)) >= 64 ? ~0ULL : ((1ULL << (2 * k - 64 * (NL - 1))) - 1);
@@ -949,7 +952,7 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
         const uint8_t b = bk[slot];
         if (b == 0xFF) continue;
         const uint32_t pos = start[b] + rk[slot];
-        key_copy<NL>(ss, pos, ks, slot);
+        perm[pos] = (uint16_t)slot;
         sb[pos] = b;
       }
       __syncthreads();
@@ -960,7 +963,7 @@ __global__ void __launch_bounds__(kCoarseBlock, 2) k_part_coarse(ReadsView R, un
         const uint64_t gi = gbase[b] + (j - start[b]);
         const uint64_t end = cv.uniform ? (uint64_t)(b + 1) * cv.uniform : cv.base[b + 1];
         if (gi < end) {
-          key_copy<NL>(cv.keys, gi, ss, j);
+          key_copy<NL>(cv.keys, gi, ks, perm[j]);
         } else {
           atomicOr(cv.err, (int)kErrRegion);
         }
