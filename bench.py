@@ -966,7 +966,8 @@ def main():
     achieved = kbytes / (kms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "dram_traffic_c2_k55.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and args.scale == 1.0 and K == 55:
+        # captured on the full-size k=55 job only
         with open(tpath) as f:
             traffic = json.load(f).get(kname)
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
