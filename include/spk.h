@@ -414,9 +414,11 @@ int spk_batch_next(spk_batch* batch, int* index, spk_result** result);
 int spk_batch_end(spk_batch* batch);
 
 /* Serving loop.  spk_serve_start starts a scheduler thread that admits
- * submitted jobs while their estimated HBM need fits in hbm_budget_bytes
- * (0 = 90% of the device memory free at start) and at most max_inflight jobs
- * run concurrently on separate streams. */
+ * submitted jobs in arrival order while at most max_inflight run, each on its
+ * own stream: jobs run side by side while their estimated HBM needs together
+ * stay within an eighth of hbm_budget_bytes (0 = 90% of the device memory
+ * free at start), a job that needs more runs alone, and a job that needs more
+ * than the whole budget is refused (SPK_E_ADMISSION). */
 int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight);
 int spk_serve_stop(spk_ctx* ctx);
 /* Estimated device bytes a job needs (Bloom + table + reads + outputs). */

@@ -15,6 +15,7 @@
 // frees (with the deleter given at construction) the results of finished jobs
 // nobody waits for, so tickets never collected do not leak their results.
 #pragma once
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstdint>
@@ -47,10 +48,14 @@ class Scheduler {
  public:
   enum { kAdmissionError = 8 /* SPK_E_ADMISSION */ };
 
-  // free_result: how to free the result of a job nobody collected (may be empty).
-  Scheduler(uint64_t budget, int max_inflight, std::function<void(void*)> free_result = nullptr)
-      : budget_(budget), max_inflight_(max_inflight < 1 ? 1 : max_inflight),
-        free_result_(std::move(free_result)) {
+  // free_result: how to free the result of a job nobody collected (may be
+  // empty).  shared_budget (0: the whole budget): jobs run side by side only
+  // while their needs together stay within it; a job that needs more than it
+  // runs alone (see submit).
+  Scheduler(uint64_t budget, int max_inflight, std::function<void(void*)> free_result = nullptr,
+            uint64_t shared_budget = 0)
+      : budget_(budget), shared_budget_(shared_budget ? std::min(shared_budget, budget) : budget),
+        max_inflight_(max_inflight < 1 ? 1 : max_inflight), free_result_(std::move(free_result)) {
     thread_ = std::thread([this] { loop(); });
   }
   ~Scheduler() {
@@ -97,12 +102,13 @@ class Scheduler {
   // exclusive: the job is admitted only when no other job runs, and no other
   // job is admitted while it runs (jobs of a large share of the budget, whose
   // neighbours would fragment the memory they need).
+  // A job that needs more than the shared budget is exclusive too.
   uint64_t submit(uint64_t need, std::function<int(void**, std::string*)> run, bool exclusive = false) {
     std::unique_lock<std::mutex> l(mu_);
     auto j = std::make_shared<SchedJob>();
     j->ticket = ++next_ticket_;
     j->need = need;
-    j->exclusive = exclusive;
+    j->exclusive = exclusive || need > shared_budget_;
     j->run = std::move(run);
     j->t_submit = std::chrono::steady_clock::now();
     jobs_[j->ticket] = j;
@@ -172,7 +178,7 @@ class Scheduler {
         if (stopping_) return true;
         if (queue_.empty() || inflight_ >= max_inflight_ || exclusive_running_) return false;
         const auto& f = queue_.front();
-        return f->exclusive ? inflight_ == 0 : in_use_ + f->need <= budget_;
+        return f->exclusive ? inflight_ == 0 : (inflight_ == 0 || in_use_ + f->need <= shared_budget_);
       });
       if (stopping_) break;
       auto j = queue_.front();
@@ -207,6 +213,7 @@ class Scheduler {
   std::map<uint64_t, std::shared_ptr<SchedJob>> jobs_;
   std::thread thread_;
   uint64_t budget_;
+  uint64_t shared_budget_;
   uint64_t in_use_ = 0;
   uint64_t next_ticket_ = 0;
   int max_inflight_;

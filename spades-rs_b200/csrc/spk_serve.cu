@@ -175,8 +175,13 @@ int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight) {
   if (!hbm_budget_bytes) hbm_budget_bytes = (uint64_t)(usable_device_memory(ctx) * 0.9);
   auto* s = new Server();
   s->budget = hbm_budget_bytes;
+  // Jobs run side by side only while together they need at most an eighth
+  // of the budget; a larger job runs alone (two jobs of 20-40 GB side by side
+  // took 5-40 times their time alone: the memory pool maps new memory for one
+  // while the other's buffers are in use).
   s->sched = std::make_shared<Scheduler>(hbm_budget_bytes, max_inflight > 0 ? max_inflight : 4,
-                                         [](void* r) { spk_result_free((spk_result*)r); });
+                                         [](void* r) { spk_result_free((spk_result*)r); },
+                                         hbm_budget_bytes / 8);
   ctx->server = s;
   return SPK_OK;
 }
@@ -203,7 +208,7 @@ int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket) {
     const int rc = run_job(ctx, j, ks, out);
     if (rc) *msg = spk_last_error();
     return rc;
-  }, need > ctx->server->budget / 4);  // a large job runs alone
+  });
   return SPK_OK;
 }
 

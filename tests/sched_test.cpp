@@ -177,9 +177,45 @@ static void exclusive_runs_alone() {
   CHECK(s.peak_inflight() >= 2);  // the small ones did share the device
 }
 
+// With a shared budget, jobs run side by side only while their needs
+// together fit it, and a job above it runs alone.
+static void shared_budget_pairs() {
+  std::atomic<int> running{0}, peak{0}, overlap_with_big{0};
+  std::atomic<bool> big_running{false};
+  Scheduler s(100, 8, nullptr, 20);
+  std::vector<uint64_t> t;
+  auto job = [&](void** out, std::string*) {
+    const int r = ++running;
+    int p = peak.load();
+    while (r > p && !peak.compare_exchange_weak(p, r)) {
+    }
+    if (big_running) overlap_with_big++;
+    std::this_thread::sleep_for(15ms);
+    running--;
+    *out = nullptr;
+    return 0;
+  };
+  for (int i = 0; i < 6; i++) t.push_back(s.submit(8, job));  // two of them fit 20 at a time
+  t.push_back(s.submit(30, [&](void**, std::string*) {        // above 20: alone
+    if (running.load() != 0) overlap_with_big++;
+    big_running = true;
+    std::this_thread::sleep_for(20ms);
+    big_running = false;
+    return 0;
+  }));
+  for (int i = 0; i < 2; i++) t.push_back(s.submit(8, job));
+  for (auto x : t) {
+    int st = -1;
+    CHECK(s.wait(x, -1, &st, nullptr, nullptr) == 1 && st == 0);
+  }
+  CHECK(peak.load() == 2);
+  CHECK(overlap_with_big.load() == 0);
+}
+
 int main() {
   admission();
   exclusive_runs_alone();
+  shared_budget_pairs();
   error_message();
   waiter_survives_stop();
   uncollected_results_freed();
