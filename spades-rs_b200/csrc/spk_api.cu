@@ -183,6 +183,38 @@ void staging_release(spk_ctx* ctx, uint64_t* block) {
   std::lock_guard<std::mutex> l(ctx->staging_mu);
   ctx->staging_free.push_back(block);
 }
+void pool_reserve(spk_ctx* ctx, uint64_t bytes) {
+  if (!ctx->pool) return;
+  std::lock_guard<std::mutex> l(ctx->pool_mu);
+  if (bytes <= ctx->pool_reserved) return;
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaMemPoolTrimTo(ctx->pool, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  size_t f = 0, t = 0;
+  if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  const uint64_t room = (uint64_t)f > (1ull << 30) ? (uint64_t)f - (1ull << 30) : 0;  // leave 1 GiB to others
+  const uint64_t n = std::min<uint64_t>(bytes, room);
+  // (a request the device cannot hold in full is not retried until a larger one comes)
+  ctx->pool_reserved = bytes;
+  if (n < (2ull << 20)) return;
+  void* p = nullptr;
+  cudaStream_t st = ctx->own_stream;
+  if (cudaMallocAsync(&p, n, st) != cudaSuccess || cudaFreeAsync(p, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    cudaGetLastError();  // a hint: without it the pool grows as the jobs need
+}
+
+void pool_trim(spk_ctx* ctx) {
+  if (!ctx->pool) return;
+  std::lock_guard<std::mutex> l(ctx->pool_mu);
+  cudaMemPoolTrimTo(ctx->pool, 0);
+  ctx->pool_reserved = 0;
+}
+
 spk_result* result_new(spk_ctx* ctx, cudaStream_t st, bool own_stream) {
   uint64_t* h = staging_acquire(ctx);
   if (!h) {
@@ -371,7 +403,7 @@ int spk_ctx_destroy(spk_ctx* ctx) {
     }
   for (uint64_t* b : ctx->staging_all) cudaFreeHost(b);
   cudaStreamDestroy(ctx->own_stream);
-  if (ctx->pool) cudaMemPoolTrimTo(ctx->pool, 0);
+  pool_trim(ctx);
   delete ctx;
   return SPK_OK;
 }

@@ -194,6 +194,10 @@ struct spk_ctx {
   std::mutex batch_mu;  // one batch at a time per context
   std::condition_variable batch_cv;
   bool batch_active = false;
+  // Bytes of the one contiguous block the memory pool was last grown by
+  // (spk::pool_reserve); 0 after the pool gave its cached memory back.
+  uint64_t pool_reserved = 0;
+  std::mutex pool_mu;
 };
 
 struct spk_bloom {
@@ -231,6 +235,18 @@ uint64_t* staging_acquire(spk_ctx* ctx);
 void staging_release(spk_ctx* ctx, uint64_t* block);
 // A new result on stream st with its own staging block, or nullptr (error set).
 spk_result* result_new(spk_ctx* ctx, cudaStream_t st, bool own_stream);
+// Grows the device memory pool by one contiguous block of at least `bytes`
+// (capped by what the device has free), unless the last such block is as
+// large already.  Jobs whose buffers come and go in sizes the pool has not
+// seen make it map new memory piece by piece, in the middle of their kernels'
+// work (about 8 ms per GB, and more when the pieces are fragmented); one
+// block mapped up front serves them all.  It waits for the whole device and
+// gives the pool's unused memory back first, so the caller makes sure no job
+// of the context is running.
+void pool_reserve(spk_ctx* ctx, uint64_t bytes);
+// The pool's cached memory given back (a job that ran out of memory runs
+// again): the reservation is gone too.
+void pool_trim(spk_ctx* ctx);
 // Count pipeline on device-resident reads (spk_count.cu).  `res` is filled
 // with one KResult per k.
 int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t max_len,

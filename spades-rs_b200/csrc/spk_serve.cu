@@ -179,6 +179,11 @@ int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight) {
   // of the budget; a larger job runs alone (two jobs of 20-40 GB side by side
   // took 5-40 times their time alone: the memory pool maps new memory for one
   // while the other's buffers are in use).
+  // The jobs that run side by side share one block of the pool, mapped here
+  // (twice their shared budget: their estimates leave out the list sort's
+  // and the edges' temporaries, and blocks freed by one job in the middle of
+  // another's are reused only once both are done).
+  pool_reserve(ctx, hbm_budget_bytes / 4);
   s->sched = std::make_shared<Scheduler>(hbm_budget_bytes, max_inflight > 0 ? max_inflight : 4,
                                          [](void* r) { spk_result_free((spk_result*)r); },
                                          hbm_budget_bytes / 8);
@@ -202,9 +207,13 @@ int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket) {
   spk_job j = *job;
   std::vector<uint32_t> ks(job->ks, job->ks + job->n_k);
   const uint64_t need = job_estimate(j, ctx->total_mem);
+  // A job above the shared budget runs alone: the pool is first grown to
+  // hold it in one block, if it has not been yet.
+  const bool alone = need > ctx->server->budget / 8;
   // The job runs on a worker thread: its error message is taken there and
   // handed to the caller of spk_wait with the status.
-  *ticket = ctx->server->sched->submit(need, [ctx, j, ks](void** out, std::string* msg) {
+  *ticket = ctx->server->sched->submit(need, [ctx, j, ks, need, alone](void** out, std::string* msg) {
+    if (alone) pool_reserve(ctx, need + (need >> 3));
     const int rc = run_job(ctx, j, ks, out);
     if (rc) *msg = spk_last_error();
     return rc;
