@@ -1797,8 +1797,7 @@ __global__ void __launch_bounds__(kApplyBlock) k_bloom_apply(RangeView rv, uint6
     const uint64_t b = range_base(rv, r);
     const uint64_t end = rv.uniform ? (uint64_t)(r + 1) * rv.uniform : rv.base[r + 1];
     const uint64_t e = min(end, b + (uint64_t)rv.fill[(uint64_t)r * kFillStride]);
-    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-      const uint32_t op = __ldcs(rv.ops + i);
+    auto apply = [&](uint32_t op) {
       const uint32_t off = op >> 1;
       const uint32_t w = off >> 5, bit = 1u << (off & 31);
       if (op & 1) {
@@ -1807,7 +1806,34 @@ __global__ void __launch_bounds__(kApplyBlock) k_bloom_apply(RangeView rv, uint6
       } else if (atomicOr(s_seen + w, bit) & bit) {
         atomicOr(s_twice + w, bit);
       }
+    };
+    // The operations stream in as 16-byte loads, two per thread in flight
+    // (one 4-byte load per thread kept too few bytes in flight: the pass ran
+    // at the latency of its loads); the unaligned head and the tail one by one.
+    const uint64_t a0 = min(e, (uint64_t)((b + 3) & ~3ULL)), a1 = max(a0, (uint64_t)(e & ~3ULL));
+    for (uint64_t i = b + threadIdx.x; i < a0; i += blockDim.x) apply(__ldcs(rv.ops + i));
+    const uint4* v = (const uint4*)(rv.ops + a0);
+    const uint64_t nv = (a1 - a0) / 4;
+    uint64_t q = threadIdx.x;
+    for (; q + blockDim.x < nv; q += 2 * blockDim.x) {
+      const uint4 x = __ldcs(v + q), y = __ldcs(v + q + blockDim.x);
+      apply(x.x);
+      apply(x.y);
+      apply(x.z);
+      apply(x.w);
+      apply(y.x);
+      apply(y.y);
+      apply(y.z);
+      apply(y.w);
     }
+    for (; q < nv; q += blockDim.x) {
+      const uint4 x = __ldcs(v + q);
+      apply(x.x);
+      apply(x.y);
+      apply(x.z);
+      apply(x.w);
+    }
+    for (uint64_t i = a1 + threadIdx.x; i < e; i += blockDim.x) apply(__ldcs(rv.ops + i));
     __syncthreads();
     const uint64_t g0 = (uint64_t)r * (W32 / 2);
     for (uint32_t i = threadIdx.x; i < W32 / 2 && g0 + i < num_words; i += blockDim.x) {
