@@ -12,10 +12,10 @@
 //   uploader   one host thread enqueues each job's upload on one upload
 //              stream (pageable memory through the context's pinned chunks),
 //              up to kAhead jobs ahead of the counts;
-//   lanes      kLanes host threads take the jobs in order and run each count
+//   lanes      kLanes (3) host threads take the jobs in order and run each count
 //              on the lane's stream once its upload has landed, so one job's
 //              copies overlap the counts of the jobs before it and a lane's
-//              host readbacks overlap the other lane's kernels;
+//              host readbacks overlap the other lanes' kernels;
 //   results    a finished job's result moves to the batch's result stream,
 //              and spk_batch_next hands the results out in job order as they
 //              finish, so the caller's downloads of one result overlap the
@@ -48,12 +48,14 @@ int upload_reads(spk_result* res, cudaStream_t st, const uint8_t* data, size_t d
 uint64_t job_estimate(const spk_job& j, uint64_t total_mem);
 uint64_t usable_device_memory(spk_ctx* ctx);
 void rehome_result(spk_result* res, cudaStream_t s);
-constexpr int kLanes = 2;   // jobs counting at once
+// jobs counting at once (64 samples of 0.05-1.2 Mb: 132 ms per batch with
+// two lanes, 125 ms with three, 126 ms with four)
+constexpr int kLanes = 3;
 constexpr int kAhead = 4;   // uploads enqueued ahead of the jobs counting
 // spk_ctx::batch_streams: [0] uploads, [1, kLanes] the lanes, [kLanes + 1]
 // the finished jobs' results
 constexpr int kResultStream = kLanes + 1;
-static_assert(kResultStream < 4, "spk_ctx::batch_streams holds four streams");
+static_assert(kResultStream < 8, "spk_ctx::batch_streams holds eight streams");
 
 namespace {
 struct BatchSlot {
@@ -284,7 +286,7 @@ int spk_batch_start(spk_ctx* ctx, const spk_job* jobs, int n_jobs, spk_batch** o
   // job maps memory piece by piece mid-way (64 samples of 0.5-12 Mb: 1.28 s
   // steady with the block, 1.30-1.86 s without).
   if (n_jobs > 0) {
-    const uint64_t side = small_max ? std::min<uint64_t>(b->budget / 8, 2 * small_max) : 0;
+    const uint64_t side = small_max ? std::min<uint64_t>(b->budget / 8, kLanes * small_max) : 0;
     const uint64_t peak = std::max(need_max, side) + (need_max >> 3) + (uint64_t)(kAhead + kLanes) * ahead;
     pool_reserve(ctx, std::min<uint64_t>(peak, b->budget));
   }

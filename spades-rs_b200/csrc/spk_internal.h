@@ -190,7 +190,7 @@ struct spk_ctx {
   // the device memory pool's allocations slow down with every stream that
   // has used it (measured: 1.4 us per allocation with 3 streams, 11 us after
   // a batch that gave every job streams of its own).
-  cudaStream_t batch_streams[4] = {};
+  cudaStream_t batch_streams[8] = {};
   std::mutex batch_mu;  // one batch at a time per context
   std::condition_variable batch_cv;
   bool batch_active = false;
