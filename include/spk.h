@@ -389,7 +389,7 @@ typedef struct spk_job {
 
 /* Counts several independent read sets as one pipeline (samples of uneven
  * size, each with its own Bloom and table): one host thread uploads the jobs'
- * reads ahead on an upload stream while two lanes count them in order, so a
+ * reads ahead on an upload stream while three lanes count them in order, so a
  * job's copies overlap the counts before it.  results[i] receives job i's
  * result, identical to spk_count on that job alone; if a job fails, every
  * result is freed and its status is returned.  Replaces the serial per-sample
