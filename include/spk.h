@@ -247,6 +247,15 @@ typedef struct spk_count_opts {
                                  (one pass over the reads each); 0 = as many as the device
                                  memory needs (usually one) */
   uint32_t reserved;
+  /* Host buffers (pageable or pinned; either may be NULL) that receive the
+   * solid list of the first k, as spk_result_solid gives it, during the count:
+   * the default job copies it while the edges are built.  solid_capacity is
+   * the k-mers they hold (keys: ceil(k/32) limbs each); a longer list is not
+   * copied.  spk_result_info.solid_copied tells whether they were filled, and
+   * n_solid how many k-mers they hold.  Borrowed for the call. */
+  uint64_t* solid_keys_out;
+  uint32_t* solid_counts_out;
+  uint64_t solid_capacity;
 } spk_count_opts;
 
 void spk_count_opts_default(spk_count_opts* opts);
@@ -305,6 +314,8 @@ typedef struct spk_result_info {
                                     counting one group of spans (read sets too large for one) */
   float ms_coarse_kernel;        /* two-level partition in one group: the coarse pass alone
                                     (ms_scatter_kernel - ms_coarse_kernel is the fine pass) */
+  uint32_t solid_copied;         /* 1: the solid list went to spk_count_opts.solid_*_out */
+  uint32_t reserved2;
 } spk_result_info;
 
 int spk_result_count(const spk_result* res, int* n_k);

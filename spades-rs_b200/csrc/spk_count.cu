@@ -3694,6 +3694,24 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
   for (int j = 0; j < nl; j++) lp[j] = kr.list[j].as<uint64_t>();
   SPK_CUDA(cudaEventRecord(e4.e, st));
 
+  // ---- the solid list for the caller's host buffers: converted here, copied
+  // on a side stream while the edges are built ----
+  const bool want_solid = (o.solid_keys_out || o.solid_counts_out) && info.n_solid <= o.solid_capacity;
+  SideStream cpy;
+  if (want_solid) {
+    uint64_t m = 0;
+    if ((rc = cpy.open())) return rc;
+    if ((rc = ordered_convert(st, nl, kr.list_len, k, kr.list, kr.list[4].as<uint32_t>(), info.cutoff,
+                              &kr.conv.keys, &kr.conv.cnt, host, &m, info.n_solid)))
+      return rc;
+    kr.conv.kind = 0;  // what spk_result_solid converts (kept for later downloads)
+    kr.conv.minc = info.cutoff;
+    kr.conv.n = m;
+    launches += 4;     // k_oc_count, the scan's two kernels, k_oc_write
+    SPK_CUDA(cudaEventRecord(cpy.fork, st));
+    SPK_CUDA(cudaStreamWaitEvent(cpy.s, cpy.fork, 0));
+  }
+
   // ---- edges ----
   kr.nle = (int)((k + 1 + 31) / 32);
   uint64_t ecap = 0;
@@ -3725,6 +3743,16 @@ int count_one_k_list(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsV
       return rc;
   }
   SPK_CUDA(cudaEventRecord(e5.e, st));
+  if (want_solid) {
+    // (the host waits here for the copy while the device builds the edges)
+    const uint64_t m = kr.conv.n;
+    if (m && o.solid_keys_out && (rc = xfer_d2h(ctx, o.solid_keys_out, kr.conv.keys.p, m * nl * 8, cpy.s)))
+      return rc;
+    if (m && o.solid_counts_out && (rc = xfer_d2h(ctx, o.solid_counts_out, kr.conv.cnt.p, m * 4, cpy.s)))
+      return rc;
+    SPK_CUDA(cudaStreamSynchronize(cpy.s));
+    info.solid_copied = 1;
+  }
   if (!(o.flags & SPK_F_KEEP_BLOOM)) {
     kr.seen.release();
     kr.twice.release();
@@ -3775,10 +3803,42 @@ void rehome_result(spk_result* res, cudaStream_t s) {
   res->reads.st = res->offs.st = res->lens.st = s;
 }
 
-// One k: the job with few round trips where it applies, else (or after an
-// overflow there) the general one.
+// The solid list into the caller's host buffers (spk_count_opts.solid_*_out)
+// after a job that did not copy it during the count.
+static int solid_copy_after(spk_ctx* ctx, cudaStream_t st, uint64_t* host, KResult& kr,
+                            const spk_count_opts& o) {
+  if (!(o.solid_keys_out || o.solid_counts_out) || kr.info.solid_copied || kr.info.n_solid > o.solid_capacity)
+    return SPK_OK;
+  KResult::Conv& cv = kr.conv;
+  uint64_t m = 0;
+  int rc = ordered_convert(st, kr.nl, kr.list_len, kr.k, kr.list, kr.list[4].as<uint32_t>(), kr.info.cutoff,
+                           &cv.keys, &cv.cnt, host, &m);
+  if (rc) return rc;
+  cv.kind = 0;
+  cv.minc = kr.info.cutoff;
+  cv.n = m;
+  if (m > o.solid_capacity) return SPK_OK;
+  if (m && o.solid_keys_out && (rc = xfer_d2h(ctx, o.solid_keys_out, cv.keys.p, m * kr.nl * 8, st))) return rc;
+  if (m && o.solid_counts_out && (rc = xfer_d2h(ctx, o.solid_counts_out, cv.cnt.p, m * 4, st))) return rc;
+  SPK_CUDA(cudaStreamSynchronize(st));
+  kr.info.solid_copied = 1;
+  return SPK_OK;
+}
+
+static int count_k_job(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv, unsigned k,
+                       const spk_count_opts& o, KResult& kr);
+// One k, and the copy of its solid list to the caller's buffers if asked for.
 static int count_k(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv, unsigned k,
                    const spk_count_opts& o, KResult& kr) {
+  const int rc = count_k_job(ctx, st, host, rv, k, o, kr);
+  if (rc) return rc;
+  return solid_copy_after(ctx, st, host, kr, o);
+}
+
+// One k: the job with few round trips where it applies, else (or after an
+// overflow there) the general one.
+static int count_k_job(spk_ctx* ctx, cudaStream_t st, uint64_t* host, const ReadsView& rv, unsigned k,
+                       const spk_count_opts& o, KResult& kr) {
   int rc = count_one_k_list(ctx, st, host, rv, k, o, kr);
   // A span with more distinct k-mers than slots: twice the slots, twice at most.
   for (uint32_t grow = 1; rc == kGrow && grow <= 2; grow++) {
@@ -3836,7 +3896,12 @@ int count_pipeline(spk_ctx* ctx, cudaStream_t st, const ReadsView& rv, uint32_t 
         rc = fail(SPK_E_CUDA, "per-k stream");
       auto kr = std::make_unique<KResult>();
       if (!rc && cudaStreamWaitEvent(s2, ready, 0) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "wait");
-      if (!rc) rc = count_k(ctx, s2, h, rv, ks[i], o, *kr);
+      spk_count_opts oi = o;
+      if (i > 0) {  // the caller's solid buffers are the first k's
+        oi.solid_keys_out = nullptr;
+        oi.solid_counts_out = nullptr;
+      }
+      if (!rc) rc = count_k(ctx, s2, h, rv, ks[i], oi, *kr);
       if (s2) {
         cudaStreamSynchronize(s2);
         rehome(*kr, st);

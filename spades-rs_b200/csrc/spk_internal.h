@@ -318,8 +318,9 @@ int sort_dev_finish(cudaStream_t st, DevSort& ds, DevBuf* keys, DevBuf* vals, ui
 // Exclusive scan of u32 in place (spk_sort.cu).
 int scan_u32(cudaStream_t st, uint32_t* a, uint64_t n, DevBuf& sums, uint32_t* launches = nullptr);
 // Ordered compaction of a sorted SoA list into AoS Kmer256 limbs; *m is the
-// number of kept items (synchronises st).
+// number of kept items (synchronises st to read it, unless the caller knows
+// it already: known_m, which must be exact).
 int ordered_convert(cudaStream_t st, int nl, uint64_t n, unsigned k, DevBuf* limbs,
                     const uint32_t* cin, uint32_t min_count, DevBuf* out, DevBuf* cout,
-                    uint64_t* h_staging, uint64_t* m);
+                    uint64_t* h_staging, uint64_t* m, uint64_t known_m = ~0ULL);
 }  // namespace spk

@@ -783,7 +783,7 @@ __global__ void __launch_bounds__(OC_BLOCK) k_oc_write(const uint64_t* l0, const
                                                         unsigned k, uint32_t min_count,
                                                         const uint32_t* __restrict__ bc,
                                                         uint64_t* __restrict__ out,
-                                                        uint32_t* __restrict__ cout) {
+                                                        uint32_t* __restrict__ cout, uint64_t out_cap) {
   __shared__ uint32_t ws[OC_BLOCK / 32];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // Thread t owns the contiguous items [t*IPT, t*IPT+IPT) of the tile.
@@ -809,6 +809,7 @@ __global__ void __launch_bounds__(OC_BLOCK) k_oc_write(const uint64_t* l0, const
 #pragma unroll 1
   for (int j = 0; j < OC_IPT; j++) {
     if (!(keepmask & (1u << j))) continue;
+    if (p >= out_cap) break;  // (a caller's count of the kept items that was short)
     const uint64_t i = base + j;
     Seq<NL> V;
     V.v[0] = l0[i];
@@ -827,7 +828,7 @@ __global__ void __launch_bounds__(OC_BLOCK) k_oc_write(const uint64_t* l0, const
 // Returns the number of kept items in *m (host value; synchronises st).
 int ordered_convert(cudaStream_t st, int nl, uint64_t n, unsigned k, DevBuf* limbs,
                     const uint32_t* cin, uint32_t min_count, DevBuf* out, DevBuf* cout,
-                    uint64_t* h_staging, uint64_t* m) {
+                    uint64_t* h_staging, uint64_t* m, uint64_t known_m) {
   int rc;
   const uint32_t nt = (uint32_t)std::max<uint64_t>((n + OC_TILE - 1) / OC_TILE, 1);
   DevBuf bc;
@@ -838,9 +839,13 @@ int ordered_convert(cudaStream_t st, int nl, uint64_t n, unsigned k, DevBuf* lim
   }
   DevBuf sums;
   if ((rc = scan_u32(st, bc.as<uint32_t>(), nt + 1, sums))) return rc;
-  SPK_CUDA(cudaMemcpyAsync(h_staging, bc.as<uint32_t>() + nt, 4, cudaMemcpyDeviceToHost, st));
-  SPK_CUDA(cudaStreamSynchronize(st));
-  *m = (uint64_t)((uint32_t*)h_staging)[0];
+  if (known_m != ~0ULL) {
+    *m = known_m;
+  } else {
+    SPK_CUDA(cudaMemcpyAsync(h_staging, bc.as<uint32_t>() + nt, 4, cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    *m = (uint64_t)((uint32_t*)h_staging)[0];
+  }
   if ((rc = out->alloc(std::max<uint64_t>(*m, 1) * nl * 8, st))) return rc;
   if (cout && (rc = cout->alloc(std::max<uint64_t>(*m, 1) * 4, st))) return rc;
   if (n && *m) {
@@ -849,10 +854,10 @@ int ordered_convert(cudaStream_t st, int nl, uint64_t n, unsigned k, DevBuf* lim
     uint64_t* o = out->as<uint64_t>();
     uint32_t* oc = cout ? cout->as<uint32_t>() : nullptr;
     switch (nl) {
-      case 1: k_oc_write<1><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
-      case 2: k_oc_write<2><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
-      case 3: k_oc_write<3><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
-      default: k_oc_write<4><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc); break;
+      case 1: k_oc_write<1><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc, *m); break;
+      case 2: k_oc_write<2><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc, *m); break;
+      case 3: k_oc_write<3><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc, *m); break;
+      default: k_oc_write<4><<<nt, OC_BLOCK, 0, st>>>(p[0], p[1], p[2], p[3], cin, n, k, min_count, bc.as<uint32_t>(), o, oc, *m); break;
     }
     SPK_CUDA(cudaGetLastError());
   }

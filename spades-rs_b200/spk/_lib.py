@@ -48,7 +48,9 @@ class CountOpts(C.Structure):
                 ("flags", C.c_uint32), ("table_log2", C.c_uint32),
                 ("prior_seqs", C.c_void_p), ("prior_offsets", C.c_void_p),
                 ("prior_lengths", C.c_void_p), ("n_prior", C.c_uint64),
-                ("span_groups_log2", C.c_uint32), ("reserved", C.c_uint32)]
+                ("span_groups_log2", C.c_uint32), ("reserved", C.c_uint32),
+                ("solid_keys_out", C.c_void_p), ("solid_counts_out", C.c_void_p),
+                ("solid_capacity", C.c_uint64)]
 
 
 class ResultInfo(C.Structure):
@@ -67,7 +69,8 @@ class ResultInfo(C.Structure):
                 ("ms_unitigs_host", C.c_float), ("unitig_launches", C.c_uint32),
                 ("n_unitigs", C.c_uint64), ("n_corrected_reads", C.c_uint64),
                 ("ms_correct", C.c_float), ("part_passes", C.c_uint32),
-                ("span_groups", C.c_uint32), ("ms_coarse_kernel", C.c_float)]
+                ("span_groups", C.c_uint32), ("ms_coarse_kernel", C.c_float),
+                ("solid_copied", C.c_uint32), ("reserved2", C.c_uint32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

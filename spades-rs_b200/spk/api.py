@@ -244,9 +244,13 @@ class PackedReads:
 def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: int = 2,
               min_coverage: float = 5.0, flags: Optional[int] = None,
               table_log2: int = 0, priors: Optional[Sequence[bytes]] = None,
-              span_groups_log2: int = 0) -> CountOpts:
+              span_groups_log2: int = 0, solid_out=None) -> CountOpts:
     """spk_count_opts.  priors: prior/trusted contigs as ASCII byte strings
-    (src/assemble.rs:244-284); the returned options keep them alive."""
+    (src/assemble.rs:244-284); the returned options keep them alive.
+    solid_out: (keys, counts) arrays (u64 (capacity, ceil(k/32)) and u32
+    (capacity,), C-contiguous; pinned host memory copies fastest) that the
+    count fills with the first k's solid list while it builds the edges
+    (CountResult.info()["solid_copied"], ["n_solid"])."""
     o = CountOpts()
     lib().spk_count_opts_default(C.byref(o))
     o.bloom_bits = bloom_bits
@@ -267,6 +271,16 @@ def make_opts(bloom_bits: int = 512 << 20, min_count: int = 0, list_min_count: i
         o.prior_offsets = offs.ctypes.data
         o.prior_lengths = lens.ctypes.data
         o.n_prior = len(seqs)
+    if solid_out is not None:
+        keys, counts = solid_out
+        if (keys.dtype != np.uint64 or counts.dtype != np.uint32 or keys.ndim != 2 or counts.ndim != 1
+                or keys.shape[0] != counts.shape[0] or not keys.flags.c_contiguous
+                or not counts.flags.c_contiguous):
+            raise SpkError(1, "solid_out must be C-contiguous u64 keys (n, limbs) and u32 counts (n,)")
+        o._solid_arrays = (keys, counts)
+        o.solid_keys_out = keys.ctypes.data
+        o.solid_counts_out = counts.ctypes.data
+        o.solid_capacity = counts.shape[0]
     return o
 
 
@@ -386,6 +400,12 @@ def _as_arrays(packed):
     return data, offsets, lengths
 
 
+def _check_solid_out(opt_kw, ks_arr) -> None:
+    so = opt_kw.get("solid_out")
+    if so is not None and ks_arr.size and so[0].ndim == 2 and so[0].shape[1] != nlimbs(int(ks_arr[0])):
+        raise SpkError(1, f"solid_out keys need {nlimbs(int(ks_arr[0]))} u64 limbs per k-mer")
+
+
 def count(packed, ks: Sequence[int] | int, ctx: Optional[Context] = None, **opt_kw) -> CountResult:
     """spk_count on host-resident packed reads (copied to the device inside the call)."""
     ctx = ctx or default_context()
@@ -396,6 +416,7 @@ def count(packed, ks: Sequence[int] | int, ctx: Optional[Context] = None, **opt_
     if offsets.size != lengths.size:
         raise SpkError(1, "offsets and lengths differ in size")
     ks_arr = np.ascontiguousarray(np.atleast_1d(ks), dtype=np.uint32)
+    _check_solid_out(opt_kw, ks_arr)
     o = make_opts(**opt_kw)
     h = vp()
     check(lib().spk_count(ctx.h, data.ctypes.data if data.size else None, data.size,
@@ -410,6 +431,7 @@ def count_device(d_data: int, data_len: int, d_offsets: int, d_lengths: int, n_r
     """spk_count_device: packed reads already resident on the device (raw pointers)."""
     ctx = ctx or default_context()
     ks_arr = np.ascontiguousarray(np.atleast_1d(ks), dtype=np.uint32)
+    _check_solid_out(opt_kw, ks_arr)
     o = make_opts(**opt_kw)
     h = vp()
     check(lib().spk_count_device(ctx.h, d_data, data_len, d_offsets, d_lengths, n_reads,

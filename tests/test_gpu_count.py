@@ -246,6 +246,49 @@ def test_multik_equals_single_k(spk):
         np.testing.assert_array_equal(multi.edges(i), one.edges(0))
 
 
+@pytest.mark.parametrize("k,flags", [(21, BASE), (55, BASE), (77, BASE), (55, BASE | GATED), (55, BASE | DIRECT)])
+def test_solid_out_buffers(spk, k, flags):
+    """spk_count_opts.solid_*_out: the count fills the caller's host buffers
+    with the first k's solid list (the default job while it builds the edges,
+    the other schedules after the job), exactly what spk_result_solid gives;
+    a list longer than the buffers is not copied and leaves them untouched."""
+    data, offs, lens = synth_small_packed()
+    want_k, want_c = spk.count((data, offs, lens), [k], bloom_bits=1 << 22, flags=flags).solid(0)
+    n = len(want_c)
+    assert n > 0
+    L = nlimbs(k)
+    keys = np.full((n + 5, L), 0xAB, dtype=np.uint64)
+    counts = np.full(n + 5, 7, dtype=np.uint32)
+    r = spk.count((data, offs, lens), [k], bloom_bits=1 << 22, flags=flags, solid_out=(keys, counts))
+    info = r.info(0)
+    assert info["solid_copied"] == 1 and info["n_solid"] == n
+    np.testing.assert_array_equal(keys[:n], want_k)
+    np.testing.assert_array_equal(counts[:n], want_c)
+    assert (keys[n:] == 0xAB).all() and (counts[n:] == 7).all()
+    gk, gc = r.solid(0)  # the download after it gives the same list
+    np.testing.assert_array_equal(gk, want_k)
+    np.testing.assert_array_equal(gc, want_c)
+    small_k = np.full((n - 1, L), 0xAB, dtype=np.uint64)
+    small_c = np.full(n - 1, 7, dtype=np.uint32)
+    r2 = spk.count((data, offs, lens), [k], bloom_bits=1 << 22, flags=flags, solid_out=(small_k, small_c))
+    assert r2.info(0)["solid_copied"] == 0
+    assert (small_k == 0xAB).all() and (small_c == 7).all()
+    np.testing.assert_array_equal(r2.solid(0)[0], want_k)
+
+
+def test_solid_out_first_k_of_several(spk):
+    """With several k, the buffers receive the first k's solid list only."""
+    data, offs, lens = synth_small_packed()
+    want_k, want_c = spk.count((data, offs, lens), [33], bloom_bits=1 << 22).solid(0)
+    n = len(want_c)
+    keys = np.zeros((n, nlimbs(33)), dtype=np.uint64)
+    counts = np.zeros(n, dtype=np.uint32)
+    r = spk.count((data, offs, lens), [33, 55], bloom_bits=1 << 22, solid_out=(keys, counts))
+    assert r.info(0)["solid_copied"] == 1 and r.info(1)["solid_copied"] == 0
+    np.testing.assert_array_equal(keys, want_k)
+    np.testing.assert_array_equal(counts, want_c)
+
+
 def test_count_device_pointers(spk):
     """spk_count_device on device-resident reads, including an unaligned base pointer."""
     import torch
