@@ -515,9 +515,8 @@ def _gk(occ, sec):
 
 def run_c3(args, ctx, log_rank0):
     """Multi-k: the 5 Mb x 100x reads (scaled by --scale) at k in {21,33,55,77},
-    one call counting the four k values concurrently against four
-    one-k calls in a row.  Both are device-resident; time = host clock around
-    synchronised calls (the concurrent call runs on several streams)."""
+    one call counting the four k values against four one-k calls in a row.
+    Both are device-resident; time = host clock around synchronised calls."""
     import numpy as np
     import torch
     import spk
@@ -563,7 +562,7 @@ def run_c3(args, ctx, log_rank0):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded; no public dataset)",
             "config": {"workload": f"c3: the 5 Mb x 100x reads at scale {args.scale}, k in {ks} in "
-                                   "one call (concurrent per-k streams)",
+                                   "one call",
                        "occurrences": occ, "bloom_bits": args.bloom_bits,
                        "timing": "host clock around synchronised calls"},
             "plain": {"what": "one call per k, in a row", "value": _gk(occ, t_plain),

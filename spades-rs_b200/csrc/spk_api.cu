@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -156,6 +157,51 @@ int DevBuf::alloc(size_t n, cudaStream_t s) {
   st = s;
   return SPK_OK;
 }
+// The results pool of the current device (created on first use; nullptr if
+// the driver refuses one: results then come from the default pool).
+static cudaMemPool_t results_pool() {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> l(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t p = nullptr;
+  if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+  } else {
+    uint64_t thr = ~0ULL;  // keep freed blocks cached, as the default pool does
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  pools[dev] = p;
+  return p;
+}
+
+int DevBuf::alloc_keep(size_t n, cudaStream_t s) {
+  cudaMemPool_t pool = results_pool();
+  if (!pool) return alloc(n, s);
+  release();
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n, pool, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+    return alloc(n, s);  // the default pool may still have room
+  }
+  bytes = n;
+  st = s;
+  return SPK_OK;
+}
+
 void DevBuf::release() {
   if (p) cudaFreeAsync(p, st);
   p = nullptr;
@@ -212,6 +258,7 @@ void pool_trim(spk_ctx* ctx) {
   if (!ctx->pool) return;
   std::lock_guard<std::mutex> l(ctx->pool_mu);
   cudaMemPoolTrimTo(ctx->pool, 0);
+  if (cudaMemPool_t rp = results_pool()) cudaMemPoolTrimTo(rp, 0);  // its unused blocks only
   ctx->pool_reserved = 0;
 }
 

@@ -53,6 +53,11 @@ struct DevBuf {
   }
   ~DevBuf() { release(); }
   int alloc(size_t n, cudaStream_t s);
+  // The same from a second pool of the device that holds only what results
+  // keep (their lists, edges and converted downloads), so that buffers kept
+  // past a job do not sit in the middle of the memory the next job's large
+  // temporaries come from (that made the pool map new memory mid-job).
+  int alloc_keep(size_t n, cudaStream_t s);
   void release();
   template <class T> T* as() const { return static_cast<T*>(p); }
 };

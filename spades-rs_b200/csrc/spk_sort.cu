@@ -846,8 +846,8 @@ int ordered_convert(cudaStream_t st, int nl, uint64_t n, unsigned k, DevBuf* lim
     SPK_CUDA(cudaStreamSynchronize(st));
     *m = (uint64_t)((uint32_t*)h_staging)[0];
   }
-  if ((rc = out->alloc(std::max<uint64_t>(*m, 1) * nl * 8, st))) return rc;
-  if (cout && (rc = cout->alloc(std::max<uint64_t>(*m, 1) * 4, st))) return rc;
+  if ((rc = out->alloc_keep(std::max<uint64_t>(*m, 1) * nl * 8, st))) return rc;
+  if (cout && (rc = cout->alloc_keep(std::max<uint64_t>(*m, 1) * 4, st))) return rc;
   if (n && *m) {
     const uint64_t* p[4] = {nullptr, nullptr, nullptr, nullptr};
     for (int j = 0; j < nl; j++) p[j] = limbs[j].as<uint64_t>();
