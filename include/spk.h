@@ -427,7 +427,7 @@ int spk_batch_end(spk_batch* batch);
 /* Serving loop.  spk_serve_start starts a scheduler thread that admits
  * submitted jobs in arrival order while at most max_inflight run, each on its
  * own stream: jobs run side by side while their estimated HBM needs together
- * stay within an eighth of hbm_budget_bytes (0 = 90% of the device memory
+ * stay within a sixteenth of hbm_budget_bytes (0 = 90% of the device memory
  * free at start), a job that needs more runs alone, and a job that needs more
  * than the whole budget is refused (SPK_E_ADMISSION). */
 int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight);

@@ -252,6 +252,14 @@ void pool_reserve(spk_ctx* ctx, uint64_t bytes) {
   if (cudaMallocAsync(&p, n, st) != cudaSuccess || cudaFreeAsync(p, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     cudaGetLastError();  // a hint: without it the pool grows as the jobs need
+  // The results' pool gets a block too (a sixteenth: lists and edges are a
+  // few percent of a job's temporaries).
+  if (cudaMemPool_t rp = results_pool()) {
+    p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, n / 16 + (2ull << 20), rp, st) != cudaSuccess ||
+        cudaFreeAsync(p, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+      cudaGetLastError();
+  }
 }
 
 void pool_trim(spk_ctx* ctx) {

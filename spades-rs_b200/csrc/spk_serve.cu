@@ -175,18 +175,21 @@ int spk_serve_start(spk_ctx* ctx, uint64_t hbm_budget_bytes, int max_inflight) {
   if (!hbm_budget_bytes) hbm_budget_bytes = (uint64_t)(usable_device_memory(ctx) * 0.9);
   auto* s = new Server();
   s->budget = hbm_budget_bytes;
-  // Jobs run side by side only while together they need at most an eighth
-  // of the budget; a larger job runs alone (two jobs of 20-40 GB side by side
-  // took 5-40 times their time alone: the memory pool maps new memory for one
-  // while the other's buffers are in use).
+  // Jobs run side by side only while together they need at most a
+  // sixteenth of the budget; a larger job runs alone.  Two jobs of 20-40 GB
+  // side by side took 5-40 times their time alone (the memory pool maps new
+  // memory for one while the other's buffers are in use), and jobs of 5-10 GB
+  // side by side still took up to 50 times their time alone now and then.
+  // At the arrival rates of a service a job takes a small share of the time
+  // between arrivals, so running most jobs alone costs little queueing.
   // The jobs that run side by side share one block of the pool, mapped here
-  // (twice their shared budget: their estimates leave out the list sort's
-  // and the edges' temporaries, and blocks freed by one job in the middle of
-  // another's are reused only once both are done).
+  // (several times their shared budget: their estimates leave out the list
+  // sort's and the edges' temporaries, and blocks freed by one job in the
+  // middle of another's are reused only once both are done).
   pool_reserve(ctx, hbm_budget_bytes / 4);
   s->sched = std::make_shared<Scheduler>(hbm_budget_bytes, max_inflight > 0 ? max_inflight : 4,
                                          [](void* r) { spk_result_free((spk_result*)r); },
-                                         hbm_budget_bytes / 8);
+                                         hbm_budget_bytes / 16);
   ctx->server = s;
   return SPK_OK;
 }
@@ -209,7 +212,7 @@ int spk_submit(spk_ctx* ctx, const spk_job* job, uint64_t* ticket) {
   const uint64_t need = job_estimate(j, ctx->total_mem);
   // A job above the shared budget runs alone: the pool is first grown to
   // hold it in one block, if it has not been yet.
-  const bool alone = need > ctx->server->budget / 8;
+  const bool alone = need > ctx->server->budget / 16;
   // The job runs on a worker thread: its error message is taken there and
   // handed to the caller of spk_wait with the status.
   *ticket = ctx->server->sched->submit(need, [ctx, j, ks, need, alone](void** out, std::string* msg) {
