@@ -461,7 +461,7 @@ def c2_config(p, occ, args, world):
             "parallelism": f"replicas x{world} (one read set per GPU, no collective)"}
 
 
-def run_parity(p, run_job, bloom_bits, timed_info):
+def run_parity(p, run_job, bloom_bits, timed_info, k=K):
     """The full result of one more (untimed) job against the oracle's
     twice-tier count of the same reads (threaded; order-free, so equal to the
     serial restatement): the whole admitted table with its counts, both Bloom
@@ -480,12 +480,12 @@ def run_parity(p, run_job, bloom_bits, timed_info):
     r.close()
     t1 = time.time()
     threads = os.cpu_count() or 1
-    o = ora.count(p.data, p.offsets, p.lengths, K, bloom_bits, mode=ora.MODE_TWICE, threads=threads)
+    o = ora.count(p.data, p.offsets, p.lengths, k, bloom_bits, mode=ora.MODE_TWICE, threads=threads)
     tk, tc = o.table(1)
     oseen, otwice = o.bloom()
     cut = ora.cutoff(tc, 5.0)
     solid = tc >= cut
-    oe = ora.edges(tk[solid], K)
+    oe = ora.edges(tk[solid], k)
     checks = {
         "table": bool(np.array_equal(gk, tk) and np.array_equal(gc, tc)),
         "count_ge2_list": bool(np.array_equal(gk[gc >= 2], tk[tc >= 2]) and np.array_equal(gc[gc >= 2], tc[tc >= 2])),
@@ -511,6 +511,82 @@ def run_parity(p, run_job, bloom_bits, timed_info):
 # ---------------------------------------------------------------------------
 def _gk(occ, sec):
     return occ / sec / 1e9
+
+
+def run_c1(args, ctx, log_rank0):
+    """Plain single-sample counting: the 1 Mb x 30x read set (2 x 150 bp
+    pairs, 0.5% substitution errors, 0.01% N) at k=21 with one-limb keys and
+    the 512 Mi-bit Bloom.  Device-resident steps timed with CUDA events (L2
+    flushed between steps); end to end through spk_count from pinned host
+    buffers, the solid list copied to pinned buffers during the count; and
+    the whole result of one more job against the oracle."""
+    import numpy as np
+    import torch
+    import spk
+    from spk import synth
+    k = 21
+    p = synth.c1(args.scale).packed
+    occ = synth.occurrences(p, k)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    d_data = torch.zeros(p.data.size + 64, dtype=torch.uint8, device=dev)
+    d_data[: p.data.size] = torch.from_numpy(p.data).to(dev)
+    d_off = torch.from_numpy(p.offsets.view(np.int64)).to(dev)
+    d_len = torch.from_numpy(p.lengths.view(np.int32)).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    opts = dict(bloom_bits=args.bloom_bits, flags=spk.SPK_F_EDGES)
+
+    def job(**kw):
+        return spk.count_device(d_data.data_ptr(), p.data.size, d_off.data_ptr(), d_len.data_ptr(),
+                                p.lengths.size, [k], ctx=ctx, **{**opts, **kw})
+
+    def timed(fn):
+        out, infos = [], []
+        for i in range(args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+            e1.synchronize()
+            if i >= args.warmup:
+                out.append(e0.elapsed_time(e1))
+                infos.append(r.info(0))
+            r.close()
+        return out, infos
+
+    step_ms, infos = timed(job)
+    ms = sum(step_ms) / len(step_ms)
+    h_data = torch.from_numpy(p.data).pin_memory()
+    h_off = torch.from_numpy(p.offsets.view(np.int64)).pin_memory()
+    h_len = torch.from_numpy(p.lengths.view(np.int32)).pin_memory()
+    packed_pinned = (h_data.numpy(), h_off.numpy().view(np.uint64), h_len.numpy().view(np.uint32))
+    n_out = int(infos[0]["n_solid"]) + 1024
+    o_keys = torch.empty((n_out, 1), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    o_counts = torch.empty(n_out, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    e2e_ms, _ = timed(lambda: spk.count(packed_pinned, [k], ctx=ctx, solid_out=(o_keys, o_counts), **opts))
+    em = sum(e2e_ms) / len(e2e_ms)
+    parity, detail = run_parity(p, job, args.bloom_bits, infos, k=k)
+    info = infos[0]
+    return {"metric": METRIC, "value": _gk(occ, ms / 1e3), "unit": "Gk-mers/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "step_ms": [round(x, 3) for x in step_ms],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": f"c1: 1 Mb genome, 2x150 bp pairs at 30x, 0.5% substitution errors, "
+                                   f"0.01% N, scale {args.scale}; canonical k=21 (u64 keys); Bloom "
+                                   f"{args.bloom_bits} bits/tier; adaptive cutoff; sorted solid list + edges",
+                       "k": k, "reads": int(len(p)), "occurrences": occ,
+                       "l2": "flushed between steps (512 MiB write)"},
+            "e2e": {"value": _gk(occ, em / 1e3), "unit": "Gk-mers/s", "ms_per_step": em,
+                    "h2d_bytes_per_step": int(p.data.nbytes + p.offsets.nbytes + p.lengths.nbytes),
+                    "d2h_bytes_per_step": int(info["n_solid"]) * 12},
+            "parity": parity, "parity_detail": detail,
+            "result": {key: int(info[key]) for key in ("n_solid", "n_edges", "cutoff", "n_table")}}
 
 
 def run_c3(args, ctx, log_rank0):
@@ -743,15 +819,17 @@ def main():
                     help="skip the full-size check of one job's result against the oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "unitigs", "correct", "ingest"],
-                    help="c2 (default): k=55 on the 5 Mb x 100x reads; c3: multi-k; "
+    ap.add_argument("--workload", default="c2",
+                    choices=["c1", "c2", "c3", "c4", "c5", "unitigs", "correct", "ingest"],
+                    help="c2 (default): k=55 on the 5 Mb x 100x reads; c1: k=21 on the 1 Mb x 30x "
+                         "reads; c3: multi-k; "
                          "c4: 64 batched samples; c5: serving; unitigs: unitig compaction "
                          "of the c2 solid k-mers; correct: c2 with error correction; ingest: c2 "
                          "as FASTQ texts")
     args = ap.parse_args()
     assert args.warmup >= 1
     if args.scale is None:
-        args.scale = {"c2": 1.0, "c3": 1.0, "c4": 1.0, "c5": 0.1, "unitigs": 1.0,
+        args.scale = {"c1": 1.0, "c2": 1.0, "c3": 1.0, "c4": 1.0, "c5": 0.1, "unitigs": 1.0,
                       "correct": 1.0, "ingest": 1.0}[args.workload]
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -787,7 +865,7 @@ def main():
             return
         torch.cuda.set_device(local_rank)
         ctx = spk.Context(local_rank)
-        fn = {"c3": run_c3, "c4": run_c4, "c5": run_c5, "unitigs": run_unitigs,
+        fn = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "unitigs": run_unitigs,
               "correct": run_correct, "ingest": run_ingest}[args.workload]
         print(json.dumps(fn(args, ctx, log)), flush=True)
         ctx.close()
