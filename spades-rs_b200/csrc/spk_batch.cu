@@ -27,9 +27,9 @@
 // and the downloads of the results before it still overlap it).  A job that
 // runs out of device memory anyway waits until no other job runs, gives the
 // memory pool's cached blocks back and runs again alone.  The batch runs on
-// a fixed handful of streams of the context
-// (spk_ctx::batch_streams).  Every result is exactly spk_count's on that
-// sample alone: the jobs share nothing but the device.
+// a fixed handful of streams of the context (spk_ctx::batch_streams).  Every
+// result is exactly spk_count's on that sample alone: the jobs share nothing
+// but the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -144,10 +144,10 @@ void spk_batch::lane(cudaStream_t st) {
     {
       std::unique_lock<std::mutex> l(mu);
       // Jobs start in order, and alone a job always starts.  Jobs count side
-      // by side only while together they need at most an
-      // eighth of the budget; a larger job runs alone.  (Two jobs of 20-40 GB
-      // side by side took 5-40 times their time alone: the memory pool then
-      // maps new memory for one job's buffers while the other's are in use.)
+      // by side only while together they need at most an eighth of the
+      // budget; a larger job runs alone.  (Two jobs of 20-40 GB side by side
+      // took 5-40 times their time alone: the memory pool then maps new
+      // memory for one job's buffers while the other's are in use.)
       cv.wait(l, [&] {
         if (next_start >= n) return true;
         if (exclusive || oom_waiting || uploaded <= next_start) return false;
