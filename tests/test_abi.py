@@ -78,3 +78,50 @@ def test_no_device_fails_loudly(spk_lib):
     with pytest.raises(spk.SpkError) as e:
         spk.Context(0)
     assert e.value.code == 7  # SPK_E_NO_DEVICE
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of the header's structs have the C sizes and field
+    offsets (a compiled probe of include/spk.h against spk._lib)."""
+    import ctypes as C
+    from spk import _lib
+    structs = {"spk_count_opts": _lib.CountOpts, "spk_result_info": _lib.ResultInfo,
+               "spk_table_view": _lib.TableView, "spk_job": _lib.JobC}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            cname, what, v = line.split()
+            got[(cname, what)] = int(v)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_solid_out_options_are_checked(spk_lib):
+    """make_opts(solid_out=...) takes C-contiguous u64 keys and u32 counts of
+    one length, and points the options at them (no device needed)."""
+    import numpy as np
+    from spk import SpkError
+    from spk.api import make_opts
+    keys = np.zeros((10, 2), dtype=np.uint64)
+    counts = np.zeros(10, dtype=np.uint32)
+    o = make_opts(solid_out=(keys, counts))
+    assert o.solid_keys_out == keys.ctypes.data and o.solid_counts_out == counts.ctypes.data
+    assert o.solid_capacity == 10
+    assert make_opts().solid_keys_out is None and make_opts().solid_capacity == 0
+    for bad in ((keys.astype(np.int64), counts), (keys, counts[:9]), (keys[:, :1][::2], counts[:5]),
+                (keys, counts.astype(np.uint64))):
+        with pytest.raises(SpkError):
+            make_opts(solid_out=bad)
