@@ -1003,7 +1003,8 @@ __global__ void k_coarse_chunks(CoarseView cv, uint32_t chunk, uint32_t* __restr
 // One thread issues cp.async.bulk (the TMA's untiled copy: 16-byte aligned
 // addresses, a multiple of 16 bytes) from this GPU's global memory into the
 // CTA's shared memory, completing on an mbarrier; the threads wait on the
-// barrier's phase with a bounded number of polls.  No multicast.
+// barrier's phase with a bounded number of polls.  Each copy lands in this
+// CTA's shared memory alone, from this GPU's own memory.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
